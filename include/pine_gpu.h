@@ -1,0 +1,263 @@
+/* pine_gpu.h - C ABI of libpinegpu.so, the B200 (sm_100a) wavefront path tracer that
+ * stands behind pine's integrator plugin surface.
+ *
+ * Reference interfaces replaced (paths are relative to the pine source tree):
+ *   Integrator::Render()              src/core/integrator.h:15-30, integrator.cpp:121-150
+ *     -> pg_render / pg_render_batch
+ *   RadianceIntegrator::Compute / Li  src/core/integrator.cpp:152-158,
+ *                                     src/impl/integrator/path.cpp:6-87   -> kernels in pg_render
+ *   Accel::Intersect (BVH)            src/core/accel.h:8-14, src/impl/accel/bvh.cpp:669-709
+ *     -> pg_intersect (batched; the per-ray synchronous Accel API cannot amortise a launch)
+ *   LoadScene + Create* factories     src/util/fileio.cpp:251-281       -> pg_load_scene_file
+ *   Scene (flattened)                 src/core/scene.h:18-27             -> pg_scene_desc
+ *   LoadVolume (.vol)                 src/util/fileio.cpp:194-202       -> pg_write_volume
+ *
+ * Conventions: plain pointers and sizes only.  The caller owns every host buffer; the
+ * library copies inputs during the call and fills caller-allocated outputs before it
+ * returns.  A context owns its device memory and streams and is not thread-safe (one
+ * context per host thread; pine calls Render() from its main thread, src/cli/main.cpp:23).
+ * No exception crosses this boundary: every entry point returns a pg_status, and
+ * pg_last_error() describes the most recent failure.
+ */
+#ifndef PINE_GPU_H
+#define PINE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pg_status {
+    PG_OK = 0,
+    PG_ERR_INVALID_ARG = 1,  /* bad pointer, size or parameter */
+    PG_ERR_OOM = 2,          /* device allocation failed */
+    PG_ERR_CUDA = 3,         /* CUDA runtime error (no device, launch failure, ...) */
+    PG_ERR_DEVICE_LIMIT = 4, /* a device loop hit its iteration cap (traversal stack,
+                                tracking steps); results of that call are incomplete */
+    PG_ERR_UNSUPPORTED = 5,  /* shape/material/node/light outside the supported set */
+    PG_ERR_IO = 6,           /* file could not be read or written */
+    PG_ERR_PARSE = 7         /* scene text does not follow pine's grammar */
+} pg_status;
+
+typedef struct pg_ctx pg_ctx;
+
+/* ---- shapes (pine's Shape variant, src/core/geometry.h:415-453) ---- */
+enum {
+    PG_SHAPE_SPHERE = 0,   /* p[0..2] centre, p[3] radius          (geometry.h:143-170) */
+    PG_SHAPE_PLANE = 1,    /* p[0..2] position, p[3..5] unit normal (geometry.h:118-141) */
+    PG_SHAPE_TRIANGLE = 2, /* p[0..8] v0, v1, v2                     (geometry.h:242-339) */
+    PG_SHAPE_RECT = 3,     /* p[0..2] position, p[3..5] ex, p[6..8] ey (raw, not normalised)
+                                                                     (geometry.h:341-367) */
+    PG_SHAPE_MESH = 4      /* triangles [mesh_first_triangle, +mesh_num_triangles) of the
+                              scene's shared index buffer            (geometry.h:369-413) */
+};
+
+typedef struct pg_shape {
+    int32_t type;
+    int32_t material;       /* index into pg_scene_desc.materials, -1 = no material
+                               (a null surface that rays cross, path.cpp:42-46) */
+    int32_t medium_inside;  /* index into media, -1 = none (geometry.cpp:396-409) */
+    int32_t medium_outside;
+    int64_t mesh_first_triangle;
+    int64_t mesh_num_triangles;
+    float p[12];
+} pg_shape;
+
+/* ---- materials (src/core/material.h:35-106, src/core/bxdf.h:18-70) ---- */
+enum { PG_BSDF_DIFFUSE = 0, PG_BSDF_CONDUCTOR = 1, PG_BSDF_DIELECTRIC = 2 };
+enum { PG_MATERIAL_LAYERED = 0, PG_MATERIAL_EMISSIVE = 1 };
+#define PG_MAX_LAYERS 4
+
+typedef struct pg_bsdf {
+    int32_t type;
+    float albedo[3];
+    float roughness; /* alpha = clamp(roughness^2, 0.001, 1) (bxdf.cpp:37,88) */
+    float eta;
+} pg_bsdf;
+
+typedef struct pg_material {
+    int32_t type;
+    int32_t num_layers;            /* layered: layers[0] is the top layer (material.cpp:33-43) */
+    pg_bsdf layers[PG_MAX_LAYERS];
+    float emission[3];             /* emissive: one-sided radiance (material.h:60-65) */
+} pg_material;
+
+/* ---- lights (src/core/light.h:136-187).  Area lights are not listed here: every shape
+ * with an emissive material becomes an area light, appended after these in shape order,
+ * exactly as LoadScene does (fileio.cpp:271-273). ---- */
+enum {
+    PG_LIGHT_POINT = 0,        /* p[0..2] position, p[3..5] color  (light.cpp:9-16) */
+    PG_LIGHT_DIRECTIONAL = 1,  /* p[0..2] direction, p[3..5] color (light.cpp:33-41) */
+    PG_LIGHT_SKY = 2,          /* p[0..2] sunDirection, p[3..5] sunColor; environment
+                                  (light.cpp:65-79, color.cpp:91-99) */
+    PG_LIGHT_CONSTANT_ENV = 3  /* p[3..5] radiance; environment of uniform radiance,
+                                  sampled uniformly over the sphere.  Not in pine, whose
+                                  environment set is {Atmosphere, Sky}. */
+};
+
+typedef struct pg_light {
+    int32_t type;
+    float p[12];
+} pg_light;
+
+/* ---- participating media (src/core/medium.h:22-77) ---- */
+enum { PG_MEDIUM_HOMOGENEOUS = 0, PG_MEDIUM_GRID = 1 };
+
+typedef struct pg_medium {
+    int32_t type;
+    float sigma_a[3];
+    float sigma_s[3];
+    float g;               /* Henyey-Greenstein asymmetry */
+    int32_t size[3];       /* grid: voxels, x fastest (medium.cpp:156-160) */
+    float position[3];     /* grid: world placement (medium.cpp:180-182) */
+    float scale;
+    int32_t interpolate;   /* grid: trilinear (1, pine's default) or nearest (0) */
+    const float* density;  /* grid: size[0]*size[1]*size[2] floats, host memory */
+} pg_medium;
+
+/* ---- camera (ThinLenCamera, src/core/camera.h:18-51) ---- */
+typedef struct pg_camera {
+    float from[3];
+    float to[3];
+    float fov;             /* full angle in radians (camera.h:29) */
+    float lens_radius;
+    float focus_distance;
+    int32_t width, height; /* film size */
+    int32_t medium;        /* medium the camera sits in, -1 = none (camera.cpp:95-101) */
+} pg_camera;
+
+enum { PG_LIGHT_SAMPLER_POWER = 0, PG_LIGHT_SAMPLER_UNIFORM = 1 };
+
+typedef struct pg_scene_desc {
+    int32_t num_shapes;
+    const pg_shape* shapes;          /* pine order; the index is the shape id */
+    int64_t num_vertices;
+    const float* vertices;           /* xyz per vertex, shared by all meshes */
+    int64_t num_triangles;
+    const uint32_t* indices;         /* 3 per triangle, indices into vertices */
+    int32_t num_materials;
+    const pg_material* materials;
+    int32_t num_media;
+    const pg_medium* media;
+    int32_t num_lights;
+    const pg_light* lights;          /* explicit lights in scene-file order */
+    pg_camera camera;
+    int32_t light_sampler;           /* PG_LIGHT_SAMPLER_* (lightsampler.cpp:41-51) */
+    int32_t max_depth;               /* Path{maxDepth}, pine's default 4 (integrator.cpp:55) */
+    int32_t samples_per_pixel;       /* Path{sampler{samplesPerPixel}} */
+} pg_scene_desc;
+
+/* ---- render requests ---- */
+enum { PG_MATH_PINE = 0, PG_MATH_FAST = 1 };
+
+typedef struct pg_render_desc {
+    int32_t spp;            /* samples per pixel; <= 0 uses the scene's */
+    int32_t max_depth;      /* <= 0 uses the scene's */
+    uint64_t seed;          /* random stream key; equal seeds give identical images */
+    int32_t sample_offset;  /* index of the first sample (progressive rendering) */
+    int32_t math_mode;      /* PG_MATH_PINE reproduces pine's pstd numerics
+                               (src/pstd/math.h); PG_MATH_FAST uses CUDA intrinsics */
+    int32_t guiding;        /* 1: MIS-combine the learned vMF proposal with BSDF/phase
+                               sampling (fraction 0.5); 0: plain path tracing */
+    int32_t accumulate;     /* 1: add to the context's film instead of clearing it */
+} pg_render_desc;
+
+typedef struct pg_render_stats {
+    double seconds;         /* device time of the render (CUDA events) */
+    int64_t paths;          /* camera samples completed */
+    int64_t rays;           /* extension + shadow rays traced */
+    int64_t volume_steps;   /* tracking steps (density lookups) in grid media */
+    int64_t dropped;        /* samples with NaN/Inf radiance, not accumulated
+                               (integrator.cpp:156-157) */
+    int64_t launches;       /* kernel launches issued */
+} pg_render_stats;
+
+/* ---- context ---- */
+pg_status pg_create(pg_ctx** out, int device);
+void pg_destroy(pg_ctx* ctx);
+/* Most recent error message for ctx (or for the process when ctx is NULL). */
+const char* pg_last_error(const pg_ctx* ctx);
+
+/* Upload a flattened scene (host arrays are copied); builds the 8-wide compressed BVH
+ * and the majorant brick grids.  Returns the scene id in *scene_id. */
+pg_status pg_upload_scene(pg_ctx* ctx, const pg_scene_desc* desc, int32_t* scene_id);
+/* Parse a pine scene file (grammar of src/util/parser.cpp:45-101, numbers through a
+ * bit-exact restatement of pstd::stof) and upload it. */
+pg_status pg_load_scene_file(pg_ctx* ctx, const char* path, int32_t* scene_id);
+pg_status pg_release_scene(pg_ctx* ctx, int32_t scene_id);
+/* Film size and defaults of an uploaded scene. */
+pg_status pg_scene_info(pg_ctx* ctx, int32_t scene_id, int32_t* width, int32_t* height,
+                        int32_t* spp, int32_t* max_depth);
+
+/* Render one image.  Outputs (any may be NULL; then nothing is copied back):
+ * out_mean  width*height*3 floats, per-pixel mean radiance (linear RGB, before pine's
+ *           tonemap and gamma), row y = film y (pine flips rows only when writing the
+ *           image, film.h:60-62);
+ * out_var   width*height*3 floats, per-pixel unbiased sample variance of the samples;
+ * out_count width*height samples accumulated per pixel. */
+pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc, float* out_mean,
+                    float* out_var, uint32_t* out_count, pg_render_stats* stats);
+
+/* Closest hit for n rays (host arrays).  rays: n x 8 floats (o.xyz, d.xyz, tmin, tmax).
+ * Outputs: shape_id (pine shape index, -1 = miss), prim_id (triangle index within the
+ * mesh, -1 otherwise), t, uv (n x 2).  Any output may be NULL. */
+pg_status pg_intersect(pg_ctx* ctx, int32_t scene_id, const float* rays, int64_t n,
+                       int32_t* shape_id, int32_t* prim_id, float* t, float* uv);
+/* Same, but every pointer is device memory and the call does not synchronise with the
+ * host beyond the launch (for callers that keep rays resident on the GPU). */
+pg_status pg_intersect_device(pg_ctx* ctx, int32_t scene_id, const float* d_rays, int64_t n,
+                              int32_t* d_shape_id, int32_t* d_prim_id, float* d_t,
+                              float* d_uv);
+
+/* ---- batched requests (many renders in one persistent, graph-captured launch) ---- */
+typedef struct pg_request {
+    int32_t scene_id;
+    int32_t width, height;  /* <= 0: the scene's film size */
+    int32_t spp;
+    int32_t max_depth;      /* <= 0: the scene's */
+    uint64_t seed;
+    float* out_mean;        /* width*height*3, may be NULL */
+} pg_request;
+
+typedef struct pg_batch_result {
+    double seconds;         /* device time of the whole batch */
+    int64_t paths;
+    double* request_seconds; /* optional, n entries: completion time of each request,
+                                measured from the batch start */
+} pg_batch_result;
+
+typedef struct pg_tuning {
+    int32_t queue_capacity; /* path slots resident in the wavefront */
+    int32_t block_size;     /* threads per block of the bounce kernels */
+    int32_t split_shadow;   /* 1: shadow rays in their own kernel; 0: fused in shading */
+} pg_tuning;
+
+pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,
+                          pg_batch_result* result);
+/* Autotuner: times candidate tunings on a short sample of the request mix and keeps the
+ * fastest for this context.  *chosen receives it (may be NULL). */
+pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n, pg_tuning* chosen);
+pg_status pg_set_tuning(pg_ctx* ctx, const pg_tuning* tuning);
+pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* tuning);
+
+/* ---- synthetic scene inputs (seeded) ---- */
+/* n^3 fractal-noise cloud, x fastest; ~nonzero_fraction of voxels > 0; max exactly 1. */
+pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fraction, float* density);
+/* Pine's uncompressed volume file: int32 sx, sy, sz then floats (fileio.cpp:194-202). */
+pg_status pg_write_volume(const char* path, int sx, int sy, int sz, const float* density);
+/* Icosphere with 20*4^subdiv triangles, displaced along its normals by 4-octave noise of
+ * amplitude*radius, written as OBJ with plain decimals (pine's parser has no exponents). */
+pg_status pg_gen_icosphere_obj(const char* path, int subdiv, float radius, float cx, float cy,
+                               float cz, float amplitude, uint64_t seed,
+                               int64_t* out_triangles);
+
+/* ---- host restatements exposed for tests ---- */
+/* pstd::stof (src/pstd/string.cpp:50-68), bit-exact. */
+float pg_pstd_stof(const char* str, int64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PINE_GPU_H */

@@ -1,0 +1,378 @@
+// Test infrastructure, not product code.
+//
+// Harness that drives the reference renderer's own code (pine, compiled from its
+// unmodified sources by oracle/Makefile) so that its results can be pinned as golden
+// vectors and its CPU integrator can be timed.  Nothing in the GPU library links this.
+//
+// Modes (all paths absolute; arrays are raw little-endian, row-major):
+//   render <scene.txt> <prefix>      per-pixel mean / sample variance / count in FP64,
+//                                    replicating PixelIntegrator::Render + Compute
+//                                    (src/core/integrator.cpp:121-158) with the scene's
+//                                    own sampler and PathIntegrator::Li.
+//   hits   <scene.txt> <rays> <out>  closest hit per ray through BVH::Intersect
+//                                    (src/impl/accel/bvh.cpp:669-709), recording the
+//                                    shape index, triangle index, t and (u, v).
+//   math   <in> <out>                pstd math (src/pstd/math.h:142-351) on (a, b) pairs.
+//   stof   <in.txt> <out>            pstd::stof / stofs (src/pstd/string.cpp:50-120).
+//   bsdf   <in> <out>                Diffuse / Conductor / Dielectric F, PDF, Sample
+//                                    (src/core/bxdf.cpp) and HG phase (src/core/medium.cpp:9-31).
+//   camera <scene.txt> <in> <out>    ThinLenCamera::GenRay (src/core/camera.cpp:31-41).
+//   density <scene.txt> <in> <out>   GridMedium::Density (src/core/medium.cpp:141-160).
+//   time   <scene.txt>               wall time of the stock Integrator::Render() only
+//                                    (BVH build and file loading excluded).
+#include <core/scene.h>
+#include <core/scattering.h>
+#include <util/fileio.h>
+#include <util/parser.h>
+#include <util/parallel.h>
+#include <impl/integrator/path.h>
+
+// BVHImpl::Intersect is a template defined in this file; it is compiled here (and left
+// out of the library objects) so that the triangle index is reachable.
+#include <impl/accel/bvh.cpp>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pine;
+
+namespace {
+
+std::vector<float> ReadF32(const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) {
+        std::fprintf(stderr, "cannot open %s\n", path);
+        std::exit(2);
+    }
+    std::fseek(f, 0, SEEK_END);
+    long n = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    std::vector<float> v(n / 4);
+    if (n && std::fread(v.data(), 4, v.size(), f) != v.size())
+        std::exit(2);
+    std::fclose(f);
+    return v;
+}
+
+void WriteRaw(const char* path, const void* data, size_t bytes) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        std::fprintf(stderr, "cannot write %s\n", path);
+        std::exit(2);
+    }
+    if (bytes)
+        std::fwrite(data, 1, bytes, f);
+    std::fclose(f);
+}
+
+// Finite check on the bit pattern: the reference is built with -ffast-math, under which
+// isnan/isinf may fold to false, so the harness inspects the exponent bits itself.
+bool Finite(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    return (b & 0x7f800000u) != 0x7f800000u;
+}
+
+Scene* Load(const char* path) {
+    Scene* scene = new Scene;
+    LoadScene(path, scene);
+    return scene;
+}
+
+int Render(const char* scenePath, const std::string& prefix) {
+    Scene* scene = Load(scenePath);
+    auto* ri = dynamic_cast<RadianceIntegrator*>(scene->integrator.get());
+    if (!ri) {
+        std::fprintf(stderr, "integrator is not a RadianceIntegrator\n");
+        return 2;
+    }
+    vec2i size = ri->filmSize;
+    int spp = ri->samplesPerPixel;
+    int total = size.x * size.y;
+    std::vector<double> sum(total * 3), sumsq(total * 3);
+    std::vector<int64_t> count(total), dropped(total);
+
+    auto t0 = std::chrono::steady_clock::now();
+    ParallelFor(total, [&](int index) {
+        vec2i p = {index % size.x, index / size.x};
+        Sampler& sampler = ri->samplers[threadIdx];
+        sampler.StartPixel(p, 0);
+        for (int s = 0; s < spp; s++) {
+            vec2 pFilm = (p + sampler.Get2D()) / vec2(size);
+            Ray ray = scene->camera.GenRay(pFilm, sampler.Get2D());
+            Spectrum L = ri->Li(ray, sampler);
+            vec3 rgb = L.ToRGB();
+            if (Finite(rgb.x) && Finite(rgb.y) && Finite(rgb.z)) {
+                for (int c = 0; c < 3; c++) {
+                    sum[index * 3 + c] += rgb[c];
+                    sumsq[index * 3 + c] += double(rgb[c]) * rgb[c];
+                }
+                count[index]++;
+            } else {
+                dropped[index]++;
+            }
+            sampler.StartNextSample();
+        }
+    });
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+    std::vector<double> mean(total * 3), var(total * 3);
+    int64_t nDropped = 0;
+    for (int i = 0; i < total; i++) {
+        nDropped += dropped[i];
+        double n = (double)count[i];
+        for (int c = 0; c < 3; c++) {
+            double m = n > 0 ? sum[i * 3 + c] / n : 0.0;
+            mean[i * 3 + c] = m;
+            var[i * 3 + c] = n > 1 ? std::max(0.0, (sumsq[i * 3 + c] - n * m * m) / (n - 1)) : 0.0;
+        }
+    }
+    WriteRaw((prefix + "_mean.f64").c_str(), mean.data(), mean.size() * 8);
+    WriteRaw((prefix + "_var.f64").c_str(), var.data(), var.size() * 8);
+    WriteRaw((prefix + "_count.i64").c_str(), count.data(), count.size() * 8);
+    std::printf("{\"width\": %d, \"height\": %d, \"spp\": %d, \"seconds\": %.6f, "
+                "\"dropped\": %lld, \"threads\": %d}\n",
+                size.x, size.y, spp, secs, (long long)nDropped, NumThreads());
+    return 0;
+}
+
+int Hits(const char* scenePath, const char* raysPath, const char* outPath) {
+    Scene* scene = Load(scenePath);
+    auto* rayInt = dynamic_cast<RayIntegrator*>(scene->integrator.get());
+    auto* bvh = rayInt ? dynamic_cast<BVH*>(rayInt->accel.get()) : nullptr;
+    if (!bvh) {
+        std::fprintf(stderr, "accelerator is not pine's BVH\n");
+        return 2;
+    }
+    std::vector<float> rays = ReadF32(raysPath);
+    size_t n = rays.size() / 8;
+    struct Rec {
+        int32_t shape, tri;
+        float t, u, v;
+    };
+    std::vector<Rec> out(n);
+    ParallelFor((int)n, [&](int i) {
+        const float* r = &rays[i * 8];
+        Ray ray(vec3(r[0], r[1], r[2]), vec3(r[3], r[4], r[5]), r[6], r[7]);
+        Interaction it;
+        Rec rec{-1, -1, 0.0f, 0.0f, 0.0f};
+        if (!scene->shapes.size()) {
+            out[i] = rec;
+            return;
+        }
+        // Mirrors BVH::Intersect (bvh.cpp:669-709) but records the shape and triangle
+        // indices instead of filling the full interaction.
+        int triangleIndex = -1;
+        bool hit = bvh->tbvh.Intersect(
+            ray, it,
+            [&](Ray& ray, Interaction& it, int lbvhIndex) {
+                auto& shape = scene->shapes[bvh->indices[lbvhIndex]];
+                if (lbvhIndex < (int)bvh->lbvh.size()) {
+                    return bvh->lbvh[lbvhIndex].Intersect(
+                        ray, it,
+                        [&](Ray& ray, Interaction& it, int index) {
+                            return shape.Be<TriangleMesh>().GetTriangle(index).Intersect(ray, it);
+                        },
+                        [&](Interaction&, int tIndex) { triangleIndex = tIndex; });
+                } else {
+                    return shape.Intersect(ray, it);
+                }
+            },
+            [&](Interaction&, int lbvhIndex) {
+                rec.shape = bvh->indices[lbvhIndex];
+                rec.tri = lbvhIndex < (int)bvh->lbvh.size() ? triangleIndex : -1;
+            });
+        if (hit) {
+            rec.t = ray.tmax;
+            rec.u = it.uv.x;
+            rec.v = it.uv.y;
+        } else {
+            rec.shape = rec.tri = -1;
+        }
+        out[i] = rec;
+    });
+    WriteRaw(outPath, out.data(), out.size() * sizeof(Rec));
+    return 0;
+}
+
+int Math(const char* inPath, const char* outPath) {
+    std::vector<float> in = ReadF32(inPath);
+    size_t n = in.size() / 2;
+    const int K = 12;
+    std::vector<float> out(n * K);
+    for (size_t i = 0; i < n; i++) {
+        float a = in[2 * i], b = in[2 * i + 1];
+        float* o = &out[i * K];
+        o[0] = pstd::sqrt(a);
+        o[1] = pstd::log2(a);
+        o[2] = pstd::log(a);
+        o[3] = pstd::exp(a);
+        o[4] = pstd::cos(a);
+        o[5] = pstd::sin(a);
+        o[6] = pstd::tan(a);
+        o[7] = pstd::acos(a);
+        o[8] = pstd::asin(a);
+        o[9] = pstd::atan(a);
+        o[10] = pstd::atan2(a, b);
+        o[11] = pstd::pow(a, b);
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+int Stof(const char* inPath, const char* outPath) {
+    FILE* f = std::fopen(inPath, "rb");
+    if (!f)
+        return 2;
+    std::vector<float> out;
+    char line[4096];
+    while (std::fgets(line, sizeof(line), f)) {
+        size_t len = std::strlen(line);
+        while (len && (line[len - 1] == '\n' || line[len - 1] == '\r'))
+            line[--len] = 0;
+        pstd::string s(line, len);
+        out.push_back(pstd::stof(s));
+        float v[3];
+        pstd::stofs(s, v, 3);
+        out.insert(out.end(), v, v + 3);
+    }
+    std::fclose(f);
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+// Input rows (18 floats): type(0 diffuse, 1 conductor, 2 dielectric, 3 HG phase),
+// albedo rgb, roughness, eta (or g), wi xyz, wo xyz, u1, u2 xy, pad x3.
+// Output rows (16 floats): F rgb, PDF, sampleOk, wo xyz, f rgb, pdf, pad x4.
+int Bsdf(const char* inPath, const char* outPath) {
+    std::vector<float> in = ReadF32(inPath);
+    const int KI = 18, KO = 16;
+    size_t n = in.size() / KI;
+    std::vector<float> out(n * KO, 0.0f);
+    for (size_t i = 0; i < n; i++) {
+        const float* r = &in[i * KI];
+        float* o = &out[i * KO];
+        int type = (int)r[0];
+        vec3 wi(r[6], r[7], r[8]), wo(r[9], r[10], r[11]);
+        float u1 = r[12];
+        vec2 u2(r[13], r[14]);
+        if (type == 3) {
+            PhaseFunction ph(r[5]);
+            float p = ph.P(wi, wo);
+            o[0] = o[1] = o[2] = p;
+            o[3] = p;
+            vec3 ws;
+            float pdf = ph.Sample(wi, ws, u2);
+            o[4] = 1.0f;
+            o[5] = ws.x, o[6] = ws.y, o[7] = ws.z;
+            o[8] = o[9] = o[10] = pdf;
+            o[11] = pdf;
+            continue;
+        }
+        char text[512];
+        const char* names[] = {"Diffuse", "Conductor", "Dielectric"};
+        std::snprintf(text, sizeof(text),
+                      "bsdf: %s{\n albedo: %.9g %.9g %.9g\n roughness: %.9g\n eta: %.9g\n}\n",
+                      names[type], r[1], r[2], r[3], r[4], r[5]);
+        // pstd::stof has no exponent support; %.9g of values in [1e-4, 1e4) never uses one.
+        Parameters params = Parse(text);
+        BSDF bsdf = CreateBSDF(params["bsdf"]);
+        NodeEvalCtx nc(vec3(0.0f), vec3(0, 0, 1), vec2(0.0f));
+        vec3 f = bsdf.F(wi, wo, nc);
+        o[0] = f.x, o[1] = f.y, o[2] = f.z;
+        o[3] = bsdf.PDF(wi, wo, nc);
+        auto bs = bsdf.Sample(wi, u1, u2, nc);
+        if (bs) {
+            o[4] = 1.0f;
+            o[5] = bs->wo.x, o[6] = bs->wo.y, o[7] = bs->wo.z;
+            o[8] = bs->f[0], o[9] = bs->f[1], o[10] = bs->f[2];
+            o[11] = bs->pdf;
+        }
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+int CameraRays(const char* scenePath, const char* inPath, const char* outPath) {
+    Scene* scene = Load(scenePath);
+    std::vector<float> in = ReadF32(inPath);
+    size_t n = in.size() / 4;
+    std::vector<float> out(n * 6);
+    for (size_t i = 0; i < n; i++) {
+        Ray ray = scene->camera.GenRay(vec2(in[i * 4], in[i * 4 + 1]),
+                                       vec2(in[i * 4 + 2], in[i * 4 + 3]));
+        for (int k = 0; k < 3; k++) {
+            out[i * 6 + k] = ray.o[k];
+            out[i * 6 + 3 + k] = ray.d[k];
+        }
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+int Density(const char* scenePath, const char* inPath, const char* outPath) {
+    Scene* scene = Load(scenePath);
+    const GridMedium* grid = nullptr;
+    for (auto& m : scene->mediums)
+        if (m.second->Is<GridMedium>())
+            grid = &m.second->Be<GridMedium>();
+    if (!grid)
+        return 2;
+    std::vector<float> in = ReadF32(inPath);
+    size_t n = in.size() / 3;
+    std::vector<float> out(n);
+    for (size_t i = 0; i < n; i++)
+        out[i] = grid->Density(vec3(in[i * 3], in[i * 3 + 1], in[i * 3 + 2]));
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+int Time(const char* scenePath) {
+    auto tl = std::chrono::steady_clock::now();
+    Scene* scene = Load(scenePath);
+    double load = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl).count();
+    auto* integ = scene->integrator.get();
+    vec2i size = integ->filmSize;
+    auto t0 = std::chrono::steady_clock::now();
+    integ->Render();
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    double paths = (double)size.x * size.y * integ->samplesPerPixel;
+    std::printf("{\"seconds\": %.6f, \"paths\": %.0f, \"mpaths_per_s\": %.6f, \"threads\": %d, "
+                "\"load_seconds\": %.3f}\n",
+                secs, paths, paths / secs * 1e-6, NumThreads(), load);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: pine_ref <mode> ...\n");
+        return 2;
+    }
+    std::string mode = argv[1];
+    // Pine's own start-up sequence (src/cli/main.cpp:17-19); the profilers are not needed.
+    SampledSpectrum::Initialize();
+    if (mode == "render" && argc == 4)
+        return Render(argv[2], argv[3]);
+    if (mode == "hits" && argc == 5)
+        return Hits(argv[2], argv[3], argv[4]);
+    if (mode == "math" && argc == 4)
+        return Math(argv[2], argv[3]);
+    if (mode == "stof" && argc == 4)
+        return Stof(argv[2], argv[3]);
+    if (mode == "bsdf" && argc == 4)
+        return Bsdf(argv[2], argv[3]);
+    if (mode == "camera" && argc == 5)
+        return CameraRays(argv[2], argv[3], argv[4]);
+    if (mode == "density" && argc == 5)
+        return Density(argv[2], argv[3], argv[4]);
+    if (mode == "time" && argc == 3)
+        return Time(argv[2]);
+    std::fprintf(stderr, "bad arguments for mode %s\n", mode.c_str());
+    return 2;
+}

@@ -1,0 +1,219 @@
+"""pine_b200: a B200 (sm_100a) wavefront path tracer behind pine's integrator surface.
+
+This module is a thin ctypes binding of the C ABI in ``include/pine_gpu.h``
+(``libpinegpu.so``, built in-tree by :mod:`pine_b200.build`).  All rendering runs in
+the CUDA library; there is no CPU fallback, and every call fails with
+:class:`PgError` when the library or a GPU is missing.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libpinegpu.so")
+HEADER = os.path.join(ROOT, "include", "pine_gpu.h")
+
+PG_OK = 0
+STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_INVALID_ARG", 2: "PG_ERR_OOM", 3: "PG_ERR_CUDA",
+                4: "PG_ERR_DEVICE_LIMIT", 5: "PG_ERR_UNSUPPORTED", 6: "PG_ERR_IO",
+                7: "PG_ERR_PARSE"}
+MATH_MODES = {"pine": 0, "fast": 1}
+
+
+class PgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class RenderDesc(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32),
+                ("seed", ctypes.c_uint64), ("sample_offset", ctypes.c_int32),
+                ("math_mode", ctypes.c_int32), ("guiding", ctypes.c_int32),
+                ("accumulate", ctypes.c_int32)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("paths", ctypes.c_int64),
+                ("rays", ctypes.c_int64), ("volume_steps", ctypes.c_int64),
+                ("dropped", ctypes.c_int64), ("launches", ctypes.c_int64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("queue_capacity", ctypes.c_int32), ("block_size", ctypes.c_int32),
+                ("split_shadow", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("scene_id", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("spp", ctypes.c_int32),
+                ("max_depth", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("out_mean", ctypes.POINTER(ctypes.c_float))]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("paths", ctypes.c_int64),
+                ("request_seconds", ctypes.POINTER(ctypes.c_double))]
+
+
+_lib = None
+_P = ctypes.POINTER
+_F = _P(ctypes.c_float)
+_I32 = _P(ctypes.c_int32)
+_U32 = _P(ctypes.c_uint32)
+
+
+def declared_functions(header: str = HEADER):
+    """Names of the functions include/pine_gpu.h declares."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:pg_status|void|const char\s*\*|float)\s+(pg_\w+)\s*\(",
+                                 text, flags=re.M)))
+
+
+def lib():
+    """Loads libpinegpu.so (raising if it was not built) and declares its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PgError(3, f"{LIB_PATH} is not built; run pine_b200.build.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    st = ctypes.c_int
+    sig = {
+        "pg_create": (st, [_P(ctypes.c_void_p), ctypes.c_int]),
+        "pg_destroy": (None, [ctypes.c_void_p]),
+        "pg_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+        "pg_upload_scene": (st, [ctypes.c_void_p, ctypes.c_void_p, _I32]),
+        "pg_load_scene_file": (st, [ctypes.c_void_p, ctypes.c_char_p, _I32]),
+        "pg_release_scene": (st, [ctypes.c_void_p, ctypes.c_int32]),
+        "pg_scene_info": (st, [ctypes.c_void_p, ctypes.c_int32, _I32, _I32, _I32, _I32]),
+        "pg_render": (st, [ctypes.c_void_p, ctypes.c_int32, _P(RenderDesc), _F, _F, _U32,
+                           _P(RenderStats)]),
+        "pg_intersect": (st, [ctypes.c_void_p, ctypes.c_int32, _F, ctypes.c_int64, _I32, _I32,
+                              _F, _F]),
+        "pg_intersect_device": (st, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                     ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p]),
+        "pg_set_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
+        "pg_get_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
+        "pg_gen_cloud_volume": (st, [ctypes.c_int, ctypes.c_uint64, ctypes.c_float, _F]),
+        "pg_write_volume": (st, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]),
+        "pg_gen_icosphere_obj": (st, [ctypes.c_char_p, ctypes.c_int, ctypes.c_float,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_float, ctypes.c_uint64, _P(ctypes.c_int64)]),
+        "pg_pstd_stof": (ctypes.c_float, [ctypes.c_char_p, ctypes.c_int64]),
+    }
+    for name, (res, args) in sig.items():
+        if hasattr(L, name):
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+    if hasattr(L, "pg_render_batch"):
+        L.pg_render_batch.restype = st
+        L.pg_render_batch.argtypes = [ctypes.c_void_p, _P(Request), ctypes.c_int32,
+                                      _P(BatchResult)]
+        L.pg_autotune.restype = st
+        L.pg_autotune.argtypes = [ctypes.c_void_p, _P(Request), ctypes.c_int32, _P(Tuning)]
+    _lib = L
+    return L
+
+
+def _fptr(a):
+    return None if a is None else a.ctypes.data_as(_F)
+
+
+class Context:
+    """One CUDA device context of libpinegpu (not thread-safe, like pg_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        self._ctx = ctypes.c_void_p()
+        self._check(self._lib.pg_create(ctypes.byref(self._ctx), int(device)), global_err=True)
+
+    def _check(self, status: int, global_err: bool = False):
+        if status != PG_OK:
+            msg = self._lib.pg_last_error(None if global_err else self._ctx)
+            raise PgError(status, (msg or b"").decode(errors="replace"))
+
+    def close(self):
+        if self._ctx:
+            self._lib.pg_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- scenes
+    def load_scene(self, path: str) -> int:
+        sid = ctypes.c_int32(-1)
+        self._check(self._lib.pg_load_scene_file(self._ctx, os.path.abspath(path).encode(),
+                                                 ctypes.byref(sid)))
+        return sid.value
+
+    def release_scene(self, scene: int):
+        self._check(self._lib.pg_release_scene(self._ctx, int(scene)))
+
+    def scene_info(self, scene: int):
+        w, h, s, d = (ctypes.c_int32() for _ in range(4))
+        self._check(self._lib.pg_scene_info(self._ctx, int(scene), ctypes.byref(w),
+                                            ctypes.byref(h), ctypes.byref(s), ctypes.byref(d)))
+        return {"width": w.value, "height": h.value, "spp": s.value, "max_depth": d.value}
+
+    # ---- rendering
+    def render(self, scene: int, spp: int = 0, max_depth: int = 0, seed: int = 0,
+               math_mode: str = "pine", sample_offset: int = 0, accumulate: bool = False,
+               guiding: bool = False, outputs: bool = True):
+        info = self.scene_info(scene)
+        w, h = info["width"], info["height"]
+        desc = RenderDesc(int(spp), int(max_depth), int(seed), int(sample_offset),
+                          MATH_MODES[math_mode], int(bool(guiding)), int(bool(accumulate)))
+        stats = RenderStats()
+        mean = var = count = None
+        if outputs:
+            mean = np.zeros((h, w, 3), np.float32)
+            var = np.zeros((h, w, 3), np.float32)
+            count = np.zeros((h, w), np.uint32)
+        self._check(self._lib.pg_render(self._ctx, int(scene), ctypes.byref(desc), _fptr(mean),
+                                        _fptr(var),
+                                        None if count is None else count.ctypes.data_as(_U32),
+                                        ctypes.byref(stats)))
+        st = {k: getattr(stats, k) for k, _ in RenderStats._fields_}
+        return {"mean": mean, "var": var, "count": count, "stats": st}
+
+    def intersect(self, scene: int, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        sid = np.empty(n, np.int32)
+        pid = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        uv = np.empty((n, 2), np.float32)
+        self._check(self._lib.pg_intersect(self._ctx, int(scene), _fptr(rays), n,
+                                           sid.ctypes.data_as(_I32), pid.ctypes.data_as(_I32),
+                                           _fptr(t), _fptr(uv)))
+        return sid, pid, t, uv
+
+    # ---- tuning and batches
+    def tuning(self) -> dict:
+        t = Tuning()
+        self._check(self._lib.pg_get_tuning(self._ctx, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
+    def set_tuning(self, queue_capacity: int, block_size: int = 128, split_shadow: int = 1):
+        t = Tuning(int(queue_capacity), int(block_size), int(split_shadow))
+        self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))

@@ -1,0 +1,696 @@
+// Device shading: BSDFs, lights, phase function, media.  Formulas and operation order
+// follow pine (file:line cited per function); M selects pine's numerics or CUDA's.
+#pragma once
+
+#include "pg_device.cuh"
+
+namespace pg {
+
+// ---------------------------------------------------------------- random numbers
+// Counter-based stream: the value of draw `dim` of sample `key0` under seed word `key1`.
+// PCG's output permutation (O'Neill 2014) used as a 32-bit hash, three rounds.
+__device__ __forceinline__ uint32_t PcgHash(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+struct Rng {
+    uint32_t key0, key1, dim;
+    __device__ __forceinline__ float Get1D() {
+        uint32_t h = PcgHash(dim + key1);
+        h = PcgHash(h ^ key0);
+        h = PcgHash(h + key1);
+        dim++;
+        return (float)(h >> 8) * 0x1p-24f;
+    }
+    __device__ __forceinline__ void Get2D(float& a, float& b) {
+        a = Get1D();
+        b = Get1D();
+    }
+};
+
+// ---------------------------------------------------------------- frames and sampling
+template <int M>
+struct Frame {
+    V3 x, y, z;
+    __device__ __forceinline__ void From(V3 n) {
+        z = n;
+        CoordinateSystem<M>(n, x, y);
+    }
+    __device__ __forceinline__ V3 ToLocal(V3 w) const {
+        return {Dot(w, x), Dot(w, y), Dot(w, z)};
+    }
+    __device__ __forceinline__ V3 ToWorld(V3 v) const {
+        return x * v.x + y * v.y + z * v.z;  // mat3 * vec3 (vecmath.h:765-767)
+    }
+};
+
+template <int M>
+__device__ __forceinline__ V3 SphericalToCartesian(float phi, float theta) {
+    float st = PMath<M>::sin(theta);  // vecmath.h:1238-1241
+    return v3(st * PMath<M>::cos(phi), st * PMath<M>::sin(phi), PMath<M>::cos(theta));
+}
+template <int M>
+__device__ __forceinline__ V3 UniformSphereSampling(float u0, float u1) {
+    return SphericalToCartesian<M>(u0 * kPi * 2, PMath<M>::acos(1.0f - 2 * u1));  // sampling.h:41-43
+}
+template <int M>
+__device__ __forceinline__ void SampleDiskConcentric(float u0, float u1, float& dx, float& dy) {
+    u0 = u0 * 2 - 1.0f, u1 = u1 * 2 - 1.0f;  // sampling.h:22-33
+    float theta, r;
+    if (Fabs(u0) > Fabs(u1)) {
+        r = u0;
+        theta = kPi / 4.0f * u1 / u0;
+    } else {
+        r = u1;
+        theta = kPi / 2.0f - kPi / 4.0f * (u0 / u1);
+    }
+    dx = r * PMath<M>::cos(theta);
+    dy = r * PMath<M>::sin(theta);
+}
+template <int M>
+__device__ __forceinline__ void SampleDiskPolar(float u0, float u1, float& dx, float& dy) {
+    float r = PMath<M>::sqrt(u0), theta = 2 * kPi * u1;  // sampling.h:16-20
+    dx = r * PMath<M>::cos(theta);
+    dy = r * PMath<M>::sin(theta);
+}
+template <int M>
+__device__ __forceinline__ V3 CosineWeightedSampling(float u0, float u1) {
+    float dx, dy;
+    SampleDiskConcentric<M>(u0, u1, dx, dy);  // sampling.h:35-39
+    return v3(dx, dy, PMath<M>::sqrt(Max(1.0f - dx * dx - dy * dy, 0.0f)));
+}
+
+// ---------------------------------------------------------------- microfacets (scattering.h)
+__device__ __forceinline__ float CosTheta(V3 w) {
+    return w.z;
+}
+__device__ __forceinline__ float AbsCosTheta(V3 w) {
+    return Fabs(w.z);
+}
+__device__ __forceinline__ bool SameHemisphere(V3 a, V3 b) {
+    return a.z * b.z > 0.0f;
+}
+
+template <int M>
+struct TrowbridgeReitz {  // scattering.h:91-145, isotropic alpha
+    float alpha;
+    __device__ __forceinline__ float Sin2Theta(V3 w) const {
+        return Max(1.0f - Sqr(w.z), 0.0f);
+    }
+    __device__ __forceinline__ float SinTheta(V3 w) const {
+        return PMath<M>::sqrt(Sin2Theta(w));
+    }
+    __device__ __forceinline__ float Tan2Theta(V3 w) const {
+        return Sin2Theta(w) / Sqr(w.z);
+    }
+    __device__ __forceinline__ float CosPhi(V3 w) const {
+        float s = SinTheta(w);
+        return s == 0 ? 1 : Clamp(w.x / s, -1.0f, 1.0f);
+    }
+    __device__ __forceinline__ float SinPhi(V3 w) const {
+        float s = SinTheta(w);
+        return s == 0 ? 1 : Clamp(w.y / s, -1.0f, 1.0f);
+    }
+    __device__ __forceinline__ float D(V3 wm) const {
+        float tan2 = Tan2Theta(wm);
+        float cos4 = Sqr(Sqr(wm.z));
+        if (cos4 < 1e-6f)
+            return 0.0f;
+        float e = tan2 * (Sqr(CosPhi(wm) / alpha) + Sqr(SinPhi(wm) / alpha));
+        return 1.0f / (kPi * alpha * alpha * cos4 * Sqr(1 + e));
+    }
+    __device__ __forceinline__ float Lambda(V3 w) const {
+        float tan2 = Tan2Theta(w);
+        float a2 = Sqr(CosPhi(w) * alpha) + Sqr(SinPhi(w) * alpha);
+        return (PMath<M>::sqrt(1.0f + a2 * tan2) - 1.0f) / 2.0f;
+    }
+    __device__ __forceinline__ float G1(V3 w) const {
+        return 1.0f / (1.0f + Lambda(w));
+    }
+    __device__ __forceinline__ float G(V3 wi, V3 wo) const {
+        return 1.0f / (1.0f + Lambda(wi) + Lambda(wo));
+    }
+    __device__ __forceinline__ float Dv(V3 w, V3 wm) const {
+        return G1(w) / AbsCosTheta(w) * D(wm) * AbsDot(w, wm);
+    }
+    __device__ __forceinline__ float PDF(V3 w, V3 wm) const {
+        return Max(Dv(w, wm), kEpsilon);
+    }
+    __device__ __forceinline__ V3 SampleWm(V3 w, float u0, float u1) const {
+        V3 wh = Normalize<M>(v3(alpha * w.x, alpha * w.y, w.z));
+        if (wh.z < 0.0f)
+            wh = -wh;
+        V3 T1 = (wh.z < 0.99999f) ? Normalize<M>(Cross(v3(0, 0, 1), wh)) : v3(1, 0, 0);
+        V3 T2 = Cross(wh, T1);
+        float px, py;
+        SampleDiskPolar<M>(u0, u1, px, py);
+        float h = PMath<M>::sqrt(1.0f - Sqr(px));
+        float t = (1.0f + wh.z) / 2;
+        py = h * (1 - t) + py * t;  // pstd::lerp(t, h, py)
+        float pz = PMath<M>::sqrt(Max(0.0f, 1.0f - (px * px + py * py)));
+        V3 nh = T1 * px + T2 * py + wh * pz;
+        return Normalize<M>(v3(alpha * nh.x, alpha * nh.y, Max(1e-6f, nh.z)));
+    }
+};
+
+__device__ __forceinline__ V3 Reflect(V3 wi, V3 n) {
+    return 2.0f * Dot(wi, n) * n - wi;  // scattering.h:45-47
+}
+template <int M>
+__device__ __forceinline__ bool Refract(V3 wi, V3 n, float eta, V3& wt) {
+    float cosI = Dot(n, wi);  // scattering.h:48-67
+    if (cosI < 0) {
+        eta = 1.0f / eta;
+        cosI = -cosI;
+        n = -n;
+    }
+    float sin2I = Max(0.0f, 1.0f - Sqr(cosI));
+    float sin2T = sin2I / Sqr(eta);
+    if (sin2T >= 1)
+        return false;
+    float cosT = PMath<M>::sqrt(1.0f - sin2T);
+    wt = -wi / eta + (cosI / eta - cosT) * n;
+    return true;
+}
+template <int M>
+__device__ __forceinline__ float FrDielectric(float cosI, float eta) {
+    cosI = Clamp(cosI, -1.0f, 1.0f);  // scattering.h:69-85
+    if (cosI < 0) {
+        eta = 1 / eta;
+        cosI = -cosI;
+    }
+    float sin2I = 1.0f - Sqr(cosI);
+    float sin2T = sin2I / Sqr(eta);
+    if (sin2T >= 1.0f)
+        return 1.0f;
+    float cosT = PMath<M>::sqrt(1.0f - sin2T);
+    float rParl = (eta * cosI - cosT) / (eta * cosI + cosT);
+    float rPerp = (cosI - eta * cosT) / (cosI + eta * cosT);
+    return (Sqr(rParl) + Sqr(rPerp)) / 2.0f;
+}
+template <int M>
+__device__ __forceinline__ V3 FrSchlick(V3 F0, float cosT) {
+    float p = M == kPine ? PstdPowi(1.0f - cosT, 5) : PMath<M>::pow5(1.0f - cosT);  // pow(x, 5.0f)
+    return F0 + (v3(1.0f) - F0) * p;
+}
+
+// ---------------------------------------------------------------- BSDFs (bxdf.cpp)
+struct BsdfSample {
+    V3 wo, f;
+    float pdf;
+};
+
+template <int M>
+__device__ bool BsdfSampleOne(const BsdfDev& b, V3 wi, float u1, float u20, float u21,
+                              BsdfSample& bs) {
+    V3 albedo = v3(b.albedo[0], b.albedo[1], b.albedo[2]);
+    if (b.type == PG_BSDF_DIFFUSE) {  // bxdf.cpp:7-19
+        V3 wo = CosineWeightedSampling<M>(u20, u21);
+        if (CosTheta(wi) < 0)
+            wo = wo * -1.0f;
+        bs.wo = wo;
+        bs.pdf = AbsCosTheta(wo) / kPi;
+        bs.f = albedo / kPi;
+        return true;
+    }
+    TrowbridgeReitz<M> distrib{b.alpha};
+    if (b.type == PG_BSDF_CONDUCTOR) {  // bxdf.cpp:33-54
+        V3 wm = distrib.SampleWm(wi, u20, u21);
+        V3 wo = Reflect(wi, wm);
+        if (!SameHemisphere(wi, wo))
+            return false;
+        V3 fr = FrSchlick<M>(albedo, AbsCosTheta(wm));
+        bs.wo = wo;
+        bs.pdf = distrib.PDF(wi, wm) / (4 * AbsDot(wi, wm));
+        bs.f = fr * distrib.D(wm) * distrib.G(wo, wi) / (4 * CosTheta(wi) * CosTheta(wo));
+        return true;
+    }
+    // Dielectric, bxdf.cpp:80-119
+    float etap = b.eta;
+    if (CosTheta(wi) < 0)
+        etap = 1.0f / etap;
+    float fr = FrDielectric<M>(AbsCosTheta(wi), etap);
+    V3 wm = distrib.SampleWm(wi, u20, u21);
+    if (u1 < fr) {
+        V3 wo = Reflect(wi, wm);
+        if (!SameHemisphere(wi, wo))
+            return false;
+        bs.wo = wo;
+        bs.pdf = fr * distrib.PDF(wi, wm) / (4 * AbsDot(wi, wm));
+        bs.f = albedo * fr * distrib.D(wm) * distrib.G(wo, wi) / (4 * CosTheta(wi) * CosTheta(wo));
+    } else {
+        V3 wo;
+        if (!Refract<M>(wi, wm, etap, wo))
+            return false;
+        float cosO = CosTheta(wo), cosI = CosTheta(wi);
+        bs.wo = wo;
+        float denom = Sqr(Dot(wo, wm) + Dot(wi, wm) / etap);
+        float dwm = AbsDot(wo, wm) / denom;
+        bs.pdf = (1.0f - fr) * distrib.PDF(wi, wm) * dwm;
+        bs.f = albedo * (1.0f - fr) * distrib.D(wm) * distrib.G(wi, wo) *
+               Fabs(Dot(wo, wm) * Dot(wi, wm) / denom / cosI / cosO);
+    }
+    return true;
+}
+
+template <int M>
+__device__ void BsdfEvalOne(const BsdfDev& b, V3 wi, V3 wo, V3& f, float& pdf) {
+    V3 albedo = v3(b.albedo[0], b.albedo[1], b.albedo[2]);
+    if (b.type == PG_BSDF_DIFFUSE) {  // bxdf.cpp:21-31
+        bool same = SameHemisphere(wi, wo);
+        f = same ? albedo / kPi : v3(0.0f);
+        pdf = same ? AbsCosTheta(wo) / kPi : kEpsilon;
+        return;
+    }
+    TrowbridgeReitz<M> distrib{b.alpha};
+    if (b.type == PG_BSDF_CONDUCTOR) {  // bxdf.cpp:56-78
+        if (!SameHemisphere(wi, wo)) {
+            f = v3(0.0f);
+            pdf = 0.0f;
+            return;
+        }
+        V3 wh = Normalize<M>(wi + wo);
+        V3 fr = FrSchlick<M>(albedo, AbsCosTheta(wh));
+        f = fr * distrib.D(wh) * distrib.G(wo, wi) / (4 * AbsCosTheta(wo) * AbsCosTheta(wi));
+        pdf = distrib.PDF(wi, wh) / (4 * AbsDot(wi, wh));
+        return;
+    }
+    // Dielectric, bxdf.cpp:121-165
+    float cosO = CosTheta(wo), cosI = CosTheta(wi);
+    bool reflect = cosI * cosO > 0;
+    float etap = b.eta;
+    if (!reflect)
+        etap = 1.0f / etap;
+    V3 wm = Normalize<M>(wi * etap + wo);
+    if (Dot(wm, v3(0, 0, 1)) < 0.0f)
+        wm = -wm;  // FaceForward(wm, (0,0,1))
+    f = v3(0.0f);
+    pdf = 0.0f;
+    if (Dot(wm, wo) * cosI < 0.0f || Dot(wm, wi) * cosO < 0.0f)
+        return;
+    float fr = FrDielectric<M>(AbsCosTheta(wi), b.eta);
+    if (reflect) {
+        f = albedo * fr * distrib.D(wm) * distrib.G(wo, wi) / (4 * cosI * cosO);
+        pdf = fr * distrib.PDF(wi, wm) / (4 * AbsDot(wi, wm));
+    } else {
+        float d2 = Sqr(Dot(wo, wm) + Dot(wi, wm) / etap);
+        float denom = d2 * cosI * cosO;
+        f = albedo * (1.0f - fr) * distrib.D(wm) * distrib.G(wi, wo) *
+            Fabs(Dot(wo, wm) * Dot(wi, wm) / denom);
+        pdf = (1.0f - fr) * distrib.PDF(wi, wm) * (AbsDot(wo, wm) / d2);
+    }
+}
+
+// LayeredMaterial (material.cpp:9-31): sample layers top-down until one reflects into the
+// incident hemisphere; F and PDF sum over all layers.
+template <int M>
+__device__ bool MaterialSample(const MaterialDev& m, V3 wi, float u1, float u20, float u21,
+                               BsdfSample& bs) {
+    bool ok = false;
+    for (int i = 0; i < m.num_layers; i++) {
+        ok = BsdfSampleOne<M>(m.layers[i], wi, u1, u20, u21, bs);
+        if (ok && SameHemisphere(wi, bs.wo))
+            break;
+    }
+    return ok;
+}
+template <int M>
+__device__ void MaterialEval(const MaterialDev& m, V3 wi, V3 wo, V3& f, float& pdf) {
+    f = v3(0.0f);
+    pdf = 0.0f;
+    for (int i = 0; i < m.num_layers; i++) {
+        V3 fi;
+        float pi;
+        BsdfEvalOne<M>(m.layers[i], wi, wo, fi, pi);
+        f += fi;
+        pdf += pi;
+    }
+}
+
+// ---------------------------------------------------------------- phase (medium.cpp:9-31)
+template <int M>
+__device__ __forceinline__ float PhaseHG(float cosT, float g) {
+    float denom = 1.0f + g * g + 2 * g * cosT;
+    return (1 - g * g) / (denom * PMath<M>::sqrt(denom) * kPi * 4);
+}
+// P uses |wi . wo| (medium.cpp:14-16), as pine does.
+template <int M>
+__device__ __forceinline__ float PhaseP(float g, V3 wi, V3 wo) {
+    return PhaseHG<M>(AbsDot(wi, wo), g);
+}
+template <int M>
+__device__ __forceinline__ float PhaseSample(float g, V3 wi, V3& wo, float u0, float u1) {
+    float cosT;
+    if (Fabs(g) < 1e-3f) {
+        cosT = 1 - 2 * u0;
+    } else {
+        float sq = (1.0f - g * g) / (1 + g - 2 * g * u0);
+        cosT = -(1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    float s2 = 1.0f - cosT * cosT;
+    float sinT = PMath<M>::sqrt(M == kPine ? s2 : Max(s2, 0.0f));
+    float phi = 2 * kPi * u1;
+    Frame<M> f;
+    f.From(wi);
+    wo = f.ToWorld(v3(sinT * PMath<M>::cos(phi), sinT * PMath<M>::sin(phi), cosT));
+    return PhaseHG<M>(cosT, g);
+}
+
+// ---------------------------------------------------------------- environment
+// SkyColor (color.cpp:91-99): exact sun direction gives 8 * sunColor; otherwise a gradient
+// in the polar angle measured from +y.
+template <int M>
+__device__ V3 SkyColor(V3 dir, V3 sunDir, V3 sunColor) {
+    if (sunDir.x == dir.x && sunDir.y == dir.y && sunDir.z == dir.z)
+        return sunColor * 8.0f;
+    float theta = PMath<M>::acos(dir.y) / kPi;  // after swapping y and z, acos(d.z)
+    V3 a = v3(0.01f, 0.03f, 0.3f), b = v3(0.3f, 0.5f, 0.8f);
+    V3 l = a * (1 - theta) + b * theta;
+    return sunColor * (l * l);
+}
+
+struct LightSample {
+    V3 Le, wo;
+    float distance, pdf;
+    bool isDelta;
+};
+
+// Light::Sample (light.cpp:9-79, geometry.h:432-442 for area lights).
+template <int M>
+__device__ void SampleLight(const SceneDev& S, const LightDev& l, V3 p, float u0, float u1,
+                            LightSample& ls) {
+    ls.distance = 1.0f;
+    ls.pdf = 1.0f;
+    ls.isDelta = false;
+    V3 a = v3(l.p[0], l.p[1], l.p[2]), c = v3(l.p[3], l.p[4], l.p[5]);
+    switch (l.type) {
+    case kLightPoint:
+        ls.wo = Normalize<M>(a - p, ls.distance);
+        ls.pdf = Sqr(ls.distance);
+        ls.Le = c;
+        ls.isDelta = true;
+        return;
+    case kLightDirectional:
+        ls.Le = c;
+        ls.wo = a;
+        ls.distance = 1e+10f;
+        ls.isDelta = true;
+        return;
+    case kLightSky:
+        ls.distance = 1e+10f;
+        ls.isDelta = true;
+        ls.wo = a;
+        ls.Le = SkyColor<M>(a, a, c);
+        return;
+    case kLightConstant:
+        ls.distance = 1e+10f;
+        ls.wo = UniformSphereSampling<M>(u0, u1);
+        ls.pdf = 1.0f / (4 * kPi);
+        ls.Le = c;
+        return;
+    default: {
+        const ShapeDev& sh = S.shapes[l.shape];
+        V3 sp, sn;
+        if (sh.type == PG_SHAPE_SPHERE) {
+            sn = UniformSphereSampling<M>(u0, u1);
+            sp = v3(sh.p[0], sh.p[1], sh.p[2]) + sh.p[3] * sn;
+        } else if (sh.type == PG_SHAPE_RECT) {
+            sp = v3(sh.p[0], sh.p[1], sh.p[2]) + v3(sh.p[3], sh.p[4], sh.p[5]) * sh.p[12] * (u0 - 0.5f) +
+                 v3(sh.p[6], sh.p[7], sh.p[8]) * sh.p[13] * (u1 - 0.5f);
+            sn = v3(sh.p[9], sh.p[10], sh.p[11]);
+        } else {  // triangle
+            if (u0 + u1 > 1.0f)
+                u0 = 1.0f - u0, u1 = 1.0f - u1;
+            V3 v0 = v3(sh.p[0], sh.p[1], sh.p[2]), v1 = v3(sh.p[3], sh.p[4], sh.p[5]),
+               v2 = v3(sh.p[6], sh.p[7], sh.p[8]);
+            sp = (1.0f - u0 - u1) * v0 + u0 * v1 + u1 * v2;
+            sn = Normalize<M>(Cross(v0 - v1, v0 - v2));
+        }
+        sp = OffsetRayOrigin(sp, sn);
+        ls.wo = Normalize<M>(sp - p, ls.distance);
+        const MaterialDev& mat = S.materials[sh.material];
+        ls.Le = Dot(-ls.wo, sn) > 0.0f ? v3(mat.emission[0], mat.emission[1], mat.emission[2])
+                                        : v3(0.0f);
+        ls.pdf = Sqr(ls.distance) / (AbsDot(-ls.wo, sn) * sh.area);
+        return;
+    }
+    }
+}
+
+// PowerLightSampler / UniformLightSampler (lightsampler.cpp:6-34, distribution.h:10-58).
+// Pine's discrete probability is func[i] / N (Distribution1D::SampleDiscrete does not
+// divide by the integral); with all powers zero the pick is uniform.
+__device__ __forceinline__ int PickLight(const SceneDev& S, float u, float& pdf) {
+    int n = S.num_lights;
+    if (n == 0)
+        return -1;
+    if (S.uniform_lights || S.light_func_int == 0.0f) {
+        int i = min((int)(u * n), n - 1);
+        pdf = 1.0f / n;
+        return i;
+    }
+    int first = 0, len = n + 1;  // FindInterval over cdf[0..n] (core/math.h:67-84)
+    while (len > 0) {
+        int half = len / 2, middle = first + half;
+        if (S.light_cdf[middle] <= u) {
+            first = middle + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    int i = max(0, min(first - 1, n - 1));
+    pdf = S.light_func[i] / n;
+    return i;
+}
+
+// ---------------------------------------------------------------- media (medium.cpp)
+__device__ __forceinline__ V3 Affine(const float* m, V3 p) {
+    return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+              m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+}
+__device__ __forceinline__ V3 Linear(const float* m, V3 d) {
+    return v3(m[0] * d.x + m[1] * d.y + m[2] * d.z, m[4] * d.x + m[5] * d.y + m[6] * d.z,
+              m[8] * d.x + m[9] * d.y + m[10] * d.z);
+}
+
+// AABB::Hit(Ray, tmin&, tmax&) against the unit cube (geometry.cpp:67-87).
+__device__ __forceinline__ bool UnitBoxHit(V3 o, V3 d, float& tmin, float& tmax) {
+    if (tmin > tmax)
+        return false;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        float oi = Comp(o, i), di = Comp(d, i);
+        float inv = 1.0f / di;
+        float tn = (0.0f - oi) * inv, tf = (1.0f - oi) * inv;
+        if (di < 0.0f) {
+            float tmp = tn;
+            tn = tf;
+            tf = tmp;
+        }
+        tmin = tn > tmin ? tn : tmin;
+        tmax = tf < tmax ? tf : tmax;
+        if (tmin > tmax)
+            return false;
+    }
+    return true;
+}
+
+// GridMedium::Density (medium.cpp:141-160): voxel-index space p * size, trilinear between
+// the integer lattice points floor(p) and floor(p)+1, zero outside the grid.
+__device__ __forceinline__ float VoxelD(const MediumDev& m, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= m.size[0] || y >= m.size[1] || z >= m.size[2])
+        return 0.0f;
+    return __ldg(&m.density[(size_t)x + (size_t)y * m.size[0] + (size_t)z * m.size[0] * m.size[1]]);
+}
+__device__ __forceinline__ float GridDensity(const MediumDev& m, float vx, float vy, float vz) {
+    int ix = (int)vx, iy = (int)vy, iz = (int)vz;
+    if (!m.interpolate)
+        return VoxelD(m, ix, iy, iz);
+    float fx = vx - ix, fy = vy - iy, fz = vz - iz;
+    float d000 = VoxelD(m, ix, iy, iz), d001 = VoxelD(m, ix, iy, iz + 1);
+    float d010 = VoxelD(m, ix, iy + 1, iz), d011 = VoxelD(m, ix, iy + 1, iz + 1);
+    float d100 = VoxelD(m, ix + 1, iy, iz), d101 = VoxelD(m, ix + 1, iy, iz + 1);
+    float d110 = VoxelD(m, ix + 1, iy + 1, iz), d111 = VoxelD(m, ix + 1, iy + 1, iz + 1);
+    float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+    return gx * (gy * (gz * d000 + fz * d001) + fy * (gz * d010 + fz * d011)) +
+           fx * (gy * (gz * d100 + fz * d101) + fy * (gz * d110 + fz * d111));
+}
+
+// Walks the 8^3-voxel bricks crossed by the medium-space ray o + t d, t in [t0, t1], in
+// order (3D DDA), calling f(tEnter, tExit, majorant) for bricks whose majorant is > 0.
+// f returns true to stop the walk.
+template <typename F>
+__device__ __forceinline__ void WalkBricks(const MediumDev& m, V3 o, V3 d, float t0, float t1,
+                                           F&& f) {
+    // Voxel-index space: v = (o + t d) * size; bricks are 8 voxels wide.
+    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
+    V3 vo = v3(o.x * sx, o.y * sy, o.z * sz), vd = v3(d.x * sx, d.y * sy, d.z * sz);
+    float px = vo.x + t0 * vd.x, py = vo.y + t0 * vd.y, pz = vo.z + t0 * vd.z;
+    int bx = min(max((int)floorf(px * 0.125f), 0), m.nb[0] - 1);
+    int by = min(max((int)floorf(py * 0.125f), 0), m.nb[1] - 1);
+    int bz = min(max((int)floorf(pz * 0.125f), 0), m.nb[2] - 1);
+    int stx = vd.x > 0.0f ? 1 : -1, sty = vd.y > 0.0f ? 1 : -1, stz = vd.z > 0.0f ? 1 : -1;
+    float inx = vd.x != 0.0f ? 1.0f / vd.x : 0.0f, iny = vd.y != 0.0f ? 1.0f / vd.y : 0.0f,
+          inz = vd.z != 0.0f ? 1.0f / vd.z : 0.0f;
+    auto nextT = [&](int b, int st, float vo_, float in) {
+        if (in == 0.0f)
+            return kFloatMax;
+        float plane = (float)((b + (st > 0 ? 1 : 0)) * 8);
+        return (plane - vo_) * in;
+    };
+    float tx = nextT(bx, stx, vo.x, inx), ty = nextT(by, sty, vo.y, iny), tz = nextT(bz, stz, vo.z, inz);
+    float dtx = inx != 0.0f ? 8.0f * Fabs(inx) : kFloatMax, dty = iny != 0.0f ? 8.0f * Fabs(iny) : kFloatMax,
+          dtz = inz != 0.0f ? 8.0f * Fabs(inz) : kFloatMax;
+    float t = t0;
+    const int maxSteps = m.nb[0] + m.nb[1] + m.nb[2] + 4;
+    for (int i = 0; i < maxSteps && t < t1; i++) {
+        float tn = Min(Min(tx, ty), Min(tz, t1));
+        float maj = __ldg(&m.majorant[bx + m.nb[0] * (by + m.nb[1] * bz)]);
+        if (maj > 0.0f && tn > t) {
+            if (f(t, tn, maj))
+                return;
+        }
+        t = tn;
+        if (tx <= ty && tx <= tz) {
+            bx += stx;
+            tx += dtx;
+            if (bx < 0 || bx >= m.nb[0])
+                return;
+        } else if (ty <= tz) {
+            by += sty;
+            ty += dty;
+            if (by < 0 || by >= m.nb[1])
+                return;
+        } else {
+            bz += stz;
+            tz += dtz;
+            if (bz < 0 || bz >= m.nb[2])
+                return;
+        }
+    }
+}
+
+struct MediumEvent {
+    bool scattered;
+    V3 p;       // world position of the scattering event
+    V3 weight;  // beta multiplier (medium.cpp:98-139 returns sigma_s/sigma_t or 1)
+};
+
+// GridMedium::Sample (medium.cpp:98-116) with per-brick majorants instead of the global
+// one; delta tracking is unbiased for any majorant that bounds the density it samples.
+// HomogeneousMedium::Sample (medium.cpp:38-53).  `tmax` is the world-space hit distance,
+// used as the bound in medium space as pine does (medium.cpp:99-101).
+template <int M>
+__device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng,
+                                  MediumEvent& ev, uint32_t& steps, uint32_t& err) {
+    ev.scattered = false;
+    ev.weight = v3(1.0f);
+    if (m.type == PG_MEDIUM_HOMOGENEOUS) {
+        V3 st = v3(m.sigma_a[0] + m.sigma_s[0], m.sigma_a[1] + m.sigma_s[1], m.sigma_a[2] + m.sigma_s[2]);
+        int ch = (int)(rng.Get1D() * 3);
+        ch = min(ch, 2);
+        float dist = -PMath<M>::log(1.0f - rng.Get1D()) / Comp(st, ch);
+        bool sampled = dist < tmax;
+        float t = Min(dist, tmax);
+        V3 tr = v3(PMath<M>::exp(-st.x * t), PMath<M>::exp(-st.y * t), PMath<M>::exp(-st.z * t));
+        if (sampled) {
+            ev.scattered = true;
+            ev.p = o + t * d;
+            float pdf = (st.x * tr.x + st.y * tr.y + st.z * tr.z) / 3.0f;
+            ev.weight = v3(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]) * tr / pdf;
+        } else {
+            float pdf = (tr.x + tr.y + tr.z) / 3.0f;
+            ev.weight = tr / pdf;
+        }
+        return;
+    }
+    V3 mo = Affine(m.w2m, o);
+    V3 md = Normalize<M>(Linear(m.w2m, d));
+    float t0 = 0.0f, t1 = tmax;
+    if (!UnitBoxHit(mo, md, t0, t1))
+        return;
+    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
+    float ts = 0.0f;
+    uint32_t n = 0;
+    bool hit = false;
+    WalkBricks(m, mo, md, t0, t1, [&](float ta, float tb, float maj) {
+        float inv = 1.0f / (m.sigma_t * maj);
+        float t = ta;
+        while (true) {
+            t -= PMath<M>::log(1.0f - rng.Get1D()) * inv;
+            if (t >= tb)
+                return false;
+            if (++n > (uint32_t)kTrackingCap) {
+                err |= kErrTrackingCap;
+                return true;
+            }
+            float dens = GridDensity(m, (mo.x + t * md.x) * sx, (mo.y + t * md.y) * sy,
+                                     (mo.z + t * md.z) * sz);
+            if (dens / maj > rng.Get1D()) {
+                ts = t;
+                hit = true;
+                return true;
+            }
+        }
+    });
+    steps += n;
+    if (hit) {
+        ev.scattered = true;
+        ev.p = Affine(m.m2w, mo + ts * md);
+        ev.weight = v3(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]) / m.sigma_t;
+    }
+}
+
+// GridMedium::Tr (medium.cpp:55-80): ratio tracking with pine's Russian roulette once the
+// transmittance estimate drops below 0.1.  HomogeneousMedium::Tr (medium.cpp:33-36).
+template <int M>
+__device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng, uint32_t& steps,
+                          uint32_t& err, V3& trRGB) {
+    if (m.type == PG_MEDIUM_HOMOGENEOUS) {
+        trRGB = v3(PMath<M>::exp(-tmax * (m.sigma_a[0] + m.sigma_s[0])),
+                   PMath<M>::exp(-tmax * (m.sigma_a[1] + m.sigma_s[1])),
+                   PMath<M>::exp(-tmax * (m.sigma_a[2] + m.sigma_s[2])));
+        return 1.0f;
+    }
+    trRGB = v3(1.0f);
+    V3 mo = Affine(m.w2m, o);
+    V3 md = Normalize<M>(Linear(m.w2m, d));
+    float t0 = 0.0f, t1 = tmax;
+    if (!UnitBoxHit(mo, md, t0, t1))
+        return 1.0f;
+    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
+    float tr = 1.0f;
+    uint32_t n = 0;
+    WalkBricks(m, mo, md, t0, t1, [&](float ta, float tb, float maj) {
+        float inv = 1.0f / (m.sigma_t * maj);
+        float t = ta;
+        while (true) {
+            t -= PMath<M>::log(1.0f - rng.Get1D()) * inv;
+            if (t >= tb)
+                return false;
+            if (++n > (uint32_t)kTrackingCap) {
+                err |= kErrTrackingCap;
+                tr = 0.0f;
+                return true;
+            }
+            float dens = GridDensity(m, (mo.x + t * md.x) * sx, (mo.y + t * md.y) * sy,
+                                     (mo.z + t * md.z) * sz);
+            tr *= 1.0f - Max(0.0f, dens / maj);
+            if (tr < 0.1f) {
+                float q = Max(0.05f, 1.0f - tr);
+                if (rng.Get1D() < q) {
+                    tr = 0.0f;
+                    return true;
+                }
+                tr /= 1.0f - q;
+            }
+        }
+    });
+    steps += n;
+    trRGB = v3(tr);
+    return tr;
+}
+
+}  // namespace pg

@@ -1,0 +1,955 @@
+// libpinegpu: C ABI entry points (include/pine_gpu.h) around the wavefront kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "bvh_build.h"
+#include "pg_kernels.cuh"
+#include "pine_gpu.h"
+#include "scene_load.h"
+
+namespace pg {
+
+// ---------------------------------------------------------------- errors
+struct Failure {
+    pg_status status;
+    std::string msg;
+};
+
+static std::mutex g_errMutex;
+static std::string g_err;
+
+static void SetGlobalError(const std::string& m) {
+    std::lock_guard<std::mutex> lk(g_errMutex);
+    g_err = m;
+}
+
+#define PG_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            throw Failure{e_ == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_CUDA,       \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+    } while (0)
+
+static void Require(bool ok, const std::string& msg, pg_status s = PG_ERR_INVALID_ARG) {
+    if (!ok)
+        throw Failure{s, msg};
+}
+
+// ---------------------------------------------------------------- device memory
+struct DevMem {
+    std::vector<void*> ptrs;
+    template <typename T>
+    T* Alloc(size_t n) {
+        void* p = nullptr;
+        if (n == 0)
+            n = 1;
+        PG_CUDA(cudaMalloc(&p, n * sizeof(T)));
+        ptrs.push_back(p);
+        return (T*)p;
+    }
+    template <typename T>
+    T* Upload(const std::vector<T>& v, cudaStream_t s) {
+        T* p = Alloc<T>(v.size());
+        if (!v.empty())
+            PG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+        return p;
+    }
+    void Free() {
+        for (void* p : ptrs)
+            cudaFree(p);
+        ptrs.clear();
+    }
+    ~DevMem() { Free(); }
+};
+
+struct DeviceScene {
+    SceneDev dev{};
+    DevMem mem;
+    int width = 0, height = 0, spp = 1, max_depth = 4;
+    bool surfaces = false;
+    int64_t prims = 0;
+    int bvh_depth = 0;
+};
+
+template <typename T>
+static T Ceil(T a, T b) {
+    return (a + b - 1) / b;
+}
+
+// ---------------------------------------------------------------- path pool
+struct Pool {
+    DevMem mem;
+    int slots = 0;
+    float4 *ray_o = nullptr, *ray_d = nullptr, *beta = nullptr, *L = nullptr, *hit = nullptr;
+    uint32_t* sample = nullptr;
+    int *state = nullptr, *active = nullptr;
+    float4 *so = nullptr, *sd = nullptr, *sc = nullptr;
+    uint32_t* skey = nullptr;
+    void Ensure(int n) {
+        if (n <= slots)
+            return;
+        mem.Free();
+        slots = n;
+        ray_o = mem.Alloc<float4>(n);
+        ray_d = mem.Alloc<float4>(n);
+        beta = mem.Alloc<float4>(n);
+        L = mem.Alloc<float4>(n);
+        hit = mem.Alloc<float4>(n);
+        sample = mem.Alloc<uint32_t>(n);
+        state = mem.Alloc<int>(n);
+        active = mem.Alloc<int>(n);
+        so = mem.Alloc<float4>(n);
+        sd = mem.Alloc<float4>(n);
+        sc = mem.Alloc<float4>(n);
+        skey = mem.Alloc<uint32_t>(n);
+    }
+};
+
+struct Film {
+    DevMem mem;
+    int64_t npix = 0;
+    double *sum = nullptr, *sq = nullptr;
+    uint32_t* n = nullptr;
+    void Ensure(int64_t np) {
+        if (np <= npix)
+            return;
+        mem.Free();
+        npix = np;
+        sum = mem.Alloc<double>(np * 3);
+        sq = mem.Alloc<double>(np * 3);
+        n = mem.Alloc<uint32_t>(np);
+    }
+};
+
+}  // namespace pg
+
+struct pg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<std::unique_ptr<pg::DeviceScene>> scenes;
+    pg::Pool pool;
+    pg::Film film;
+    pg::DevMem small;
+    int* counts = nullptr;                 // [0] active, [1] shadow
+    unsigned long long* next_sample = nullptr;
+    unsigned long long* stats = nullptr;   // 4 counters
+    uint32_t* err = nullptr;
+    int* h_counts = nullptr;               // pinned
+    std::string last_error;
+    pg_tuning tuning{1 << 21, 128, 1};
+};
+
+namespace pg {
+
+static pg_status Fail(pg_ctx* ctx, const Failure& f) {
+    if (ctx)
+        ctx->last_error = f.msg;
+    SetGlobalError(f.msg);
+    return f.status;
+}
+
+template <typename F>
+static pg_status Guard(pg_ctx* ctx, F&& f) {
+    try {
+        f();
+        return PG_OK;
+    } catch (const Failure& e) {
+        return Fail(ctx, e);
+    } catch (const SceneError& e) {
+        return Fail(ctx, Failure{e.status, e.what()});
+    } catch (const std::bad_alloc&) {
+        return Fail(ctx, Failure{PG_ERR_OOM, "host allocation failed"});
+    } catch (const std::exception& e) {
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, e.what()});
+    }
+}
+
+// ---------------------------------------------------------------- scene upload
+static V3 L3(const float* p) {
+    return v3(p[0], p[1], p[2]);
+}
+
+static void Put(float* dst, V3 v) {
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z;
+}
+
+static void BuildMajorants(const float* dens, const int size[3], std::vector<float>& maj, int nb[3]) {
+    for (int k = 0; k < 3; k++)
+        nb[k] = (size[k] + 7) / 8;
+    maj.assign((size_t)nb[0] * nb[1] * nb[2], 0.0f);
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++)
+        th.emplace_back([&]() {
+            for (int bz; (bz = next.fetch_add(1)) < nb[2];) {
+                for (int by = 0; by < nb[1]; by++)
+                    for (int bx = 0; bx < nb[0]; bx++) {
+                        // The trilinear footprint of points in brick b reaches voxel 8b+8.
+                        float m = 0.0f;
+                        for (int z = 8 * bz; z <= std::min(8 * bz + 8, size[2] - 1); z++)
+                            for (int y = 8 * by; y <= std::min(8 * by + 8, size[1] - 1); y++) {
+                                const float* row = dens + (size_t)z * size[0] * size[1] + (size_t)y * size[0];
+                                for (int x = 8 * bx; x <= std::min(8 * bx + 8, size[0] - 1); x++)
+                                    m = std::max(m, row[x]);
+                            }
+                        maj[(size_t)bx + (size_t)nb[0] * (by + (size_t)nb[1] * bz)] = m;
+                    }
+            }
+        });
+    for (auto& t : th)
+        t.join();
+}
+
+static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
+    Require(d != nullptr && sceneId != nullptr, "null scene description or scene id pointer");
+    Require(d->num_shapes >= 0 && (d->num_shapes == 0 || d->shapes), "bad shapes array");
+    Require(d->num_materials >= 0 && (d->num_materials == 0 || d->materials), "bad materials array");
+    Require(d->num_media >= 0 && (d->num_media == 0 || d->media), "bad media array");
+    Require(d->num_lights >= 0 && (d->num_lights == 0 || d->lights), "bad lights array");
+    Require(d->num_triangles >= 0 && (d->num_triangles == 0 || d->indices), "bad index array");
+    Require(d->num_vertices >= 0 && (d->num_vertices == 0 || d->vertices), "bad vertex array");
+    Require(d->camera.width > 0 && d->camera.height > 0, "film size must be positive");
+    Require(d->camera.medium >= -1 && d->camera.medium < d->num_media, "camera medium out of range");
+    for (int64_t i = 0; i < 3 * d->num_triangles; i++)
+        Require((int64_t)d->indices[i] < d->num_vertices, "triangle index out of range");
+
+    auto sc = std::make_unique<DeviceScene>();
+    cudaStream_t st = ctx->stream;
+    SceneDev& S = sc->dev;
+    const int ns = d->num_shapes;
+
+    // Materials: alpha = clamp(roughness^2, 0.001, 1) (bxdf.cpp:37,88).
+    std::vector<MaterialDev> mats(d->num_materials);
+    for (int i = 0; i < d->num_materials; i++) {
+        const pg_material& m = d->materials[i];
+        MaterialDev& o = mats[i];
+        std::memset(&o, 0, sizeof(o));
+        Require(m.type == PG_MATERIAL_LAYERED || m.type == PG_MATERIAL_EMISSIVE, "unknown material type",
+                PG_ERR_UNSUPPORTED);
+        o.type = m.type;
+        std::memcpy(o.emission, m.emission, sizeof(o.emission));
+        Require(m.type == PG_MATERIAL_EMISSIVE || (m.num_layers >= 0 && m.num_layers <= PG_MAX_LAYERS),
+                "material layer count out of range");
+        o.num_layers = m.type == PG_MATERIAL_LAYERED ? m.num_layers : 0;
+        for (int l = 0; l < o.num_layers; l++) {
+            const pg_bsdf& b = m.layers[l];
+            Require(b.type >= PG_BSDF_DIFFUSE && b.type <= PG_BSDF_DIELECTRIC, "unknown BSDF type",
+                    PG_ERR_UNSUPPORTED);
+            o.layers[l].type = b.type;
+            std::memcpy(o.layers[l].albedo, b.albedo, sizeof(b.albedo));
+            o.layers[l].alpha = Clamp(Sqr(b.roughness), 0.001f, 1.0f);
+            o.layers[l].eta = b.eta;
+        }
+    }
+
+    // Shapes and their derived constants, computed with pine's numerics.
+    std::vector<ShapeDev> shapes(ns);
+    std::vector<int> planes;
+    bool nullSurfaces = false;
+    int64_t numPrims = 0;
+    for (int i = 0; i < ns; i++) {
+        const pg_shape& s = d->shapes[i];
+        ShapeDev& o = shapes[i];
+        std::memset(&o, 0, sizeof(o));
+        o.type = s.type;
+        o.material = s.material;
+        o.med_in = s.medium_inside;
+        o.med_out = s.medium_outside;
+        o.light = -1;
+        Require(s.material >= -1 && s.material < d->num_materials, "shape material out of range");
+        Require(s.medium_inside >= -1 && s.medium_inside < d->num_media, "shape medium out of range");
+        Require(s.medium_outside >= -1 && s.medium_outside < d->num_media, "shape medium out of range");
+        if (s.material < 0)
+            nullSurfaces = true;
+        switch (s.type) {
+        case PG_SHAPE_SPHERE:
+            Put(o.p, L3(s.p));
+            o.p[3] = s.p[3];
+            o.area = 4 * kPi * s.p[3] * s.p[3];
+            numPrims++;
+            break;
+        case PG_SHAPE_PLANE: {
+            V3 n = L3(s.p + 3), t, b;
+            CoordinateSystem<kPine>(n, t, b);
+            Put(o.p, L3(s.p));
+            Put(o.p + 3, n);
+            Put(o.p + 6, t);
+            Put(o.p + 9, b);
+            o.area = kFloatMax;
+            planes.push_back(i);
+            break;
+        }
+        case PG_SHAPE_RECT: {
+            V3 ex = L3(s.p + 3), ey = L3(s.p + 6);
+            Put(o.p, L3(s.p));
+            Put(o.p + 3, Normalize<kPine>(ex));
+            Put(o.p + 6, Normalize<kPine>(ey));
+            Put(o.p + 9, Normalize<kPine>(Cross(ex, ey)));
+            o.p[12] = Length<kPine>(ex);
+            o.p[13] = Length<kPine>(ey);
+            o.area = o.p[12] * o.p[13];
+            numPrims++;
+            break;
+        }
+        case PG_SHAPE_TRIANGLE: {
+            std::memcpy(o.p, s.p, 9 * sizeof(float));
+            V3 v0 = L3(s.p), v1 = L3(s.p + 3), v2 = L3(s.p + 6);
+            o.area = Length<kPine>(Cross(v1 - v0, v2 - v0)) / 2;
+            numPrims++;
+            break;
+        }
+        case PG_SHAPE_MESH:
+            Require(s.mesh_first_triangle >= 0 && s.mesh_num_triangles >= 0 &&
+                        s.mesh_first_triangle + s.mesh_num_triangles <= d->num_triangles,
+                    "mesh triangle range out of range");
+            numPrims += s.mesh_num_triangles;
+            break;
+        default:
+            throw Failure{PG_ERR_UNSUPPORTED, "unsupported shape type"};
+        }
+    }
+
+    // Lights: explicit ones in order, then one area light per emissive shape
+    // (fileio.cpp:265-276).  Power as pine computes it: PointLight color*4pi; area lights
+    // evaluate Le with a zero direction and get zero (light.cpp:61-63); others zero.
+    std::vector<LightDev> lights;
+    std::vector<float> power;
+    int env = -1;
+    for (int i = 0; i < d->num_lights; i++) {
+        const pg_light& l = d->lights[i];
+        LightDev o;
+        std::memset(&o, 0, sizeof(o));
+        o.shape = -1;
+        V3 a = L3(l.p), c = L3(l.p + 3);
+        float pw = 0.0f;
+        switch (l.type) {
+        case PG_LIGHT_POINT:
+            o.type = kLightPoint;
+            Put(o.p, a);
+            pw = Luminance(c * (4 * kPi));
+            break;
+        case PG_LIGHT_DIRECTIONAL:
+            o.type = kLightDirectional;
+            Put(o.p, Normalize<kPine>(a));
+            break;
+        case PG_LIGHT_SKY:
+            o.type = kLightSky;
+            Put(o.p, Normalize<kPine>(a));
+            env = (int)lights.size();
+            break;
+        case PG_LIGHT_CONSTANT_ENV:
+            o.type = kLightConstant;
+            env = (int)lights.size();
+            break;
+        default:
+            throw Failure{PG_ERR_UNSUPPORTED, "unsupported light type"};
+        }
+        Put(o.p + 3, c);
+        lights.push_back(o);
+        power.push_back(pw);
+    }
+    for (int i = 0; i < ns; i++) {
+        int m = d->shapes[i].material;
+        if (m < 0 || d->materials[m].type != PG_MATERIAL_EMISSIVE)
+            continue;
+        Require(d->shapes[i].type != PG_SHAPE_MESH && d->shapes[i].type != PG_SHAPE_PLANE,
+                "emissive meshes and planes cannot be sampled as lights (pine aborts on them)",
+                PG_ERR_UNSUPPORTED);
+        LightDev o;
+        std::memset(&o, 0, sizeof(o));
+        o.type = kLightArea;
+        o.shape = i;
+        shapes[i].light = (int)lights.size();
+        lights.push_back(o);
+        power.push_back(0.0f);
+    }
+    // Distribution1D over the powers (distribution.h:13-25).
+    int nl = (int)lights.size();
+    std::vector<float> cdf(nl + 1, 0.0f);
+    float dx = nl ? 1.0f / nl : 0.0f, funcInt = 0.0f;
+    for (int i = 1; i <= nl; i++)
+        cdf[i] = cdf[i - 1] + power[i - 1] * dx;
+    funcInt = nl ? cdf[nl] : 0.0f;
+    if (funcInt != 0.0f)
+        for (auto& c : cdf)
+            c /= funcInt;
+    bool uniform = d->light_sampler == PG_LIGHT_SAMPLER_UNIFORM;
+    if (env >= 0 && lights[env].type == kLightConstant)
+        lights[env].p[0] = (uniform || funcInt == 0.0f) ? 1.0f / nl : power[env] / nl;
+
+    // Media.
+    std::vector<MediumDev> media(d->num_media);
+    for (int i = 0; i < d->num_media; i++) {
+        const pg_medium& m = d->media[i];
+        MediumDev& o = media[i];
+        std::memset(&o, 0, sizeof(o));
+        o.type = m.type;
+        std::memcpy(o.sigma_a, m.sigma_a, sizeof(o.sigma_a));
+        std::memcpy(o.sigma_s, m.sigma_s, sizeof(o.sigma_s));
+        o.sigma_t = m.sigma_a[0] + m.sigma_s[0];
+        o.g = m.g;
+        if (m.type == PG_MEDIUM_HOMOGENEOUS)
+            continue;
+        Require(m.type == PG_MEDIUM_GRID, "unknown medium type", PG_ERR_UNSUPPORTED);
+        Require(m.size[0] > 0 && m.size[1] > 0 && m.size[2] > 0 && m.density, "bad grid medium");
+        size_t nvox = (size_t)m.size[0] * m.size[1] * m.size[2];
+        float maxD = 0.0f;
+        for (size_t v = 0; v < nvox; v++)
+            maxD = std::max(maxD, m.density[v]);
+        o.inv_max_density = 1.0f / maxD;
+        std::memcpy(o.size, m.size, sizeof(o.size));
+        o.interpolate = m.interpolate;
+        float* dd = sc->mem.Alloc<float>(nvox);
+        PG_CUDA(cudaMemcpyAsync(dd, m.density, nvox * 4, cudaMemcpyHostToDevice, st));
+        o.density = dd;
+        std::vector<float> maj;
+        BuildMajorants(m.density, m.size, maj, o.nb);
+        o.majorant = sc->mem.Upload(maj, st);
+        // w2m = Translate(0.5 - position) * Scale(1 / normalizedSize / scale) (medium.cpp:180-182).
+        float mx = (float)std::max(m.size[0], std::max(m.size[1], m.size[2]));
+        float s3[3];
+        for (int k = 0; k < 3; k++) {
+            float ns_ = (float)m.size[k] / mx;
+            s3[k] = 1.0f / ns_ / m.scale;
+        }
+        std::memset(o.w2m, 0, sizeof(o.w2m));
+        std::memset(o.m2w, 0, sizeof(o.m2w));
+        for (int k = 0; k < 3; k++) {
+            o.w2m[4 * k + k] = s3[k];
+            o.w2m[4 * k + 3] = 0.5f - m.position[k];
+            o.m2w[4 * k + k] = 1.0f / s3[k];
+            o.m2w[4 * k + 3] = -(0.5f - m.position[k]) / s3[k];
+        }
+    }
+
+    // Camera: c2w = LookAt(from, to), fov2d from pine's tan (camera.h:23-33, vecmath.h:1212-1221).
+    const pg_camera& cam = d->camera;
+    {
+        V3 from = L3(cam.from), to = L3(cam.to), up = v3(0, 1, 0);
+        V3 z = Normalize<kPine>(to - from);
+        if (Fabs(Dot(z, up)) > 0.999f)
+            z = Normalize<kPine>(z + v3(0.0f, 0.0f, 1e-5f));
+        V3 x = Normalize<kPine>(Cross(up, z));
+        V3 y = Cross(z, x);
+        float* m = S.cam.c2w;
+        m[0] = x.x, m[1] = y.x, m[2] = z.x, m[3] = from.x;
+        m[4] = x.y, m[5] = y.y, m[6] = z.y, m[7] = from.y;
+        m[8] = x.z, m[9] = y.z, m[10] = z.z, m[11] = from.z;
+        float tanHalf = PstdTan(cam.fov / 2);
+        float aspect = (float)cam.width / (float)cam.height;
+        S.cam.fov2d[0] = tanHalf * aspect;
+        S.cam.fov2d[1] = tanHalf;
+        S.cam.lens_radius = cam.lens_radius;
+        S.cam.focal_distance = cam.focus_distance;
+        S.cam.width = cam.width;
+        S.cam.height = cam.height;
+        S.cam.medium = cam.medium;
+    }
+
+    // Primitives and the 8-wide BVH.
+    struct PrimRef {
+        int shape;
+        int64_t local;
+    };
+    std::vector<PrimRef> refs;
+    refs.reserve(numPrims);
+    std::vector<Box> boxes;
+    boxes.reserve(numPrims);
+    auto vtx = [&](uint32_t i) { return L3(d->vertices + 3 * (size_t)i); };
+    auto triBox = [&](V3 a, V3 b, V3 c) {
+        Box bx;
+        V3 lo = Min(Min(a, b), c), hi = Max(Max(a, b), c);
+        Put(bx.lo, lo);
+        Put(bx.hi, hi);
+        return bx;
+    };
+    for (int i = 0; i < ns; i++) {
+        const pg_shape& s = d->shapes[i];
+        const ShapeDev& o = shapes[i];
+        if (s.type == PG_SHAPE_MESH) {
+            for (int64_t t = 0; t < s.mesh_num_triangles; t++) {
+                const uint32_t* id = d->indices + 3 * (s.mesh_first_triangle + t);
+                boxes.push_back(triBox(vtx(id[0]), vtx(id[1]), vtx(id[2])));
+                refs.push_back({i, t});
+            }
+        } else if (s.type == PG_SHAPE_TRIANGLE) {
+            boxes.push_back(triBox(L3(s.p), L3(s.p + 3), L3(s.p + 6)));
+            refs.push_back({i, -1});
+        } else if (s.type == PG_SHAPE_SPHERE) {
+            Box bx;
+            for (int k = 0; k < 3; k++)
+                bx.lo[k] = s.p[k] - s.p[3], bx.hi[k] = s.p[k] + s.p[3];
+            boxes.push_back(bx);
+            refs.push_back({i, -1});
+        } else if (s.type == PG_SHAPE_RECT) {
+            V3 c = L3(o.p), ex = L3(o.p + 3) * (o.p[12] * 0.5f), ey = L3(o.p + 6) * (o.p[13] * 0.5f);
+            Box bx;
+            V3 lo = Min(Min(c + ex + ey, c + ex - ey), Min(c - ex + ey, c - ex - ey));
+            V3 hi = Max(Max(c + ex + ey, c + ex - ey), Max(c - ex + ey, c - ex - ey));
+            for (int k = 0; k < 3; k++) {
+                float pad = 1e-6f * std::max(1.0f, std::fabs(Comp(hi, k)) + std::fabs(Comp(lo, k)));
+                bx.lo[k] = Comp(lo, k) - pad, bx.hi[k] = Comp(hi, k) + pad;
+            }
+            boxes.push_back(bx);
+            refs.push_back({i, -1});
+        }
+    }
+    Require((int64_t)boxes.size() < (1ll << 30), "too many primitives");
+    WideBVH bvh = BuildWideBVH(boxes);
+    sc->prims = (int64_t)boxes.size();
+    sc->bvh_depth = bvh.max_depth;
+    if (!boxes.empty()) {
+        Require(bvh.max_depth < kStackSize, "BVH deeper than the traversal stack", PG_ERR_DEVICE_LIMIT);
+        size_t np = bvh.prim_order.size();
+        std::vector<float4> pr(np * 3);
+        std::vector<int> pshape(np), plocal(np);
+        for (size_t k = 0; k < np; k++) {
+            const PrimRef& r = refs[bvh.prim_order[k]];
+            const pg_shape& s = d->shapes[r.shape];
+            pshape[k] = r.shape;
+            plocal[k] = (int)r.local;
+            float4* f = &pr[3 * k];
+            if (s.type == PG_SHAPE_MESH || s.type == PG_SHAPE_TRIANGLE) {
+                V3 a, b, c;
+                if (s.type == PG_SHAPE_MESH) {
+                    const uint32_t* id = d->indices + 3 * (s.mesh_first_triangle + r.local);
+                    a = vtx(id[0]), b = vtx(id[1]), c = vtx(id[2]);
+                } else {
+                    a = L3(s.p), b = L3(s.p + 3), c = L3(s.p + 6);
+                    plocal[k] = -1;
+                }
+                V3 e1 = b - a, e2 = c - a;  // Triangle::Intersect's E1, E2 (geometry.h:272-273)
+                int ty = kPrimTriangle;
+                f[0] = make_float4(a.x, a.y, a.z, BitsFloat((uint32_t)ty));
+                f[1] = make_float4(e1.x, e1.y, e1.z, 0.0f);
+                f[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
+            } else if (s.type == PG_SHAPE_SPHERE) {
+                int ty = kPrimSphere;
+                f[0] = make_float4(s.p[0], s.p[1], s.p[2], BitsFloat((uint32_t)ty));
+                f[1] = make_float4(s.p[3], 0.0f, 0.0f, 0.0f);
+                f[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            } else {
+                int ty = kPrimRect;
+                f[0] = make_float4(0.0f, 0.0f, 0.0f, BitsFloat((uint32_t)ty));
+                f[1] = f[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+        }
+        S.nodes = (const WideNodeDev*)sc->mem.Alloc<WideNode>(bvh.nodes.size());
+        PG_CUDA(cudaMemcpyAsync((void*)S.nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(WideNode),
+                                cudaMemcpyHostToDevice, st));
+        S.prims = sc->mem.Upload(pr, st);
+        S.prim_shape = sc->mem.Upload(pshape, st);
+        S.prim_local = sc->mem.Upload(plocal, st);
+        S.has_bvh = 1;
+    }
+    S.shapes = sc->mem.Upload(shapes, st);
+    S.num_shapes = ns;
+    S.planes = sc->mem.Upload(planes, st);
+    S.num_planes = (int)planes.size();
+    S.materials = sc->mem.Upload(mats, st);
+    S.lights = sc->mem.Upload(lights, st);
+    S.num_lights = nl;
+    S.light_func = sc->mem.Upload(power, st);
+    S.light_cdf = sc->mem.Upload(cdf, st);
+    S.light_func_int = funcInt;
+    S.uniform_lights = uniform ? 1 : 0;
+    S.env_light = env;
+    S.media = sc->mem.Upload(media, st);
+    S.num_media = d->num_media;
+    S.has_null_surfaces = nullSurfaces ? 1 : 0;
+    PG_CUDA(cudaStreamSynchronize(st));
+
+    sc->width = d->camera.width;
+    sc->height = d->camera.height;
+    sc->spp = std::max(1, d->samples_per_pixel);
+    sc->max_depth = d->max_depth > 0 ? d->max_depth : 4;
+    sc->surfaces = S.has_bvh || !planes.empty();
+    for (size_t i = 0; i < ctx->scenes.size(); i++)
+        if (!ctx->scenes[i]) {
+            ctx->scenes[i] = std::move(sc);
+            *sceneId = (int32_t)i;
+            return;
+        }
+    ctx->scenes.push_back(std::move(sc));
+    *sceneId = (int32_t)ctx->scenes.size() - 1;
+}
+
+static DeviceScene& GetScene(pg_ctx* ctx, int32_t id) {
+    Require(id >= 0 && id < (int32_t)ctx->scenes.size() && ctx->scenes[id], "unknown scene id");
+    return *ctx->scenes[id];
+}
+
+// ---------------------------------------------------------------- rendering
+static pg_status DeviceErrorStatus(uint32_t e, std::string& msg) {
+    if (!e)
+        return PG_OK;
+    msg = "device iteration cap reached:";
+    if (e & kErrStackOverflow)
+        msg += " traversal stack overflow";
+    if (e & kErrTraversalCap)
+        msg += " traversal step cap";
+    if (e & kErrTrackingCap)
+        msg += " volume tracking step cap";
+    return PG_ERR_DEVICE_LIMIT;
+}
+
+static uint32_t PcgHashHost(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+
+template <int M>
+static void LaunchIteration(pg_ctx* ctx, const RenderParams& P, const SceneDev& S, bool surfaces,
+                            int n) {
+    cudaStream_t st = ctx->stream;
+    int tb = 128;
+    size_t smem = (size_t)tb * kStackSize * sizeof(uint2);
+    if (surfaces)
+        k_trace<<<Ceil(n, tb), tb, smem, st>>>(P, S);
+    int sb = ctx->tuning.block_size > 0 ? ctx->tuning.block_size : 128;
+    k_shade<M><<<Ceil(n, sb), sb, 0, st>>>(P, S);
+    k_shadow<M><<<Ceil(n, tb), tb, smem, st>>>(P, S);
+}
+
+struct RenderResult {
+    double seconds = 0;
+    unsigned long long stats[4] = {};
+    int64_t launches = 0;
+};
+
+static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
+                       int sampleOffset, int mathMode, bool accumulate, RenderResult& res) {
+    Require(spp > 0 && maxDepth > 0, "spp and max depth must be positive");
+    Require(mathMode == PG_MATH_PINE || mathMode == PG_MATH_FAST, "unknown math mode");
+    Require(sampleOffset >= 0, "sample offset must be >= 0");
+    int64_t npix = (int64_t)sc.width * sc.height;
+    uint64_t total = (uint64_t)npix * (uint64_t)spp;
+    Require(total + (uint64_t)sampleOffset * npix < (1ull << 32),
+            "width*height*(spp+offset) must stay below 2^32 per render call");
+    cudaStream_t st = ctx->stream;
+    ctx->film.Ensure(npix);
+    if (!accumulate) {
+        PG_CUDA(cudaMemsetAsync(ctx->film.sum, 0, npix * 3 * sizeof(double), st));
+        PG_CUDA(cudaMemsetAsync(ctx->film.sq, 0, npix * 3 * sizeof(double), st));
+        PG_CUDA(cudaMemsetAsync(ctx->film.n, 0, npix * sizeof(uint32_t), st));
+    }
+    int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
+    ctx->pool.Ensure(slots);
+    Pool& pl = ctx->pool;
+    PG_CUDA(cudaMemsetAsync(pl.state, 0, (size_t)slots * sizeof(int), st));
+    PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, 4 * sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+
+    RenderParams P{};
+    P.slots = slots;
+    P.width = sc.width;
+    P.height = sc.height;
+    P.npix = (int)npix;
+    P.total = total;
+    P.sample_offset = sampleOffset;
+    P.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
+    P.max_depth = maxDepth;
+    P.ray_o = pl.ray_o, P.ray_d = pl.ray_d, P.beta = pl.beta, P.L = pl.L, P.hit = pl.hit;
+    P.sample = pl.sample, P.state = pl.state, P.active = pl.active, P.counts = ctx->counts;
+    P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
+    P.film_sum = ctx->film.sum, P.film_sq = ctx->film.sq, P.film_n = ctx->film.n;
+    P.next_sample = ctx->next_sample;
+    P.stats = ctx->stats;
+    P.err = ctx->err;
+
+    const SceneDev& S = sc.dev;
+    int64_t launches = 0;
+    // Every path ends within max_depth counted events; null-surface crossings do not
+    // count, so the cap leaves room for them.
+    const int64_t maxIter = ((int64_t)total / slots + 2) * ((int64_t)maxDepth * 4 + 64) + 4096;
+    PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    int64_t iter = 0;
+    for (;; iter++) {
+        Require(iter < maxIter, "render loop did not converge", PG_ERR_DEVICE_LIMIT);
+        PG_CUDA(cudaMemsetAsync(ctx->counts, 0, 2 * sizeof(int), st));
+        if (mathMode == PG_MATH_PINE)
+            k_regen<kPine><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
+        else
+            k_regen<kFast><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
+        launches++;
+        PG_CUDA(cudaMemcpyAsync(ctx->h_counts, ctx->counts, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PG_CUDA(cudaStreamSynchronize(st));
+        int n = ctx->h_counts[0];
+        if (n == 0)
+            break;
+        if (mathMode == PG_MATH_PINE)
+            LaunchIteration<kPine>(ctx, P, S, sc.surfaces, n);
+        else
+            LaunchIteration<kFast>(ctx, P, S, sc.surfaces, n);
+        launches += sc.surfaces ? 3 : 2;
+        PG_CUDA(cudaGetLastError());
+    }
+    PG_CUDA(cudaEventRecord(ctx->ev1, st));
+    PG_CUDA(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    res.seconds = ms * 1e-3;
+    res.launches = launches;
+    PG_CUDA(cudaMemcpy(res.stats, ctx->stats, sizeof(res.stats), cudaMemcpyDeviceToHost));
+    uint32_t e = 0;
+    PG_CUDA(cudaMemcpy(&e, ctx->err, sizeof(e), cudaMemcpyDeviceToHost));
+    std::string msg;
+    if (pg_status s = DeviceErrorStatus(e, msg))
+        throw Failure{s, msg};
+}
+
+static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_t* count) {
+    if (!mean && !var && !count)
+        return;
+    std::vector<double> sum(npix * 3), sq(npix * 3);
+    std::vector<uint32_t> n(npix);
+    PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum, npix * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    PG_CUDA(cudaMemcpy(sq.data(), ctx->film.sq, npix * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    PG_CUDA(cudaMemcpy(n.data(), ctx->film.n, npix * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < npix; i++) {
+        double k = n[i];
+        for (int c = 0; c < 3; c++) {
+            double m = k > 0 ? sum[3 * i + c] / k : 0.0;
+            if (mean)
+                mean[3 * i + c] = (float)m;
+            if (var)
+                var[3 * i + c] = k > 1 ? (float)std::max(0.0, (sq[3 * i + c] - k * m * m) / (k - 1)) : 0.0f;
+        }
+        if (count)
+            count[i] = n[i];
+    }
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+// ================================================================ C ABI
+extern "C" pg_status pg_create(pg_ctx** out, int device) {
+    if (!out)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null output pointer"});
+    *out = nullptr;
+    auto ctx = std::make_unique<pg_ctx>();
+    pg_status s = Guard(ctx.get(), [&]() {
+        int count = 0;
+        PG_CUDA(cudaGetDeviceCount(&count));
+        Require(device >= 0 && device < count, "device index out of range");
+        PG_CUDA(cudaSetDevice(device));
+        ctx->device = device;
+        PG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        PG_CUDA(cudaEventCreate(&ctx->ev0));
+        PG_CUDA(cudaEventCreate(&ctx->ev1));
+        ctx->counts = ctx->small.Alloc<int>(4);
+        ctx->next_sample = ctx->small.Alloc<unsigned long long>(1);
+        ctx->stats = ctx->small.Alloc<unsigned long long>(4);
+        ctx->err = ctx->small.Alloc<uint32_t>(1);
+        PG_CUDA(cudaMallocHost(&ctx->h_counts, 4 * sizeof(int)));
+    });
+    if (s != PG_OK) {
+        SetGlobalError(ctx->last_error);
+        return s;
+    }
+    *out = ctx.release();
+    return PG_OK;
+}
+
+extern "C" void pg_destroy(pg_ctx* ctx) {
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    ctx->scenes.clear();
+    ctx->pool.mem.Free();
+    ctx->film.mem.Free();
+    ctx->small.Free();
+    if (ctx->h_counts)
+        cudaFreeHost(ctx->h_counts);
+    if (ctx->ev0)
+        cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1)
+        cudaEventDestroy(ctx->ev1);
+    if (ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char* pg_last_error(const pg_ctx* ctx) {
+    if (ctx)
+        return ctx->last_error.c_str();
+    std::lock_guard<std::mutex> lk(g_errMutex);
+    static thread_local std::string copy;
+    copy = g_err;
+    return copy.c_str();
+}
+
+extern "C" pg_status pg_upload_scene(pg_ctx* ctx, const pg_scene_desc* desc, int32_t* scene_id) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        UploadScene(ctx, desc, scene_id);
+    });
+}
+
+extern "C" pg_status pg_load_scene_file(pg_ctx* ctx, const char* path, int32_t* scene_id) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(path != nullptr && scene_id != nullptr, "null path or scene id pointer");
+        HostScene hs;
+        LoadSceneFile(path, hs);
+        pg_scene_desc d;
+        hs.Describe(d);
+        PG_CUDA(cudaSetDevice(ctx->device));
+        UploadScene(ctx, &d, scene_id);
+    });
+}
+
+extern "C" pg_status pg_release_scene(pg_ctx* ctx, int32_t scene_id) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        GetScene(ctx, scene_id);
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->scenes[scene_id].reset();
+    });
+}
+
+extern "C" pg_status pg_scene_info(pg_ctx* ctx, int32_t scene_id, int32_t* width, int32_t* height,
+                                   int32_t* spp, int32_t* max_depth) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        DeviceScene& s = GetScene(ctx, scene_id);
+        if (width)
+            *width = s.width;
+        if (height)
+            *height = s.height;
+        if (spp)
+            *spp = s.spp;
+        if (max_depth)
+            *max_depth = s.max_depth;
+    });
+}
+
+extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc,
+                               float* out_mean, float* out_var, uint32_t* out_count,
+                               pg_render_stats* stats) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(desc != nullptr, "null render description");
+        Require(desc->guiding == 0 || desc->guiding == 1, "guiding must be 0 or 1");
+        Require(desc->guiding == 0, "guided rendering is not available in this build",
+                PG_ERR_UNSUPPORTED);
+        PG_CUDA(cudaSetDevice(ctx->device));
+        DeviceScene& sc = GetScene(ctx, scene_id);
+        int spp = desc->spp > 0 ? desc->spp : sc.spp;
+        int md = desc->max_depth > 0 ? desc->max_depth : sc.max_depth;
+        RenderResult r;
+        RenderFilm(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
+                   desc->accumulate != 0, r);
+        ReadFilm(ctx, (int64_t)sc.width * sc.height, out_mean, out_var, out_count);
+        if (stats) {
+            stats->seconds = r.seconds;
+            stats->rays = (int64_t)r.stats[0];
+            stats->volume_steps = (int64_t)r.stats[1];
+            stats->dropped = (int64_t)r.stats[2];
+            stats->paths = (int64_t)r.stats[3];
+            stats->launches = r.launches;
+        }
+    });
+}
+
+static pg_status Intersect(pg_ctx* ctx, int32_t scene_id, const float* rays, int64_t n,
+                           int32_t* sid, int32_t* pid, float* t, float* uv, bool device) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(n >= 0 && (n == 0 || rays), "bad ray array");
+        PG_CUDA(cudaSetDevice(ctx->device));
+        DeviceScene& sc = GetScene(ctx, scene_id);
+        if (n == 0)
+            return;
+        cudaStream_t st = ctx->stream;
+        DevMem tmp;
+        const float* dRays = rays;
+        int32_t *dS = sid, *dP = pid;
+        float *dT = t, *dUV = uv;
+        if (!device) {
+            float* r = tmp.Alloc<float>(n * 8);
+            PG_CUDA(cudaMemcpyAsync(r, rays, n * 8 * sizeof(float), cudaMemcpyHostToDevice, st));
+            dRays = r;
+            dS = sid ? tmp.Alloc<int32_t>(n) : nullptr;
+            dP = pid ? tmp.Alloc<int32_t>(n) : nullptr;
+            dT = t ? tmp.Alloc<float>(n) : nullptr;
+            dUV = uv ? tmp.Alloc<float>(n * 2) : nullptr;
+        }
+        PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+        int tb = 128;
+        size_t smem = (size_t)tb * kStackSize * sizeof(uint2);
+        k_intersect<<<(unsigned)Ceil<int64_t>(n, tb), tb, smem, st>>>(sc.dev, dRays, n, dS, dP, dT, dUV,
+                                                                      ctx->err);
+        PG_CUDA(cudaGetLastError());
+        if (!device) {
+            if (sid)
+                PG_CUDA(cudaMemcpyAsync(sid, dS, n * 4, cudaMemcpyDeviceToHost, st));
+            if (pid)
+                PG_CUDA(cudaMemcpyAsync(pid, dP, n * 4, cudaMemcpyDeviceToHost, st));
+            if (t)
+                PG_CUDA(cudaMemcpyAsync(t, dT, n * 4, cudaMemcpyDeviceToHost, st));
+            if (uv)
+                PG_CUDA(cudaMemcpyAsync(uv, dUV, n * 8, cudaMemcpyDeviceToHost, st));
+        }
+        uint32_t e = 0;
+        PG_CUDA(cudaMemcpyAsync(&e, ctx->err, sizeof(e), cudaMemcpyDeviceToHost, st));
+        PG_CUDA(cudaStreamSynchronize(st));
+        std::string msg;
+        if (pg_status s = DeviceErrorStatus(e, msg))
+            throw Failure{s, msg};
+    });
+}
+
+extern "C" pg_status pg_intersect(pg_ctx* ctx, int32_t scene_id, const float* rays, int64_t n,
+                                  int32_t* shape_id, int32_t* prim_id, float* t, float* uv) {
+    return Intersect(ctx, scene_id, rays, n, shape_id, prim_id, t, uv, false);
+}
+
+extern "C" pg_status pg_intersect_device(pg_ctx* ctx, int32_t scene_id, const float* d_rays,
+                                         int64_t n, int32_t* d_shape_id, int32_t* d_prim_id,
+                                         float* d_t, float* d_uv) {
+    return Intersect(ctx, scene_id, d_rays, n, d_shape_id, d_prim_id, d_t, d_uv, true);
+}
+
+extern "C" pg_status pg_set_tuning(pg_ctx* ctx, const pg_tuning* t) {
+    if (!ctx || !t)
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or tuning"});
+    if (t->queue_capacity < 1024 || t->queue_capacity > (1 << 26) || t->block_size < 32 ||
+        t->block_size > 1024 || (t->block_size & 31))
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "tuning out of range"});
+    ctx->tuning = *t;
+    return PG_OK;
+}
+
+extern "C" pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* t) {
+    if (!ctx || !t)
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or tuning"});
+    *t = ctx->tuning;
+    return PG_OK;
+}

@@ -1,0 +1,713 @@
+// Host-side scene loading: pine's scene-file grammar and factories, flattened into the
+// pg_scene_desc arrays that pg_upload_scene takes.
+//
+//   Parse / ParseBlock        src/util/parser.cpp:9-110
+//   Parameters                src/util/parameters.h:13-89, parameters.cpp:20-163
+//   pstd::stof/stoi/stofs     src/pstd/string.cpp:37-120
+//   LoadObj                   src/util/objloader.cpp:12-100
+//   LoadVolume                src/util/fileio.cpp:194-202
+//   LoadScene                 src/util/fileio.cpp:251-281
+//   Create{Material,BSDF,Node,Medium,Light,Shape,Camera,Film,Integrator}
+//                             material.cpp:65-82, bxdf.cpp:170-196, node.cpp:33-97,
+//                             medium.cpp:190-224, light.cpp:141-182, geometry.cpp:323-411,
+//                             camera.cpp:9-14,86-107, film.cpp:7-12, integrator.cpp:20-56
+//
+// Unknown types follow pine: a warning and pine's fallback, except where pine's fallback
+// is a component this library does not implement (texture nodes, Cylinder/Disk/Line,
+// Atmosphere, emissive meshes), which fail with PG_ERR_UNSUPPORTED.
+#include "scene_load.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+#include "pg_math.h"
+
+namespace pg {
+
+// ---------------------------------------------------------------- pstd string parsing
+static bool IsNumber(char c) {
+    return c >= '0' && c <= '9';
+}
+static bool IsSpace(char c) {
+    return c == ' ' || c == '\n' || c == '\t' || c == '\r' || c == '\f';
+}
+
+// pstd::stof (string.cpp:50-68): a digit accumulator, no exponent, not correctly rounded.
+// The integer part is accumulated as number*10 + digit and each fraction digit is added
+// as digit*scale with scale *= 0.1f.  The reference is compiled with -ffast-math, under
+// which GCC folds (number*10 + c) - '0' into number*10 + (c - '0'); the fixtures built
+// from the reference pin this form.
+float Stof(const char* s, size_t n) {
+    float number = 0.0f;
+    bool neg = false, dot = false;
+    float scale = 0.1f;
+    for (size_t j = 0; j < n; j++) {
+        char c = s[j];
+        if (j == 0 && c == '-')
+            neg = true;
+        else if (!dot && c == '.')
+            dot = true;
+        else if (!dot)
+            number = number * 10 + (float)(c - '0');
+        else {
+            number += (float)(c - '0') * scale;
+            scale *= 0.1f;
+        }
+    }
+    return neg ? -number : number;
+}
+
+// pstd::stoi (string.cpp:37-48): stops at '.', leading '-'.
+int Stoi(const char* s, size_t n) {
+    int number = 0;
+    bool neg = false;
+    for (size_t j = 0; j < n; j++) {
+        if (s[j] == '.')
+            break;
+        if (j == 0 && s[j] == '-')
+            neg = true;
+        else
+            number = number * 10 + s[j] - '0';
+    }
+    return neg ? -number : number;
+}
+
+// pstd::stofs / stois (string.cpp:71-120): tokens of [0-9.-]; missing components repeat
+// the last value read; an empty string gives 0.
+template <typename T, typename F>
+static void Tokens(const std::string& str, T* ptr, int N, F&& conv, bool allowDot) {
+    int dim = 0, start = -1;
+    for (int i = 0; i < (int)str.size(); i++) {
+        char c = str[i];
+        if (IsNumber(c) || c == '-' || (allowDot && c == '.')) {
+            if (start == -1)
+                start = i;
+        } else if (start != -1) {
+            ptr[dim++] = conv(str.data() + start, (size_t)(i - start));
+            start = -1;
+            if (dim == N)
+                return;
+        }
+    }
+    if (start != -1)
+        ptr[dim++] = conv(str.data() + start, str.size() - start);
+    if (dim == 0) {
+        ptr[0] = 0;
+        dim++;
+    }
+    for (int i = dim; i < N; i++)
+        ptr[i] = ptr[dim - 1];
+}
+void Stofs(const std::string& str, float* ptr, int N) {
+    Tokens(str, ptr, N, Stof, true);
+}
+void Stois(const std::string& str, int* ptr, int N) {
+    Tokens(str, ptr, N, Stoi, false);
+}
+
+// ---------------------------------------------------------------- Parameters
+const std::string* Params::Value(const std::string& name) const {
+    auto it = values.find(name);
+    return it == values.end() ? nullptr : &it->second;
+}
+bool Params::HasValue(const std::string& name) const {
+    return values.count(name) != 0;
+}
+bool Params::HasSubset(const std::string& name) const {
+    return subset.count(name) != 0 || HasValue(name);
+}
+Params& Params::AddSubset(const std::string& name) {
+    auto& sub = subset[name];
+    sub.emplace_back();
+    return sub.back();
+}
+// parameters.cpp:26-44: a plain value "k: v" also serves as subset k with "@" = v.
+Params& Params::operator[](const std::string& name) {
+    auto& ss = subset[name];
+    if (HasValue(name) && ss.empty())
+        AddSubset(name).values["@"] = values[name];
+    if (ss.empty())
+        ss.resize(1);
+    return subset[name].back();
+}
+std::optional<std::string> Params::TryString(const std::string& name) const {
+    if (auto v = Value(name))
+        return *v;
+    if (name == "type" && HasValue("@"))
+        return values.at("@");
+    return std::nullopt;
+}
+std::string Params::String(const std::string& name, const char* fallback) const {
+    if (auto v = TryString(name))
+        return *v;
+    if (fallback)
+        return fallback;
+    throw SceneError(PG_ERR_PARSE, "[Parameters][GetString]cannot find \"" + name + "\"");
+}
+std::optional<float> Params::TryFloat(const std::string& name) const {
+    if (auto v = Value(name))
+        return Stof(v->data(), v->size());
+    return std::nullopt;
+}
+float Params::Float(const std::string& name) const {
+    if (auto v = TryFloat(name))
+        return *v;
+    throw SceneError(PG_ERR_PARSE, "[Parameters][GetFloat]cannot find \"" + name + "\"");
+}
+float Params::Float(const std::string& name, float fallback) const {
+    auto v = TryFloat(name);
+    return v ? *v : fallback;
+}
+std::optional<int> Params::TryInt(const std::string& name) const {
+    if (auto v = Value(name))
+        return Stoi(v->data(), v->size());
+    return std::nullopt;
+}
+int Params::Int(const std::string& name) const {
+    if (auto v = TryInt(name))
+        return *v;
+    throw SceneError(PG_ERR_PARSE, "[Parameters][GetInt]cannot find \"" + name + "\"");
+}
+int Params::Int(const std::string& name, int fallback) const {
+    auto v = TryInt(name);
+    return v ? *v : fallback;
+}
+bool Params::Bool(const std::string& name, bool fallback) const {
+    auto v = Value(name);
+    if (!v)
+        return fallback;
+    std::string s = *v;
+    for (auto& c : s)
+        if ('A' <= c && c <= 'Z')
+            c += 'a' - 'A';
+    if (s == "true")
+        return true;
+    if (s == "false")
+        return false;
+    return Stoi(s.data(), s.size()) != 0;
+}
+std::optional<std::array<float, 3>> Params::TryVec3(const std::string& name) const {
+    auto v = Value(name);
+    if (!v)
+        return std::nullopt;
+    std::array<float, 3> r;
+    Stofs(*v, r.data(), 3);
+    return r;
+}
+std::array<float, 3> Params::Vec3(const std::string& name) const {
+    if (auto v = TryVec3(name))
+        return *v;
+    throw SceneError(PG_ERR_PARSE, "[Parameters][GetVec3]cannot find \"" + name + "\"");
+}
+std::array<float, 3> Params::Vec3(const std::string& name, std::array<float, 3> fb) const {
+    auto v = TryVec3(name);
+    return v ? *v : fb;
+}
+std::array<int, 2> Params::Vec2i(const std::string& name, std::array<int, 2> fb) const {
+    auto v = Value(name);
+    if (!v)
+        return fb;
+    std::array<int, 2> r;
+    Stois(*v, r.data(), 2);
+    return r;
+}
+
+// ---------------------------------------------------------------- parser
+namespace {
+
+bool IsLetter(char s) {
+    return (s >= 'A' && s <= 'z') || (s >= '0' && s <= '9') || s == '_';  // parser.cpp:17-19
+}
+
+struct View {
+    const char* p;
+    size_t n;
+    char at(size_t i) const {
+        return i < n ? p[i] : '\0';
+    }
+    void drop(size_t k) {
+        k = std::min(k, n);
+        p += k;
+        n -= k;
+    }
+};
+
+template <typename F>
+std::optional<size_t> FirstOfF(const View& v, F&& f) {
+    for (size_t i = 0; i < v.n; i++)
+        if (f(v.p[i]))
+            return i;
+    return std::nullopt;
+}
+
+// parser.cpp:34-43: skip whitespace; a "//" comment is recognised after a whitespace
+// character and runs to the end of the line.
+void EscapeSpace(View& s) {
+    while (s.n && IsSpace(s.p[0])) {
+        s.drop(1);
+        if (s.n >= 2 && s.p[0] == '/' && s.p[1] == '/') {
+            while (s.n && s.p[0] != '\n' && s.p[0] != '\r')
+                s.drop(1);
+            s.drop(1);
+        }
+    }
+}
+
+Params ParseBlock(View& block, int depth) {
+    if (depth > 64)
+        throw SceneError(PG_ERR_PARSE, "scene nesting deeper than 64 blocks");
+    Params params;
+    while (true) {
+        EscapeSpace(block);
+        if (!FirstOfF(block, IsLetter))
+            break;
+        auto sep = FirstOfF(block, [](char c) { return c == ':' || c == '=' || c == '{'; });
+        if (!sep)
+            throw SceneError(PG_ERR_PARSE, "expected ':', '=' or '{' after a key");
+        if (auto end = FirstOfF(block, [](char c) { return c == '}'; }))
+            if (*sep > *end)
+                break;
+        auto keyEnd = FirstOfF(block, [](char c) { return !IsLetter(c); });
+        if (!keyEnd)
+            throw SceneError(PG_ERR_PARSE, "unterminated key");
+        std::string key(block.p, *keyEnd);
+        std::string name;
+        for (size_t i = *keyEnd; i < *sep; i++)
+            if (IsLetter(block.p[i]))
+                name += block.p[i];
+        block.drop(*sep);
+        bool typed = false;
+        std::string value;
+        if (block.at(0) != '{') {
+            typed = true;
+            block.drop(1);
+            EscapeSpace(block);
+            auto valueEnd =
+                FirstOfF(block, [](char c) { return c == '\n' || c == '\r' || c == '{'; });
+            if (!valueEnd)
+                throw SceneError(PG_ERR_PARSE, "value of \"" + key + "\" has no line end");
+            value.assign(block.p, *valueEnd);
+            params.values[key] = value;
+            block.drop(*valueEnd);
+        }
+        EscapeSpace(block);
+        if (block.at(0) == '{') {
+            block.drop(1);
+            Params sub = ParseBlock(block, depth + 1);
+            Params& dst = params.AddSubset(key);
+            dst = std::move(sub);
+            if (typed)
+                dst.values["@"] = value;
+            if (!name.empty() && !dst.HasValue("name"))
+                dst.values["name"] = name;
+        }
+    }
+    if (auto end = FirstOfF(block, [](char c) { return c == '}'; }))
+        block.drop(*end + 1);
+    return params;
+}
+
+}  // namespace
+
+Params ParseScene(const std::string& text) {
+    View v{text.data(), text.size()};
+    return ParseBlock(v, 0);
+}
+
+// ---------------------------------------------------------------- files
+static std::string ReadFile(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw SceneError(PG_ERR_IO, "cannot open \"" + path + "\"");
+    std::ostringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+// objloader.cpp:12-100 for the forms pine handles: "v x y z", "f a b c", "f a b c d" and
+// the slash forms; lines are only those terminated by '\n'; indices are 1-based, negative
+// ones are relative, and the smallest index is subtracted at the end.
+void LoadObj(const std::string& path, std::vector<float>& verts, std::vector<uint32_t>& idx) {
+    std::string raw = ReadFile(path);
+    std::vector<float> v;
+    std::vector<uint32_t> ind;
+    size_t pos = 0;
+    std::string face;
+    while (true) {
+        size_t nl = raw.find('\n', pos);
+        if (nl == std::string::npos)
+            break;
+        std::string line = raw.substr(pos, nl - pos);
+        pos = nl + 1;
+        if (line.size() >= 2 && line[0] == 'v' && line[1] != 't' && line[1] != 'n') {
+            float p[3];
+            Stofs(line.substr(2), p, 3);
+            v.insert(v.end(), p, p + 3);
+        } else if (!line.empty() && line[0] == 'f') {
+            std::string l = line.size() > 2 ? line.substr(2) : std::string();
+            size_t slashes = std::count(l.begin(), l.end(), '/');
+            face.clear();
+            auto takeVertex = [&](bool last) {
+                face += l.substr(0, l.find('/'));
+                size_t sp = l.find(' ');
+                l = sp == std::string::npos ? std::string() : l.substr(sp + 1);
+                if (!last)
+                    face += " ";
+            };
+            if (slashes == 0) {
+                face = l;
+            } else if (slashes == 6) {
+                takeVertex(false), takeVertex(false), takeVertex(true);
+            } else {
+                takeVertex(false), takeVertex(false), takeVertex(false), takeVertex(true);
+            }
+            size_t spaces = std::count(face.begin(), face.end(), ' ');
+            int64_t nverts = (int64_t)(v.size() / 3);
+            auto fix = [&](int i) { return (uint32_t)(i < 0 ? nverts + i : i - 1); };
+            if (spaces == 2) {
+                int f[3];
+                Stois(face, f, 3);
+                ind.insert(ind.end(), {fix(f[0]), fix(f[1]), fix(f[2])});
+            } else if (spaces == 3) {
+                int f[4];
+                Stois(face, f, 4);
+                uint32_t a = fix(f[0]), b = fix(f[1]), c = fix(f[2]), d = fix(f[3]);
+                ind.insert(ind.end(), {a, b, c, a, c, d});
+            }
+        }
+    }
+    if (!ind.empty()) {
+        uint32_t mn = *std::min_element(ind.begin(), ind.end());
+        for (auto& i : ind)
+            i -= mn;
+    }
+    for (auto i : ind)
+        if ((uint64_t)i * 3 + 2 >= v.size())
+            throw SceneError(PG_ERR_PARSE, "OBJ index out of range in \"" + path + "\"");
+    verts.swap(v);
+    idx.swap(ind);
+}
+
+// fileio.cpp:194-202: int32 sx, sy, sz then sx*sy*sz floats, x fastest.
+void LoadVolume(const std::string& path, std::vector<float>& density, int size[3]) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw SceneError(PG_ERR_IO, "cannot open volume \"" + path + "\"");
+    int32_t hdr[3];
+    if (!f.read((char*)hdr, 12))
+        throw SceneError(PG_ERR_IO, "truncated volume header in \"" + path + "\"");
+    if (hdr[0] <= 0 || hdr[1] <= 0 || hdr[2] <= 0 || (int64_t)hdr[0] * hdr[1] * hdr[2] > (1ll << 33))
+        throw SceneError(PG_ERR_PARSE, "bad volume size in \"" + path + "\"");
+    size_t n = (size_t)hdr[0] * hdr[1] * hdr[2];
+    density.resize(n);
+    if (!f.read((char*)density.data(), (std::streamsize)(n * 4)))
+        throw SceneError(PG_ERR_IO, "truncated volume data in \"" + path + "\"");
+    size[0] = hdr[0], size[1] = hdr[1], size[2] = hdr[2];
+}
+
+// ---------------------------------------------------------------- factories
+namespace {
+
+void Warn(const std::string& msg) {
+    std::fprintf(stderr, "[pine-gpu] %s\n", msg.c_str());
+}
+
+// node.cpp:33-97, restricted to constants: "k: v" literal values and Constant{float vec3}.
+struct ConstNode {
+    float f;
+    std::array<float, 3> v;
+};
+ConstNode CreateNode(Params& p, const std::string& what) {
+    std::string type = p.String("type", "");
+    if (type == "Constant")
+        return {p.Float("float"), p.Vec3("vec3")};
+    static const char* kTextured[] = {"Position", "Normal",   "TexCoord",     "Decompose",
+                                      "Composite", "Add",     "Substract",    "Multiply",
+                                      "Divide",    "MultiplyAdd", "Length",   "Sqr",
+                                      "Sqrt",      "Pow",     "Sin",          "Cos",
+                                      "Tan",       "Fract",   "Checkerboard", "Noise",
+                                      "Noise3D",   "Texture", "Invert"};
+    for (auto t : kTextured)
+        if (type == t)
+            throw SceneError(PG_ERR_UNSUPPORTED,
+                             "texture node \"" + type + "\" (" + what + ") is not supported");
+    if (p.HasValue("@") && !p.values["@"].empty()) {
+        // The literal case (node.cpp:89-91): float from stof of the whole text, vec3 from
+        // stofs.  Only EvalVec3 of albedo/color and EvalFloat of scalars are ever used.
+        ConstNode n;
+        n.f = p.Float("float", p.Float("@"));
+        n.v = p.Vec3("vec3", p.Vec3("@"));
+        return n;
+    }
+    if (type.empty())
+        throw SceneError(PG_ERR_PARSE, "[Parameters][GetString]cannot find \"type\" (" + what + ")");
+    Warn("[NodeInput][Create]Unknown type \"" + type + "\"");
+    return {p.Float("float", 0.5f), p.Vec3("vec3", {0.5f, 0.5f, 0.5f})};
+}
+
+pg_bsdf CreateBSDF(Params& p) {
+    std::string type = p.String("type");
+    pg_bsdf b{};
+    if (type == "Conductor") {
+        b.type = PG_BSDF_CONDUCTOR;
+    } else if (type == "Dielectric") {
+        b.type = PG_BSDF_DIELECTRIC;
+    } else {
+        if (type != "Diffuse")
+            Warn("[BSDF][Create]Unknown type \"" + type + "\"");
+        b.type = PG_BSDF_DIFFUSE;
+    }
+    if (b.type == PG_BSDF_DIELECTRIC && !p.HasSubset("albedo")) {
+        b.albedo[0] = b.albedo[1] = b.albedo[2] = 1.0f;  // bxdf.cpp:176-181
+    } else {
+        ConstNode a = CreateNode(p["albedo"], "albedo");
+        std::copy(a.v.begin(), a.v.end(), b.albedo);
+    }
+    if (b.type != PG_BSDF_DIFFUSE)
+        b.roughness = CreateNode(p["roughness"], "roughness").f;
+    if (b.type == PG_BSDF_DIELECTRIC)
+        b.eta = CreateNode(p["eta"], "eta").f;
+    return b;
+}
+
+pg_material CreateMaterial(Params& p) {
+    std::string type = p.String("type");
+    pg_material m{};
+    if (p.HasSubset("bumpMap"))
+        throw SceneError(PG_ERR_UNSUPPORTED, "bump maps are not supported");
+    if (type == "Emissive") {
+        m.type = PG_MATERIAL_EMISSIVE;
+        ConstNode c = CreateNode(p["color"], "color");
+        std::copy(c.v.begin(), c.v.end(), m.emission);
+        return m;
+    }
+    if (type != "Layered")
+        Warn("[Material][Create]Unknown type \"" + type + "\"");
+    m.type = PG_MATERIAL_LAYERED;
+    // material.cpp:33-43: "layerN" subsets, ordered by N descending (top layer first).
+    std::vector<std::pair<int, Params*>> layers;
+    for (auto& kv : p.subset)
+        if (kv.first.compare(0, 5, "layer") == 0 && !kv.second.empty())
+            layers.push_back({Stoi(kv.first.data() + 5, kv.first.size() - 5), &kv.second.back()});
+    std::stable_sort(layers.begin(), layers.end(),
+                     [](const auto& a, const auto& b) { return a.first > b.first; });
+    if ((int)layers.size() > PG_MAX_LAYERS)
+        throw SceneError(PG_ERR_UNSUPPORTED, "more than 4 layers in a material");
+    for (auto& l : layers)
+        m.layers[m.num_layers++] = CreateBSDF(*l.second);
+    return m;
+}
+
+}  // namespace
+
+void LoadSceneFile(const std::string& path, HostScene& s) {
+    std::string text = ReadFile(path);
+    Params params = ParseScene(text);
+    // fileio.cpp:40-48,256: every file in the scene is relative to the scene's directory.
+    std::string dir;
+    size_t slash = path.find_last_of('/');
+    dir = slash == std::string::npos ? std::string("./") : path.substr(0, slash + 1);
+
+    std::map<std::string, int> materials, media;
+    for (auto& p : params.subset["Material"]) {
+        materials[p.String("name")] = (int)s.materials.size();
+        s.materials.push_back(CreateMaterial(p));
+    }
+    for (auto& p : params.subset["Medium"]) {
+        std::string type = p.String("type");
+        pg_medium m{};
+        m.g = p.Float("g", 0.0f);
+        auto sa = p.Vec3("sigma_a"), ss = p.Vec3("sigma_s");
+        std::copy(sa.begin(), sa.end(), m.sigma_a);
+        std::copy(ss.begin(), ss.end(), m.sigma_s);
+        if (type == "Grid") {
+            m.type = PG_MEDIUM_GRID;
+            s.densities.emplace_back();
+            LoadVolume(dir + p.String("file"), s.densities.back(), m.size);
+            auto pos = p.Vec3("position");
+            std::copy(pos.begin(), pos.end(), m.position);
+            m.scale = p.Float("scale", 1.0f);
+            m.interpolate = p.Bool("interpolate", true) ? 1 : 0;
+            std::string method = p.String("samplingMethod", "deltaTracking");
+            if (method != "deltaTracking")
+                throw SceneError(PG_ERR_UNSUPPORTED, "grid sampling method \"" + method + "\"");
+        } else {
+            if (type != "Homogeneous")
+                Warn("[Medium][Create]Unknown type \"" + type + "\"");
+            m.type = PG_MEDIUM_HOMOGENEOUS;
+            s.densities.emplace_back();
+        }
+        media[p.String("name")] = (int)s.media.size();
+        s.media.push_back(m);
+    }
+    for (auto& p : params.subset["Light"]) {
+        std::string type = p.String("type");
+        pg_light l{};
+        if (type == "Directional") {
+            l.type = PG_LIGHT_DIRECTIONAL;
+            auto d = p.Vec3("direction"), c = p.Vec3("color");
+            std::copy(d.begin(), d.end(), l.p);
+            std::copy(c.begin(), c.end(), l.p + 3);
+        } else if (type == "Environment") {
+            Params& e = p["environment"];
+            std::string et = e.String("type");
+            if (et == "Sky") {
+                l.type = PG_LIGHT_SKY;
+                auto d = e.Vec3("sunDirection"), c = e.Vec3("sunColor");
+                std::copy(d.begin(), d.end(), l.p);
+                std::copy(c.begin(), c.end(), l.p + 3);
+            } else if (et == "Constant") {
+                l.type = PG_LIGHT_CONSTANT_ENV;
+                auto c = e.Vec3("color");
+                std::copy(c.begin(), c.end(), l.p + 3);
+            } else {
+                throw SceneError(PG_ERR_UNSUPPORTED, "environment \"" + et + "\" is not supported");
+            }
+        } else {
+            if (type != "Point")
+                Warn("[Light][Create]Unknown type \"" + type + "\"");
+            l.type = PG_LIGHT_POINT;
+            auto q = p.Vec3("position"), c = p.Vec3("color");
+            std::copy(q.begin(), q.end(), l.p);
+            std::copy(c.begin(), c.end(), l.p + 3);
+        }
+        s.lights.push_back(l);
+    }
+    for (auto& p : params.subset["Shape"]) {
+        std::string type = p.String("type");
+        pg_shape sh{};
+        sh.material = -1;
+        sh.medium_inside = sh.medium_outside = -1;
+        auto put = [&](int off, std::array<float, 3> v) {
+            std::copy(v.begin(), v.end(), sh.p + off);
+        };
+        if (type == "Plane") {
+            sh.type = PG_SHAPE_PLANE;
+            put(0, p.Vec3("position"));
+            // Plane::Create normalises with pine's sqrt (geometry.cpp:346-348).
+            auto n = p.Vec3("normal");
+            V3 nn = Normalize<kPine>(v3(n[0], n[1], n[2]));
+            put(3, {nn.x, nn.y, nn.z});
+        } else if (type == "Triangle") {
+            sh.type = PG_SHAPE_TRIANGLE;
+            put(0, p.Vec3("v0")), put(3, p.Vec3("v1")), put(6, p.Vec3("v2"));
+        } else if (type == "Rect") {
+            sh.type = PG_SHAPE_RECT;
+            put(0, p.Vec3("position")), put(3, p.Vec3("ex")), put(6, p.Vec3("ey"));
+        } else if (type == "TriangleMesh") {
+            sh.type = PG_SHAPE_MESH;
+            std::vector<float> v;
+            std::vector<uint32_t> ind;
+            LoadObj(dir + p.String("file"), v, ind);
+            if (auto sc = p.TryVec3("scale"))
+                for (size_t i = 0; i < v.size(); i++)
+                    v[i] *= (*sc)[i % 3];
+            if (auto ps = p.TryVec3("position"))
+                for (size_t i = 0; i < v.size(); i++)
+                    v[i] += (*ps)[i % 3];
+            uint32_t base = (uint32_t)(s.vertices.size() / 3);
+            sh.mesh_first_triangle = (int64_t)(s.indices.size() / 3);
+            sh.mesh_num_triangles = (int64_t)(ind.size() / 3);
+            s.vertices.insert(s.vertices.end(), v.begin(), v.end());
+            for (auto i : ind)
+                s.indices.push_back(i + base);
+        } else if (type == "Cylinder" || type == "Disk" || type == "Line") {
+            throw SceneError(PG_ERR_UNSUPPORTED, "shape \"" + type + "\" is not supported");
+        } else {
+            if (type != "Sphere")
+                Warn("[Shape][Create]Unknown type \"" + type + "\"");
+            sh.type = PG_SHAPE_SPHERE;
+            put(0, p.Vec3("position"));
+            sh.p[3] = p.Float("radius");
+        }
+        if (auto name = p.TryString("material")) {
+            auto it = materials.find(*name);
+            if (it == materials.end())
+                throw SceneError(PG_ERR_PARSE, "[Shape][Create]Material \"" + *name + "\" is not found");
+            sh.material = it->second;
+        }
+        auto medium = [&](const char* key, int& slot) {
+            if (auto name = p.TryString(key)) {
+                auto it = media.find(*name);
+                if (it == media.end())
+                    throw SceneError(PG_ERR_PARSE, "[Shape][Create]Medium \"" + *name + "\" is not found");
+                slot = it->second;
+            }
+        };
+        medium("medium", sh.medium_inside);
+        medium("mediumInside", sh.medium_inside);
+        medium("mediumOutside", sh.medium_outside);
+        s.shapes.push_back(sh);
+    }
+
+    // Camera (camera.cpp:86-107) and film (film.cpp:7-12).
+    Params& cam = params["Camera"];
+    std::string ctype = cam.String("type", "ThinLen");
+    if (ctype != "ThinLen")
+        Warn("[Camera][Create]Unknown type \"" + ctype + "\"");
+    Params& film = cam["film"];
+    auto size = film.Vec2i("size", {720, 480});
+    pg_camera& c = s.camera;
+    auto from = cam.Vec3("from"), to = cam.Vec3("to");
+    std::copy(from.begin(), from.end(), c.from);
+    std::copy(to.begin(), to.end(), c.to);
+    c.fov = cam.Float("fov");
+    c.lens_radius = cam.Float("lensRadius", 0.0f);
+    c.focus_distance = cam.Float("focusDistance", 1.0f);
+    c.width = size[0];
+    c.height = size[1];
+    c.medium = -1;
+    if (auto name = cam.TryString("medium")) {
+        auto it = media.find(*name);
+        if (it == media.end())
+            throw SceneError(PG_ERR_PARSE, "[Camera][Create]Medium \"" + *name + "\" is not found");
+        c.medium = it->second;
+    }
+    if (c.width <= 0 || c.height <= 0)
+        throw SceneError(PG_ERR_PARSE, "film size must be positive");
+
+    // Integrator (integrator.cpp:20-56): maxDepth default 4, sampler spp, light sampler.
+    Params& integ = params["Integrator"];
+    std::string itype = integ.String("type", "Path");
+    if (itype != "Path" && itype != "GpuPath")
+        Warn("[Integrator][Create]Integrator \"" + itype + "\" is rendered as GpuPath");
+    s.max_depth = integ.Int("maxDepth", 4);
+    s.spp = integ["sampler"].Int("samplesPerPixel", 1);
+    std::string ls = integ["lightSampler"].String("type", "Power");
+    s.light_sampler = ls == "Uniform" ? PG_LIGHT_SAMPLER_UNIFORM : PG_LIGHT_SAMPLER_POWER;
+}
+
+void HostScene::Describe(pg_scene_desc& d) {
+    std::memset(&d, 0, sizeof(d));
+    for (size_t i = 0; i < media.size(); i++)
+        media[i].density = densities[i].empty() ? nullptr : densities[i].data();
+    d.num_shapes = (int32_t)shapes.size();
+    d.shapes = shapes.data();
+    d.num_vertices = (int64_t)(vertices.size() / 3);
+    d.vertices = vertices.data();
+    d.num_triangles = (int64_t)(indices.size() / 3);
+    d.indices = indices.data();
+    d.num_materials = (int32_t)materials.size();
+    d.materials = materials.data();
+    d.num_media = (int32_t)media.size();
+    d.media = media.data();
+    d.num_lights = (int32_t)lights.size();
+    d.lights = lights.data();
+    d.camera = camera;
+    d.light_sampler = light_sampler;
+    d.max_depth = max_depth;
+    d.samples_per_pixel = spp;
+}
+
+}  // namespace pg
+
+extern "C" float pg_pstd_stof(const char* str, int64_t len) {
+    if (!str || len < 0)
+        return 0.0f;
+    return pg::Stof(str, (size_t)len);
+}
