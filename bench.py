@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 wavefront path tracer (Mpaths/s).
+
+Workload (default ``volume``): the heterogeneous-volume scene -- a 512^3 FP32 fractal-noise
+cloud (about 30% of voxels non-zero, max sigma_t 20 per unit, albedo 0.99, HG g = 0.8),
+lit by a directional sun (irradiance 5) and a constant sky (0.3), 1280x720, 256 spp, up to
+128 scattering events.  One step renders that whole image.  ``spheres`` and ``mesh`` run
+the other two scenes (640x360x64 spp; 1920x1080x256 spp over ~1.3M triangles).
+
+Arms:
+* ours (default): ``value`` is device time (CUDA events on the library's stream) with the
+  scene resident in HBM; ``e2e`` is wall time through the public C ABI with host buffers:
+  each step uploads the scene from pinned host memory (pg_upload_scene), renders and reads
+  the film back (mean, variance, count) into pinned host memory.
+* ``--impl reference``: pine's own CPU integrator (the reference compiled from source into
+  oracle/_ref) on the same scene, with pine's Sky standing in for the constant sky, which
+  pine cannot express; all host threads, one bounded sample of the image per step.
+
+Multi-GPU (``torchrun --nproc-per-node N bench.py --gpus N``): independent replicas, each
+rank renders the full workload with its own seed (weak scaling); times are the max over
+ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "pine_ref")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "volume_traffic.md")
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "volume": dict(kind="volume", width=1280, height=720, spp=256, max_depth=128, n=512),
+    "spheres": dict(kind="spheres", width=640, height=360, spp=64, max_depth=8),
+    "mesh": dict(kind="mesh", width=1920, height=1080, spp=256, max_depth=16, subdiv=8),
+}
+# ncu case: the same 512^3 grid (larger than L2) with one sample per pixel.
+PROFILE_CASE = dict(kind="volume", width=1280, height=720, spp=1, max_depth=128, n=512)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="volume")
+    ap.add_argument("--math", choices=["pine", "fast"], default="fast")
+    ap.add_argument("--cache", default=os.environ.get("PINE_B200_SCENES",
+                                                      os.path.join(tempfile.gettempdir(),
+                                                                   "pine_b200_scenes")))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="render the small ncu case once and print its per-kernel counters")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- scenes
+def scene_path(cfg, cache, env, spp=None, size=None):
+    from pine_b200 import lib, scenegen
+    os.makedirs(cache, exist_ok=True)
+    w, h = size or (cfg["width"], cfg["height"])
+    spp = cfg["spp"] if spp is None else spp
+    kind = cfg["kind"]
+    name = f"{kind}_{env}_{w}x{h}_{spp}.txt"
+    path = os.path.join(cache, name)
+    if kind == "volume":
+        scenegen.volume_scene(path, lib(), n=cfg["n"], width=w, height=h, spp=spp,
+                              max_depth=cfg["max_depth"], env=env,
+                              env_radiance=0.3 if env == "constant" else 1.0)
+    elif kind == "spheres":
+        scenegen.spheres_scene(path, width=w, height=h, spp=spp, max_depth=cfg["max_depth"],
+                               env=env, env_radiance=0.2 if env == "constant" else 0.5)
+    else:
+        scenegen.mesh_scene(path, lib(), subdiv=cfg["subdiv"], width=w, height=h, spp=spp,
+                            max_depth=cfg["max_depth"], env="none")
+    return path
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) == len(self.FIELDS)]
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- roofline
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# Algorithmic bytes: per path iteration of k_shade 128 B of path state (64 B read, 64 B
+# written); per shadow ray of k_shadow 64 B (48 B ray read, 16 B radiance update); per
+# volume tracking step 32 B (the 8 voxels of a trilinear lookup); 4 B per majorant brick.
+STATE_BYTES = {"shade": 128, "shadow": 64, "trace": 48, "regen": 16}
+
+
+def algorithmic_bytes(name, k):
+    return STATE_BYTES[name] * k["items"] + 32 * k["volume_steps"] + 4 * k["bricks"]
+
+
+def read_traffic():
+    """DRAM bytes per tracking step of each kernel, from the committed ncu summary."""
+    out = {}
+    try:
+        for line in open(TRAFFIC_FILE):
+            if line.startswith("dram_bytes_per_step"):
+                _, rest = line.split(":", 1)
+                for kv in rest.split():
+                    k, v = kv.split("=")
+                    out[k] = float(v)
+    except OSError:
+        pass
+    return out
+
+
+def roofline(kernels, peak, peak_kind):
+    timed = {n: k for n, k in kernels.items() if k["seconds"] > 0 and k["launches"] > 0}
+    if not timed:
+        return None
+    name = max(timed, key=lambda n: timed[n]["seconds"])
+    k = timed[name]
+    per_launch_bytes = algorithmic_bytes(name, k) / k["launches"]
+    launch_s = k["seconds"] / k["launches"]
+    achieved = per_launch_bytes / launch_s / 1e9
+    traffic = None
+    tr = read_traffic()
+    if name in tr and k["volume_steps"]:
+        traffic = tr[name] * k["volume_steps"] / k["launches"]
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+            "kernel": "k_" + name, "algorithmic_bytes_per_launch": per_launch_bytes,
+            "avg_launch_ms": launch_s * 1e3, "launches": k["launches"],
+            "share_of_device_time": k["seconds"] / sum(v["seconds"] for v in timed.values())}
+
+
+def add_kernels(acc, k):
+    for name, v in k.items():
+        a = acc.setdefault(name, {key: 0 for key in v})
+        for key, val in v.items():
+            a[key] += val
+
+
+# ---------------------------------------------------------------- CPU baseline (pine)
+def run_pine(scene, repeats, spp):
+    p = subprocess.run([REF_BIN, "time", scene, str(repeats), str(spp)], capture_output=True,
+                       text=True, cwd=os.path.dirname(scene))
+    lines = [json.loads(l) for l in p.stdout.splitlines() if l.startswith("{")]
+    if p.returncode != 0 or not lines:
+        raise RuntimeError(f"pine_ref failed ({p.returncode}): {p.stderr[-500:]}")
+    return lines
+
+
+def cpu_baseline(cfg, cache):
+    """pine's Path integrator on the host cores: a 1-spp calibration run sizes a sample of
+    about 10 s, which is then timed (scene loading and BVH build excluded)."""
+    if not os.path.exists(REF_BIN):
+        return None
+    scene = scene_path(cfg, cache, "sky", spp=1)
+    cal = run_pine(scene, 1, 1)[0]
+    spp = int(max(1, min(cfg["spp"], 10.0 / max(cal["seconds"], 1e-3))))
+    run = run_pine(scene, 1, spp)[0]
+    return {"value": run["mpaths_per_s"], "unit": "Mpaths/s", "cores": run["threads"],
+            "kind": "reference",
+            "sample": f"{cfg['width']}x{cfg['height']} at {spp} spp of the same scene with "
+                      f"pine's Sky in place of the constant sky ({run['paths']:.0f} paths, "
+                      f"{run['seconds']:.2f} s)"}
+
+
+def reference_arm(args, cfg, rank):
+    if rank != 0:
+        return 0
+    line = {"metric": "Mpaths/s", "unit": "Mpaths/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: pine Path integrator (CPU), scene as "
+                                   "ours with Sky for the constant sky"}}
+    if not os.path.exists(REF_BIN):
+        line["unavailable"] = "oracle/_ref/pine_ref is not built (needs the pine sources)"
+        print(json.dumps(line))
+        return 0
+    scene = scene_path(cfg, args.cache, "sky", spp=1)
+    cal = run_pine(scene, 1, 1)[0]
+    # Steps sized so that warmup + steps finish in about two minutes.
+    per_step = 120.0 / max(1, args.steps + args.warmup)
+    spp = int(max(1, min(cfg["spp"], per_step / max(cal["seconds"], 1e-3))))
+    runs = run_pine(scene, args.warmup + args.steps, spp)[args.warmup:]
+    secs = sum(r["seconds"] for r in runs)
+    paths = sum(r["paths"] for r in runs)
+    value = paths / secs / 1e6
+    line.update({"value": value, "ms_per_step": secs / len(runs) * 1e3,
+                 "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": runs[0]["threads"],
+                                  "kind": "reference",
+                                  "sample": f"{cfg['width']}x{cfg['height']} at {spp} spp per step"},
+                 "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    line["config"].update({"width": cfg["width"], "height": cfg["height"], "spp_per_step": spp,
+                           "max_depth": cfg["max_depth"]})
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse_args()
+    cfg = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, cfg, rank)
+
+    import pine_b200 as pb
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = tdist
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    env = "constant" if cfg["kind"] != "mesh" else "none"
+    if args.profile_case:
+        path = scene_path(PROFILE_CASE, args.cache, "constant")
+        ctx = pb.Context(local)
+        sid = ctx.load_scene(path)
+        r = ctx.render(sid, seed=1, math_mode=args.math, outputs=False)
+        print(json.dumps({"profile_case": PROFILE_CASE, "stats": r["stats"]}))
+        ctx.close()
+        return 0
+
+    # Scene files are generated once per cache directory (rank 0 first).
+    if rank == 0:
+        path = scene_path(cfg, args.cache, env)
+    barrier()
+    if rank != 0:
+        path = scene_path(cfg, args.cache, env)
+
+    ctx = pb.Context(local)
+    sid = ctx.load_scene(path)
+    info = ctx.scene_info(sid)
+    paths_per_step = info["width"] * info["height"] * cfg["spp"]
+    seed0 = 1000 * rank
+
+    for w in range(args.warmup):
+        ctx.render(sid, seed=seed0 + w, math_mode=args.math, outputs=False)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    device_s = 0.0
+    launches = 0
+    kernels = {}
+    stats_acc = {"rays": 0, "volume_steps": 0, "paths": 0, "dropped": 0}
+    for s in range(args.steps):
+        r = ctx.render(sid, seed=seed0 + 100 + s, math_mode=args.math, outputs=False,
+                       profile=True)
+        st = r["stats"]
+        device_s += st["seconds"]
+        launches += st["launches"]
+        add_kernels(kernels, st["kernels"])
+        for k in stats_acc:
+            stats_acc[k] += st[k]
+    barrier()
+    clk = clocks.stop()
+    device_s_max = max_over_ranks(device_s)
+
+    # End-to-end through the public API: upload from pinned host memory, render, read the
+    # film back into pinned host memory, release; wall clock, max over ranks.
+    import torch
+    parsed = pb.ParsedScene(path)
+    desc = parsed.desc
+    pinned = []
+    h2d = 0
+    for m in range(desc.num_media):
+        med = desc.media[m]
+        if med.density:
+            n = med.size[0] * med.size[1] * med.size[2]
+            src = np.ctypeslib.as_array(med.density, shape=(n,))
+            buf = torch.empty(n, dtype=torch.float32, pin_memory=True)
+            buf.numpy()[:] = src
+            pinned.append(buf)
+            med.density = ctypes_float_ptr(buf.data_ptr())
+            h2d += n * 4
+    h2d += desc.num_vertices * 12 + desc.num_triangles * 12
+    w, h = info["width"], info["height"]
+    out_mean = torch.empty((h, w, 3), dtype=torch.float32, pin_memory=True).numpy()
+    out_var = torch.empty((h, w, 3), dtype=torch.float32, pin_memory=True).numpy()
+    out_cnt = torch.empty((h, w), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    d2h = out_mean.nbytes + out_var.nbytes + out_cnt.nbytes
+    e2e_steps = max(1, min(args.steps, 4))
+    sid2 = ctx.upload_scene(desc)
+    ctx.render(sid2, spp=1, seed=7, math_mode=args.math, into=(out_mean, out_var, out_cnt))
+    ctx.release_scene(sid2)
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        sid2 = ctx.upload_scene(desc)
+        ctx.render(sid2, seed=seed0 + 500 + s, math_mode=args.math,
+                   into=(out_mean, out_var, out_cnt))
+        ctx.release_scene(sid2)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    parsed.close()
+
+    value = paths_per_step * args.steps * world / device_s_max / 1e6
+    e2e = paths_per_step * e2e_steps * world / e2e_s / 1e6
+    peak, peak_kind = hbm_peak()
+    line = {
+        "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": device_s_max / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; no dataset)",
+        "config": {"workload": f"{args.workload}: " + describe(cfg), "width": info["width"],
+                   "height": info["height"], "spp": cfg["spp"], "max_depth": cfg["max_depth"],
+                   "math_mode": args.math, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (512 MiB density grid vs 126 MB L2)"
+                         if cfg["kind"] == "volume" else "scene resident; no flush"},
+        "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                "timing": "wall clock: pg_upload_scene + pg_render + film readback + release"},
+        "gpu_launches": launches,
+        "mrays_per_s": stats_acc["rays"] * world / device_s_max / 1e6,
+        "gsteps_per_s": stats_acc["volume_steps"] * world / device_s_max / 1e9,
+        "dropped_samples": stats_acc["dropped"],
+        "roofline": roofline(kernels, peak, peak_kind),
+        "kernels": {n: {"launches": k["launches"], "seconds": k["seconds"],
+                        "items": k["items"], "volume_steps": k["volume_steps"]}
+                    for n, k in kernels.items()},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(cfg, args.cache)
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_float_ptr(addr):
+    import ctypes
+    return ctypes.cast(ctypes.c_void_p(addr), ctypes.POINTER(ctypes.c_float))
+
+
+def describe(cfg):
+    if cfg["kind"] == "volume":
+        return (f"{cfg['n']}^3 FP32 cloud grid, sigma_t 20, albedo 0.99, HG g 0.8, sun 5 + "
+                f"constant sky 0.3, {cfg['width']}x{cfg['height']}, {cfg['spp']} spp, "
+                f"max {cfg['max_depth']} events")
+    if cfg["kind"] == "spheres":
+        return (f"64 spheres + plane + rect light + constant env 0.2, {cfg['width']}x"
+                f"{cfg['height']}, {cfg['spp']} spp, depth {cfg['max_depth']}")
+    return (f"icosphere 20*4^{cfg['subdiv']} triangles in a Cornell box, {cfg['width']}x"
+            f"{cfg['height']}, {cfg['spp']} spp, depth {cfg['max_depth']}")
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -161,7 +161,21 @@ typedef struct pg_render_desc {
     int32_t guiding;        /* 1: MIS-combine the learned vMF proposal with BSDF/phase
                                sampling (fraction 0.5); 0: plain path tracing */
     int32_t accumulate;     /* 1: add to the context's film instead of clearing it */
+    int32_t profile;        /* 1: time every kernel launch with CUDA events (per-kernel
+                               totals in pg_render_stats.kernels) */
 } pg_render_desc;
+
+/* Kernels of the wavefront loop, in pg_render_stats.kernels order. */
+enum { PG_KERNEL_REGEN = 0, PG_KERNEL_TRACE = 1, PG_KERNEL_SHADE = 2, PG_KERNEL_SHADOW = 3,
+       PG_NUM_KERNELS = 4 };
+
+typedef struct pg_kernel_stats {
+    int64_t launches;
+    double seconds;         /* summed device time of its launches (profile = 1 only) */
+    int64_t items;          /* queue entries processed (paths or shadow rays) */
+    int64_t volume_steps;   /* density lookups (8 voxels each) */
+    int64_t bricks;         /* majorant bricks entered */
+} pg_kernel_stats;
 
 typedef struct pg_render_stats {
     double seconds;         /* device time of the render (CUDA events) */
@@ -171,6 +185,7 @@ typedef struct pg_render_stats {
     int64_t dropped;        /* samples with NaN/Inf radiance, not accumulated
                                (integrator.cpp:156-157) */
     int64_t launches;       /* kernel launches issued */
+    pg_kernel_stats kernels[PG_NUM_KERNELS];
 } pg_render_stats;
 
 /* ---- context ---- */
@@ -185,6 +200,10 @@ pg_status pg_upload_scene(pg_ctx* ctx, const pg_scene_desc* desc, int32_t* scene
 /* Parse a pine scene file (grammar of src/util/parser.cpp:45-101, numbers through a
  * bit-exact restatement of pstd::stof) and upload it. */
 pg_status pg_load_scene_file(pg_ctx* ctx, const char* path, int32_t* scene_id);
+/* Parse a pine scene file into a flattened description without touching the GPU.  The
+ * arrays *out points into stay valid until pg_free_parsed_scene(*handle). */
+pg_status pg_parse_scene_file(const char* path, pg_scene_desc* out, void** handle);
+void pg_free_parsed_scene(void* handle);
 pg_status pg_release_scene(pg_ctx* ctx, int32_t scene_id);
 /* Film size and defaults of an uploaded scene. */
 pg_status pg_scene_info(pg_ctx* ctx, int32_t scene_id, int32_t* width, int32_t* height,

@@ -18,8 +18,8 @@
 //                                    (src/core/bxdf.cpp) and HG phase (src/core/medium.cpp:9-31).
 //   camera <scene.txt> <in> <out>    ThinLenCamera::GenRay (src/core/camera.cpp:31-41).
 //   density <scene.txt> <in> <out>   GridMedium::Density (src/core/medium.cpp:141-160).
-//   time   <scene.txt>               wall time of the stock Integrator::Render() only
-//                                    (BVH build and file loading excluded).
+//   time   <scene.txt> [repeats] [spp]  wall time of the stock Integrator::Render() only
+//                                    (BVH build and file loading excluded), repeated.
 #include <core/scene.h>
 #include <core/scattering.h>
 #include <util/fileio.h>
@@ -331,19 +331,26 @@ int Density(const char* scenePath, const char* inPath, const char* outPath) {
     return 0;
 }
 
-int Time(const char* scenePath) {
+int Time(const char* scenePath, int repeats, int spp) {
     auto tl = std::chrono::steady_clock::now();
     Scene* scene = Load(scenePath);
     double load = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl).count();
     auto* integ = scene->integrator.get();
+    // PixelIntegrator::Render loops samplesPerPixel times per pixel (integrator.cpp:139-145).
+    if (spp > 0)
+        integ->samplesPerPixel = spp;
     vec2i size = integ->filmSize;
-    auto t0 = std::chrono::steady_clock::now();
-    integ->Render();
-    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     double paths = (double)size.x * size.y * integ->samplesPerPixel;
-    std::printf("{\"seconds\": %.6f, \"paths\": %.0f, \"mpaths_per_s\": %.6f, \"threads\": %d, "
-                "\"load_seconds\": %.3f}\n",
-                secs, paths, paths / secs * 1e-6, NumThreads(), load);
+    // One JSON line per repetition of the stock Render(); the scene is loaded once.
+    for (int r = 0; r < repeats; r++) {
+        auto t0 = std::chrono::steady_clock::now();
+        integ->Render();
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("{\"seconds\": %.6f, \"paths\": %.0f, \"mpaths_per_s\": %.6f, \"threads\": %d, "
+                    "\"load_seconds\": %.3f}\n",
+                    secs, paths, paths / secs * 1e-6, NumThreads(), load);
+        std::fflush(stdout);
+    }
     return 0;
 }
 
@@ -371,8 +378,8 @@ int main(int argc, char** argv) {
         return CameraRays(argv[2], argv[3], argv[4]);
     if (mode == "density" && argc == 5)
         return Density(argv[2], argv[3], argv[4]);
-    if (mode == "time" && argc == 3)
-        return Time(argv[2]);
+    if (mode == "time" && argc >= 3 && argc <= 5)
+        return Time(argv[2], argc >= 4 ? std::atoi(argv[3]) : 1, argc == 5 ? std::atoi(argv[4]) : 0);
     std::fprintf(stderr, "bad arguments for mode %s\n", mode.c_str());
     return 2;
 }

@@ -36,13 +36,80 @@ class RenderDesc(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32),
                 ("seed", ctypes.c_uint64), ("sample_offset", ctypes.c_int32),
                 ("math_mode", ctypes.c_int32), ("guiding", ctypes.c_int32),
-                ("accumulate", ctypes.c_int32)]
+                ("accumulate", ctypes.c_int32), ("profile", ctypes.c_int32)]
+
+
+KERNELS = ["regen", "trace", "shade", "shadow"]
+
+
+class KernelStats(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64), ("seconds", ctypes.c_double),
+                ("items", ctypes.c_int64), ("volume_steps", ctypes.c_int64),
+                ("bricks", ctypes.c_int64)]
 
 
 class RenderStats(ctypes.Structure):
     _fields_ = [("seconds", ctypes.c_double), ("paths", ctypes.c_int64),
                 ("rays", ctypes.c_int64), ("volume_steps", ctypes.c_int64),
-                ("dropped", ctypes.c_int64), ("launches", ctypes.c_int64)]
+                ("dropped", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("kernels", KernelStats * 4)]
+
+    def to_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "kernels"}
+        d["kernels"] = {name: {k: getattr(self.kernels[i], k) for k, _ in KernelStats._fields_}
+                        for i, name in enumerate(KERNELS)}
+        return d
+
+
+# Flattened scene description (pg_scene_desc and the records it points to).
+class Shape(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("material", ctypes.c_int32),
+                ("medium_inside", ctypes.c_int32), ("medium_outside", ctypes.c_int32),
+                ("mesh_first_triangle", ctypes.c_int64), ("mesh_num_triangles", ctypes.c_int64),
+                ("p", ctypes.c_float * 12)]
+
+
+class Bsdf(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("albedo", ctypes.c_float * 3),
+                ("roughness", ctypes.c_float), ("eta", ctypes.c_float)]
+
+
+class Material(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("num_layers", ctypes.c_int32),
+                ("layers", Bsdf * 4), ("emission", ctypes.c_float * 3)]
+
+
+class Light(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("p", ctypes.c_float * 12)]
+
+
+class Medium(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("sigma_a", ctypes.c_float * 3),
+                ("sigma_s", ctypes.c_float * 3), ("g", ctypes.c_float),
+                ("size", ctypes.c_int32 * 3), ("position", ctypes.c_float * 3),
+                ("scale", ctypes.c_float), ("interpolate", ctypes.c_int32),
+                ("density", ctypes.POINTER(ctypes.c_float))]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [("from_", ctypes.c_float * 3), ("to", ctypes.c_float * 3),
+                ("fov", ctypes.c_float), ("lens_radius", ctypes.c_float),
+                ("focus_distance", ctypes.c_float), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("medium", ctypes.c_int32)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("num_shapes", ctypes.c_int32), ("shapes", ctypes.POINTER(Shape)),
+                ("num_vertices", ctypes.c_int64), ("vertices", ctypes.POINTER(ctypes.c_float)),
+                ("num_triangles", ctypes.c_int64), ("indices", ctypes.POINTER(ctypes.c_uint32)),
+                ("num_materials", ctypes.c_int32), ("materials", ctypes.POINTER(Material)),
+                ("num_media", ctypes.c_int32), ("media", ctypes.POINTER(Medium)),
+                ("num_lights", ctypes.c_int32), ("lights", ctypes.POINTER(Light)),
+                ("camera", Camera), ("light_sampler", ctypes.c_int32),
+                ("max_depth", ctypes.c_int32), ("samples_per_pixel", ctypes.c_int32)]
+
+
+SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
 
 
 class Tuning(ctypes.Structure):
@@ -109,6 +176,8 @@ def lib():
                                       ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                       ctypes.c_float, ctypes.c_uint64, _P(ctypes.c_int64)]),
         "pg_pstd_stof": (ctypes.c_float, [ctypes.c_char_p, ctypes.c_int64]),
+        "pg_parse_scene_file": (st, [ctypes.c_char_p, _P(SceneDesc), _P(ctypes.c_void_p)]),
+        "pg_free_parsed_scene": (None, [ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         if hasattr(L, name):
@@ -127,6 +196,31 @@ def lib():
 
 def _fptr(a):
     return None if a is None else a.ctypes.data_as(_F)
+
+
+class ParsedScene:
+    """A pine scene file parsed into a flattened SceneDesc (host memory owned by the
+    library until close())."""
+
+    def __init__(self, path: str):
+        self._lib = lib()
+        self.desc = SceneDesc()
+        self._h = ctypes.c_void_p()
+        st = self._lib.pg_parse_scene_file(os.path.abspath(path).encode(),
+                                          ctypes.byref(self.desc), ctypes.byref(self._h))
+        if st != PG_OK:
+            raise PgError(st, (self._lib.pg_last_error(None) or b"").decode(errors="replace"))
+
+    def close(self):
+        if self._h:
+            self._lib.pg_free_parsed_scene(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -160,6 +254,11 @@ class Context:
             pass
 
     # ---- scenes
+    def upload_scene(self, desc: "SceneDesc") -> int:
+        sid = ctypes.c_int32(-1)
+        self._check(self._lib.pg_upload_scene(self._ctx, ctypes.byref(desc), ctypes.byref(sid)))
+        return sid.value
+
     def load_scene(self, path: str) -> int:
         sid = ctypes.c_int32(-1)
         self._check(self._lib.pg_load_scene_file(self._ctx, os.path.abspath(path).encode(),
@@ -178,14 +277,19 @@ class Context:
     # ---- rendering
     def render(self, scene: int, spp: int = 0, max_depth: int = 0, seed: int = 0,
                math_mode: str = "pine", sample_offset: int = 0, accumulate: bool = False,
-               guiding: bool = False, outputs: bool = True):
+               guiding: bool = False, outputs: bool = True, profile: bool = False, into=None):
+        """Renders one image.  ``into`` may give preallocated (mean, var, count) arrays
+        (e.g. pinned host memory) to fill instead of new ones."""
         info = self.scene_info(scene)
         w, h = info["width"], info["height"]
         desc = RenderDesc(int(spp), int(max_depth), int(seed), int(sample_offset),
-                          MATH_MODES[math_mode], int(bool(guiding)), int(bool(accumulate)))
+                          MATH_MODES[math_mode], int(bool(guiding)), int(bool(accumulate)),
+                          int(bool(profile)))
         stats = RenderStats()
         mean = var = count = None
-        if outputs:
+        if into is not None:
+            mean, var, count = into
+        elif outputs:
             mean = np.zeros((h, w, 3), np.float32)
             var = np.zeros((h, w, 3), np.float32)
             count = np.zeros((h, w), np.uint32)
@@ -193,8 +297,7 @@ class Context:
                                         _fptr(var),
                                         None if count is None else count.ctypes.data_as(_U32),
                                         ctypes.byref(stats)))
-        st = {k: getattr(stats, k) for k, _ in RenderStats._fields_}
-        return {"mean": mean, "var": var, "count": count, "stats": st}
+        return {"mean": mean, "var": var, "count": count, "stats": stats.to_dict()}
 
     def intersect(self, scene: int, rays: np.ndarray):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)

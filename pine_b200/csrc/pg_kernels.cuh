@@ -17,6 +17,13 @@
 
 namespace pg {
 
+enum StatIndex {
+    kStatRays = 0, kStatSteps, kStatDropped, kStatPaths,
+    kStatShadeItems, kStatShadeSteps, kStatShadeBricks,
+    kStatShadowItems, kStatShadowSteps, kStatShadowBricks,
+    kStatTraceItems, kStatRegenItems, kNumStats = 16
+};
+
 enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlotDead = 3 };
 
 struct RenderParams {
@@ -45,7 +52,7 @@ struct RenderParams {
     double* film_sq;       // npix * 3
     uint32_t* film_n;      // npix
     unsigned long long* next_sample;
-    unsigned long long* stats;  // [0] rays, [1] volume steps, [2] dropped, [3] paths
+    unsigned long long* stats;  // kStat* counters
     uint32_t* err;
 };
 
@@ -152,8 +159,9 @@ __global__ void k_regen(RenderParams P, SceneDev S) {
     int slot = WarpAppend(&P.counts[0], st == kSlotActive);
     if (slot >= 0)
         P.active[slot] = i;
-    WarpAdd(&P.stats[3], (uint32_t)done);
-    WarpAdd(&P.stats[2], (uint32_t)dropped);
+    WarpAdd(&P.stats[kStatPaths], (uint32_t)done);
+    WarpAdd(&P.stats[kStatDropped], (uint32_t)dropped);
+    WarpAdd(&P.stats[kStatRegenItems], 1u);
 }
 
 __global__ void k_trace(RenderParams P, SceneDev S) {
@@ -171,7 +179,8 @@ __global__ void k_trace(RenderParams P, SceneDev S) {
     P.hit[i] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
     if (err)
         atomicOr(P.err, err);
-    WarpAdd(&P.stats[0], 1u);
+    WarpAdd(&P.stats[kStatRays], 1u);
+    WarpAdd(&P.stats[kStatTraceItems], 1u);
 }
 
 struct SurfaceInfo {
@@ -296,7 +305,7 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
     V3 beta = v3(bt.x, bt.y, bt.z), L = v3(Lw.x, Lw.y, Lw.z);
     int depth = __float_as_int(bt.w);
     Rng rng{P.sample[i], P.key1, __float_as_uint(Lw.w)};
-    uint32_t err = 0, steps = 0;
+    uint32_t err = 0, steps = 0, bricks = 0;
     int prim = __float_as_int(h.y);
     bool found = prim != -1;
     float tHit = found ? h.x : kFloatMax;
@@ -307,7 +316,7 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
     MediumEvent ev;
     ev.scattered = false;
     if (medium >= 0) {
-        MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, steps, err);
+        MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, steps, bricks, err);
         beta *= ev.weight;
     }
     if (ev.scattered) {
@@ -410,7 +419,10 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
     }
     if (err)
         atomicOr(P.err, err);
-    WarpAdd(&P.stats[1], steps);
+    WarpAdd(&P.stats[kStatSteps], steps);
+    WarpAdd(&P.stats[kStatShadeSteps], steps);
+    WarpAdd(&P.stats[kStatShadeBricks], bricks);
+    WarpAdd(&P.stats[kStatShadeItems], 1u);
 }
 
 template <int M>
@@ -426,7 +438,7 @@ __global__ void k_shadow(RenderParams P, SceneDev S) {
     float tmax = so.w;
     int medium = __float_as_int(sd.w);
     Rng rng{P.sample[slot], P.skey[q], 0};
-    uint32_t err = 0, steps = 0;
+    uint32_t err = 0, steps = 0, bricks = 0;
     V3 tr = v3(1.0f);
     int traced = 1;
     if (!S.has_null_surfaces) {
@@ -435,7 +447,7 @@ __global__ void k_shadow(RenderParams P, SceneDev S) {
             tr = v3(0.0f);
         } else if (medium >= 0) {
             V3 t3;
-            MediumTr<M>(S.media[medium], o, d, tmax, rng, steps, err, t3);
+            MediumTr<M>(S.media[medium], o, d, tmax, rng, steps, bricks, err, t3);
             tr = t3;
         }
     } else {
@@ -446,7 +458,7 @@ __global__ void k_shadow(RenderParams P, SceneDev S) {
             bool hitS = Traverse<false>(S, o, d, 0.0f, tmax, h, stack + threadIdx.x, blockDim.x, err);
             if (medium >= 0) {
                 V3 t3;
-                MediumTr<M>(S.media[medium], o, d, hitS ? h.t : tmax, rng, steps, err, t3);
+                MediumTr<M>(S.media[medium], o, d, hitS ? h.t : tmax, rng, steps, bricks, err, t3);
                 tr *= t3;
             }
             if (!hitS)
@@ -475,8 +487,29 @@ __global__ void k_shadow(RenderParams P, SceneDev S) {
     }
     if (err)
         atomicOr(P.err, err);
-    WarpAdd(&P.stats[0], (uint32_t)traced);
-    WarpAdd(&P.stats[1], steps);
+    WarpAdd(&P.stats[kStatRays], (uint32_t)traced);
+    WarpAdd(&P.stats[kStatSteps], steps);
+    WarpAdd(&P.stats[kStatShadowSteps], steps);
+    WarpAdd(&P.stats[kStatShadowBricks], bricks);
+    WarpAdd(&P.stats[kStatShadowItems], 1u);
+}
+
+// Brick majorants: the largest density over voxels [8b, 8b+8] of each axis (the
+// trilinear footprint of points inside brick b), one thread per brick.
+__global__ void k_majorant(const float* dens, int sx, int sy, int sz, int nbx, int nby, int nbz,
+                           float* maj) {
+    int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= (int64_t)nbx * nby * nbz)
+        return;
+    int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+    float m = 0.0f;
+    for (int z = 8 * bz; z <= min(8 * bz + 8, sz - 1); z++)
+        for (int y = 8 * by; y <= min(8 * by + 8, sy - 1); y++) {
+            const float* row = dens + (size_t)z * sx * sy + (size_t)y * sx;
+            for (int x = 8 * bx; x <= min(8 * bx + 8, sx - 1); x++)
+                m = fmaxf(m, __ldg(&row[x]));
+        }
+    maj[b] = m;
 }
 
 // pg_intersect: closest hit per ray with pine's shape index and triangle index.

@@ -523,7 +523,7 @@ __device__ __forceinline__ float GridDensity(const MediumDev& m, float vx, float
 // f returns true to stop the walk.
 template <typename F>
 __device__ __forceinline__ void WalkBricks(const MediumDev& m, V3 o, V3 d, float t0, float t1,
-                                           F&& f) {
+                                           uint32_t& bricks, F&& f) {
     // Voxel-index space: v = (o + t d) * size; bricks are 8 voxels wide.
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     V3 vo = v3(o.x * sx, o.y * sy, o.z * sz), vd = v3(d.x * sx, d.y * sy, d.z * sz);
@@ -549,6 +549,7 @@ __device__ __forceinline__ void WalkBricks(const MediumDev& m, V3 o, V3 d, float
         float tn = Min(Min(tx, ty), Min(tz, t1));
         float maj = __ldg(&m.majorant[bx + m.nb[0] * (by + m.nb[1] * bz)]);
         if (maj > 0.0f && tn > t) {
+            bricks++;
             if (f(t, tn, maj))
                 return;
         }
@@ -584,7 +585,8 @@ struct MediumEvent {
 // used as the bound in medium space as pine does (medium.cpp:99-101).
 template <int M>
 __device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng,
-                                  MediumEvent& ev, uint32_t& steps, uint32_t& err) {
+                                  MediumEvent& ev, uint32_t& steps, uint32_t& bricks,
+                                  uint32_t& err) {
     ev.scattered = false;
     ev.weight = v3(1.0f);
     if (m.type == PG_MEDIUM_HOMOGENEOUS) {
@@ -615,7 +617,7 @@ __device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rn
     float ts = 0.0f;
     uint32_t n = 0;
     bool hit = false;
-    WalkBricks(m, mo, md, t0, t1, [&](float ta, float tb, float maj) {
+    WalkBricks(m, mo, md, t0, t1, bricks, [&](float ta, float tb, float maj) {
         float inv = 1.0f / (m.sigma_t * maj);
         float t = ta;
         while (true) {
@@ -647,7 +649,7 @@ __device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rn
 // transmittance estimate drops below 0.1.  HomogeneousMedium::Tr (medium.cpp:33-36).
 template <int M>
 __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng, uint32_t& steps,
-                          uint32_t& err, V3& trRGB) {
+                          uint32_t& bricks, uint32_t& err, V3& trRGB) {
     if (m.type == PG_MEDIUM_HOMOGENEOUS) {
         trRGB = v3(PMath<M>::exp(-tmax * (m.sigma_a[0] + m.sigma_s[0])),
                    PMath<M>::exp(-tmax * (m.sigma_a[1] + m.sigma_s[1])),
@@ -663,7 +665,7 @@ __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng, 
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     float tr = 1.0f;
     uint32_t n = 0;
-    WalkBricks(m, mo, md, t0, t1, [&](float ta, float tb, float maj) {
+    WalkBricks(m, mo, md, t0, t1, bricks, [&](float ta, float tb, float maj) {
         float inv = 1.0f / (m.sigma_t * maj);
         float t = ta;
         while (true) {

@@ -144,7 +144,8 @@ struct pg_ctx {
     pg::DevMem small;
     int* counts = nullptr;                 // [0] active, [1] shadow
     unsigned long long* next_sample = nullptr;
-    unsigned long long* stats = nullptr;   // 4 counters
+    unsigned long long* stats = nullptr;   // kNumStats counters
+    std::vector<cudaEvent_t> events;       // profiling events, reused
     uint32_t* err = nullptr;
     int* h_counts = nullptr;               // pinned
     std::string last_error;
@@ -183,34 +184,6 @@ static V3 L3(const float* p) {
 
 static void Put(float* dst, V3 v) {
     dst[0] = v.x, dst[1] = v.y, dst[2] = v.z;
-}
-
-static void BuildMajorants(const float* dens, const int size[3], std::vector<float>& maj, int nb[3]) {
-    for (int k = 0; k < 3; k++)
-        nb[k] = (size[k] + 7) / 8;
-    maj.assign((size_t)nb[0] * nb[1] * nb[2], 0.0f);
-    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
-    std::atomic<int> next{0};
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; t++)
-        th.emplace_back([&]() {
-            for (int bz; (bz = next.fetch_add(1)) < nb[2];) {
-                for (int by = 0; by < nb[1]; by++)
-                    for (int bx = 0; bx < nb[0]; bx++) {
-                        // The trilinear footprint of points in brick b reaches voxel 8b+8.
-                        float m = 0.0f;
-                        for (int z = 8 * bz; z <= std::min(8 * bz + 8, size[2] - 1); z++)
-                            for (int y = 8 * by; y <= std::min(8 * by + 8, size[1] - 1); y++) {
-                                const float* row = dens + (size_t)z * size[0] * size[1] + (size_t)y * size[0];
-                                for (int x = 8 * bx; x <= std::min(8 * bx + 8, size[0] - 1); x++)
-                                    m = std::max(m, row[x]);
-                            }
-                        maj[(size_t)bx + (size_t)nb[0] * (by + (size_t)nb[1] * bz)] = m;
-                    }
-            }
-        });
-    for (auto& t : th)
-        t.join();
 }
 
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
@@ -406,18 +379,20 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         Require(m.type == PG_MEDIUM_GRID, "unknown medium type", PG_ERR_UNSUPPORTED);
         Require(m.size[0] > 0 && m.size[1] > 0 && m.size[2] > 0 && m.density, "bad grid medium");
         size_t nvox = (size_t)m.size[0] * m.size[1] * m.size[2];
-        float maxD = 0.0f;
-        for (size_t v = 0; v < nvox; v++)
-            maxD = std::max(maxD, m.density[v]);
-        o.inv_max_density = 1.0f / maxD;
         std::memcpy(o.size, m.size, sizeof(o.size));
         o.interpolate = m.interpolate;
         float* dd = sc->mem.Alloc<float>(nvox);
         PG_CUDA(cudaMemcpyAsync(dd, m.density, nvox * 4, cudaMemcpyHostToDevice, st));
         o.density = dd;
-        std::vector<float> maj;
-        BuildMajorants(m.density, m.size, maj, o.nb);
-        o.majorant = sc->mem.Upload(maj, st);
+        // Brick majorants are built on the device from the uploaded grid.
+        for (int k = 0; k < 3; k++)
+            o.nb[k] = (m.size[k] + 7) / 8;
+        int64_t nbTot = (int64_t)o.nb[0] * o.nb[1] * o.nb[2];
+        float* maj = sc->mem.Alloc<float>(nbTot);
+        k_majorant<<<(unsigned)Ceil<int64_t>(nbTot, 256), 256, 0, st>>>(dd, m.size[0], m.size[1], m.size[2],
+                                                                      o.nb[0], o.nb[1], o.nb[2], maj);
+        PG_CUDA(cudaGetLastError());
+        o.majorant = maj;
         // w2m = Translate(0.5 - position) * Scale(1 / normalizedSize / scale) (medium.cpp:180-182).
         float mx = (float)std::max(m.size[0], std::max(m.size[1], m.size[2]));
         float s3[3];
@@ -612,27 +587,77 @@ static uint32_t PcgHashHost(uint32_t v) {
     return (w >> 22u) ^ w;
 }
 
-template <int M>
-static void LaunchIteration(pg_ctx* ctx, const RenderParams& P, const SceneDev& S, bool surfaces,
-                            int n) {
-    cudaStream_t st = ctx->stream;
-    int tb = 128;
-    size_t smem = (size_t)tb * kStackSize * sizeof(uint2);
-    if (surfaces)
-        k_trace<<<Ceil(n, tb), tb, smem, st>>>(P, S);
-    int sb = ctx->tuning.block_size > 0 ? ctx->tuning.block_size : 128;
-    k_shade<M><<<Ceil(n, sb), sb, 0, st>>>(P, S);
-    k_shadow<M><<<Ceil(n, tb), tb, smem, st>>>(P, S);
-}
 
 struct RenderResult {
     double seconds = 0;
-    unsigned long long stats[4] = {};
+    unsigned long long stats[kNumStats] = {};
     int64_t launches = 0;
+    int64_t kernelLaunches[PG_NUM_KERNELS] = {};
+    double kernelSeconds[PG_NUM_KERNELS] = {};
 };
 
+// Optional per-launch timing: a start/stop event pair around each kernel launch.
+struct LaunchTimer {
+    pg_ctx* ctx;
+    bool on;
+    size_t used = 0;
+    std::vector<std::pair<int, size_t>> marks;  // kernel, index of its start event
+    cudaEvent_t Next();
+    template <typename F>
+    void Time(int kernel, F&& launch);
+    void Collect(RenderResult& r);
+};
+
+cudaEvent_t LaunchTimer::Next() {
+    if (used == ctx->events.size()) {
+        cudaEvent_t e;
+        PG_CUDA(cudaEventCreate(&e));
+        ctx->events.push_back(e);
+    }
+    return ctx->events[used++];
+}
+
+template <typename F>
+void LaunchTimer::Time(int kernel, F&& launch) {
+    if (!on) {
+        launch();
+        return;
+    }
+    size_t first = used;
+    PG_CUDA(cudaEventRecord(Next(), ctx->stream));
+    launch();
+    PG_CUDA(cudaEventRecord(Next(), ctx->stream));
+    marks.push_back({kernel, first});
+}
+
+void LaunchTimer::Collect(RenderResult& r) {
+    for (auto& m : marks) {
+        float ms = 0.0f;
+        PG_CUDA(cudaEventElapsedTime(&ms, ctx->events[m.second], ctx->events[m.second + 1]));
+        r.kernelSeconds[m.first] += ms * 1e-3;
+    }
+}
+
+template <int M>
+static void LaunchIteration(pg_ctx* ctx, LaunchTimer& timer, RenderResult& res,
+                            const RenderParams& P, const SceneDev& S, bool surfaces, int n) {
+    cudaStream_t st = ctx->stream;
+    int tb = 128;
+    size_t smem = (size_t)tb * kStackSize * sizeof(uint2);
+    if (surfaces) {
+        timer.Time(PG_KERNEL_TRACE, [&]() { k_trace<<<Ceil(n, tb), tb, smem, st>>>(P, S); });
+        res.kernelLaunches[PG_KERNEL_TRACE]++;
+    }
+    int sb = ctx->tuning.block_size > 0 ? ctx->tuning.block_size : 128;
+    timer.Time(PG_KERNEL_SHADE, [&]() { k_shade<M><<<Ceil(n, sb), sb, 0, st>>>(P, S); });
+    timer.Time(PG_KERNEL_SHADOW, [&]() { k_shadow<M><<<Ceil(n, tb), tb, smem, st>>>(P, S); });
+    res.kernelLaunches[PG_KERNEL_SHADE]++;
+    res.kernelLaunches[PG_KERNEL_SHADOW]++;
+}
+
 static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
-                       int sampleOffset, int mathMode, bool accumulate, RenderResult& res) {
+                       int sampleOffset, int mathMode, bool accumulate, bool profile,
+                       RenderResult& res) {
     Require(spp > 0 && maxDepth > 0, "spp and max depth must be positive");
     Require(mathMode == PG_MATH_PINE || mathMode == PG_MATH_FAST, "unknown math mode");
     Require(sampleOffset >= 0, "sample offset must be >= 0");
@@ -652,7 +677,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     Pool& pl = ctx->pool;
     PG_CUDA(cudaMemsetAsync(pl.state, 0, (size_t)slots * sizeof(int), st));
     PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
-    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, 4 * sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
     PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
 
     RenderParams P{};
@@ -674,6 +699,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
 
     const SceneDev& S = sc.dev;
     int64_t launches = 0;
+    LaunchTimer timer{ctx, profile};
     // Every path ends within max_depth counted events; null-surface crossings do not
     // count, so the cap leaves room for them.
     const int64_t maxIter = ((int64_t)total / slots + 2) * ((int64_t)maxDepth * 4 + 64) + 4096;
@@ -682,10 +708,13 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     for (;; iter++) {
         Require(iter < maxIter, "render loop did not converge", PG_ERR_DEVICE_LIMIT);
         PG_CUDA(cudaMemsetAsync(ctx->counts, 0, 2 * sizeof(int), st));
-        if (mathMode == PG_MATH_PINE)
-            k_regen<kPine><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
-        else
-            k_regen<kFast><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
+        timer.Time(PG_KERNEL_REGEN, [&]() {
+            if (mathMode == PG_MATH_PINE)
+                k_regen<kPine><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
+            else
+                k_regen<kFast><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
+        });
+        res.kernelLaunches[PG_KERNEL_REGEN]++;
         launches++;
         PG_CUDA(cudaMemcpyAsync(ctx->h_counts, ctx->counts, sizeof(int), cudaMemcpyDeviceToHost, st));
         PG_CUDA(cudaStreamSynchronize(st));
@@ -693,9 +722,9 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
         if (n == 0)
             break;
         if (mathMode == PG_MATH_PINE)
-            LaunchIteration<kPine>(ctx, P, S, sc.surfaces, n);
+            LaunchIteration<kPine>(ctx, timer, res, P, S, sc.surfaces, n);
         else
-            LaunchIteration<kFast>(ctx, P, S, sc.surfaces, n);
+            LaunchIteration<kFast>(ctx, timer, res, P, S, sc.surfaces, n);
         launches += sc.surfaces ? 3 : 2;
         PG_CUDA(cudaGetLastError());
     }
@@ -705,6 +734,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     res.seconds = ms * 1e-3;
     res.launches = launches;
+    timer.Collect(res);
     PG_CUDA(cudaMemcpy(res.stats, ctx->stats, sizeof(res.stats), cudaMemcpyDeviceToHost));
     uint32_t e = 0;
     PG_CUDA(cudaMemcpy(&e, ctx->err, sizeof(e), cudaMemcpyDeviceToHost));
@@ -756,7 +786,7 @@ extern "C" pg_status pg_create(pg_ctx** out, int device) {
         PG_CUDA(cudaEventCreate(&ctx->ev1));
         ctx->counts = ctx->small.Alloc<int>(4);
         ctx->next_sample = ctx->small.Alloc<unsigned long long>(1);
-        ctx->stats = ctx->small.Alloc<unsigned long long>(4);
+        ctx->stats = ctx->small.Alloc<unsigned long long>(kNumStats);
         ctx->err = ctx->small.Alloc<uint32_t>(1);
         PG_CUDA(cudaMallocHost(&ctx->h_counts, 4 * sizeof(int)));
     });
@@ -784,6 +814,8 @@ extern "C" void pg_destroy(pg_ctx* ctx) {
         cudaEventDestroy(ctx->ev0);
     if (ctx->ev1)
         cudaEventDestroy(ctx->ev1);
+    for (auto e : ctx->events)
+        cudaEventDestroy(e);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -819,6 +851,24 @@ extern "C" pg_status pg_load_scene_file(pg_ctx* ctx, const char* path, int32_t* 
         PG_CUDA(cudaSetDevice(ctx->device));
         UploadScene(ctx, &d, scene_id);
     });
+}
+
+extern "C" pg_status pg_parse_scene_file(const char* path, pg_scene_desc* out, void** handle) {
+    if (!path || !out || !handle)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null path, description or handle"});
+    *handle = nullptr;
+    auto hs = std::make_unique<HostScene>();
+    pg_status s = Guard(nullptr, [&]() {
+        LoadSceneFile(path, *hs);
+        hs->Describe(*out);
+    });
+    if (s == PG_OK)
+        *handle = hs.release();
+    return s;
+}
+
+extern "C" void pg_free_parsed_scene(void* handle) {
+    delete static_cast<HostScene*>(handle);
 }
 
 extern "C" pg_status pg_release_scene(pg_ctx* ctx, int32_t scene_id) {
@@ -864,15 +914,27 @@ extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_de
         int md = desc->max_depth > 0 ? desc->max_depth : sc.max_depth;
         RenderResult r;
         RenderFilm(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
-                   desc->accumulate != 0, r);
+                   desc->accumulate != 0, desc->profile != 0, r);
         ReadFilm(ctx, (int64_t)sc.width * sc.height, out_mean, out_var, out_count);
         if (stats) {
             stats->seconds = r.seconds;
-            stats->rays = (int64_t)r.stats[0];
-            stats->volume_steps = (int64_t)r.stats[1];
-            stats->dropped = (int64_t)r.stats[2];
-            stats->paths = (int64_t)r.stats[3];
+            stats->rays = (int64_t)r.stats[kStatRays];
+            stats->volume_steps = (int64_t)r.stats[kStatSteps];
+            stats->dropped = (int64_t)r.stats[kStatDropped];
+            stats->paths = (int64_t)r.stats[kStatPaths];
             stats->launches = r.launches;
+            const int items[PG_NUM_KERNELS] = {kStatRegenItems, kStatTraceItems, kStatShadeItems,
+                                               kStatShadowItems};
+            const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps};
+            const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks};
+            for (int k = 0; k < PG_NUM_KERNELS; k++) {
+                pg_kernel_stats& ks = stats->kernels[k];
+                ks.launches = r.kernelLaunches[k];
+                ks.seconds = r.kernelSeconds[k];
+                ks.items = (int64_t)r.stats[items[k]];
+                ks.volume_steps = steps[k] >= 0 ? (int64_t)r.stats[steps[k]] : 0;
+                ks.bricks = bricks[k] >= 0 ? (int64_t)r.stats[bricks[k]] : 0;
+            }
         }
     });
 }

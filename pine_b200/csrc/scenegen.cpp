@@ -123,7 +123,7 @@ extern "C" pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fra
     ParallelRange(total, [&](int64_t i) {
         int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((int64_t)n * n));
         float px = (x + 0.5f) / n, py = (y + 0.5f) / n, pz = (z + 0.5f) / n;
-        float ex = (px - 0.5f) / 0.42f, ey = (py - 0.5f) / 0.30f, ez = (pz - 0.5f) / 0.38f;
+        float ex = (px - 0.5f) / 0.49f, ey = (py - 0.5f) / 0.42f, ez = (pz - 0.5f) / 0.47f;
         float r2 = ex * ex + ey * ey + ez * ez;
         float fall = r2 < 1.0f ? (1.0f - r2) * (1.0f - r2) : 0.0f;
         float f = Fbm(px * 4.0f, py * 4.0f, pz * 4.0f, 6, s) * 0.5f + 0.5f;
