@@ -290,12 +290,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, f"cuda:{local}")
 
     env = "constant" if cfg["kind"] != "mesh" else "none"
     if args.profile_case:
@@ -381,8 +376,8 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     parsed.close()
 
-    value = paths_per_step * args.steps * world / device_s_max / 1e6
-    e2e = paths_per_step * e2e_steps * world / e2e_s / 1e6
+    value = aggregate(paths_per_step, args.steps, world, device_s_max)
+    e2e = aggregate(paths_per_step, e2e_steps, world, e2e_s)
     peak, peak_kind = hbm_peak()
     line = {
         "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world,
@@ -419,6 +414,21 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def reduce_max(x, dist, device):
+    """Max of x over the ranks of the process group (x itself without one)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(paths_per_step, steps, world, device_seconds_max):
+    """Whole-job throughput in Mpaths/s: every rank renders paths_per_step per step."""
+    return paths_per_step * steps * world / device_seconds_max / 1e6
 
 
 def ctypes_float_ptr(addr):

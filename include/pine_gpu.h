@@ -248,8 +248,10 @@ typedef struct pg_batch_result {
 
 typedef struct pg_tuning {
     int32_t queue_capacity; /* path slots resident in the wavefront */
-    int32_t block_size;     /* threads per block of the bounce kernels */
-    int32_t split_shadow;   /* 1: shadow rays in their own kernel; 0: fused in shading */
+    int32_t block_size;     /* threads per block of the shading kernel */
+    int32_t split_shadow;   /* 1: shadow rays in their own kernel; 0: traced inside the
+                               shading kernel */
+    int32_t majorant_brick; /* voxels per edge of a grid medium's majorant brick: 8, 16, 32 */
 } pg_tuning;
 
 pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,

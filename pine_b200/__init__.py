@@ -114,7 +114,7 @@ SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
 
 class Tuning(ctypes.Structure):
     _fields_ = [("queue_capacity", ctypes.c_int32), ("block_size", ctypes.c_int32),
-                ("split_shadow", ctypes.c_int32)]
+                ("split_shadow", ctypes.c_int32), ("majorant_brick", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):
@@ -317,6 +317,49 @@ class Context:
         self._check(self._lib.pg_get_tuning(self._ctx, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
-    def set_tuning(self, queue_capacity: int, block_size: int = 128, split_shadow: int = 1):
-        t = Tuning(int(queue_capacity), int(block_size), int(split_shadow))
+    def set_tuning(self, queue_capacity: int = 1 << 21, block_size: int = 128,
+                   split_shadow: int = 1, majorant_brick: int = 16):
+        t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))
+
+    @staticmethod
+    def _requests(reqs, outputs):
+        arr = (Request * len(reqs))()
+        outs = []
+        for i, r in enumerate(reqs):
+            arr[i].scene_id = int(r["scene"])
+            arr[i].width = int(r.get("width", 0))
+            arr[i].height = int(r.get("height", 0))
+            arr[i].spp = int(r["spp"])
+            arr[i].max_depth = int(r.get("max_depth", 0))
+            arr[i].seed = int(r.get("seed", i))
+            out = None
+            if outputs:
+                out = np.zeros((int(r["out_height"]), int(r["out_width"]), 3), np.float32)
+                arr[i].out_mean = out.ctypes.data_as(_F)
+            outs.append(out)
+        return arr, outs
+
+    def render_batch(self, reqs, outputs: bool = True):
+        """Renders many requests (dicts: scene, spp, width, height, max_depth, seed) in one
+        graph-captured wavefront.  Returns per-request means, per-request completion times
+        (seconds from the batch start) and the batch's device time."""
+        sizes = []
+        for r in reqs:
+            info = self.scene_info(int(r["scene"]))
+            w = int(r.get("width", 0)) or info["width"]
+            h = int(r.get("height", 0)) or info["height"]
+            sizes.append((w, h))
+        full = [dict(r, out_width=w, out_height=h) for r, (w, h) in zip(reqs, sizes)]
+        arr, outs = self._requests(full, outputs)
+        times = (ctypes.c_double * len(reqs))()
+        res = BatchResult(0.0, 0, ctypes.cast(times, _P(ctypes.c_double)))
+        self._check(self._lib.pg_render_batch(self._ctx, arr, len(reqs), ctypes.byref(res)))
+        return {"means": outs, "request_seconds": list(times), "seconds": res.seconds,
+                "paths": res.paths}
+
+    def autotune(self, reqs) -> dict:
+        arr, _ = self._requests(reqs, False)
+        t = Tuning()
+        self._check(self._lib.pg_autotune(self._ctx, arr, len(reqs), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}

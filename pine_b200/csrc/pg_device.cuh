@@ -59,8 +59,10 @@ struct MediumDev {
     float inv_max_density;
     int interpolate;
     const float* density;   // x fastest
-    const float* majorant;  // per 8^3 brick, covering the trilinear footprint
+    const float* majorant;  // per brick of bsize^3 voxels, covering the trilinear footprint
     int nb[3];
+    int bsize;              // voxels per brick edge (8, 16 or 32)
+    float inv_bsize;
 };
 
 struct CameraDev {
@@ -104,6 +106,7 @@ enum DeviceError : uint32_t {
     kErrStackOverflow = 1u,
     kErrTraversalCap = 2u,
     kErrTrackingCap = 4u,
+    kErrLoopCap = 8u,
 };
 
 constexpr int kStackSize = 32;

@@ -2,15 +2,25 @@
 // (src/impl/integrator/path.cpp:6-87) per launch sequence, over a pool of path slots that
 // are refilled with new camera samples as paths finish.
 //
-//   k_regen   flush finished paths to the film (Film::AddSample with a box filter of
-//             radius 0.5: one pixel per sample, film.h:26-45), claim new camera samples
-//             (RadianceIntegrator::Compute + ThinLenCamera::GenRay, integrator.cpp:152-158,
-//             camera.cpp:31-41) and compact the active slots into a queue.
+// One iteration runs, in order:
+//   k_regen   for the slots shading marked finished: flush the path to the film
+//             (Film::AddSample with a box filter of radius 0.5: one pixel per sample,
+//             film.h:26-45), claim a new camera sample (RadianceIntegrator::Compute +
+//             ThinLenCamera::GenRay, integrator.cpp:152-158, camera.cpp:31-41) and append
+//             the slot to the next active queue.
+//   k_swap    one thread: the next queue becomes the active one; decides whether the loop
+//             goes on (host loop, or the condition of a graph while-node).
 //   k_trace   closest hit of every active ray (BVH::Intersect, bvh.cpp:669-709).
-//   k_shade   medium sampling, surface/medium events, next-event estimation (queues a
-//             shadow ray), BSDF/phase sampling and Russian roulette.
+//   k_shade   medium sampling, surface/medium events, next-event estimation (a shadow ray
+//             queued for k_shadow, or traced in place), BSDF/phase sampling, Russian
+//             roulette; appends each slot to the next queue or to the finished list.
 //   k_shadow  occlusion and transmittance of the queued shadow rays
 //             (RayIntegrator::IntersectTr, integrator.cpp:68-87), added to the path.
+// Queues are compacted with warp-aggregated atomics.  Every kernel is grid-stride, so a
+// fixed (persistent) grid serves any queue length; that is what a graph captures.
+//
+// Several render requests can share one wavefront (pg_render_batch): each slot carries
+// its request, whose scene, film region, sample range and seed it uses.
 #pragma once
 
 #include "pg_shade.cuh"
@@ -21,39 +31,56 @@ enum StatIndex {
     kStatRays = 0, kStatSteps, kStatDropped, kStatPaths,
     kStatShadeItems, kStatShadeSteps, kStatShadeBricks,
     kStatShadowItems, kStatShadowSteps, kStatShadowBricks,
-    kStatTraceItems, kStatRegenItems, kNumStats = 16
+    kStatTraceItems, kStatRegenItems, kStatIterations, kNumStats = 16
 };
 
 enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlotDead = 3 };
 
+// Counters in device memory (RenderParams::counts).
+enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
+                  kCntIter = 5, kNumCounts = 8 };
+
+struct RequestDev {
+    unsigned long long sample_begin;  // first global sample id of this request
+    uint32_t total;                   // samples = npix * spp
+    int npix, width, height;
+    unsigned long long film_base;     // first pixel of its film region
+    uint32_t key1;                    // seed word of its random streams
+    uint32_t key0_offset;             // sample_offset * npix (progressive passes)
+    int max_depth;
+};
+
 struct RenderParams {
     int slots;
-    int width, height;
-    int npix;
-    uint64_t total;        // samples to render
-    int sample_offset;     // first sample index (progressive passes)
-    uint32_t key1;         // seed word of the random streams
-    int max_depth;
-    int block;             // threads per block of the queue kernels
-    float4* ray_o;         // o.xyz, bsdfPdf
-    float4* ray_d;         // d.xyz, medium (int bits, -1 none)
-    float4* beta;          // beta.rgb, depth (int bits)
-    float4* L;             // L.rgb, rng dim (uint bits)
-    float4* hit;           // t, prim (int bits), u, v
-    uint32_t* sample;      // sample id within this render
+    int nreq;
+    unsigned long long total;    // samples over all requests
+    const RequestDev* reqs;
+    const SceneDev* scenes;      // one per request (batched renders)
+    int* slot_req;               // request of each slot (batched renders)
+    float4* ray_o;               // o.xyz, bsdfPdf
+    float4* ray_d;               // d.xyz, medium (int bits, -1 none)
+    float4* beta;                // beta.rgb, depth (int bits)
+    float4* L;                   // L.rgb, rng dim (uint bits)
+    float4* hit;                 // t, prim (int bits), u, v
+    uint32_t* sample;            // sample id within its request
     int* state;
-    int* active;
-    int* counts;           // [0] active, [1] shadow
-    float4* so;            // shadow: o.xyz, tmax
-    float4* sd;            // shadow: d.xyz, medium
-    float4* sc;            // shadow: unoccluded contribution rgb, slot
-    uint32_t* skey;        // shadow: random stream word
-    double* film_sum;      // npix * 3
-    double* film_sq;       // npix * 3
-    uint32_t* film_n;      // npix
+    int* lists;                  // two queues of `slots` entries, alternating by parity
+    int* finished;
+    int* counts;                 // CountIndex
+    float4* so;                  // shadow: o.xyz, tmax
+    float4* sd;                  // shadow: d.xyz, medium
+    float4* sc;                  // shadow: unoccluded contribution rgb, slot
+    uint32_t* skey;              // shadow: random stream word
+    float4* film_acc;            // per pixel: sum r, g, b, count (this call)
+    float4* film_acc2;           // per pixel: sum of squares r, g, b (this call)
     unsigned long long* next_sample;
-    unsigned long long* stats;  // kStat* counters
+    unsigned long long* stats;   // StatIndex
+    uint32_t* req_done;          // completed paths per request
+    unsigned long long* req_time;  // globaltimer (ns) at each request's completion
     uint32_t* err;
+    int max_iter;
+    int use_cond;                // k_swap sets the graph while-condition
+    cudaGraphConditionalHandle cond;
 };
 
 __device__ __forceinline__ int WarpAppend(int* counter, bool pred) {
@@ -82,6 +109,49 @@ __device__ __forceinline__ bool Finite(V3 c) {
     return isfinite(c.x) && isfinite(c.y) && isfinite(c.z);
 }
 
+// red.global.add.v4.f32 (sm_90+): one 16-byte atomic add of four floats.
+__device__ __forceinline__ void RedAdd4(float4* p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
+                 "f"(d)
+                 : "memory");
+}
+
+// Adds a call's float film into the FP64 film (sum, sum of squares, count).
+__global__ void k_fold(const float4* acc, const float4* acc2, size_t npix, double* sum, double* sq,
+                       uint32_t* n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float4 a = acc[i], b = acc2[i];
+        sum[3 * i] += a.x, sum[3 * i + 1] += a.y, sum[3 * i + 2] += a.z;
+        sq[3 * i] += b.x, sq[3 * i + 1] += b.y, sq[3 * i + 2] += b.z;
+        n[i] += (uint32_t)a.w;
+    }
+}
+
+__device__ __forceinline__ unsigned long long GlobalTimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int* ActiveList(const RenderParams& P) {
+    return P.lists + (size_t)(P.counts[kCntParity] & 1) * P.slots;
+}
+__device__ __forceinline__ int* NextList(const RenderParams& P) {
+    return P.lists + (size_t)((P.counts[kCntParity] + 1) & 1) * P.slots;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ const SceneDev& SceneOf(const RenderParams& P, const SceneDev& S0, int slot) {
+    if (MULTI)
+        return P.scenes[P.slot_req[slot]];
+    return S0;
+}
+template <bool MULTI>
+__device__ __forceinline__ const RequestDev& RequestOf(const RenderParams& P, int slot) {
+    return P.reqs[MULTI ? P.slot_req[slot] : 0];
+}
+
 template <int M>
 __device__ void CameraRay(const CameraDev& cam, float fx, float fy, float l0, float l1, V3& o,
                           V3& d) {
@@ -99,88 +169,140 @@ __device__ void CameraRay(const CameraDev& cam, float fx, float fy, float l0, fl
     d = Linear(m, Normalize<M>(focus - lens));
 }
 
-template <int M>
-__global__ void k_regen(RenderParams P, SceneDev S) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.slots)
-        return;
-    int st = P.state[i];
-    uint32_t dropped = 0, done = 0;
-    if (st == kSlotFinished) {
-        float4 L = P.L[i];
-        V3 c = v3(L.x, L.y, L.z);
-        uint32_t id = P.sample[i];
-        int pix = (int)(id % (uint32_t)P.npix);
-        if (Finite(c)) {
-            atomicAdd(&P.film_sum[3 * pix + 0], (double)c.x);
-            atomicAdd(&P.film_sum[3 * pix + 1], (double)c.y);
-            atomicAdd(&P.film_sum[3 * pix + 2], (double)c.z);
-            atomicAdd(&P.film_sq[3 * pix + 0], (double)c.x * c.x);
-            atomicAdd(&P.film_sq[3 * pix + 1], (double)c.y * c.y);
-            atomicAdd(&P.film_sq[3 * pix + 2], (double)c.z * c.z);
-            atomicAdd(&P.film_n[pix], 1u);
-        } else {
-            dropped = 1;
-        }
-        done = 1;
-        st = kSlotEmpty;
+__device__ __forceinline__ int FindRequest(const RenderParams& P, unsigned long long id) {
+    int lo = 0, hi = P.nreq - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (P.reqs[mid].sample_begin <= id)
+            lo = mid;
+        else
+            hi = mid - 1;
     }
-    if (st == kSlotEmpty) {
-        unsigned mask = __activemask();
-        unsigned want = __ballot_sync(mask, true);
-        int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
-        unsigned long long base = 0;
-        if (lane == leader)
-            base = atomicAdd(P.next_sample, (unsigned long long)__popc(want));
-        base = __shfl_sync(want, base, leader);
-        unsigned long long id = base + __popc(want & ((1u << lane) - 1u));
-        if (id < P.total) {
-            uint32_t sid = (uint32_t)id;
-            int pix = (int)(sid % (uint32_t)P.npix);
-            int px = pix % P.width, py = pix / P.width;
-            uint32_t key0 = sid + (uint32_t)P.sample_offset * (uint32_t)P.npix;
-            Rng rng{key0, P.key1, 0};
-            float u0, u1, l0, l1;
-            rng.Get2D(u0, u1);
-            rng.Get2D(l0, l1);
-            V3 o, d;
-            CameraRay<M>(S.cam, (px + u0) / (float)P.width, (py + u1) / (float)P.height, l0, l1, o, d);
-            P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
-            P.ray_d[i] = make_float4(d.x, d.y, d.z, __int_as_float(S.cam.medium));
-            P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
-            P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng.dim));
-            P.sample[i] = key0;
-            st = kSlotActive;
-        } else {
-            st = kSlotDead;
-        }
-    }
-    P.state[i] = st;
-    int slot = WarpAppend(&P.counts[0], st == kSlotActive);
-    if (slot >= 0)
-        P.active[slot] = i;
-    WarpAdd(&P.stats[kStatPaths], (uint32_t)done);
-    WarpAdd(&P.stats[kStatDropped], (uint32_t)dropped);
-    WarpAdd(&P.stats[kStatRegenItems], 1u);
+    return lo;
 }
 
-__global__ void k_trace(RenderParams P, SceneDev S) {
+template <int M, bool MULTI>
+__global__ void k_regen(RenderParams P, SceneDev S0) {
+    const int n = P.counts[kCntFinished];
+    int* next = NextList(P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
+         q += gridDim.x * blockDim.x) {
+        bool live = q < n;
+        int i = live ? P.finished[q] : 0;
+        int st = live ? P.state[i] : kSlotDead;
+        uint32_t dropped = 0, done = 0;
+        if (live && st == kSlotFinished) {
+            const RequestDev& R = RequestOf<MULTI>(P, i);
+            float4 L = P.L[i];
+            V3 c = v3(L.x, L.y, L.z);
+            uint32_t sid = P.sample[i] - R.key0_offset;
+            size_t pix = (size_t)R.film_base + sid % (uint32_t)R.npix;
+            if (Finite(c)) {
+                // Two 16-byte vector reductions per sample into this call's float film,
+                // folded into the FP64 film once the call's paths are done (k_fold).
+                RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
+                RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
+            } else {
+                dropped = 1;
+            }
+            if (MULTI) {
+                int r = P.slot_req[i];
+                if (atomicAdd(&P.req_done[r], 1u) + 1u == R.total)
+                    P.req_time[r] = GlobalTimer();
+            }
+            done = 1;
+            st = kSlotEmpty;
+        }
+        bool claim = live && st == kSlotEmpty;
+        unsigned mask = __ballot_sync(__activemask(), claim);
+        if (claim) {
+            int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+            unsigned long long base = 0;
+            if (lane == leader)
+                base = atomicAdd(P.next_sample, (unsigned long long)__popc(mask));
+            base = __shfl_sync(mask, base, leader);
+            unsigned long long id = base + __popc(mask & ((1u << lane) - 1u));
+            if (id < P.total) {
+                int r = MULTI ? FindRequest(P, id) : 0;
+                const RequestDev& R = P.reqs[r];
+                if (MULTI)
+                    P.slot_req[i] = r;
+                const SceneDev& S = MULTI ? P.scenes[r] : S0;
+                uint32_t sid = (uint32_t)(id - R.sample_begin);
+                int pix = (int)(sid % (uint32_t)R.npix);
+                int px = pix % R.width, py = pix / R.width;
+                uint32_t key0 = sid + R.key0_offset;
+                Rng rng{key0, R.key1, 0};
+                float u0, u1, l0, l1;
+                rng.Get2D(u0, u1);
+                rng.Get2D(l0, l1);
+                V3 o, d;
+                CameraRay<M>(S.cam, (px + u0) / (float)R.width, (py + u1) / (float)R.height, l0, l1,
+                             o, d);
+                P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+                P.ray_d[i] = make_float4(d.x, d.y, d.z, __int_as_float(S.cam.medium));
+                P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
+                P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng.dim));
+                P.sample[i] = key0;
+                st = kSlotActive;
+            } else {
+                st = kSlotDead;
+            }
+        }
+        if (live)
+            P.state[i] = st;
+        int slot = WarpAppend(&P.counts[kCntNext], live && st == kSlotActive);
+        if (slot >= 0)
+            next[slot] = i;
+        WarpAdd(&P.stats[kStatPaths], done);
+        WarpAdd(&P.stats[kStatDropped], dropped);
+        WarpAdd(&P.stats[kStatRegenItems], live ? 1u : 0u);
+    }
+}
+
+// Makes the next queue the active one and decides whether the loop continues.
+__global__ void k_swap(RenderParams P) {
+    int* c = P.counts;
+    int active = c[kCntNext];
+    c[kCntActive] = active;
+    c[kCntNext] = 0;
+    c[kCntFinished] = 0;
+    c[kCntShadow] = 0;
+    c[kCntParity] ^= 1;
+    int it = ++c[kCntIter];
+    bool more = active > 0;
+    if (it > P.max_iter) {
+        atomicOr(P.err, kErrLoopCap);
+        more = false;
+        c[kCntActive] = 0;
+    }
+    P.stats[kStatIterations] = it;
+    if (P.use_cond)
+        cudaGraphSetConditional(P.cond, more ? 1u : 0u);
+}
+
+template <bool MULTI>
+__global__ void k_trace(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.counts[0];
-    if (q >= n)
-        return;
-    int i = P.active[q];
-    float4 ro = P.ray_o[i], rd = P.ray_d[i];
-    Hit h;
-    uint32_t err = 0;
-    Traverse<false>(S, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), 0.0f, kFloatMax, h,
-                    stack + threadIdx.x, blockDim.x, err);
-    P.hit[i] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
-    if (err)
-        atomicOr(P.err, err);
-    WarpAdd(&P.stats[kStatRays], 1u);
-    WarpAdd(&P.stats[kStatTraceItems], 1u);
+    const int n = P.counts[kCntActive];
+    const int* active = ActiveList(P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
+         q += gridDim.x * blockDim.x) {
+        if (q < n) {
+            int i = active[q];
+            const SceneDev& S = SceneOf<MULTI>(P, S0, i);
+            float4 ro = P.ray_o[i], rd = P.ray_d[i];
+            Hit h;
+            uint32_t err = 0;
+            Traverse<false>(S, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), 0.0f, kFloatMax, h,
+                            stack + threadIdx.x, blockDim.x, err);
+            P.hit[i] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+            if (err)
+                atomicOr(P.err, err);
+        }
+        WarpAdd(&P.stats[kStatRays], q < n ? 1u : 0u);
+        WarpAdd(&P.stats[kStatTraceItems], q < n ? 1u : 0u);
+    }
 }
 
 struct SurfaceInfo {
@@ -226,13 +348,66 @@ __device__ void Surface(const SceneDev& S, V3 o, V3 d, float4 h, SurfaceInfo& si
     }
 }
 
-// Next-event estimation (RayIntegrator::EstimateDirect, integrator.cpp:88-119): picks a
-// light, samples it, evaluates the BSDF (surface) or phase function (medium) and queues a
-// shadow ray carrying the unoccluded contribution beta * f * w * Le / pdf.
+// Transmittance of a shadow ray (RayIntegrator::IntersectTr, integrator.cpp:68-87):
+// zero if a surface with a material blocks it, otherwise the product of the media's
+// transmittances along the segments between null surfaces.
 template <int M>
-__device__ void QueueNEE(const RenderParams& P, const SceneDev& S, int slot, Rng& rng, V3 p,
-                         V3 n, V3 wiWorld, bool surface, const MaterialDev* mat,
-                         const Frame<M>* frame, float g, int medIn, int medOut, V3 beta) {
+__device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, Rng& rng,
+                       uint2* stack, int stride, uint32_t& steps, uint32_t& bricks, uint32_t& err,
+                       int& traced) {
+    V3 tr = v3(1.0f);
+    traced = 1;
+    bool surfaces = S.has_bvh || S.num_planes;
+    if (!S.has_null_surfaces) {
+        Hit h;
+        if (surfaces && Traverse<true>(S, o, d, 0.0f, tmax, h, stack, stride, err))
+            return v3(0.0f);
+        if (medium >= 0)
+            MediumTr<M>(S.media[medium], o, d, tmax, rng, steps, bricks, err, tr);
+        return tr;
+    }
+    V3 p2 = o + tmax * d;
+    for (int k = 0; k < 64; k++) {
+        Hit h;
+        bool hitS = Traverse<false>(S, o, d, 0.0f, tmax, h, stack, stride, err);
+        if (medium >= 0) {
+            V3 t3;
+            MediumTr<M>(S.media[medium], o, d, hitS ? h.t : tmax, rng, steps, bricks, err, t3);
+            tr *= t3;
+        }
+        if (!hitS)
+            break;
+        SurfaceInfo si;
+        Surface<M>(S, o, d, make_float4(h.t, __int_as_float(h.prim), h.u, h.v), si);
+        const ShapeDev& sh = S.shapes[si.shape];
+        if (sh.material >= 0)
+            return v3(0.0f);
+        int medIn = sh.med_in, medOut = sh.med_out;
+        if (medIn == medOut)
+            medIn = medOut = medium;
+        float dist;
+        d = Normalize<M>(p2 - si.p, dist);  // Interaction::SpawnRayTo (interaction.h:27-36)
+        o = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, d));
+        tmax = dist * (1.0f - 1e-3f);
+        medium = Dot(d, si.n) > 0 ? medOut : medIn;
+        traced++;
+    }
+    return tr;
+}
+
+struct ShadeCounters {
+    uint32_t steps = 0, bricks = 0, err = 0, shadowSteps = 0, shadowBricks = 0, shadowRays = 0;
+};
+
+// Next-event estimation (RayIntegrator::EstimateDirect, integrator.cpp:88-119): picks a
+// light, samples it, evaluates the BSDF (surface) or phase function (medium) and either
+// queues a shadow ray carrying the unoccluded contribution beta * f * w * Le / pdf for
+// k_shadow or, with FUSED, traces it here and adds the result to L.
+template <int M, bool FUSED>
+__device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, uint32_t key1, Rng& rng,
+                          V3 p, V3 n, V3 wiWorld, bool surface, const MaterialDev* mat,
+                          const Frame<M>* frame, float g, int medIn, int medOut, V3 beta, V3& L,
+                          uint2* stack, ShadeCounters& ct) {
     float lightPdf;
     int li = PickLight(S, rng.Get1D(), lightPdf);
     float u0, u1;
@@ -266,11 +441,22 @@ __device__ void QueueNEE(const RenderParams& P, const SceneDev& S, int slot, Rng
     // Interaction::SpawnRay(wo, distance) (interaction.h:37-44).
     V3 o = OffsetRayOrigin(p, FaceSameHemisphere(n, ls.wo));
     int med = Dot(ls.wo, n) > 0 ? medOut : medIn;
-    int q = atomicAdd(&P.counts[1], 1);
-    P.so[q] = make_float4(o.x, o.y, o.z, ls.distance * (1.0f - 1e-3f));
+    float tmax = ls.distance * (1.0f - 1e-3f);
+    uint32_t key = PcgHash(rng.dim ^ 0x68bc21ebu) ^ key1;
+    if (FUSED) {
+        Rng srng{P.sample[slot], key, 0};
+        int traced;
+        V3 tr = ShadowTr<M>(S, o, ls.wo, tmax, med, srng, stack, blockDim.x, ct.shadowSteps,
+                            ct.shadowBricks, ct.err, traced);
+        L += c * tr;
+        ct.shadowRays += traced;
+        return;
+    }
+    int q = atomicAdd(&P.counts[kCntShadow], 1);
+    P.so[q] = make_float4(o.x, o.y, o.z, tmax);
     P.sd[q] = make_float4(ls.wo.x, ls.wo.y, ls.wo.z, __int_as_float(med));
     P.sc[q] = make_float4(c.x, c.y, c.z, __int_as_float(slot));
-    P.skey[q] = PcgHash(rng.dim ^ 0x68bc21ebu) ^ P.key1;
+    P.skey[q] = key;
 }
 
 // Environment radiance for an escaped ray and its MIS light pdf (path.cpp:29-40).
@@ -288,13 +474,9 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
     return c;
 }
 
-template <int M>
-__global__ void k_shade(RenderParams P, SceneDev S) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.counts[0];
-    if (q >= n)
-        return;
-    int i = P.active[q];
+template <int M, bool FUSED>
+__device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
+                         uint2* stack, ShadeCounters& ct, bool& finished) {
     float4 ro = P.ray_o[i], rd = P.ray_d[i], bt = P.beta[i], Lw = P.L[i];
     // Scenes without surfaces skip k_trace: every ray misses.
     float4 h = (S.has_bvh || S.num_planes) ? P.hit[i]
@@ -304,29 +486,29 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
     int medium = __float_as_int(rd.w);
     V3 beta = v3(bt.x, bt.y, bt.z), L = v3(Lw.x, Lw.y, Lw.z);
     int depth = __float_as_int(bt.w);
-    Rng rng{P.sample[i], P.key1, __float_as_uint(Lw.w)};
-    uint32_t err = 0, steps = 0, bricks = 0;
+    const int maxDepth = R.max_depth;
+    Rng rng{P.sample[i], R.key1, __float_as_uint(Lw.w)};
     int prim = __float_as_int(h.y);
     bool found = prim != -1;
     float tHit = found ? h.x : kFloatMax;
-    bool finished = false;
+    finished = false;
     V3 no = o, nd = d;
     int nmed = medium;
 
     MediumEvent ev;
     ev.scattered = false;
     if (medium >= 0) {
-        MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, steps, bricks, err);
+        MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, ct.steps, ct.bricks, ct.err);
         beta *= ev.weight;
     }
     if (ev.scattered) {
         // Medium interaction (path.cpp:19-27).
-        if (depth + 1 == P.max_depth) {
+        if (depth + 1 == maxDepth) {
             finished = true;
         } else {
             const MediumDev& m = S.media[medium];
-            QueueNEE<M>(P, S, i, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr, m.g, medium,
-                        medium, beta);
+            NextEvent<M, FUSED>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
+                                m.g, medium, medium, beta, L, stack, ct);
             float u0, u1;
             rng.Get2D(u0, u1);
             V3 wo;
@@ -352,9 +534,8 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
         Surface<M>(S, o, d, h, si);
         const ShapeDev& sh = S.shapes[si.shape];
         int medIn = sh.med_in, medOut = sh.med_out;
-        if (medIn == medOut) {
+        if (medIn == medOut)
             medIn = medOut = medium;  // no transition: the ray's medium (bvh.cpp:701-707)
-        }
         if (sh.material < 0) {
             // Null surface: continue through without counting a bounce (path.cpp:42-46).
             no = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, d));
@@ -372,13 +553,13 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
                     L += beta * le * PowerHeuristic(bsdfPdf, lightPdf);
                 }
                 finished = true;
-            } else if (depth + 1 == P.max_depth) {
+            } else if (depth + 1 == maxDepth) {
                 finished = true;
             } else {
                 Frame<M> fr;
                 fr.From(si.n);
-                QueueNEE<M>(P, S, i, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f, medIn, medOut,
-                            beta);
+                NextEvent<M, FUSED>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
+                                    medIn, medOut, beta, L, stack, ct);
                 float u1 = rng.Get1D(), u20, u21;
                 rng.Get2D(u20, u21);
                 BsdfSample bs;
@@ -417,99 +598,85 @@ __global__ void k_shade(RenderParams P, SceneDev S) {
         P.ray_d[i] = make_float4(nd.x, nd.y, nd.z, __int_as_float(nmed));
         P.beta[i] = make_float4(beta.x, beta.y, beta.z, __int_as_float(depth));
     }
-    if (err)
-        atomicOr(P.err, err);
-    WarpAdd(&P.stats[kStatSteps], steps);
-    WarpAdd(&P.stats[kStatShadeSteps], steps);
-    WarpAdd(&P.stats[kStatShadeBricks], bricks);
-    WarpAdd(&P.stats[kStatShadeItems], 1u);
 }
 
-template <int M>
-__global__ void k_shadow(RenderParams P, SceneDev S) {
+template <int M, bool MULTI, bool FUSED>
+__global__ void k_shade(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = P.counts[1];
-    if (q >= n)
-        return;
-    float4 so = P.so[q], sd = P.sd[q], sc = P.sc[q];
-    int slot = __float_as_int(sc.w);
-    V3 o = v3(so.x, so.y, so.z), d = v3(sd.x, sd.y, sd.z);
-    float tmax = so.w;
-    int medium = __float_as_int(sd.w);
-    Rng rng{P.sample[slot], P.skey[q], 0};
-    uint32_t err = 0, steps = 0, bricks = 0;
-    V3 tr = v3(1.0f);
-    int traced = 1;
-    if (!S.has_null_surfaces) {
-        Hit h;
-        if (Traverse<true>(S, o, d, 0.0f, tmax, h, stack + threadIdx.x, blockDim.x, err)) {
-            tr = v3(0.0f);
-        } else if (medium >= 0) {
-            V3 t3;
-            MediumTr<M>(S.media[medium], o, d, tmax, rng, steps, bricks, err, t3);
-            tr = t3;
-        }
-    } else {
-        // Closest-hit loop through null surfaces (integrator.cpp:68-87).
-        V3 p2 = o + tmax * d;
-        for (int k = 0; k < 64; k++) {
-            Hit h;
-            bool hitS = Traverse<false>(S, o, d, 0.0f, tmax, h, stack + threadIdx.x, blockDim.x, err);
-            if (medium >= 0) {
-                V3 t3;
-                MediumTr<M>(S.media[medium], o, d, hitS ? h.t : tmax, rng, steps, bricks, err, t3);
-                tr *= t3;
-            }
-            if (!hitS)
-                break;
-            SurfaceInfo si;
-            Surface<M>(S, o, d, make_float4(h.t, __int_as_float(h.prim), h.u, h.v), si);
-            const ShapeDev& sh = S.shapes[si.shape];
-            if (sh.material >= 0) {
-                tr = v3(0.0f);
-                break;
-            }
-            int medIn = sh.med_in, medOut = sh.med_out;
-            if (medIn == medOut)
-                medIn = medOut = medium;
-            float dist;
-            d = Normalize<M>(p2 - si.p, dist);  // Interaction::SpawnRayTo (interaction.h:27-36)
-            o = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, d));
-            tmax = dist * (1.0f - 1e-3f);
-            medium = Dot(d, si.n) > 0 ? medOut : medIn;
-            traced++;
-        }
+    const int n = P.counts[kCntActive];
+    const int* active = ActiveList(P);
+    int* next = NextList(P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
+         q += gridDim.x * blockDim.x) {
+        ShadeCounters ct;
+        bool live = q < n, finished = true;
+        int i = live ? active[q] : 0;
+        if (live)
+            ShadeOne<M, FUSED>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
+                               stack + threadIdx.x, ct, finished);
+        int a = WarpAppend(&P.counts[kCntNext], live && !finished);
+        if (a >= 0)
+            next[a] = i;
+        int f = WarpAppend(&P.counts[kCntFinished], live && finished);
+        if (f >= 0)
+            P.finished[f] = i;
+        if (ct.err)
+            atomicOr(P.err, ct.err);
+        WarpAdd(&P.stats[kStatSteps], ct.steps + ct.shadowSteps);
+        WarpAdd(&P.stats[kStatShadeSteps], ct.steps + ct.shadowSteps);
+        WarpAdd(&P.stats[kStatShadeBricks], ct.bricks + ct.shadowBricks);
+        WarpAdd(&P.stats[kStatShadeItems], live ? 1u : 0u);
+        WarpAdd(&P.stats[kStatRays], ct.shadowRays);
     }
-    if (!IsBlack(tr)) {
-        float4 Lw = P.L[slot];
-        P.L[slot] = make_float4(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z, Lw.w);
-    }
-    if (err)
-        atomicOr(P.err, err);
-    WarpAdd(&P.stats[kStatRays], (uint32_t)traced);
-    WarpAdd(&P.stats[kStatSteps], steps);
-    WarpAdd(&P.stats[kStatShadowSteps], steps);
-    WarpAdd(&P.stats[kStatShadowBricks], bricks);
-    WarpAdd(&P.stats[kStatShadowItems], 1u);
 }
 
-// Brick majorants: the largest density over voxels [8b, 8b+8] of each axis (the
-// trilinear footprint of points inside brick b), one thread per brick.
-__global__ void k_majorant(const float* dens, int sx, int sy, int sz, int nbx, int nby, int nbz,
-                           float* maj) {
-    int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= (int64_t)nbx * nby * nbz)
+template <int M, bool MULTI>
+__global__ void k_shadow(RenderParams P, SceneDev S0) {
+    extern __shared__ uint2 stack[];
+    const int n = P.counts[kCntShadow];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
+         q += gridDim.x * blockDim.x) {
+        uint32_t err = 0, steps = 0, bricks = 0;
+        int traced = 0;
+        if (q < n) {
+            float4 so = P.so[q], sd = P.sd[q], sc = P.sc[q];
+            int slot = __float_as_int(sc.w);
+            const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
+            Rng rng{P.sample[slot], P.skey[q], 0};
+            V3 tr = ShadowTr<M>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
+                                __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x, steps,
+                                bricks, err, traced);
+            if (!IsBlack(tr)) {
+                float4 Lw = P.L[slot];
+                P.L[slot] = make_float4(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z, Lw.w);
+            }
+            if (err)
+                atomicOr(P.err, err);
+        }
+        WarpAdd(&P.stats[kStatRays], (uint32_t)traced);
+        WarpAdd(&P.stats[kStatSteps], steps);
+        WarpAdd(&P.stats[kStatShadowSteps], steps);
+        WarpAdd(&P.stats[kStatShadowBricks], bricks);
+        WarpAdd(&P.stats[kStatShadowItems], q < n ? 1u : 0u);
+    }
+}
+
+// Brick majorants: the largest density over voxels [b*k, b*k + b] of each axis (the
+// trilinear footprint of points inside brick k of edge b voxels), one thread per brick.
+__global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int nbx, int nby,
+                           int nbz, float* maj) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)nbx * nby * nbz)
         return;
-    int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+    int bx = (int)(k % nbx), by = (int)((k / nbx) % nby), bz = (int)(k / ((int64_t)nbx * nby));
     float m = 0.0f;
-    for (int z = 8 * bz; z <= min(8 * bz + 8, sz - 1); z++)
-        for (int y = 8 * by; y <= min(8 * by + 8, sy - 1); y++) {
+    for (int z = b * bz; z <= min(b * bz + b, sz - 1); z++)
+        for (int y = b * by; y <= min(b * by + b, sy - 1); y++) {
             const float* row = dens + (size_t)z * sx * sy + (size_t)y * sx;
-            for (int x = 8 * bx; x <= min(8 * bx + 8, sx - 1); x++)
+            for (int x = b * bx; x <= min(b * bx + b, sx - 1); x++)
                 m = fmaxf(m, __ldg(&row[x]));
         }
-    maj[b] = m;
+    maj[k] = m;
 }
 
 // pg_intersect: closest hit per ray with pine's shape index and triangle index.

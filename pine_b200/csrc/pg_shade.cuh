@@ -145,7 +145,7 @@ struct TrowbridgeReitz {  // scattering.h:91-145, isotropic alpha
         V3 T2 = Cross(wh, T1);
         float px, py;
         SampleDiskPolar<M>(u0, u1, px, py);
-        float h = PMath<M>::sqrt(1.0f - Sqr(px));
+        float h = PMath<M>::sqrt(Max(1.0f - Sqr(px), 0.0f));
         float t = (1.0f + wh.z) / 2;
         py = h * (1 - t) + py * t;  // pstd::lerp(t, h, py)
         float pz = PMath<M>::sqrt(Max(0.0f, 1.0f - (px * px + py * py)));
@@ -348,8 +348,11 @@ __device__ __forceinline__ float PhaseSample(float g, V3 wi, V3& wo, float u0, f
         float sq = (1.0f - g * g) / (1 + g - 2 * g * u0);
         cosT = -(1.0f + g * g - sq * sq) / (2.0f * g);
     }
-    float s2 = 1.0f - cosT * cosT;
-    float sinT = PMath<M>::sqrt(M == kPine ? s2 : Max(s2, 0.0f));
+    // 1 - cos^2 can round below zero; pine's Newton sqrt (math.h:142-151) then reaches
+    // x = 0 at -2^-22 and diverges to -inf, giving a NaN direction that its uncapped
+    // delta-tracking loop (medium.cpp:104-116) never leaves.  Clamped at 0 here.
+    float s2 = Max(1.0f - cosT * cosT, 0.0f);
+    float sinT = PMath<M>::sqrt(s2);
     float phi = 2 * kPi * u1;
     Frame<M> f;
     f.From(wi);
@@ -475,6 +478,13 @@ __device__ __forceinline__ V3 Linear(const float* m, V3 d) {
               m[8] * d.x + m[9] * d.y + m[10] * d.z);
 }
 
+// A ray with a non-finite origin or direction (only reachable through a NaN upstream)
+// is treated as missing the grid instead of walking it without end.
+__device__ __forceinline__ bool FiniteRay(V3 o, V3 d) {
+    return isfinite(o.x) && isfinite(o.y) && isfinite(o.z) && isfinite(d.x) && isfinite(d.y) &&
+           isfinite(d.z);
+}
+
 // AABB::Hit(Ray, tmin&, tmax&) against the unit cube (geometry.cpp:67-87).
 __device__ __forceinline__ bool UnitBoxHit(V3 o, V3 d, float& tmin, float& tmax) {
     if (tmin > tmax)
@@ -518,31 +528,32 @@ __device__ __forceinline__ float GridDensity(const MediumDev& m, float vx, float
            fx * (gy * (gz * d100 + fz * d101) + fy * (gz * d110 + fz * d111));
 }
 
-// Walks the 8^3-voxel bricks crossed by the medium-space ray o + t d, t in [t0, t1], in
-// order (3D DDA), calling f(tEnter, tExit, majorant) for bricks whose majorant is > 0.
-// f returns true to stop the walk.
+// Walks the majorant bricks (m.bsize^3 voxels each) crossed by the medium-space ray
+// o + t d, t in [t0, t1], in order (3D DDA), calling f(tEnter, tExit, majorant) for bricks
+// whose majorant is > 0.  f returns true to stop the walk.
 template <typename F>
 __device__ __forceinline__ void WalkBricks(const MediumDev& m, V3 o, V3 d, float t0, float t1,
                                            uint32_t& bricks, F&& f) {
-    // Voxel-index space: v = (o + t d) * size; bricks are 8 voxels wide.
+    // Voxel-index space: v = (o + t d) * size; bricks are bsize voxels wide.
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     V3 vo = v3(o.x * sx, o.y * sy, o.z * sz), vd = v3(d.x * sx, d.y * sy, d.z * sz);
     float px = vo.x + t0 * vd.x, py = vo.y + t0 * vd.y, pz = vo.z + t0 * vd.z;
-    int bx = min(max((int)floorf(px * 0.125f), 0), m.nb[0] - 1);
-    int by = min(max((int)floorf(py * 0.125f), 0), m.nb[1] - 1);
-    int bz = min(max((int)floorf(pz * 0.125f), 0), m.nb[2] - 1);
+    const float inb = m.inv_bsize, bs = (float)m.bsize;
+    int bx = min(max((int)floorf(px * inb), 0), m.nb[0] - 1);
+    int by = min(max((int)floorf(py * inb), 0), m.nb[1] - 1);
+    int bz = min(max((int)floorf(pz * inb), 0), m.nb[2] - 1);
     int stx = vd.x > 0.0f ? 1 : -1, sty = vd.y > 0.0f ? 1 : -1, stz = vd.z > 0.0f ? 1 : -1;
     float inx = vd.x != 0.0f ? 1.0f / vd.x : 0.0f, iny = vd.y != 0.0f ? 1.0f / vd.y : 0.0f,
           inz = vd.z != 0.0f ? 1.0f / vd.z : 0.0f;
     auto nextT = [&](int b, int st, float vo_, float in) {
         if (in == 0.0f)
             return kFloatMax;
-        float plane = (float)((b + (st > 0 ? 1 : 0)) * 8);
+        float plane = (float)(b + (st > 0 ? 1 : 0)) * bs;
         return (plane - vo_) * in;
     };
     float tx = nextT(bx, stx, vo.x, inx), ty = nextT(by, sty, vo.y, iny), tz = nextT(bz, stz, vo.z, inz);
-    float dtx = inx != 0.0f ? 8.0f * Fabs(inx) : kFloatMax, dty = iny != 0.0f ? 8.0f * Fabs(iny) : kFloatMax,
-          dtz = inz != 0.0f ? 8.0f * Fabs(inz) : kFloatMax;
+    float dtx = inx != 0.0f ? bs * Fabs(inx) : kFloatMax, dty = iny != 0.0f ? bs * Fabs(iny) : kFloatMax,
+          dtz = inz != 0.0f ? bs * Fabs(inz) : kFloatMax;
     float t = t0;
     const int maxSteps = m.nb[0] + m.nb[1] + m.nb[2] + 4;
     for (int i = 0; i < maxSteps && t < t1; i++) {
@@ -611,7 +622,7 @@ __device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rn
     V3 mo = Affine(m.w2m, o);
     V3 md = Normalize<M>(Linear(m.w2m, d));
     float t0 = 0.0f, t1 = tmax;
-    if (!UnitBoxHit(mo, md, t0, t1))
+    if (!FiniteRay(mo, md) || !UnitBoxHit(mo, md, t0, t1))
         return;
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     float ts = 0.0f;
@@ -660,7 +671,7 @@ __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng, 
     V3 mo = Affine(m.w2m, o);
     V3 md = Normalize<M>(Linear(m.w2m, d));
     float t0 = 0.0f, t1 = tmax;
-    if (!UnitBoxHit(mo, md, t0, t1))
+    if (!FiniteRay(mo, md) || !UnitBoxHit(mo, md, t0, t1))
         return 1.0f;
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     float tr = 1.0f;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -73,9 +74,13 @@ struct DevMem {
     ~DevMem() { Free(); }
 };
 
+// Majorant brick edges a grid medium is prepared for (selected by pg_tuning).
+constexpr int kBrickSizes[4] = {8, 16, 32, 64};
+
 struct DeviceScene {
     SceneDev dev{};
     DevMem mem;
+    const MediumDev* media_dev[4] = {nullptr, nullptr, nullptr, nullptr};  // per brick size
     int width = 0, height = 0, spp = 1, max_depth = 4;
     bool surfaces = false;
     int64_t prims = 0;
@@ -93,7 +98,7 @@ struct Pool {
     int slots = 0;
     float4 *ray_o = nullptr, *ray_d = nullptr, *beta = nullptr, *L = nullptr, *hit = nullptr;
     uint32_t* sample = nullptr;
-    int *state = nullptr, *active = nullptr;
+    int *state = nullptr, *lists = nullptr, *finished = nullptr, *slot_req = nullptr;
     float4 *so = nullptr, *sd = nullptr, *sc = nullptr;
     uint32_t* skey = nullptr;
     void Ensure(int n) {
@@ -108,7 +113,9 @@ struct Pool {
         hit = mem.Alloc<float4>(n);
         sample = mem.Alloc<uint32_t>(n);
         state = mem.Alloc<int>(n);
-        active = mem.Alloc<int>(n);
+        lists = mem.Alloc<int>(2 * (size_t)n);
+        finished = mem.Alloc<int>(n);
+        slot_req = mem.Alloc<int>(n);
         so = mem.Alloc<float4>(n);
         sd = mem.Alloc<float4>(n);
         sc = mem.Alloc<float4>(n);
@@ -119,16 +126,21 @@ struct Pool {
 struct Film {
     DevMem mem;
     int64_t npix = 0;
-    double *sum = nullptr, *sq = nullptr;
+    double *sum = nullptr, *sq = nullptr;  // accumulated over calls (progressive passes)
     uint32_t* n = nullptr;
+    float4 *acc = nullptr, *acc2 = nullptr;  // this call's samples, vector-atomic targets
     void Ensure(int64_t np) {
         if (np <= npix)
             return;
+        if (npix > 0)
+            throw Failure{PG_ERR_INVALID_ARG, "film grew while accumulating"};
         mem.Free();
         npix = np;
         sum = mem.Alloc<double>(np * 3);
         sq = mem.Alloc<double>(np * 3);
         n = mem.Alloc<uint32_t>(np);
+        acc = mem.Alloc<float4>(np);
+        acc2 = mem.Alloc<float4>(np);
     }
 };
 
@@ -142,14 +154,16 @@ struct pg_ctx {
     pg::Pool pool;
     pg::Film film;
     pg::DevMem small;
-    int* counts = nullptr;                 // [0] active, [1] shadow
+    int* counts = nullptr;                 // CountIndex
     unsigned long long* next_sample = nullptr;
     unsigned long long* stats = nullptr;   // kNumStats counters
     std::vector<cudaEvent_t> events;       // profiling events, reused
     uint32_t* err = nullptr;
     int* h_counts = nullptr;               // pinned
+    pg::DevMem req_buf;                    // per-call request table
     std::string last_error;
-    pg_tuning tuning{1 << 21, 128, 1};
+    pg_tuning tuning{1 << 21, 128, 1, 32};
+    int num_sms = 148;
 };
 
 namespace pg {
@@ -365,6 +379,8 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
 
     // Media.
     std::vector<MediumDev> media(d->num_media);
+    std::vector<std::array<const float*, 4>> majVariants(d->num_media);
+    std::vector<std::array<std::array<int, 3>, 4>> nbVariants(d->num_media);
     for (int i = 0; i < d->num_media; i++) {
         const pg_medium& m = d->media[i];
         MediumDev& o = media[i];
@@ -384,15 +400,21 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         float* dd = sc->mem.Alloc<float>(nvox);
         PG_CUDA(cudaMemcpyAsync(dd, m.density, nvox * 4, cudaMemcpyHostToDevice, st));
         o.density = dd;
-        // Brick majorants are built on the device from the uploaded grid.
-        for (int k = 0; k < 3; k++)
-            o.nb[k] = (m.size[k] + 7) / 8;
-        int64_t nbTot = (int64_t)o.nb[0] * o.nb[1] * o.nb[2];
-        float* maj = sc->mem.Alloc<float>(nbTot);
-        k_majorant<<<(unsigned)Ceil<int64_t>(nbTot, 256), 256, 0, st>>>(dd, m.size[0], m.size[1], m.size[2],
-                                                                      o.nb[0], o.nb[1], o.nb[2], maj);
-        PG_CUDA(cudaGetLastError());
-        o.majorant = maj;
+        // Brick majorants are built on the device from the uploaded grid, for each brick
+        // size a tuning may select; variant 0 is kept in `media`, the others below.
+        for (int v = 0; v < 4; v++) {
+            int b = kBrickSizes[v];
+            int nb[3];
+            for (int k = 0; k < 3; k++)
+                nb[k] = (m.size[k] + b - 1) / b;
+            int64_t nbTot = (int64_t)nb[0] * nb[1] * nb[2];
+            float* maj = sc->mem.Alloc<float>(nbTot);
+            k_majorant<<<(unsigned)Ceil<int64_t>(nbTot, 128), 128, 0, st>>>(
+                dd, m.size[0], m.size[1], m.size[2], b, nb[0], nb[1], nb[2], maj);
+            PG_CUDA(cudaGetLastError());
+            majVariants[i][v] = maj;
+            nbVariants[i][v] = {nb[0], nb[1], nb[2]};
+        }
         // w2m = Translate(0.5 - position) * Scale(1 / normalizedSize / scale) (medium.cpp:180-182).
         float mx = (float)std::max(m.size[0], std::max(m.size[1], m.size[2]));
         float s3[3];
@@ -542,7 +564,20 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     S.light_func_int = funcInt;
     S.uniform_lights = uniform ? 1 : 0;
     S.env_light = env;
-    S.media = sc->mem.Upload(media, st);
+    for (int v = 0; v < 4; v++) {
+        std::vector<MediumDev> mv = media;
+        for (int i = 0; i < d->num_media; i++) {
+            if (mv[i].type != PG_MEDIUM_GRID)
+                continue;
+            mv[i].majorant = majVariants[i][v];
+            for (int k = 0; k < 3; k++)
+                mv[i].nb[k] = nbVariants[i][v][k];
+            mv[i].bsize = kBrickSizes[v];
+            mv[i].inv_bsize = 1.0f / kBrickSizes[v];
+        }
+        sc->media_dev[v] = sc->mem.Upload(mv, st);
+    }
+    S.media = sc->media_dev[0];
     S.num_media = d->num_media;
     S.has_null_surfaces = nullSurfaces ? 1 : 0;
     PG_CUDA(cudaStreamSynchronize(st));
@@ -602,57 +637,274 @@ struct LaunchTimer {
     bool on;
     size_t used = 0;
     std::vector<std::pair<int, size_t>> marks;  // kernel, index of its start event
-    cudaEvent_t Next();
+    cudaEvent_t Next() {
+        if (used == ctx->events.size()) {
+            cudaEvent_t e;
+            PG_CUDA(cudaEventCreate(&e));
+            ctx->events.push_back(e);
+        }
+        return ctx->events[used++];
+    }
     template <typename F>
-    void Time(int kernel, F&& launch);
-    void Collect(RenderResult& r);
+    void Time(int kernel, F&& launch) {
+        if (!on) {
+            launch();
+            return;
+        }
+        size_t first = used;
+        PG_CUDA(cudaEventRecord(Next(), ctx->stream));
+        launch();
+        PG_CUDA(cudaEventRecord(Next(), ctx->stream));
+        marks.push_back({kernel, first});
+    }
+    void Collect(RenderResult& r) {
+        for (auto& m : marks) {
+            float ms = 0.0f;
+            PG_CUDA(cudaEventElapsedTime(&ms, ctx->events[m.second], ctx->events[m.second + 1]));
+            r.kernelSeconds[m.first] += ms * 1e-3;
+        }
+    }
 };
 
-cudaEvent_t LaunchTimer::Next() {
-    if (used == ctx->events.size()) {
-        cudaEvent_t e;
-        PG_CUDA(cudaEventCreate(&e));
-        ctx->events.push_back(e);
-    }
-    return ctx->events[used++];
+__global__ void k_iota(int* a, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        a[i] = i;
+}
+__global__ void k_timestamp(unsigned long long* t) {
+    *t = GlobalTimer();
 }
 
-template <typename F>
-void LaunchTimer::Time(int kernel, F&& launch) {
-    if (!on) {
-        launch();
-        return;
-    }
-    size_t first = used;
-    PG_CUDA(cudaEventRecord(Next(), ctx->stream));
-    launch();
-    PG_CUDA(cudaEventRecord(Next(), ctx->stream));
-    marks.push_back({kernel, first});
-}
+// One wavefront: its parameters, kernels and launch shapes.
+struct Wave {
+    RenderParams P{};
+    SceneDev S0{};
+    bool multi = false, surfaces = false, fused = false;
+    int mode = PG_MATH_FAST;
+    int shadeBlock = 128;
+    size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
+};
 
-void LaunchTimer::Collect(RenderResult& r) {
-    for (auto& m : marks) {
-        float ms = 0.0f;
-        PG_CUDA(cudaEventElapsedTime(&ms, ctx->events[m.second], ctx->events[m.second + 1]));
-        r.kernelSeconds[m.first] += ms * 1e-3;
-    }
-}
-
-template <int M>
-static void LaunchIteration(pg_ctx* ctx, LaunchTimer& timer, RenderResult& res,
-                            const RenderParams& P, const SceneDev& S, bool surfaces, int n) {
+template <int M, bool MULTI, bool FUSED>
+static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                       RenderResult* res) {
     cudaStream_t st = ctx->stream;
-    int tb = 128;
-    size_t smem = (size_t)tb * kStackSize * sizeof(uint2);
-    if (surfaces) {
-        timer.Time(PG_KERNEL_TRACE, [&]() { k_trace<<<Ceil(n, tb), tb, smem, st>>>(P, S); });
-        res.kernelLaunches[PG_KERNEL_TRACE]++;
+    const int sms = ctx->num_sms;
+    const int tb = 128;
+    auto grid = [&](int block, int perSm) {
+        int cap = sms * perSm;
+        return persistent ? cap : std::max(1, std::min(Ceil(n, block), cap * 8));
+    };
+    auto time = [&](int k, auto&& f) {
+        if (timer)
+            timer->Time(k, f);
+        else
+            f();
+        if (res)
+            res->kernelLaunches[k]++;
+    };
+    if (w.surfaces)
+        time(PG_KERNEL_TRACE, [&]() {
+            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+    const size_t shadeSmem = FUSED ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    if (FUSED && shadeSmem > 48 * 1024)
+        PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)shadeSmem));
+    time(PG_KERNEL_SHADE, [&]() {
+        k_shade<M, MULTI, FUSED><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
+    });
+    if (!FUSED)
+        time(PG_KERNEL_SHADOW, [&]() {
+            k_shadow<M, MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+}
+
+template <int M, bool MULTI>
+static void LaunchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
+    auto f = [&]() {
+        k_regen<M, MULTI><<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(w.P, w.S0);
+        k_swap<<<1, 1, 0, ctx->stream>>>(w.P);
+    };
+    if (timer)
+        timer->Time(PG_KERNEL_REGEN, f);
+    else
+        f();
+    if (res)
+        res->kernelLaunches[PG_KERNEL_REGEN]++;
+}
+
+template <int M, bool MULTI>
+static void Body(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer, RenderResult* res) {
+    if (w.fused)
+        LaunchBody<M, MULTI, true>(ctx, w, n, persistent, timer, res);
+    else
+        LaunchBody<M, MULTI, false>(ctx, w, n, persistent, timer, res);
+}
+
+static void DispatchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
+    if (w.mode == PG_MATH_PINE)
+        w.multi ? LaunchRegen<kPine, true>(ctx, w, timer, res) : LaunchRegen<kPine, false>(ctx, w, timer, res);
+    else
+        w.multi ? LaunchRegen<kFast, true>(ctx, w, timer, res) : LaunchRegen<kFast, false>(ctx, w, timer, res);
+}
+
+static void DispatchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                         RenderResult* res) {
+    if (w.mode == PG_MATH_PINE)
+        w.multi ? Body<kPine, true>(ctx, w, n, persistent, timer, res)
+                : Body<kPine, false>(ctx, w, n, persistent, timer, res);
+    else
+        w.multi ? Body<kFast, true>(ctx, w, n, persistent, timer, res)
+                : Body<kFast, false>(ctx, w, n, persistent, timer, res);
+}
+
+// Fills the pool pointers of a wave and resets its queues: every slot starts empty and
+// listed as finished, so the first k_regen fills all of them.
+static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int maxIter) {
+    cudaStream_t st = ctx->stream;
+    ctx->pool.Ensure(slots);
+    Pool& pl = ctx->pool;
+    RenderParams& P = w.P;
+    P.slots = slots;
+    P.total = total;
+    P.ray_o = pl.ray_o, P.ray_d = pl.ray_d, P.beta = pl.beta, P.L = pl.L, P.hit = pl.hit;
+    P.sample = pl.sample, P.state = pl.state, P.lists = pl.lists, P.finished = pl.finished;
+    P.slot_req = pl.slot_req;
+    P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
+    P.counts = ctx->counts;
+    P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2;
+    P.next_sample = ctx->next_sample;
+    P.stats = ctx->stats;
+    P.err = ctx->err;
+    P.max_iter = maxIter;
+    PG_CUDA(cudaMemsetAsync(pl.state, 0, (size_t)slots * sizeof(int), st));
+    k_iota<<<ctx->num_sms * 4, 256, 0, st>>>(pl.finished, slots);
+    PG_CUDA(cudaGetLastError());
+    std::vector<int> c(kNumCounts, 0);
+    c[kCntFinished] = slots;
+    PG_CUDA(cudaMemcpyAsync(ctx->counts, c.data(), kNumCounts * sizeof(int), cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+}
+
+// Host-driven loop: the active count is read back after each k_swap so that every launch
+// is sized to its queue (and can be timed per kernel).
+static void RunHostLoop(pg_ctx* ctx, Wave& w, bool profile, RenderResult& res) {
+    cudaStream_t st = ctx->stream;
+    LaunchTimer timer{ctx, profile};
+    PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    for (int64_t iter = 0;; iter++) {
+        DispatchRegen(ctx, w, &timer, &res);
+        PG_CUDA(cudaMemcpyAsync(ctx->h_counts, ctx->counts, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PG_CUDA(cudaStreamSynchronize(st));
+        int n = ctx->h_counts[0];
+        if (n == 0)
+            break;
+        DispatchBody(ctx, w, n, false, &timer, &res);
+        PG_CUDA(cudaGetLastError());
     }
-    int sb = ctx->tuning.block_size > 0 ? ctx->tuning.block_size : 128;
-    timer.Time(PG_KERNEL_SHADE, [&]() { k_shade<M><<<Ceil(n, sb), sb, 0, st>>>(P, S); });
-    timer.Time(PG_KERNEL_SHADOW, [&]() { k_shadow<M><<<Ceil(n, tb), tb, smem, st>>>(P, S); });
-    res.kernelLaunches[PG_KERNEL_SHADE]++;
-    res.kernelLaunches[PG_KERNEL_SHADOW]++;
+    PG_CUDA(cudaStreamSynchronize(st));
+    timer.Collect(res);
+}
+
+// Device-driven loop: the whole render is one CUDA graph whose while-node repeats
+// regen/swap/trace/shade/shadow with persistent (fixed, grid-stride) launches until k_swap
+// finds the active queue empty or the iteration cap reached.
+static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res) {
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    PG_CUDA(cudaGraphCreate(&graph, 0));
+    struct Cleanup {
+        cudaGraph_t& g;
+        cudaGraphExec_t& e;
+        ~Cleanup() {
+            if (e)
+                cudaGraphExecDestroy(e);
+            if (g)
+                cudaGraphDestroy(g);
+        }
+    } cleanup{graph, exec};
+    cudaGraphConditionalHandle cond;
+    PG_CUDA(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    PG_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    w.P.use_cond = 1;
+    w.P.cond = cond;
+    PG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    DispatchRegen(ctx, w, nullptr, nullptr);
+    DispatchBody(ctx, w, w.P.slots, true, nullptr, nullptr);
+    cudaGraph_t captured = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(st, &captured);
+    if (ce != cudaSuccess)
+        throw Failure{PG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)};
+    PG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    PG_CUDA(cudaGraphLaunch(exec, st));
+    w.P.use_cond = 0;
+}
+
+// Ends the timed region (after the film fold) and collects counters and device errors.
+static void FinishWave(pg_ctx* ctx, RenderResult& res) {
+    PG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    PG_CUDA(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    res.seconds = ms * 1e-3;
+    PG_CUDA(cudaMemcpy(res.stats, ctx->stats, sizeof(res.stats), cudaMemcpyDeviceToHost));
+    res.launches = 0;
+    for (int k = 0; k < PG_NUM_KERNELS; k++)
+        res.launches += res.kernelLaunches[k];
+    uint32_t e = 0;
+    PG_CUDA(cudaMemcpy(&e, ctx->err, sizeof(e), cudaMemcpyDeviceToHost));
+    std::string msg;
+    if (pg_status s = DeviceErrorStatus(e, msg))
+        throw Failure{s, msg};
+}
+
+static int MediaVariant(const pg_tuning& t) {
+    return t.majorant_brick >= 64 ? 3 : (t.majorant_brick >= 32 ? 2 : (t.majorant_brick >= 16 ? 1 : 0));
+}
+
+// Ensures film storage for npix pixels; growing discards what it held.
+static void EnsureFilm(pg_ctx* ctx, int64_t npix) {
+    if (npix > ctx->film.npix) {
+        ctx->film.mem.Free();
+        ctx->film.npix = 0;
+    }
+    ctx->film.Ensure(npix);
+}
+
+static void ClearCallFilm(pg_ctx* ctx, int64_t npix) {
+    PG_CUDA(cudaMemsetAsync(ctx->film.acc, 0, npix * sizeof(float4), ctx->stream));
+    PG_CUDA(cudaMemsetAsync(ctx->film.acc2, 0, npix * sizeof(float4), ctx->stream));
+}
+
+static void FoldFilm(pg_ctx* ctx, int64_t npix) {
+    k_fold<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(ctx->film.acc, ctx->film.acc2, (size_t)npix,
+                                                     ctx->film.sum, ctx->film.sq, ctx->film.n);
+    PG_CUDA(cudaGetLastError());
+}
+
+static void ClearFilm(pg_ctx* ctx, int64_t npix) {
+    EnsureFilm(ctx, npix);
+    cudaStream_t st = ctx->stream;
+    PG_CUDA(cudaMemsetAsync(ctx->film.sum, 0, npix * 3 * sizeof(double), st));
+    PG_CUDA(cudaMemsetAsync(ctx->film.sq, 0, npix * 3 * sizeof(double), st));
+    PG_CUDA(cudaMemsetAsync(ctx->film.n, 0, npix * sizeof(uint32_t), st));
+}
+
+static int64_t IterationCap(uint64_t total, int slots, int maxDepth) {
+    // Every path ends within max_depth counted events; null-surface crossings do not
+    // count, so the cap leaves generous room for them.
+    return ((int64_t)(total / (uint64_t)slots) + 2) * ((int64_t)maxDepth * 4 + 64) + 4096;
 }
 
 static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
@@ -666,81 +918,39 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     Require(total + (uint64_t)sampleOffset * npix < (1ull << 32),
             "width*height*(spp+offset) must stay below 2^32 per render call");
     cudaStream_t st = ctx->stream;
-    ctx->film.Ensure(npix);
-    if (!accumulate) {
-        PG_CUDA(cudaMemsetAsync(ctx->film.sum, 0, npix * 3 * sizeof(double), st));
-        PG_CUDA(cudaMemsetAsync(ctx->film.sq, 0, npix * 3 * sizeof(double), st));
-        PG_CUDA(cudaMemsetAsync(ctx->film.n, 0, npix * sizeof(uint32_t), st));
-    }
+    if (!accumulate)
+        ClearFilm(ctx, npix);
+    else
+        Require(ctx->film.npix >= npix, "accumulate needs a film from an earlier call of this size");
+    ClearCallFilm(ctx, npix);
+
+    Wave w;
+    w.mode = mathMode;
+    w.surfaces = sc.surfaces;
+    w.fused = ctx->tuning.split_shadow == 0;
+    w.shadeBlock = ctx->tuning.block_size;
+    w.S0 = sc.dev;
+    w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
-    ctx->pool.Ensure(slots);
-    Pool& pl = ctx->pool;
-    PG_CUDA(cudaMemsetAsync(pl.state, 0, (size_t)slots * sizeof(int), st));
-    PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
-    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
-    PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
-
-    RenderParams P{};
-    P.slots = slots;
-    P.width = sc.width;
-    P.height = sc.height;
-    P.npix = (int)npix;
-    P.total = total;
-    P.sample_offset = sampleOffset;
-    P.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
-    P.max_depth = maxDepth;
-    P.ray_o = pl.ray_o, P.ray_d = pl.ray_d, P.beta = pl.beta, P.L = pl.L, P.hit = pl.hit;
-    P.sample = pl.sample, P.state = pl.state, P.active = pl.active, P.counts = ctx->counts;
-    P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
-    P.film_sum = ctx->film.sum, P.film_sq = ctx->film.sq, P.film_n = ctx->film.n;
-    P.next_sample = ctx->next_sample;
-    P.stats = ctx->stats;
-    P.err = ctx->err;
-
-    const SceneDev& S = sc.dev;
-    int64_t launches = 0;
-    LaunchTimer timer{ctx, profile};
-    // Every path ends within max_depth counted events; null-surface crossings do not
-    // count, so the cap leaves room for them.
-    const int64_t maxIter = ((int64_t)total / slots + 2) * ((int64_t)maxDepth * 4 + 64) + 4096;
-    PG_CUDA(cudaEventRecord(ctx->ev0, st));
-    int64_t iter = 0;
-    for (;; iter++) {
-        Require(iter < maxIter, "render loop did not converge", PG_ERR_DEVICE_LIMIT);
-        PG_CUDA(cudaMemsetAsync(ctx->counts, 0, 2 * sizeof(int), st));
-        timer.Time(PG_KERNEL_REGEN, [&]() {
-            if (mathMode == PG_MATH_PINE)
-                k_regen<kPine><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
-            else
-                k_regen<kFast><<<Ceil(slots, 256), 256, 0, st>>>(P, S);
-        });
-        res.kernelLaunches[PG_KERNEL_REGEN]++;
-        launches++;
-        PG_CUDA(cudaMemcpyAsync(ctx->h_counts, ctx->counts, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PG_CUDA(cudaStreamSynchronize(st));
-        int n = ctx->h_counts[0];
-        if (n == 0)
-            break;
-        if (mathMode == PG_MATH_PINE)
-            LaunchIteration<kPine>(ctx, timer, res, P, S, sc.surfaces, n);
-        else
-            LaunchIteration<kFast>(ctx, timer, res, P, S, sc.surfaces, n);
-        launches += sc.surfaces ? 3 : 2;
-        PG_CUDA(cudaGetLastError());
-    }
-    PG_CUDA(cudaEventRecord(ctx->ev1, st));
-    PG_CUDA(cudaEventSynchronize(ctx->ev1));
-    float ms = 0;
-    PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    res.seconds = ms * 1e-3;
-    res.launches = launches;
-    timer.Collect(res);
-    PG_CUDA(cudaMemcpy(res.stats, ctx->stats, sizeof(res.stats), cudaMemcpyDeviceToHost));
-    uint32_t e = 0;
-    PG_CUDA(cudaMemcpy(&e, ctx->err, sizeof(e), cudaMemcpyDeviceToHost));
-    std::string msg;
-    if (pg_status s = DeviceErrorStatus(e, msg))
-        throw Failure{s, msg};
+    PrepareWave(ctx, w, slots, total, (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30));
+    RequestDev rq{};
+    rq.sample_begin = 0;
+    rq.total = (uint32_t)total;
+    rq.npix = (int)npix;
+    rq.width = sc.width;
+    rq.height = sc.height;
+    rq.film_base = 0;
+    rq.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
+    rq.key0_offset = (uint32_t)sampleOffset * (uint32_t)npix;
+    rq.max_depth = maxDepth;
+    RequestDev* dReq = ctx->req_buf.Alloc<RequestDev>(1);
+    PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
+    w.P.reqs = dReq;
+    w.P.nreq = 1;
+    RunHostLoop(ctx, w, profile, res);
+    FoldFilm(ctx, npix);
+    FinishWave(ctx, res);
+    ctx->req_buf.Free();
 }
 
 static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_t* count) {
@@ -767,6 +977,9 @@ static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_
 
 }  // namespace pg
 
+namespace pg {
+static bool ValidTuning(const pg_tuning& t);
+}
 using namespace pg;
 
 // ================================================================ C ABI
@@ -784,11 +997,12 @@ extern "C" pg_status pg_create(pg_ctx** out, int device) {
         PG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         PG_CUDA(cudaEventCreate(&ctx->ev0));
         PG_CUDA(cudaEventCreate(&ctx->ev1));
-        ctx->counts = ctx->small.Alloc<int>(4);
+        ctx->counts = ctx->small.Alloc<int>(kNumCounts);
         ctx->next_sample = ctx->small.Alloc<unsigned long long>(1);
         ctx->stats = ctx->small.Alloc<unsigned long long>(kNumStats);
         ctx->err = ctx->small.Alloc<uint32_t>(1);
-        PG_CUDA(cudaMallocHost(&ctx->h_counts, 4 * sizeof(int)));
+        PG_CUDA(cudaMallocHost(&ctx->h_counts, kNumCounts * sizeof(int)));
+        PG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
     });
     if (s != PG_OK) {
         SetGlobalError(ctx->last_error);
@@ -1002,8 +1216,7 @@ extern "C" pg_status pg_intersect_device(pg_ctx* ctx, int32_t scene_id, const fl
 extern "C" pg_status pg_set_tuning(pg_ctx* ctx, const pg_tuning* t) {
     if (!ctx || !t)
         return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or tuning"});
-    if (t->queue_capacity < 1024 || t->queue_capacity > (1 << 26) || t->block_size < 32 ||
-        t->block_size > 1024 || (t->block_size & 31))
+    if (!ValidTuning(*t))
         return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "tuning out of range"});
     ctx->tuning = *t;
     return PG_OK;
@@ -1014,4 +1227,185 @@ extern "C" pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* t) {
         return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or tuning"});
     *t = ctx->tuning;
     return PG_OK;
+}
+
+// ================================================================ batched requests
+namespace pg {
+
+struct BatchOutcome {
+    RenderResult res;
+    std::vector<double> requestSeconds;
+};
+
+// Renders many requests in one graph-captured persistent wavefront.  sppDivisor > 1 runs
+// a proportionally smaller sample of each request (used by the autotuner).
+static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning& tune,
+                     bool outputs, int sppDivisor, BatchOutcome& out) {
+    Require(reqs != nullptr && n > 0 && n <= (1 << 16), "bad request array");
+    cudaStream_t st = ctx->stream;
+    std::vector<RequestDev> rq(n);
+    std::vector<SceneDev> scenes(n);
+    uint64_t total = 0, pixels = 0;
+    bool surfaces = false;
+    int maxDepth = 1;
+    const int variant = MediaVariant(tune);
+    for (int i = 0; i < n; i++) {
+        const pg_request& r = reqs[i];
+        DeviceScene& sc = GetScene(ctx, r.scene_id);
+        int w = r.width > 0 ? r.width : sc.width, h = r.height > 0 ? r.height : sc.height;
+        Require(r.spp > 0, "request spp must be positive");
+        int spp = std::max(1, r.spp / std::max(1, sppDivisor));
+        int md = r.max_depth > 0 ? r.max_depth : sc.max_depth;
+        uint64_t cnt = (uint64_t)w * h * spp;
+        Require(cnt < (1ull << 32), "a request's width*height*spp must stay below 2^32");
+        RequestDev& d = rq[i];
+        d.sample_begin = total;
+        d.total = (uint32_t)cnt;
+        d.npix = w * h;
+        d.width = w;
+        d.height = h;
+        d.film_base = pixels;
+        d.key1 = PcgHashHost((uint32_t)r.seed ^ PcgHashHost(0x9e3779b9u + (uint32_t)i)) ^
+                 (uint32_t)(r.seed >> 32);
+        d.key0_offset = 0;
+        d.max_depth = md;
+        total += cnt;
+        pixels += (uint64_t)w * h;
+        maxDepth = std::max(maxDepth, md);
+        SceneDev s = sc.dev;
+        s.media = sc.media_dev[variant];
+        // The request's film size sets the aspect ratio (camera.h:29-30).
+        s.cam.width = w;
+        s.cam.height = h;
+        s.cam.fov2d[0] = s.cam.fov2d[1] * ((float)w / (float)h);
+        scenes[i] = s;
+        surfaces = surfaces || sc.surfaces;
+    }
+    ClearFilm(ctx, (int64_t)pixels);
+    ClearCallFilm(ctx, (int64_t)pixels);
+    RequestDev* dReq = ctx->req_buf.Upload(rq, st);
+    SceneDev* dScenes = ctx->req_buf.Upload(scenes, st);
+    uint32_t* done = ctx->req_buf.Alloc<uint32_t>(n);
+    unsigned long long* times = ctx->req_buf.Alloc<unsigned long long>(n + 1);
+    PG_CUDA(cudaMemsetAsync(done, 0, n * sizeof(uint32_t), st));
+    PG_CUDA(cudaMemsetAsync(times, 0, (n + 1) * sizeof(unsigned long long), st));
+
+    Wave w;
+    w.multi = true;
+    w.mode = PG_MATH_FAST;
+    w.surfaces = surfaces;
+    w.fused = tune.split_shadow == 0;
+    w.shadeBlock = tune.block_size;
+    w.S0 = scenes[0];
+    int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, tune.queue_capacity), total);
+    PrepareWave(ctx, w, slots, total, (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30));
+    w.P.reqs = dReq;
+    w.P.nreq = n;
+    w.P.scenes = dScenes;
+    w.P.req_done = done;
+    w.P.req_time = times + 1;
+    k_timestamp<<<1, 1, 0, st>>>(times);
+    RunGraph(ctx, w, out.res);
+    FoldFilm(ctx, (int64_t)pixels);
+    FinishWave(ctx, out.res);
+    std::vector<unsigned long long> t(n + 1);
+    PG_CUDA(cudaMemcpy(t.data(), times, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    out.requestSeconds.resize(n);
+    for (int i = 0; i < n; i++)
+        out.requestSeconds[i] = t[i + 1] >= t[0] ? (double)(t[i + 1] - t[0]) * 1e-9 : -1.0;
+    if (outputs) {
+        for (int i = 0; i < n; i++) {
+            if (!reqs[i].out_mean)
+                continue;
+            const RequestDev& d = rq[i];
+            std::vector<double> sum((size_t)d.npix * 3);
+            std::vector<uint32_t> cnt(d.npix);
+            PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum + d.film_base * 3, sum.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+            PG_CUDA(cudaMemcpy(cnt.data(), ctx->film.n + d.film_base, cnt.size() * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+            for (int p = 0; p < d.npix; p++)
+                for (int c = 0; c < 3; c++)
+                    reqs[i].out_mean[3 * p + c] = cnt[p] ? (float)(sum[3 * p + c] / cnt[p]) : 0.0f;
+        }
+    }
+    ctx->req_buf.Free();
+}
+
+static bool ValidTuning(const pg_tuning& t) {
+    return t.queue_capacity >= 1024 && t.queue_capacity <= (1 << 26) && t.block_size >= 32 &&
+           t.block_size <= 1024 && (t.block_size & 31) == 0 && (t.split_shadow == 0 || t.split_shadow == 1) &&
+           (t.majorant_brick == 8 || t.majorant_brick == 16 || t.majorant_brick == 32 ||
+            t.majorant_brick == 64);
+}
+
+}  // namespace pg
+
+extern "C" pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,
+                                     pg_batch_result* result) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        BatchOutcome o;
+        RunBatch(ctx, reqs, n, ctx->tuning, true, 1, o);
+        if (result) {
+            result->seconds = o.res.seconds;
+            result->paths = (int64_t)o.res.stats[kStatPaths];
+            if (result->request_seconds)
+                for (int i = 0; i < n; i++)
+                    result->request_seconds[i] = o.requestSeconds[i];
+        }
+    });
+}
+
+// Coordinate descent over the tuning space on a 1/8-spp sample of the request mix: brick
+// size, shadow split, shading block size, queue capacity, each chosen with the others
+// fixed, keeping a value only when it is at least 2% faster.
+extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n, pg_tuning* chosen) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        pg_tuning best = ctx->tuning;
+        auto measure = [&](const pg_tuning& t) {
+            double m = 1e30;
+            for (int rep = 0; rep < 2; rep++) {
+                BatchOutcome o;
+                RunBatch(ctx, reqs, n, t, false, 8, o);
+                m = std::min(m, o.res.seconds);
+            }
+            return m;
+        };
+        double bestT = measure(best);
+        const int bricks[] = {8, 16, 32, 64}, blocks[] = {64, 128, 256};
+        const int caps[] = {1 << 19, 1 << 20, 1 << 21, 1 << 22};
+        for (int dim = 0; dim < 4; dim++) {
+            std::vector<pg_tuning> cands;
+            for (int k = 0; k < (dim == 1 ? 2 : (dim == 2 ? 3 : 4)); k++) {
+                pg_tuning t = best;
+                if (dim == 0)
+                    t.majorant_brick = bricks[k];
+                else if (dim == 1)
+                    t.split_shadow = k;
+                else if (dim == 2)
+                    t.block_size = blocks[k];
+                else
+                    t.queue_capacity = caps[k];
+                cands.push_back(t);
+            }
+            for (auto& t : cands) {
+                if (std::memcmp(&t, &best, sizeof(t)) == 0)
+                    continue;
+                double s = measure(t);
+                if (s < bestT * 0.98) {
+                    bestT = s;
+                    best = t;
+                }
+            }
+        }
+        ctx->tuning = best;
+        if (chosen)
+            *chosen = best;
+    });
 }

@@ -1,0 +1,203 @@
+"""Regenerates the golden fixtures in tests/golden/ by running the reference renderer.
+
+The reference is pine built from its own sources by oracle/Makefile (oracle/_ref/pine_ref,
+a harness that calls pine's functions; see oracle/ref_harness.cpp).  Scene inputs come
+from the seeded generators in pine_b200.scenegen; everything a test needs to replay a case
+(scene text, OBJ/volume assets, rays, outputs) is stored in the .npz so that the tests do
+not depend on the generators or on the reference being present.
+
+    python tests/golden/make_golden.py           # needs oracle/_ref/pine_ref
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+REF = os.path.join(ROOT, "oracle", "_ref", "pine_ref")
+
+HIT_DTYPE = np.dtype([("shape", "<i4"), ("tri", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+
+
+def run(*args, cwd=None):
+    p = subprocess.run([REF, *args], capture_output=True, text=True, cwd=cwd)
+    if p.returncode != 0:
+        raise RuntimeError(f"pine_ref {args[0]} failed: {p.stderr[-2000:]}")
+    return p.stdout
+
+
+def math_kat(tmp, rng):
+    a = np.concatenate([
+        np.exp(rng.uniform(-30, 30, 1024)),            # sqrt / log domain, many magnitudes
+        rng.uniform(1e-4, 4.0, 512),
+        rng.uniform(-20, 20, 1024),                     # cos / sin / tan / atan
+        rng.uniform(-1, 1, 512),                        # acos / asin
+        np.array([0.0, 1.0, -1.0, 0.5, 2.0, 1e-20, 1e20, 3.14159265, 1.5707963]),
+    ]).astype(np.float32)
+    b = rng.uniform(-5, 5, a.size).astype(np.float32)
+    b[-9:] = [1, 1, 2, 0.5, 5, 1, 1, -1, 3]
+    inp = np.stack([a, b], 1).astype(np.float32)
+    inp.tofile(f"{tmp}/m.in")
+    run("math", f"{tmp}/m.in", f"{tmp}/m.out")
+    out = np.fromfile(f"{tmp}/m.out", np.float32).reshape(-1, 12)
+    names = np.array(["sqrt", "log2", "log", "exp", "cos", "sin", "tan", "acos", "asin", "atan",
+                      "atan2", "pow"])
+    np.savez_compressed(f"{HERE}/pstd_math.npz", inputs=inp, outputs=out, names=names)
+
+
+def stof_kat(tmp, rng):
+    strs = ["0", "1", "-1", "0.5", "-0.5", "0.785398", "3.14159265", "10", "255", "1000000",
+            "123456789", "0.1", "0.2", "0.3", "19.8", "0.000001", "-0.000001", ".5", "-.25",
+            "1.", "5 0 0", "0 0 5", "-0.4 0.8 0.45", "1 2", "1e-5", "2.5e3", "", "  7", "abc",
+            "1.5.2", "-", "12 -3.5 .75 9", "0.123456789012", "99999.999999"]
+    for _ in range(600):
+        x = rng.uniform(-1000, 1000) * 10.0 ** int(rng.integers(-4, 2))
+        strs.append("%.*f" % (int(rng.integers(0, 8)), x))
+    for _ in range(200):
+        v = rng.uniform(-10, 10, 3)
+        strs.append(" ".join("%.6f" % t for t in v))
+    with open(f"{tmp}/s.in", "w") as f:
+        f.write("\n".join(strs) + "\n")
+    run("stof", f"{tmp}/s.in", f"{tmp}/s.out")
+    out = np.fromfile(f"{tmp}/s.out", np.float32).reshape(-1, 4)
+    np.savez_compressed(f"{HERE}/pstd_stof.npz", strings=np.array(strs, dtype=object),
+                        outputs=out, allow_pickle=True)
+
+
+def unit(v):
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def bsdf_kat(tmp, rng):
+    rows = []
+    for i in range(3000):
+        typ = i % 4
+        albedo = rng.uniform(0.05, 1.0, 3)
+        rough = rng.choice([0.0, 0.05, 0.2, 0.5, 0.9, 1.0]) if typ != 0 else 0.5
+        eta = rng.choice([1.33, 1.5, 2.4]) if typ == 2 else (rng.uniform(-0.9, 0.9) if typ == 3 else 1.5)
+        wi = unit(rng.normal(size=3))
+        if typ in (1, 2) and rng.uniform() < 0.7:
+            wi[2] = abs(wi[2])
+        wo = unit(rng.normal(size=3))
+        if rng.uniform() < 0.5:
+            wo[2] = np.sign(wi[2]) * abs(wo[2])
+        u1 = rng.uniform()
+        u2 = rng.uniform(size=2)
+        rows.append([typ, *albedo, rough, eta, *wi, *wo, u1, *u2, 0, 0, 0])
+    inp = np.array(rows, np.float32)
+    inp.tofile(f"{tmp}/b.in")
+    run("bsdf", f"{tmp}/b.in", f"{tmp}/b.out")
+    out = np.fromfile(f"{tmp}/b.out", np.float32).reshape(-1, 16)
+    np.savez_compressed(f"{HERE}/bsdf.npz", inputs=inp, outputs=out)
+
+
+def read_assets(paths):
+    return {os.path.basename(p): open(p, "rb").read() for p in paths}
+
+
+def pack_scene(scene_path, extra_assets=()):
+    d = os.path.dirname(scene_path)
+    assets = read_assets([os.path.join(d, a) for a in extra_assets])
+    return {"scene_text": np.array(open(scene_path).read()),
+            "asset_names": np.array(list(assets.keys()), dtype=object),
+            "asset_blobs": np.array([np.frombuffer(v, np.uint8) for v in assets.values()],
+                                    dtype=object)}
+
+
+def rays_for(rng, n, lo, hi):
+    o = rng.uniform(lo, hi, (n, 3))
+    d = unit(rng.normal(size=(n, 3)))
+    r = np.concatenate([o, d, np.zeros((n, 1)), np.full((n, 1), 3.4e38)], 1).astype(np.float32)
+    return r
+
+
+def hits_case(tmp, name, scene, assets, rays):
+    rays.tofile(f"{tmp}/{name}.rays")
+    run("hits", scene, f"{tmp}/{name}.rays", f"{tmp}/{name}.hits")
+    rec = np.fromfile(f"{tmp}/{name}.hits", HIT_DTYPE)
+    np.savez_compressed(f"{HERE}/hits_{name}.npz", rays=rays, hits=rec,
+                        **pack_scene(scene, assets), allow_pickle=True)
+    return rec
+
+
+def camera_rays(rng, scene):
+    n = 2048
+    inp = rng.uniform(0, 1, (n, 4)).astype(np.float32)
+    inp[:8, :2] = [[0, 0], [1, 1], [0.5, 0.5], [0, 1], [1, 0], [0.25, 0.75], [0.999, 0.001], [0.5, 0]]
+    d = os.path.dirname(scene)
+    inp.tofile(f"{d}/cam.in")
+    run("camera", scene, f"{d}/cam.in", f"{d}/cam.out")
+    out = np.fromfile(f"{d}/cam.out", np.float32).reshape(-1, 6)
+    return inp, out
+
+
+def image_case(name, scene, assets):
+    d = os.path.dirname(scene)
+    info = json.loads(run("render", scene, f"{d}/{name}").strip().splitlines()[-1])
+    h, w = info["height"], info["width"]
+    mean = np.fromfile(f"{d}/{name}_mean.f64").reshape(h, w, 3)
+    var = np.fromfile(f"{d}/{name}_var.f64").reshape(h, w, 3)
+    cnt = np.fromfile(f"{d}/{name}_count.i64", np.int64).reshape(h, w)
+    np.savez_compressed(f"{HERE}/image_{name}.npz", mean=mean.astype(np.float32),
+                        var=var.astype(np.float32), count=cnt.astype(np.int32),
+                        info=np.array(json.dumps(info)), **pack_scene(scene, assets),
+                        allow_pickle=True)
+
+
+def main():
+    if not os.path.exists(REF):
+        sys.exit("oracle/_ref/pine_ref is missing: run `make -C oracle ref` first")
+    import pine_b200
+    from pine_b200 import scenegen
+    L = pine_b200.lib()
+    rng = np.random.default_rng(20261203)
+    with tempfile.TemporaryDirectory() as tmp:
+        math_kat(tmp, rng)
+        stof_kat(tmp, rng)
+        bsdf_kat(tmp, rng)
+
+        # Spheres (pine Sky in place of the constant environment pine lacks).
+        sp = scenegen.spheres_scene(f"{tmp}/spheres.txt", width=48, height=27, spp=1024,
+                                    env="sky", env_radiance=0.5)
+        hits_case(tmp, "spheres", sp, [], rays_for(rng, 8000, [-6, 0.5, -6], [6, 5, 6]))
+        cam_in, cam_out = camera_rays(rng, sp)
+        np.savez_compressed(f"{HERE}/camera.npz", inputs=cam_in, outputs=cam_out,
+                            **pack_scene(sp), allow_pickle=True)
+        image_case("spheres", sp, [])
+
+        # Mesh: 5120-triangle displaced icosphere in the 12-triangle box.
+        ms = scenegen.mesh_scene(f"{tmp}/mesh.txt", L, subdiv=4, width=48, height=27,
+                                 spp=512, max_depth=16)
+        mesh_assets = ["ico4_s0.obj", "cornell.obj"]
+        # Rays from inside the box toward the sphere and walls, and from the camera side.
+        r1 = rays_for(rng, 6000, [-2.8, 0.2, -2.8], [2.8, 5.8, 2.8])
+        r2 = rays_for(rng, 2000, [-6, 1, -12], [6, 5, -6])
+        hits_case(tmp, "mesh", ms, mesh_assets, np.concatenate([r1, r2]))
+        image_case("mesh", ms, mesh_assets)
+
+        # Volume: 32^3 cloud for density lookups, 64^3 for the image.
+        vs = scenegen.volume_scene(f"{tmp}/vol32.txt", L, n=32, width=16, height=9, spp=1,
+                                   env="sky", env_radiance=1.0)
+        pts = np.concatenate([rng.uniform(-0.05, 1.05, (3000, 3)),
+                              rng.integers(0, 33, (200, 3)) / 32.0]).astype(np.float32)
+        pts.tofile(f"{tmp}/p.in")
+        run("density", vs, f"{tmp}/p.in", f"{tmp}/p.out")
+        dens = np.fromfile(f"{tmp}/p.out", np.float32)
+        np.savez_compressed(f"{HERE}/density.npz", points=pts, density=dens,
+                            **pack_scene(vs, ["cloud32_s0.vol"]), allow_pickle=True)
+        vi = scenegen.volume_scene(f"{tmp}/volume.txt", L, n=64, width=48, height=27,
+                                   spp=1024, env="sky", env_radiance=1.0)
+        image_case("volume", vi, ["cloud64_s0.vol"])
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,73 @@
+"""Batched requests in one graph-captured persistent wavefront (pg_render_batch) and the
+autotuner (pg_autotune)."""
+
+import numpy as np
+import pytest
+
+from conftest import golden, write_fixture_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_matches_individual_renders(ctx, tmp_path):
+    names = ["spheres", "volume", "mesh"]
+    ids = [ctx.load_scene(write_fixture_scene(golden(f"image_{n}.npz"), str(tmp_path / n)))
+           for n in names]
+    reqs = [dict(scene=ids[0], spp=256, seed=1),
+            dict(scene=ids[1], spp=256, seed=2),
+            dict(scene=ids[2], spp=128, seed=3),
+            dict(scene=ids[1], spp=64, width=40, height=30, seed=4),
+            dict(scene=ids[0], spp=32, width=17, height=9, seed=5)]
+    out = ctx.render_batch(reqs)
+    assert out["paths"] == sum(r["spp"] * (r.get("width", 48) * r.get("height", 27)) for r in reqs)
+    t = np.array(out["request_seconds"])
+    assert (t > 0).all() and (t <= out["seconds"] * 1.01 + 1e-3).all()
+    for r, mean in zip(reqs[:3], out["means"][:3]):
+        single = ctx.render(r["scene"], spp=r["spp"], seed=100 + r["seed"])
+        se = np.sqrt(single["var"].astype(float) / r["spp"] * 2)
+        v = se > 0
+        z = np.abs(mean - single["mean"])[v] / se[v]
+        # Different random streams: agreement within Monte Carlo error (the 128-spp mesh
+        # request has heavy-tailed pixels, hence 95% rather than 99%).
+        assert np.mean(z < 2.576) > 0.95
+        assert abs(mean.mean() - single["mean"].mean()) < 0.03 * single["mean"].mean() + 1e-3
+    # A request with its own film size renders that size.
+    assert out["means"][3].shape == (30, 40, 3) and out["means"][4].shape == (9, 17, 3)
+    assert np.isfinite(out["means"][3]).all() and out["means"][3].mean() > 0
+    for i in ids:
+        ctx.release_scene(i)
+
+
+def test_autotune_returns_a_valid_tuning(ctx, tmp_path):
+    ids = [ctx.load_scene(write_fixture_scene(golden(f"image_{n}.npz"), str(tmp_path / n)))
+           for n in ["volume", "spheres"]]
+    before = ctx.tuning()
+    t = ctx.autotune([dict(scene=ids[0], spp=64), dict(scene=ids[1], spp=64)])
+    assert t["majorant_brick"] in (8, 16, 32) and t["split_shadow"] in (0, 1)
+    assert t["block_size"] in (64, 128, 256) and 1 << 19 <= t["queue_capacity"] <= 1 << 22
+    assert ctx.tuning() == t
+    # Whatever was chosen renders the same image statistically.
+    r = ctx.render(ids[1], spp=256, seed=9)
+    ctx.set_tuning(**before)
+    q = ctx.render(ids[1], spp=256, seed=10)
+    se = np.sqrt((r["var"] + q["var"]).astype(float) / 256)
+    v = se > 0
+    assert np.mean(np.abs(r["mean"] - q["mean"])[v] / se[v] < 2.576) > 0.97
+    for i in ids:
+        ctx.release_scene(i)
+
+
+@pytest.mark.parametrize("split,brick", [(0, 8), (1, 32), (0, 16)])
+def test_tunings_agree(ctx, tmp_path, split, brick):
+    """Every shadow split and majorant brick size renders the same image statistically."""
+    z = golden("image_volume.npz")
+    sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
+    before = ctx.tuning()
+    ctx.set_tuning(queue_capacity=1 << 20, block_size=128, split_shadow=split,
+                   majorant_brick=brick)
+    r = ctx.render(sid, spp=1024, seed=31)
+    ctx.set_tuning(**before)
+    se = np.sqrt(r["var"].astype(float) / 1024 + z["var"] / z["count"][..., None])
+    v = se > 0
+    assert np.mean(np.abs(r["mean"] - z["mean"])[v] / se[v] < 2.576) >= 0.98
+    ctx.release_scene(sid)
