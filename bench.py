@@ -164,11 +164,11 @@ def algorithmic_bytes(name, k):
 
 
 def read_traffic():
-    """DRAM bytes per tracking step of each kernel, from the committed ncu summary."""
+    """DRAM bytes per algorithmic byte of each kernel, from the committed ncu summary."""
     out = {}
     try:
         for line in open(TRAFFIC_FILE):
-            if line.startswith("dram_bytes_per_step"):
+            if line.startswith("dram_bytes_per_algorithmic_byte"):
                 _, rest = line.split(":", 1)
                 for kv in rest.split():
                     k, v = kv.split("=")
@@ -189,8 +189,8 @@ def roofline(kernels, peak, peak_kind):
     achieved = per_launch_bytes / launch_s / 1e9
     traffic = None
     tr = read_traffic()
-    if name in tr and k["volume_steps"]:
-        traffic = tr[name] * k["volume_steps"] / k["launches"]
+    if name in tr:
+        traffic = tr[name] * per_launch_bytes
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
             "kernel": "k_" + name, "algorithmic_bytes_per_launch": per_launch_bytes,

@@ -248,10 +248,12 @@ typedef struct pg_batch_result {
 
 typedef struct pg_tuning {
     int32_t queue_capacity; /* path slots resident in the wavefront */
-    int32_t block_size;     /* threads per block of the shading kernel */
+    int32_t block_size;     /* threads per block of the shading kernel: a multiple of 32,
+                               at most 128 (the kernel's launch bound) */
     int32_t split_shadow;   /* 1: shadow rays in their own kernel; 0: traced inside the
                                shading kernel */
-    int32_t majorant_brick; /* voxels per edge of a grid medium's majorant brick: 8, 16, 32 */
+    int32_t majorant_brick; /* voxels per edge of a grid medium's majorant brick: 8, 16, 32
+                               or 64 */
 } pg_tuning;
 
 pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,

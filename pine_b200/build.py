@@ -39,12 +39,14 @@ def _stale(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, defines=(), out: str = None) -> str:
+    """Builds libpinegpu.so (or `out`, with extra -D `defines`) when a source changed."""
+    lib_path = out or LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "pine_gpu.h"),
                                                             __file__]
-    if force or _stale(LIB, deps):
-        objdir = os.path.join(HERE, "_build")
+    if force or _stale(lib_path, deps):
+        objdir = os.path.join(HERE, "_build", os.path.basename(lib_path))
         os.makedirs(objdir, exist_ok=True)
         objs = []
         procs = []
@@ -52,7 +54,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             obj = os.path.join(objdir, os.path.basename(src) + ".o")
             objs.append(obj)
             cmd = [_nvcc(), "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
-                   "-Xcompiler", "-pthread", "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+                   "-Xcompiler", "-pthread", "-I", INCLUDE, "-I", CSRC,
+                   *[f"-D{d}" for d in defines], "-c", src, "-o", obj]
             if src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"] if verbose else []
             procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
@@ -67,10 +70,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if failed:
             msg = "\n".join(" ".join(c) + "\n" + o for c, o in failed)
             raise RuntimeError("libpinegpu build failed:\n" + msg)
-        tmp = LIB + ".tmp"
+        tmp = lib_path + ".tmp"
         subprocess.run([_nvcc(), "-shared", *ARCH, "-o", tmp, *objs, "-Xcompiler", "-pthread"],
                        check=True)
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib_path)
+    if out:
+        return lib_path
     cli_src = os.path.join(CSRC, "pine_cli.cpp")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB])):
         subprocess.run(["g++", "-std=c++17", "-O2", "-I", INCLUDE, cli_src, "-o", CLI,

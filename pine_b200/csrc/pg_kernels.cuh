@@ -25,6 +25,21 @@
 
 #include "pg_shade.cuh"
 
+// Build-time register cap of the shading kernel.  Measured on B200 (volume benchmark):
+// (128 threads, 6 blocks) -> 85 registers, 1160 Mpaths/s; no cap -> 128 registers, 1128;
+// (64, 12) -> 1162.  Blocks of up to PG_SHADE_MAX_THREADS threads can be launched.
+#ifndef PG_SHADE_MAX_THREADS
+#define PG_SHADE_MAX_THREADS 128
+#endif
+#ifndef PG_SHADE_MIN_BLOCKS
+#define PG_SHADE_MIN_BLOCKS 6
+#endif
+#if PG_SHADE_MIN_BLOCKS > 0
+#define PG_SHADE_BOUNDS __launch_bounds__(PG_SHADE_MAX_THREADS, PG_SHADE_MIN_BLOCKS)
+#else
+#define PG_SHADE_BOUNDS
+#endif
+
 namespace pg {
 
 enum StatIndex {
@@ -94,6 +109,44 @@ __device__ __forceinline__ int WarpAppend(int* counter, bool pred) {
         base = atomicAdd(counter, __popc(mask));
     base = __shfl_sync(mask, base, leader);
     return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Block-aggregated appends: every thread of the block calls these together (the
+// grid-stride loops move whole blocks in lockstep); each returns the calling thread's
+// index in the queue its predicate selects, or -1, with one global atomic per queue per
+// block instead of one per warp or per thread.
+template <int K>
+struct BlockQueues {
+    int base[K];
+    int warpOff[K][32];
+};
+
+template <int K>
+__device__ __forceinline__ void BlockAppend(int* const (&counters)[K], const bool (&pred)[K],
+                                            int (&slot)[K], BlockQueues<K>& sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    unsigned mask[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        mask[k] = __ballot_sync(0xffffffffu, pred[k]);
+        if (lane == 0)
+            sh.warpOff[k][warp] = __popc(mask[k]);
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        int k = threadIdx.x, tot = 0;
+        for (int w = 0; w < nw; w++) {
+            int c = sh.warpOff[k][w];
+            sh.warpOff[k][w] = tot;
+            tot += c;
+        }
+        sh.base[k] = tot ? atomicAdd(counters[k], tot) : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++)
+        slot[k] = pred[k] ? sh.base[k] + sh.warpOff[k][warp] + __popc(mask[k] & ((1u << lane) - 1u)) : -1;
+    __syncthreads();
 }
 
 // Adds v (summed over the calling threads of the warp) to a 64-bit counter with one
@@ -181,81 +234,101 @@ __device__ __forceinline__ int FindRequest(const RenderParams& P, unsigned long 
     return lo;
 }
 
+// Adds a finished path's radiance to its pixel (Film::AddSample with a box filter of
+// radius 0.5) and, in a batch, completes its request when it was the last path.
+template <bool MULTI>
+__device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, uint32_t& dropped) {
+    const RequestDev& R = RequestOf<MULTI>(P, i);
+    uint32_t sid = P.sample[i] - R.key0_offset;
+    size_t pix = (size_t)R.film_base + sid % (uint32_t)R.npix;
+    if (Finite(c)) {
+        RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
+        RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
+    } else {
+        dropped++;
+    }
+    if (MULTI) {
+        int r = P.slot_req[i];
+        if (atomicAdd(&P.req_done[r], 1u) + 1u == R.total)
+            P.req_time[r] = GlobalTimer();
+    }
+}
+
+// Starts camera sample `id` in slot i (RadianceIntegrator::Compute + ThinLenCamera::GenRay,
+// integrator.cpp:152-158, camera.cpp:31-41).
+template <int M, bool MULTI>
+__device__ void SpawnPath(const RenderParams& P, const SceneDev& S0, int i, unsigned long long id) {
+    int r = MULTI ? FindRequest(P, id) : 0;
+    const RequestDev& R = P.reqs[r];
+    if (MULTI)
+        P.slot_req[i] = r;
+    const SceneDev& S = MULTI ? P.scenes[r] : S0;
+    uint32_t sid = (uint32_t)(id - R.sample_begin);
+    int pix = (int)(sid % (uint32_t)R.npix);
+    int px = pix % R.width, py = pix / R.width;
+    uint32_t key0 = sid + R.key0_offset;
+    Rng rng{key0, R.key1, 0};
+    float u0, u1, l0, l1;
+    rng.Get2D(u0, u1);
+    rng.Get2D(l0, l1);
+    V3 o, d;
+    CameraRay<M>(S.cam, (px + u0) / (float)R.width, (py + u1) / (float)R.height, l0, l1, o, d);
+    P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+    P.ray_d[i] = make_float4(d.x, d.y, d.z, __int_as_float(S.cam.medium));
+    P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
+    P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng.dim));
+    P.sample[i] = key0;
+}
+
+// Block-aggregated claim of new camera samples for the threads with `want`; returns the
+// sample id, or ~0ull when the render has no samples left.  Called by whole blocks.
+__device__ __forceinline__ unsigned long long BlockClaim(const RenderParams& P, bool want,
+                                                         int* off, unsigned long long* base) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (lane == 0)
+        off[warp] = __popc(mask);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < nw; w++) {
+            int c = off[w];
+            off[w] = tot;
+            tot += c;
+        }
+        *base = tot ? atomicAdd(P.next_sample, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long id = *base + off[warp] + __popc(mask & ((1u << lane) - 1u));
+    __syncthreads();
+    return want && id < P.total ? id : ~0ull;
+}
+
+// Fills the slots listed in the finished queue with new camera samples (the start of a
+// render; afterwards shading and shadow kernels refill slots themselves).
 template <int M, bool MULTI>
 __global__ void k_regen(RenderParams P, SceneDev S0) {
+    __shared__ int claimOff[32];
+    __shared__ unsigned long long claimBase;
+    __shared__ BlockQueues<1> q1;
     const int n = P.counts[kCntFinished];
     int* next = NextList(P);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
          q += gridDim.x * blockDim.x) {
         bool live = q < n;
         int i = live ? P.finished[q] : 0;
-        int st = live ? P.state[i] : kSlotDead;
-        uint32_t dropped = 0, done = 0;
-        if (live && st == kSlotFinished) {
-            const RequestDev& R = RequestOf<MULTI>(P, i);
-            float4 L = P.L[i];
-            V3 c = v3(L.x, L.y, L.z);
-            uint32_t sid = P.sample[i] - R.key0_offset;
-            size_t pix = (size_t)R.film_base + sid % (uint32_t)R.npix;
-            if (Finite(c)) {
-                // Two 16-byte vector reductions per sample into this call's float film,
-                // folded into the FP64 film once the call's paths are done (k_fold).
-                RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
-                RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
-            } else {
-                dropped = 1;
-            }
-            if (MULTI) {
-                int r = P.slot_req[i];
-                if (atomicAdd(&P.req_done[r], 1u) + 1u == R.total)
-                    P.req_time[r] = GlobalTimer();
-            }
-            done = 1;
-            st = kSlotEmpty;
-        }
-        bool claim = live && st == kSlotEmpty;
-        unsigned mask = __ballot_sync(__activemask(), claim);
-        if (claim) {
-            int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
-            unsigned long long base = 0;
-            if (lane == leader)
-                base = atomicAdd(P.next_sample, (unsigned long long)__popc(mask));
-            base = __shfl_sync(mask, base, leader);
-            unsigned long long id = base + __popc(mask & ((1u << lane) - 1u));
-            if (id < P.total) {
-                int r = MULTI ? FindRequest(P, id) : 0;
-                const RequestDev& R = P.reqs[r];
-                if (MULTI)
-                    P.slot_req[i] = r;
-                const SceneDev& S = MULTI ? P.scenes[r] : S0;
-                uint32_t sid = (uint32_t)(id - R.sample_begin);
-                int pix = (int)(sid % (uint32_t)R.npix);
-                int px = pix % R.width, py = pix / R.width;
-                uint32_t key0 = sid + R.key0_offset;
-                Rng rng{key0, R.key1, 0};
-                float u0, u1, l0, l1;
-                rng.Get2D(u0, u1);
-                rng.Get2D(l0, l1);
-                V3 o, d;
-                CameraRay<M>(S.cam, (px + u0) / (float)R.width, (py + u1) / (float)R.height, l0, l1,
-                             o, d);
-                P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
-                P.ray_d[i] = make_float4(d.x, d.y, d.z, __int_as_float(S.cam.medium));
-                P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
-                P.L[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng.dim));
-                P.sample[i] = key0;
-                st = kSlotActive;
-            } else {
-                st = kSlotDead;
-            }
-        }
+        unsigned long long id = BlockClaim(P, live, claimOff, &claimBase);
+        bool spawned = id != ~0ull;
+        if (spawned)
+            SpawnPath<M, MULTI>(P, S0, i, id);
         if (live)
-            P.state[i] = st;
-        int slot = WarpAppend(&P.counts[kCntNext], live && st == kSlotActive);
-        if (slot >= 0)
-            next[slot] = i;
-        WarpAdd(&P.stats[kStatPaths], done);
-        WarpAdd(&P.stats[kStatDropped], dropped);
+            P.state[i] = spawned ? kSlotActive : kSlotDead;
+        int* const ctr[1] = {&P.counts[kCntNext]};
+        const bool pr[1] = {spawned};
+        int sl[1];
+        BlockAppend<1>(ctr, pr, sl, q1);
+        if (sl[0] >= 0)
+            next[sl[0]] = i;
         WarpAdd(&P.stats[kStatRegenItems], live ? 1u : 0u);
     }
 }
@@ -399,6 +472,13 @@ struct ShadeCounters {
     uint32_t steps = 0, bricks = 0, err = 0, shadowSteps = 0, shadowBricks = 0, shadowRays = 0;
 };
 
+// The shadow-queue entry a shading step produced (-1: none).  The top bit of the slot
+// word of an entry marks the path's last shadow ray: k_shadow then finishes the path.
+struct PendingShadow {
+    int idx = -1;
+};
+constexpr uint32_t kFinalShadow = 0x80000000u;
+
 // Next-event estimation (RayIntegrator::EstimateDirect, integrator.cpp:88-119): picks a
 // light, samples it, evaluates the BSDF (surface) or phase function (medium) and either
 // queues a shadow ray carrying the unoccluded contribution beta * f * w * Le / pdf for
@@ -407,7 +487,7 @@ template <int M, bool FUSED>
 __device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, uint32_t key1, Rng& rng,
                           V3 p, V3 n, V3 wiWorld, bool surface, const MaterialDev* mat,
                           const Frame<M>* frame, float g, int medIn, int medOut, V3 beta, V3& L,
-                          uint2* stack, ShadeCounters& ct) {
+                          uint2* stack, ShadeCounters& ct, PendingShadow& ps) {
     float lightPdf;
     int li = PickLight(S, rng.Get1D(), lightPdf);
     float u0, u1;
@@ -452,11 +532,14 @@ __device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, ui
         ct.shadowRays += traced;
         return;
     }
-    int q = atomicAdd(&P.counts[kCntShadow], 1);
+    // Appended where it is produced (warp-aggregated), so nothing stays live in registers;
+    // shading marks the record final afterwards if the path ends at this vertex.
+    int q = WarpAppend(&P.counts[kCntShadow], true);
     P.so[q] = make_float4(o.x, o.y, o.z, tmax);
     P.sd[q] = make_float4(ls.wo.x, ls.wo.y, ls.wo.z, __int_as_float(med));
     P.sc[q] = make_float4(c.x, c.y, c.z, __int_as_float(slot));
     P.skey[q] = key;
+    ps.idx = q;
 }
 
 // Environment radiance for an escaped ray and its MIS light pdf (path.cpp:29-40).
@@ -476,7 +559,8 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
 
 template <int M, bool FUSED>
 __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
-                         uint2* stack, ShadeCounters& ct, bool& finished) {
+                         uint2* stack, ShadeCounters& ct, PendingShadow& ps, bool& finished,
+                         V3& Lout) {
     float4 ro = P.ray_o[i], rd = P.ray_d[i], bt = P.beta[i], Lw = P.L[i];
     // Scenes without surfaces skip k_trace: every ray misses.
     float4 h = (S.has_bvh || S.num_planes) ? P.hit[i]
@@ -508,7 +592,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
         } else {
             const MediumDev& m = S.media[medium];
             NextEvent<M, FUSED>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
-                                m.g, medium, medium, beta, L, stack, ct);
+                                m.g, medium, medium, beta, L, stack, ct, ps);
             float u0, u1;
             rng.Get2D(u0, u1);
             V3 wo;
@@ -559,7 +643,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
                 Frame<M> fr;
                 fr.From(si.n);
                 NextEvent<M, FUSED>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
-                                    medIn, medOut, beta, L, stack, ct);
+                                    medIn, medOut, beta, L, stack, ct, ps);
                 float u1 = rng.Get1D(), u20, u21;
                 rng.Get2D(u20, u21);
                 BsdfSample bs;
@@ -591,8 +675,11 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
         }
     }
     P.L[i] = make_float4(L.x, L.y, L.z, __uint_as_float(rng.dim));
+    Lout = L;
     if (finished) {
         P.state[i] = kSlotFinished;
+        if (ps.idx >= 0)
+            reinterpret_cast<uint32_t*>(&P.sc[ps.idx])[3] = (uint32_t)i | kFinalShadow;
     } else {
         P.ray_o[i] = make_float4(no.x, no.y, no.z, bsdfPdf);
         P.ray_d[i] = make_float4(nd.x, nd.y, nd.z, __int_as_float(nmed));
@@ -601,25 +688,42 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
 }
 
 template <int M, bool MULTI, bool FUSED>
-__global__ void k_shade(RenderParams P, SceneDev S0) {
+__global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
+    __shared__ BlockQueues<1> q1;
+    __shared__ int claimOff[32];
+    __shared__ unsigned long long claimBase;
     const int n = P.counts[kCntActive];
     const int* active = ActiveList(P);
     int* next = NextList(P);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
          q += gridDim.x * blockDim.x) {
         ShadeCounters ct;
+        PendingShadow ps;
         bool live = q < n, finished = true;
         int i = live ? active[q] : 0;
+        V3 L;
         if (live)
             ShadeOne<M, FUSED>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
-                               stack + threadIdx.x, ct, finished);
-        int a = WarpAppend(&P.counts[kCntNext], live && !finished);
-        if (a >= 0)
-            next[a] = i;
-        int f = WarpAppend(&P.counts[kCntFinished], live && finished);
-        if (f >= 0)
-            P.finished[f] = i;
+                               stack + threadIdx.x, ct, ps, finished, L);
+        // A path that ends here with no shadow ray in flight is flushed now and its slot
+        // takes the next camera sample; one with a shadow ray pending ends in k_shadow.
+        bool endHere = live && finished && ps.idx < 0;
+        uint32_t dropped = 0;
+        if (endHere)
+            FlushPath<MULTI>(P, i, L, dropped);
+        unsigned long long id = BlockClaim(P, endHere, claimOff, &claimBase);
+        bool spawned = id != ~0ull;
+        if (spawned)
+            SpawnPath<M, MULTI>(P, S0, i, id);
+        else if (endHere)
+            P.state[i] = kSlotDead;
+        int* const ctr[1] = {&P.counts[kCntNext]};
+        const bool pr[1] = {(live && !finished) || spawned};
+        int sl[1];
+        BlockAppend<1>(ctr, pr, sl, q1);
+        if (sl[0] >= 0)
+            next[sl[0]] = i;
         if (ct.err)
             atomicOr(P.err, ct.err);
         WarpAdd(&P.stats[kStatSteps], ct.steps + ct.shadowSteps);
@@ -627,37 +731,63 @@ __global__ void k_shade(RenderParams P, SceneDev S0) {
         WarpAdd(&P.stats[kStatShadeBricks], ct.bricks + ct.shadowBricks);
         WarpAdd(&P.stats[kStatShadeItems], live ? 1u : 0u);
         WarpAdd(&P.stats[kStatRays], ct.shadowRays);
+        WarpAdd(&P.stats[kStatPaths], endHere ? 1u : 0u);
+        WarpAdd(&P.stats[kStatDropped], dropped);
     }
 }
 
 template <int M, bool MULTI>
 __global__ void k_shadow(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
+    __shared__ BlockQueues<1> q1;
+    __shared__ int claimOff[32];
+    __shared__ unsigned long long claimBase;
     const int n = P.counts[kCntShadow];
+    int* next = NextList(P);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
          q += gridDim.x * blockDim.x) {
-        uint32_t err = 0, steps = 0, bricks = 0;
-        int traced = 0;
+        uint32_t err = 0, steps = 0, bricks = 0, dropped = 0;
+        int traced = 0, slot = 0;
+        bool last = false;
         if (q < n) {
             float4 so = P.so[q], sd = P.sd[q], sc = P.sc[q];
-            int slot = __float_as_int(sc.w);
+            uint32_t w = __float_as_uint(sc.w);
+            slot = (int)(w & ~kFinalShadow);
+            last = (w & kFinalShadow) != 0;
             const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
             Rng rng{P.sample[slot], P.skey[q], 0};
             V3 tr = ShadowTr<M>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
                                 __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x, steps,
                                 bricks, err, traced);
-            if (!IsBlack(tr)) {
-                float4 Lw = P.L[slot];
-                P.L[slot] = make_float4(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z, Lw.w);
-            }
+            float4 Lw = P.L[slot];
+            V3 L = v3(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z);
+            if (last)
+                FlushPath<MULTI>(P, slot, L, dropped);
+            else if (!IsBlack(tr))
+                P.L[slot] = make_float4(L.x, L.y, L.z, Lw.w);
             if (err)
                 atomicOr(P.err, err);
         }
+        // The path's last shadow ray: the slot takes the next camera sample.
+        unsigned long long id = BlockClaim(P, last, claimOff, &claimBase);
+        bool spawned = id != ~0ull;
+        if (spawned)
+            SpawnPath<M, MULTI>(P, S0, slot, id);
+        else if (last)
+            P.state[slot] = kSlotDead;
+        int* const ctr[1] = {&P.counts[kCntNext]};
+        const bool pr[1] = {spawned};
+        int sl[1];
+        BlockAppend<1>(ctr, pr, sl, q1);
+        if (sl[0] >= 0)
+            next[sl[0]] = slot;
         WarpAdd(&P.stats[kStatRays], (uint32_t)traced);
         WarpAdd(&P.stats[kStatSteps], steps);
         WarpAdd(&P.stats[kStatShadowSteps], steps);
         WarpAdd(&P.stats[kStatShadowBricks], bricks);
         WarpAdd(&P.stats[kStatShadowItems], q < n ? 1u : 0u);
+        WarpAdd(&P.stats[kStatPaths], last ? 1u : 0u);
+        WarpAdd(&P.stats[kStatDropped], dropped);
     }
 }
 
@@ -676,6 +806,23 @@ __global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int
             for (int x = b * bx; x <= min(b * bx + b, sx - 1); x++)
                 m = fmaxf(m, __ldg(&row[x]));
         }
+    maj[k] = m;
+}
+
+// Majorants of bricks of edge 2s from those of edge s: the footprint of brick b
+// ([2s*b, 2s*b + 2s] per axis) is the union of its children's (2b and 2b+1), so the
+// maximum over the existing children is exact.
+__global__ void k_majorant_coarsen(const float* fine, int fx, int fy, int fz, int nbx, int nby,
+                                   int nbz, float* maj) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)nbx * nby * nbz)
+        return;
+    int bx = (int)(k % nbx), by = (int)((k / nbx) % nby), bz = (int)(k / ((int64_t)nbx * nby));
+    float m = 0.0f;
+    for (int z = 2 * bz; z <= min(2 * bz + 1, fz - 1); z++)
+        for (int y = 2 * by; y <= min(2 * by + 1, fy - 1); y++)
+            for (int x = 2 * bx; x <= min(2 * bx + 1, fx - 1); x++)
+                m = fmaxf(m, fine[x + (size_t)fx * (y + (size_t)fy * z)]);
     maj[k] = m;
 }
 

@@ -162,7 +162,7 @@ struct pg_ctx {
     int* h_counts = nullptr;               // pinned
     pg::DevMem req_buf;                    // per-call request table
     std::string last_error;
-    pg_tuning tuning{1 << 21, 128, 1, 32};
+    pg_tuning tuning{1 << 21, 64, 1, 64};
     int num_sms = 148;
 };
 
@@ -409,8 +409,14 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
                 nb[k] = (m.size[k] + b - 1) / b;
             int64_t nbTot = (int64_t)nb[0] * nb[1] * nb[2];
             float* maj = sc->mem.Alloc<float>(nbTot);
-            k_majorant<<<(unsigned)Ceil<int64_t>(nbTot, 128), 128, 0, st>>>(
-                dd, m.size[0], m.size[1], m.size[2], b, nb[0], nb[1], nb[2], maj);
+            if (v == 0) {
+                k_majorant<<<(unsigned)Ceil<int64_t>(nbTot, 128), 128, 0, st>>>(
+                    dd, m.size[0], m.size[1], m.size[2], b, nb[0], nb[1], nb[2], maj);
+            } else {
+                const auto& f = nbVariants[i][v - 1];
+                k_majorant_coarsen<<<(unsigned)Ceil<int64_t>(nbTot, 128), 128, 0, st>>>(
+                    majVariants[i][v - 1], f[0], f[1], f[2], nb[0], nb[1], nb[2], maj);
+            }
             PG_CUDA(cudaGetLastError());
             majVariants[i][v] = maj;
             nbVariants[i][v] = {nb[0], nb[1], nb[2]};
@@ -717,8 +723,12 @@ static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer
         time(PG_KERNEL_SHADOW, [&]() {
             k_shadow<M, MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
         });
+    // Queue swap; counted with the fill kernel.
+    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
 }
 
+// The initial fill of every slot and the first swap.  Later refills happen inside k_shade
+// and k_shadow as paths end.
 template <int M, bool MULTI>
 static void LaunchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
     auto f = [&]() {
@@ -794,8 +804,8 @@ static void RunHostLoop(pg_ctx* ctx, Wave& w, bool profile, RenderResult& res) {
     cudaStream_t st = ctx->stream;
     LaunchTimer timer{ctx, profile};
     PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    DispatchRegen(ctx, w, &timer, &res);
     for (int64_t iter = 0;; iter++) {
-        DispatchRegen(ctx, w, &timer, &res);
         PG_CUDA(cudaMemcpyAsync(ctx->h_counts, ctx->counts, sizeof(int), cudaMemcpyDeviceToHost, st));
         PG_CUDA(cudaStreamSynchronize(st));
         int n = ctx->h_counts[0];
@@ -808,10 +818,11 @@ static void RunHostLoop(pg_ctx* ctx, Wave& w, bool profile, RenderResult& res) {
     timer.Collect(res);
 }
 
-// Device-driven loop: the whole render is one CUDA graph whose while-node repeats
-// regen/swap/trace/shade/shadow with persistent (fixed, grid-stride) launches until k_swap
-// finds the active queue empty or the iteration cap reached.
-static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res) {
+// Device-driven loop: after the initial fill, the whole render is one CUDA graph whose
+// while-node repeats trace/shade/shadow/swap with persistent (fixed, grid-stride) launches
+// until k_swap finds the active queue empty or the iteration cap reached.  The condition
+// starts at 1: the fill always leaves at least one active path.
+static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res, unsigned long long* startTime) {
     cudaStream_t st = ctx->stream;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -839,16 +850,18 @@ static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res) {
     w.P.use_cond = 1;
     w.P.cond = cond;
     PG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    DispatchRegen(ctx, w, nullptr, nullptr);
     DispatchBody(ctx, w, w.P.slots, true, nullptr, nullptr);
     cudaGraph_t captured = nullptr;
     cudaError_t ce = cudaStreamEndCapture(st, &captured);
     if (ce != cudaSuccess)
         throw Failure{PG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)};
     PG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    PG_CUDA(cudaEventRecord(ctx->ev0, st));
-    PG_CUDA(cudaGraphLaunch(exec, st));
     w.P.use_cond = 0;
+    PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    if (startTime)
+        k_timestamp<<<1, 1, 0, st>>>(startTime);
+    DispatchRegen(ctx, w, nullptr, nullptr);
+    PG_CUDA(cudaGraphLaunch(exec, st));
 }
 
 // Ends the timed region (after the film fold) and collects counters and device errors.
@@ -1304,8 +1317,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.P.scenes = dScenes;
     w.P.req_done = done;
     w.P.req_time = times + 1;
-    k_timestamp<<<1, 1, 0, st>>>(times);
-    RunGraph(ctx, w, out.res);
+    RunGraph(ctx, w, out.res, times);
     FoldFilm(ctx, (int64_t)pixels);
     FinishWave(ctx, out.res);
     std::vector<unsigned long long> t(n + 1);
@@ -1332,9 +1344,14 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     ctx->req_buf.Free();
 }
 
+// Largest shading block: the kernel's launch bound when it has one; otherwise what the
+// fused variant's traversal stacks (256 bytes a thread) leave of shared memory.
+constexpr int kMaxShadeBlock = PG_SHADE_MIN_BLOCKS > 0 ? PG_SHADE_MAX_THREADS : 512;
+
 static bool ValidTuning(const pg_tuning& t) {
     return t.queue_capacity >= 1024 && t.queue_capacity <= (1 << 26) && t.block_size >= 32 &&
-           t.block_size <= 1024 && (t.block_size & 31) == 0 && (t.split_shadow == 0 || t.split_shadow == 1) &&
+           t.block_size <= kMaxShadeBlock && (t.block_size & 31) == 0 &&
+           (t.split_shadow == 0 || t.split_shadow == 1) &&
            (t.majorant_brick == 8 || t.majorant_brick == 16 || t.majorant_brick == 32 ||
             t.majorant_brick == 64);
 }
@@ -1378,7 +1395,7 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
             return m;
         };
         double bestT = measure(best);
-        const int bricks[] = {8, 16, 32, 64}, blocks[] = {64, 128, 256};
+        const int bricks[] = {8, 16, 32, 64}, blocks[] = {32, 64, 128};
         const int caps[] = {1 << 19, 1 << 20, 1 << 21, 1 << 22};
         for (int dim = 0; dim < 4; dim++) {
             std::vector<pg_tuning> cands;
@@ -1389,7 +1406,7 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
                 else if (dim == 1)
                     t.split_shadow = k;
                 else if (dim == 2)
-                    t.block_size = blocks[k];
+                    t.block_size = std::min(blocks[k], kMaxShadeBlock);
                 else
                     t.queue_capacity = caps[k];
                 cands.push_back(t);
