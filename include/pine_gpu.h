@@ -218,6 +218,23 @@ pg_status pg_scene_info(pg_ctx* ctx, int32_t scene_id, int32_t* width, int32_t* 
 pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc, float* out_mean,
                     float* out_var, uint32_t* out_count, pg_render_stats* stats);
 
+/* pg_render without device allocation, for callers that may not allocate GPU memory
+ * while they render: an application whose device memory belongs to its own allocator,
+ * or a thread that cannot take the device-wide synchronisation cudaMalloc and cudaFree
+ * may cause.  No counterpart in the reference (pine renders on the host).
+ * Path state and the film accumulators live in one fixed array inside the library,
+ * about 26 MiB on every GPU that loads it, held until the process exits: at most 65536
+ * path slots and films of at most 524288 pixels (larger films: PG_ERR_INVALID_ARG).
+ * mean_device: caller-owned DEVICE memory of width*height*3 floats on the context's
+ * GPU; it receives the per-pixel mean as pg_render's out_mean does.  desc->accumulate
+ * and desc->profile must be 0.  stats may be NULL; its per-kernel entries stay zero.
+ * The first call on each GPU looks up the array's device address; make that first call
+ * before any stream capture.  All contexts on a GPU share the array: calls that overlap
+ * in time on the same GPU (other host threads, other contexts) race and must be
+ * serialised by the caller. */
+pg_status pg_render_noalloc(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc,
+                            float* mean_device, pg_render_stats* stats);
+
 /* Closest hit for n rays (host arrays).  rays: n x 8 floats (o.xyz, d.xyz, tmin, tmax).
  * Outputs: shape_id (pine shape index, -1 = miss), prim_id (triangle index within the
  * mesh, -1 otherwise), t, uv (n x 2).  Any output may be NULL. */

@@ -163,6 +163,8 @@ def lib():
         "pg_scene_info": (st, [ctypes.c_void_p, ctypes.c_int32, _I32, _I32, _I32, _I32]),
         "pg_render": (st, [ctypes.c_void_p, ctypes.c_int32, _P(RenderDesc), _F, _F, _U32,
                            _P(RenderStats)]),
+        "pg_render_noalloc": (st, [ctypes.c_void_p, ctypes.c_int32, _P(RenderDesc),
+                                   ctypes.c_void_p, _P(RenderStats)]),
         "pg_intersect": (st, [ctypes.c_void_p, ctypes.c_int32, _F, ctypes.c_int64, _I32, _I32,
                               _F, _F]),
         "pg_intersect_device": (st, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,

@@ -1426,3 +1426,163 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
             *chosen = best;
     });
 }
+// ================================================================ allocation-free render
+// pg_render_noalloc: the same wavefront as pg_render, for callers that must not allocate
+// device memory during a render (an application whose GPU memory is owned by its own
+// allocator, or a thread that cannot take the device-wide synchronisation cudaMalloc and
+// cudaFree may imply).  Path slots, shadow queue and the call's film accumulators live in
+// one fixed array of device memory that the library defines; the context's counters, the
+// uploaded scene and the caller's output buffer are used as they are.
+namespace pg {
+
+constexpr int kNoAllocSlots = 1 << 16;       // path slots of the wavefront
+constexpr int64_t kNoAllocPixels = 1 << 19;  // largest film (e.g. 1024 x 512)
+
+constexpr size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Byte offsets of the regions inside the array, each 256-byte aligned.
+struct NoAllocLayout {
+    static constexpr size_t kF4 = (size_t)kNoAllocSlots * sizeof(float4);
+    static constexpr size_t kI = (size_t)kNoAllocSlots * sizeof(int);
+    // ray_o, ray_d, beta, L, hit, so, sd, sc
+    static constexpr size_t float4s = 0;
+    // sample, skey, state, finished, slot_req, lists (2 x slots)
+    static constexpr size_t ints = float4s + 8 * Align256(kF4);
+    static constexpr size_t film = ints + 7 * Align256(kI);
+    static constexpr size_t filmBytes = Align256((size_t)kNoAllocPixels * sizeof(float4));
+    static constexpr size_t request = film + 2 * filmBytes;
+    static constexpr size_t total = request + Align256(sizeof(RequestDev));
+};
+
+// The array: about 26 MiB on every GPU that loads the library, held until the process
+// exits.  All calls on a device share it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
+
+// Device address of the array per device, looked up by the first call on that device.
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[64] = {};
+
+static unsigned char* NoAllocScratch(int device) {
+    Require(device >= 0 && device < 64, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw Failure{PG_ERR_CUDA, std::string("scratch address lookup: ") + cudaGetErrorString(e)};
+        g_noalloc_addr[device] = p;
+    }
+    return static_cast<unsigned char*>(g_noalloc_addr[device]);
+}
+
+__global__ void k_noalloc_mean(const float4* acc, int64_t npix, float* mean) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float4 a = acc[i];
+        float k = a.w;
+        mean[3 * i] = k > 0.0f ? a.x / k : 0.0f;
+        mean[3 * i + 1] = k > 0.0f ? a.y / k : 0.0f;
+        mean[3 * i + 2] = k > 0.0f ? a.z / k : 0.0f;
+    }
+}
+
+static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
+                          int sampleOffset, int mathMode, float* meanDevice, RenderResult& res) {
+    Require(spp > 0 && maxDepth > 0, "spp and max depth must be positive");
+    Require(mathMode == PG_MATH_PINE || mathMode == PG_MATH_FAST, "unknown math mode");
+    Require(sampleOffset >= 0, "sample offset must be >= 0");
+    int64_t npix = (int64_t)sc.width * sc.height;
+    Require(npix <= kNoAllocPixels, "film larger than the 524288 pixels pg_render_noalloc holds");
+    uint64_t total = (uint64_t)npix * (uint64_t)spp;
+    Require(total + (uint64_t)sampleOffset * npix < (1ull << 32),
+            "width*height*(spp+offset) must stay below 2^32 per render call");
+    unsigned char* base = NoAllocScratch(ctx->device);
+    cudaStream_t st = ctx->stream;
+    using L = NoAllocLayout;
+    auto f4 = [&](int k) { return reinterpret_cast<float4*>(base + L::float4s + k * Align256(L::kF4)); };
+    auto i32 = [&](int k) { return reinterpret_cast<int*>(base + L::ints + k * Align256(L::kI)); };
+    float4* acc = reinterpret_cast<float4*>(base + L::film);
+    float4* acc2 = reinterpret_cast<float4*>(base + L::film + L::filmBytes);
+    RequestDev* dReq = reinterpret_cast<RequestDev*>(base + L::request);
+
+    Wave w;
+    w.mode = mathMode;
+    w.surfaces = sc.surfaces;
+    w.fused = ctx->tuning.split_shadow == 0;
+    w.shadeBlock = ctx->tuning.block_size;
+    w.S0 = sc.dev;
+    w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
+    const int slots = (int)std::min<uint64_t>((uint64_t)kNoAllocSlots, total);
+    RenderParams& P = w.P;
+    P.slots = slots;
+    P.total = total;
+    P.ray_o = f4(0), P.ray_d = f4(1), P.beta = f4(2), P.L = f4(3), P.hit = f4(4);
+    P.so = f4(5), P.sd = f4(6), P.sc = f4(7);
+    P.sample = reinterpret_cast<uint32_t*>(i32(0));
+    P.skey = reinterpret_cast<uint32_t*>(i32(1));
+    P.state = i32(2), P.finished = i32(3), P.slot_req = i32(4), P.lists = i32(5);
+    P.counts = ctx->counts;
+    P.film_acc = acc, P.film_acc2 = acc2;
+    P.next_sample = ctx->next_sample;
+    P.stats = ctx->stats;
+    P.err = ctx->err;
+    P.max_iter = (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30);
+    P.reqs = dReq;
+    P.nreq = 1;
+    // What must start at zero: slot states, the film accumulators of this film, counters.
+    PG_CUDA(cudaMemsetAsync(P.state, 0, (size_t)slots * sizeof(int), st));
+    PG_CUDA(cudaMemsetAsync(acc, 0, (size_t)npix * sizeof(float4), st));
+    PG_CUDA(cudaMemsetAsync(acc2, 0, (size_t)npix * sizeof(float4), st));
+    k_iota<<<ctx->num_sms * 4, 256, 0, st>>>(P.finished, slots);
+    PG_CUDA(cudaGetLastError());
+    int c[kNumCounts] = {};
+    c[kCntFinished] = slots;
+    PG_CUDA(cudaMemcpyAsync(ctx->counts, c, sizeof(c), cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
+    PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+    RequestDev rq{};
+    rq.total = (uint32_t)total;
+    rq.npix = (int)npix;
+    rq.width = sc.width;
+    rq.height = sc.height;
+    rq.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
+    rq.key0_offset = (uint32_t)sampleOffset * (uint32_t)npix;
+    rq.max_depth = maxDepth;
+    PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
+    RunHostLoop(ctx, w, false, res);
+    k_noalloc_mean<<<ctx->num_sms * 4, 256, 0, st>>>(acc, npix, meanDevice);
+    PG_CUDA(cudaGetLastError());
+    FinishWave(ctx, res);
+}
+
+}  // namespace pg
+
+extern "C" pg_status pg_render_noalloc(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc,
+                                       float* mean_device, pg_render_stats* stats) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(desc != nullptr && mean_device != nullptr, "null render description or output");
+        Require(desc->guiding == 0, "guided rendering is not available in this build",
+                PG_ERR_UNSUPPORTED);
+        Require(desc->accumulate == 0 && desc->profile == 0,
+                "pg_render_noalloc takes neither accumulate nor profile");
+        PG_CUDA(cudaSetDevice(ctx->device));
+        DeviceScene& sc = GetScene(ctx, scene_id);
+        int spp = desc->spp > 0 ? desc->spp : sc.spp;
+        int md = desc->max_depth > 0 ? desc->max_depth : sc.max_depth;
+        RenderResult r;
+        RenderNoAlloc(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
+                      mean_device, r);
+        if (stats) {
+            *stats = pg_render_stats{};
+            stats->seconds = r.seconds;
+            stats->rays = (int64_t)r.stats[kStatRays];
+            stats->volume_steps = (int64_t)r.stats[kStatSteps];
+            stats->dropped = (int64_t)r.stats[kStatDropped];
+            stats->paths = (int64_t)r.stats[kStatPaths];
+            stats->launches = r.launches;
+        }
+    });
+}
