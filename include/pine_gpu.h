@@ -281,6 +281,48 @@ pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n, pg_tuning*
 pg_status pg_set_tuning(pg_ctx* ctx, const pg_tuning* tuning);
 pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* tuning);
 
+/* ---- neural path guiding (no counterpart in pine, which has no guiding) ----
+ * Each context owns one guiding network: 32 encoded vertex features -> 5 hidden layers of
+ * 64 (ReLU) -> 40 outputs, an 8-lobe von Mises-Fisher mixture over world directions
+ * (per lobe: axis v/|v|, log kappa clamped to [-3, 7], softmax logit).  FP16 weights and
+ * activations on the tensor cores with FP32 accumulation; FP32 master weights and Adam.
+ * pg_render with desc->guiding = 1 trains it online; these entry points expose it.
+ * Weights: PG_GUIDE_WEIGHTS floats, [layer 0..5][output 0..63][input 0..63]; the first
+ * layer reads features 0..31 and a constant 1 at input 32; the last layer writes outputs
+ * 0..39.  Other entries stay zero. */
+#define PG_GUIDE_WEIGHTS (6 * 64 * 64)
+#define PG_GUIDE_FEATURES 32
+#define PG_GUIDE_OUTPUTS 40
+/* Glorot-uniform weights from `seed`, Adam state cleared. */
+pg_status pg_guide_reset(pg_ctx* ctx, uint64_t seed);
+pg_status pg_guide_get_weights(pg_ctx* ctx, float* weights);
+pg_status pg_guide_set_weights(pg_ctx* ctx, const float* weights);
+/* Raw outputs (n x 40) of n feature rows (n x 32), on the GPU. */
+pg_status pg_guide_forward(pg_ctx* ctx, const float* features, int64_t n, float* raw);
+/* Mean gradient over n samples of -w log q(d) with respect to the weights (grad:
+ * PG_GUIDE_WEIGHTS floats), on the GPU; dir_weight: n x 4 (d.xyz unit, w).  *loss
+ * receives the mean loss.  Per-output gradients are clipped to +-1e4. */
+pg_status pg_guide_gradient(pg_ctx* ctx, const float* features, const float* dir_weight,
+                            int64_t n, float* grad, double* loss);
+/* One training step as the renderer takes it: weights divided by their mean, gradient,
+ * Adam (lr, beta1 0.9, beta2 0.99, eps 1e-8). */
+pg_status pg_guide_train_step(pg_ctx* ctx, const float* features, const float* dir_weight,
+                              int64_t n, float lr, double* loss);
+/* Host restatements of the device functions the renderer uses.
+ * Encoding: pos_unit (n x 3, scene bounds mapped to [0,1]^3), normal (n x 3; a NaN x
+ * marks a medium vertex), wo (n x 3) -> features (n x 32). */
+void pg_guide_encode(const float* pos_unit, const float* normal, const float* wo, int64_t n,
+                     float* features);
+/* raw (n x 40) -> lobes (n x 8 x 5: axis xyz, kappa, weight). */
+void pg_guide_mixture(const float* raw, int64_t n, float* lobes);
+/* Mixture density of dirs (n x 3) under raw (n x 40). */
+void pg_guide_pdf(const float* raw, const float* dirs, int64_t n, float* pdf);
+/* Directions drawn from raw's mixture with uniforms u (n x 3). */
+void pg_guide_sample(const float* raw, const float* u, int64_t n, float* dirs);
+/* Per-sample loss -w log q(d) and its gradient with respect to the 40 raw outputs. */
+void pg_guide_loss_grad(const float* raw, const float* dir_weight, int64_t n, float* grad,
+                        float* loss);
+
 /* ---- synthetic scene inputs (seeded) ---- */
 /* n^3 fractal-noise cloud, x fastest; ~nonzero_fraction of voxels > 0; max exactly 1. */
 pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fraction, float* density);

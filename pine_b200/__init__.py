@@ -180,6 +180,19 @@ def lib():
         "pg_pstd_stof": (ctypes.c_float, [ctypes.c_char_p, ctypes.c_int64]),
         "pg_parse_scene_file": (st, [ctypes.c_char_p, _P(SceneDesc), _P(ctypes.c_void_p)]),
         "pg_free_parsed_scene": (None, [ctypes.c_void_p]),
+        "pg_guide_reset": (st, [ctypes.c_void_p, ctypes.c_uint64]),
+        "pg_guide_get_weights": (st, [ctypes.c_void_p, _F]),
+        "pg_guide_set_weights": (st, [ctypes.c_void_p, _F]),
+        "pg_guide_forward": (st, [ctypes.c_void_p, _F, ctypes.c_int64, _F]),
+        "pg_guide_gradient": (st, [ctypes.c_void_p, _F, _F, ctypes.c_int64, _F,
+                                   _P(ctypes.c_double)]),
+        "pg_guide_train_step": (st, [ctypes.c_void_p, _F, _F, ctypes.c_int64, ctypes.c_float,
+                                     _P(ctypes.c_double)]),
+        "pg_guide_encode": (None, [_F, _F, _F, ctypes.c_int64, _F]),
+        "pg_guide_mixture": (None, [_F, ctypes.c_int64, _F]),
+        "pg_guide_pdf": (None, [_F, _F, ctypes.c_int64, _F]),
+        "pg_guide_sample": (None, [_F, _F, ctypes.c_int64, _F]),
+        "pg_guide_loss_grad": (None, [_F, _F, ctypes.c_int64, _F, _F]),
     }
     for name, (res, args) in sig.items():
         if hasattr(L, name):
@@ -198,6 +211,54 @@ def lib():
 
 def _fptr(a):
     return None if a is None else a.ctypes.data_as(_F)
+
+
+GUIDE_WEIGHTS = 6 * 64 * 64
+GUIDE_FEATURES = 32
+GUIDE_OUTPUTS = 40
+
+
+def _f32(a, cols):
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1, cols)
+
+
+def guide_encode(pos_unit, normal, wo):
+    """Features (n x 32) of path vertices; a NaN normal marks a medium vertex."""
+    p, nn, w = _f32(pos_unit, 3), _f32(normal, 3), _f32(wo, 3)
+    out = np.empty((p.shape[0], GUIDE_FEATURES), np.float32)
+    lib().pg_guide_encode(_fptr(p), _fptr(nn), _fptr(w), p.shape[0], _fptr(out))
+    return out
+
+
+def guide_mixture(raw):
+    """Lobes (n x 8 x 5: axis xyz, kappa, weight) of raw network outputs (n x 40)."""
+    r = _f32(raw, GUIDE_OUTPUTS)
+    out = np.empty((r.shape[0], 8, 5), np.float32)
+    lib().pg_guide_mixture(_fptr(r), r.shape[0], _fptr(out))
+    return out
+
+
+def guide_pdf(raw, dirs):
+    r, d = _f32(raw, GUIDE_OUTPUTS), _f32(dirs, 3)
+    out = np.empty(r.shape[0], np.float32)
+    lib().pg_guide_pdf(_fptr(r), _fptr(d), r.shape[0], _fptr(out))
+    return out
+
+
+def guide_sample(raw, u):
+    r, uu = _f32(raw, GUIDE_OUTPUTS), _f32(u, 3)
+    out = np.empty((r.shape[0], 3), np.float32)
+    lib().pg_guide_sample(_fptr(r), _fptr(uu), r.shape[0], _fptr(out))
+    return out
+
+
+def guide_loss_grad(raw, dir_weight):
+    """Per-sample loss -w log q(d) and its gradient with respect to the raw outputs."""
+    r, dw = _f32(raw, GUIDE_OUTPUTS), _f32(dir_weight, 4)
+    g = np.empty_like(r)
+    loss = np.empty(r.shape[0], np.float32)
+    lib().pg_guide_loss_grad(_fptr(r), _fptr(dw), r.shape[0], _fptr(g), _fptr(loss))
+    return loss, g
 
 
 class ParsedScene:
@@ -312,6 +373,40 @@ class Context:
                                            sid.ctypes.data_as(_I32), pid.ctypes.data_as(_I32),
                                            _fptr(t), _fptr(uv)))
         return sid, pid, t, uv
+
+    # ---- guiding network
+    def guide_reset(self, seed: int = 0):
+        self._check(self._lib.pg_guide_reset(self._ctx, int(seed)))
+
+    def guide_weights(self) -> np.ndarray:
+        w = np.empty((6, 64, 64), np.float32)
+        self._check(self._lib.pg_guide_get_weights(self._ctx, _fptr(w)))
+        return w
+
+    def set_guide_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32).reshape(6, 64, 64)
+        self._check(self._lib.pg_guide_set_weights(self._ctx, _fptr(w)))
+
+    def guide_forward(self, features) -> np.ndarray:
+        f = _f32(features, GUIDE_FEATURES)
+        out = np.empty((f.shape[0], GUIDE_OUTPUTS), np.float32)
+        self._check(self._lib.pg_guide_forward(self._ctx, _fptr(f), f.shape[0], _fptr(out)))
+        return out
+
+    def guide_gradient(self, features, dir_weight):
+        f, dw = _f32(features, GUIDE_FEATURES), _f32(dir_weight, 4)
+        g = np.empty((6, 64, 64), np.float32)
+        loss = ctypes.c_double()
+        self._check(self._lib.pg_guide_gradient(self._ctx, _fptr(f), _fptr(dw), f.shape[0],
+                                                _fptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def guide_train_step(self, features, dir_weight, lr: float = 1e-2) -> float:
+        f, dw = _f32(features, GUIDE_FEATURES), _f32(dir_weight, 4)
+        loss = ctypes.c_double()
+        self._check(self._lib.pg_guide_train_step(self._ctx, _fptr(f), _fptr(dw), f.shape[0],
+                                                  float(lr), ctypes.byref(loss)))
+        return loss.value
 
     # ---- tuning and batches
     def tuning(self) -> dict:

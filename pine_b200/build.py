@@ -20,9 +20,10 @@ LIB = os.path.join(HERE, "libpinegpu.so")
 CLI = os.path.join(HERE, "pine-gpu")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["pine_gpu.cu", "batch.cu", "scene_load.cpp", "bvh_build.cpp", "scenegen.cpp"]
+SOURCES = ["pine_gpu.cu", "guide_mlp.cu", "batch.cu", "scene_load.cpp", "bvh_build.cpp",
+           "scenegen.cpp"]
 HEADERS = ["pg_math.h", "pg_device.cuh", "pg_shade.cuh", "pg_kernels.cuh", "scene_load.h",
-           "bvh_build.h"]
+           "bvh_build.h", "guide_net.cuh", "guide_mlp.h"]
 
 
 def _nvcc() -> str:

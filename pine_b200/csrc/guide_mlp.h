@@ -1,0 +1,53 @@
+// Host interface of the guiding network's GPU kernels (guide_mlp.cu): inference,
+// gradient of the training loss, and the Adam step.  All device buffers are owned by the
+// caller (pg_ctx); every launch goes to the given stream.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pg {
+
+struct GuideNetDev {
+    __half* w16 = nullptr;      // FP16 weights in the kernels' shared-memory image (48 KiB)
+    float* w32 = nullptr;       // FP32 master weights [6][64][64], rows = outputs
+    float* adam_m = nullptr;    // Adam first and second moments, same layout
+    float* adam_v = nullptr;
+    float* grad = nullptr;      // mean gradient of the last step, same layout
+    float* partial = nullptr;   // per-block gradient sums [blocks][6][64][64]
+    float* loss = nullptr;      // loss sum of the last gradient pass
+    float* wsum = nullptr;      // sum of the sample weights of a batch
+    uint32_t* err = nullptr;    // bit 0: a tensor-core wait timed out
+    int blocks = 0;             // blocks of the gradient kernel (partial rows)
+    int step = 0;               // Adam steps taken
+};
+
+// Device memory a GuideNetDev needs for `blocks` gradient blocks.
+size_t GuideNetBytes(int blocks);
+// Points the fields at `mem` (GuideNetBytes(blocks) bytes, 256-byte aligned).
+void GuideNetBind(GuideNetDev& net, void* mem, int blocks);
+
+// Rebuilds the FP16 image from the FP32 master weights.
+cudaError_t GuidePack(const GuideNetDev& net, cudaStream_t st);
+
+// Raw network outputs (n x 40 FP32) for n rows of 64 FP16 features (128-byte rows).
+cudaError_t GuideForward(const GuideNetDev& net, const __half* feat, int64_t n, float* out,
+                         int sms, cudaStream_t st);
+
+// Mean over the n rows of the gradient of -weight * log q(dir) with respect to the FP32
+// weights (net.grad) and the loss sum (net.loss).  dirw: n x float4 (dir.xyz, weight);
+// weights are divided by `weightScale` first.  Per-output gradients are clipped to
+// +-kGuideGradClip before the FP16 backward pass.
+cudaError_t GuideGradient(GuideNetDev& net, const __half* feat, const float4* dirw, int64_t n,
+                          float weightScale, cudaStream_t st);
+
+// Sum of the n sample weights (dirw[i].w) into net.wsum.
+cudaError_t GuideWeightSum(GuideNetDev& net, const float4* dirw, int64_t n, cudaStream_t st);
+
+// One Adam step (beta1 0.9, beta2 0.99, eps 1e-8) from net.grad, then GuidePack.
+cudaError_t GuideAdam(GuideNetDev& net, float lr, cudaStream_t st);
+
+constexpr float kGuideGradClip = 1.0e4f;
+
+}  // namespace pg

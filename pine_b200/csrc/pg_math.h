@@ -10,12 +10,13 @@
 
 #include <stdint.h>
 
+#include <cmath>
+#include <cstring>
+
 #ifdef __CUDACC__
 #define PG_HD __host__ __device__ __forceinline__
 #else
 #define PG_HD inline
-#include <cmath>
-#include <cstring>
 #endif
 
 namespace pg {

@@ -14,6 +14,8 @@
 #include <vector>
 
 #include "bvh_build.h"
+#include "guide_mlp.h"
+#include "guide_net.cuh"
 #include "pg_kernels.cuh"
 #include "pine_gpu.h"
 #include "scene_load.h"
@@ -164,6 +166,8 @@ struct pg_ctx {
     std::string last_error;
     pg_tuning tuning{1 << 21, 64, 1, 64};
     int num_sms = 148;
+    pg::DevMem guide_mem;                  // guiding network (allocated on first use)
+    pg::GuideNetDev guide;
 };
 
 namespace pg {
@@ -1585,4 +1589,222 @@ extern "C" pg_status pg_render_noalloc(pg_ctx* ctx, int32_t scene_id, const pg_r
             stats->launches = r.launches;
         }
     });
+}
+
+// ================================================================ guiding network
+namespace pg {
+
+// Allocates the context's guiding network on first use (Glorot-uniform weights, seed 0).
+static GuideNetDev& EnsureGuide(pg_ctx* ctx);
+
+static void GuideInit(pg_ctx* ctx, uint64_t seed) {
+    GuideNetDev& g = ctx->guide;
+    std::vector<float> w(kGuideWeights, 0.0f);
+    for (int l = 0; l < kGuideLayers; l++) {
+        int fanIn = l == 0 ? kGuideFeatures + 1 : kGuideDim;
+        int fanOut = l == kGuideLayers - 1 ? kGuideOutputs : kGuideDim;
+        float lim = std::sqrt(6.0f / (float)(fanIn + fanOut));
+        for (int o = 0; o < fanOut; o++)
+            for (int i = 0; i < fanIn; i++) {
+                uint32_t idx = (uint32_t)((l * kGuideDim + o) * kGuideDim + i);
+                uint32_t h = PcgHashHost(PcgHashHost(idx ^ (uint32_t)seed) ^ (uint32_t)(seed >> 32) ^
+                                         0x85ebca6bu);
+                float u = (float)(h >> 8) * (1.0f / 16777216.0f);
+                w[idx] = (2.0f * u - 1.0f) * lim;
+            }
+    }
+    cudaStream_t st = ctx->stream;
+    PG_CUDA(cudaMemcpyAsync(g.w32, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaMemsetAsync(g.adam_m, 0, kGuideWeights * sizeof(float), st));
+    PG_CUDA(cudaMemsetAsync(g.adam_v, 0, kGuideWeights * sizeof(float), st));
+    PG_CUDA(cudaMemsetAsync(g.err, 0, sizeof(uint32_t), st));
+    PG_CUDA(GuidePack(g, st));
+    g.step = 0;
+}
+
+static GuideNetDev& EnsureGuide(pg_ctx* ctx) {
+    if (!ctx->guide.w16) {
+        void* mem = ctx->guide_mem.Alloc<uint8_t>(GuideNetBytes(ctx->num_sms));
+        GuideNetBind(ctx->guide, mem, ctx->num_sms);
+        GuideInit(ctx, 0);
+    }
+    return ctx->guide;
+}
+
+// Host feature rows (n x 32 FP32) -> device rows of 64 FP16 with the constant input.
+static __half* UploadFeatures(pg_ctx* ctx, DevMem& mem, const float* f, int64_t n) {
+    std::vector<__half> rows((size_t)n * kGuideDim, __float2half(0.0f));
+    for (int64_t r = 0; r < n; r++) {
+        for (int i = 0; i < kGuideFeatures; i++)
+            rows[(size_t)r * kGuideDim + i] = __float2half(f[r * kGuideFeatures + i]);
+        rows[(size_t)r * kGuideDim + kGuideFeatures] = __float2half(1.0f);
+    }
+    return mem.Upload(rows, ctx->stream);
+}
+
+static void CheckGuideErr(pg_ctx* ctx) {
+    uint32_t e = 0;
+    PG_CUDA(cudaMemcpy(&e, ctx->guide.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e)
+        throw Failure{PG_ERR_DEVICE_LIMIT, "guiding network: a tensor-core wait timed out"};
+}
+
+static void GuideGradientHost(pg_ctx* ctx, const float* features, const float* dw, int64_t n,
+                              bool normalise, DevMem& tmp, double& loss) {
+    GuideNetDev& g = EnsureGuide(ctx);
+    cudaStream_t st = ctx->stream;
+    __half* feat = UploadFeatures(ctx, tmp, features, n);
+    std::vector<float> h(dw, dw + 4 * n);
+    float4* dirw = reinterpret_cast<float4*>(tmp.Upload(h, st));
+    float scale = 1.0f;
+    if (normalise) {
+        double s = 0;
+        for (int64_t i = 0; i < n; i++)
+            s += dw[4 * i + 3];
+        scale = s > 0 ? (float)(s / (double)n) : 1.0f;
+    }
+    PG_CUDA(GuideGradient(g, feat, dirw, n, scale, st));
+    float ls = 0;
+    PG_CUDA(cudaMemcpyAsync(&ls, g.loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+    PG_CUDA(cudaStreamSynchronize(st));
+    CheckGuideErr(ctx);
+    loss = n > 0 ? ls / (double)n : 0.0;
+}
+
+}  // namespace pg
+
+extern "C" pg_status pg_guide_reset(pg_ctx* ctx, uint64_t seed) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        EnsureGuide(ctx);
+        GuideInit(ctx, seed);
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" pg_status pg_guide_get_weights(pg_ctx* ctx, float* weights) {
+    if (!ctx || !weights)
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or output"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        GuideNetDev& g = EnsureGuide(ctx);
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        PG_CUDA(cudaMemcpy(weights, g.w32, kGuideWeights * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" pg_status pg_guide_set_weights(pg_ctx* ctx, const float* weights) {
+    if (!ctx || !weights)
+        return Fail(ctx, Failure{PG_ERR_INVALID_ARG, "null context or input"});
+    return Guard(ctx, [&]() {
+        PG_CUDA(cudaSetDevice(ctx->device));
+        GuideNetDev& g = EnsureGuide(ctx);
+        PG_CUDA(cudaMemcpyAsync(g.w32, weights, kGuideWeights * sizeof(float),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        PG_CUDA(GuidePack(g, ctx->stream));
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" pg_status pg_guide_forward(pg_ctx* ctx, const float* features, int64_t n, float* raw) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(n >= 0 && (n == 0 || (features && raw)), "bad feature or output arrays");
+        PG_CUDA(cudaSetDevice(ctx->device));
+        GuideNetDev& g = EnsureGuide(ctx);
+        if (n == 0)
+            return;
+        DevMem tmp;
+        __half* feat = UploadFeatures(ctx, tmp, features, n);
+        float* out = tmp.Alloc<float>((size_t)n * kGuideOutputs);
+        PG_CUDA(GuideForward(g, feat, n, out, ctx->num_sms, ctx->stream));
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        CheckGuideErr(ctx);
+        PG_CUDA(cudaMemcpy(raw, out, (size_t)n * kGuideOutputs * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" pg_status pg_guide_gradient(pg_ctx* ctx, const float* features, const float* dir_weight,
+                                       int64_t n, float* grad, double* loss) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(n > 0 && features && dir_weight && grad, "bad arrays");
+        PG_CUDA(cudaSetDevice(ctx->device));
+        DevMem tmp;
+        double l = 0;
+        GuideGradientHost(ctx, features, dir_weight, n, false, tmp, l);
+        PG_CUDA(cudaMemcpy(grad, ctx->guide.grad, kGuideWeights * sizeof(float), cudaMemcpyDeviceToHost));
+        if (loss)
+            *loss = l;
+    });
+}
+
+extern "C" pg_status pg_guide_train_step(pg_ctx* ctx, const float* features, const float* dir_weight,
+                                         int64_t n, float lr, double* loss) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(n > 0 && features && dir_weight, "bad arrays");
+        Require(lr > 0 && lr < 1, "learning rate out of range");
+        PG_CUDA(cudaSetDevice(ctx->device));
+        DevMem tmp;
+        double l = 0;
+        GuideGradientHost(ctx, features, dir_weight, n, true, tmp, l);
+        PG_CUDA(GuideAdam(ctx->guide, lr, ctx->stream));
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (loss)
+            *loss = l;
+    });
+}
+
+extern "C" void pg_guide_encode(const float* pos_unit, const float* normal, const float* wo,
+                                int64_t n, float* features) {
+    for (int64_t i = 0; i < n; i++) {
+        const float* p = pos_unit + 3 * i;
+        const float* nn = normal + 3 * i;
+        const float* w = wo + 3 * i;
+        GuideEncode(v3(p[0], p[1], p[2]), v3(nn[0], nn[1], nn[2]), !std::isnan(nn[0]),
+                    v3(w[0], w[1], w[2]), features + kGuideFeatures * i);
+    }
+}
+
+extern "C" void pg_guide_mixture(const float* raw, int64_t n, float* lobes) {
+    for (int64_t i = 0; i < n; i++) {
+        VmfLobe l[kGuideLobes];
+        GuideMixture(raw + kGuideOutputs * i, l);
+        for (int k = 0; k < kGuideLobes; k++) {
+            float* o = lobes + (i * kGuideLobes + k) * 5;
+            o[0] = l[k].mu.x, o[1] = l[k].mu.y, o[2] = l[k].mu.z, o[3] = l[k].kappa, o[4] = l[k].weight;
+        }
+    }
+}
+
+extern "C" void pg_guide_pdf(const float* raw, const float* dirs, int64_t n, float* pdf) {
+    for (int64_t i = 0; i < n; i++) {
+        VmfLobe l[kGuideLobes];
+        GuideMixture(raw + kGuideOutputs * i, l);
+        pdf[i] = GuidePdf(l, v3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+    }
+}
+
+extern "C" void pg_guide_sample(const float* raw, const float* u, int64_t n, float* dirs) {
+    for (int64_t i = 0; i < n; i++) {
+        VmfLobe l[kGuideLobes];
+        GuideMixture(raw + kGuideOutputs * i, l);
+        V3 d = GuideSample(l, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+        dirs[3 * i] = d.x, dirs[3 * i + 1] = d.y, dirs[3 * i + 2] = d.z;
+    }
+}
+
+extern "C" void pg_guide_loss_grad(const float* raw, const float* dir_weight, int64_t n, float* grad,
+                                   float* loss) {
+    for (int64_t i = 0; i < n; i++) {
+        const float* d = dir_weight + 4 * i;
+        loss[i] = GuideLossGrad(raw + kGuideOutputs * i, v3(d[0], d[1], d[2]), d[3], 1.0f,
+                                grad + kGuideOutputs * i);
+    }
 }
