@@ -165,9 +165,11 @@ typedef struct pg_render_desc {
                                totals in pg_render_stats.kernels) */
 } pg_render_desc;
 
-/* Kernels of the wavefront loop, in pg_render_stats.kernels order. */
+/* Kernels of the wavefront loop, in pg_render_stats.kernels order.  GUIDE (network
+ * inference and guided direction sampling) and TRAIN (gradient and Adam between passes)
+ * run only in guided renders. */
 enum { PG_KERNEL_REGEN = 0, PG_KERNEL_TRACE = 1, PG_KERNEL_SHADE = 2, PG_KERNEL_SHADOW = 3,
-       PG_NUM_KERNELS = 4 };
+       PG_KERNEL_GUIDE = 4, PG_KERNEL_TRAIN = 5, PG_NUM_KERNELS = 6 };
 
 typedef struct pg_kernel_stats {
     int64_t launches;

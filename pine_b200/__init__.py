@@ -39,7 +39,7 @@ class RenderDesc(ctypes.Structure):
                 ("accumulate", ctypes.c_int32), ("profile", ctypes.c_int32)]
 
 
-KERNELS = ["regen", "trace", "shade", "shadow"]
+KERNELS = ["regen", "trace", "shade", "shadow", "guide", "train"]
 
 
 class KernelStats(ctypes.Structure):
@@ -52,7 +52,7 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("seconds", ctypes.c_double), ("paths", ctypes.c_int64),
                 ("rays", ctypes.c_int64), ("volume_steps", ctypes.c_int64),
                 ("dropped", ctypes.c_int64), ("launches", ctypes.c_int64),
-                ("kernels", KernelStats * 4)]
+                ("kernels", KernelStats * 6)]
 
     def to_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "kernels"}

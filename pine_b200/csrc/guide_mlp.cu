@@ -203,6 +203,34 @@ __device__ __forceinline__ void Teardown(uint64_t* bar, uint32_t phase, bool abo
     }
 }
 
+// Writes input row `row` (tile row r) into a swizzled block: a copied FP16 feature row, or
+// the encoding of a path vertex.  Rows past the end are zero.
+__device__ __forceinline__ void LoadInputRow(const GuideInput& in, int64_t row, bool valid,
+                                             uint8_t* blk, uint32_t r) {
+    if (!in.vert) {
+        const uint4 z = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            *reinterpret_cast<uint4*>(blk + SwzOff(r, c)) = valid ? in.feat[row * 8 + c] : z;
+        return;
+    }
+    float f[kGuideDim];
+#pragma unroll
+    for (int i = 0; i < kGuideDim; i++)
+        f[i] = 0.0f;
+    if (valid) {
+        const float4* v = in.vert + row * in.stride;
+        float4 p = v[0], n = v[1], w = v[2];
+        V3 pu = v3((p.x - in.lo[0]) * in.inv[0], (p.y - in.lo[1]) * in.inv[1],
+                   (p.z - in.lo[2]) * in.inv[2]);
+        GuideEncode(pu, v3(n.x, n.y, n.z), !isnan(n.x), v3(w.x, w.y, w.z), f);
+        f[kGuideFeatures] = 1.0f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        StoreRow16(blk, r, q, f + 16 * q);
+}
+
 // Issues D[tmem] = A(128 x 64, K-major block) * B(64 x 64 weights, K-major)^T.
 __device__ __forceinline__ void IssueForward(uint32_t tmem, const uint8_t* act, const uint8_t* w) {
     uint32_t a = SmemU32(act), b = SmemU32(w);
@@ -214,7 +242,7 @@ __device__ __forceinline__ void IssueForward(uint32_t tmem, const uint8_t* act, 
 
 // ---------------------------------------------------------------- inference
 __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict__ w16,
-                                                       const uint4* __restrict__ feat, int64_t n,
+                                                       GuideInput in, int64_t nMax,
                                                        float* __restrict__ out, uint32_t* err) {
     extern __shared__ uint8_t smemRaw[];
     __shared__ uint64_t bar;
@@ -229,13 +257,11 @@ __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict_
     const uint32_t tmem = tmemSlot;
     const uint32_t lane = tmem + ((uint32_t)(warp * 32) << 16);
     uint32_t phase = 0;
+    const int64_t n = in.count ? min((int64_t)*in.count, nMax) : nMax;
     const int64_t tiles = (n + kTileRows - 1) / kTileRows;
     for (int64_t t = blockIdx.x; t < tiles && !abortFlag; t += gridDim.x) {
         const int64_t row = t * kTileRows + tid;
-        const uint4 z = make_uint4(0, 0, 0, 0);
-#pragma unroll
-        for (int c = 0; c < 8; c++)
-            *reinterpret_cast<uint4*>(sA[0] + SwzOff(tid, c)) = row < n ? feat[row * 8 + c] : z;
+        LoadInputRow(in, row, row < n, sA[0], tid);
         FenceProxyAsync();
         FenceBefore();
         __syncthreads();
@@ -289,7 +315,7 @@ __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict_
 
 // ---------------------------------------------------------------- training gradient
 __global__ void __launch_bounds__(128, 1) k_guide_grad(const __half* __restrict__ w16,
-                                                       const uint4* __restrict__ feat,
+                                                       GuideInput in,
                                                        const float4* __restrict__ dirw, int64_t n,
                                                        float invWeightScale,
                                                        float* __restrict__ partial,
@@ -318,10 +344,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_grad(const __half* __restrict_
     const int64_t tiles = (n + kTileRows - 1) / kTileRows;
     for (int64_t t = blockIdx.x; t < tiles && !abortFlag; t += gridDim.x) {
         const int64_t row = t * kTileRows + tid;
-        const uint4 z = make_uint4(0, 0, 0, 0);
-#pragma unroll
-        for (int c = 0; c < 8; c++)
-            *reinterpret_cast<uint4*>(sH + SwzOff(tid, c)) = row < n ? feat[row * 8 + c] : z;
+        LoadInputRow(in, row, row < n, sH, tid);
         const float4 dw = row < n ? dirw[row] : make_float4(0.0f, 0.0f, 1.0f, 0.0f);
         FenceProxyAsync();
         FenceBefore();
@@ -532,7 +555,7 @@ cudaError_t GuidePack(const GuideNetDev& net, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t GuideForward(const GuideNetDev& net, const __half* feat, int64_t n, float* out,
+cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n, float* out,
                          int sms, cudaStream_t st) {
     if (n <= 0)
         return cudaSuccess;
@@ -542,12 +565,11 @@ cudaError_t GuideForward(const GuideNetDev& net, const __half* feat, int64_t n, 
         return e;
     int64_t tiles = (n + kTileRows - 1) / kTileRows;
     int grid = (int)std::min<int64_t>(tiles, (int64_t)sms * 2);
-    k_guide_forward<<<grid, 128, kFwdSmem, st>>>(net.w16, reinterpret_cast<const uint4*>(feat), n,
-                                                 out, net.err);
+    k_guide_forward<<<grid, 128, kFwdSmem, st>>>(net.w16, in, n, out, net.err);
     return cudaGetLastError();
 }
 
-cudaError_t GuideGradient(GuideNetDev& net, const __half* feat, const float4* dirw, int64_t n,
+cudaError_t GuideGradient(GuideNetDev& net, const GuideInput& in, const float4* dirw, int64_t n,
                           float weightScale, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_guide_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kTrainSmem);
@@ -555,9 +577,8 @@ cudaError_t GuideGradient(GuideNetDev& net, const __half* feat, const float4* di
         return e;
     if ((e = cudaMemsetAsync(net.loss, 0, sizeof(float), st)) != cudaSuccess)
         return e;
-    k_guide_grad<<<net.blocks, 128, kTrainSmem, st>>>(net.w16, reinterpret_cast<const uint4*>(feat),
-                                                      dirw, n, 1.0f / weightScale, net.partial,
-                                                      net.loss, net.err);
+    k_guide_grad<<<net.blocks, 128, kTrainSmem, st>>>(net.w16, in, dirw, n, 1.0f / weightScale,
+                                                      net.partial, net.loss, net.err);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     k_guide_reduce<<<48, 512, 0, st>>>(net.partial, net.blocks, n > 0 ? 1.0f / (float)n : 0.0f,

@@ -23,6 +23,16 @@ struct GuideNetDev {
     int step = 0;               // Adam steps taken
 };
 
+// Rows the kernels read: FP16 feature rows, or path vertices they encode themselves.
+struct GuideInput {
+    const uint4* feat = nullptr;    // n rows of 64 FP16 (128 bytes): features, 1, zeros
+    const float4* vert = nullptr;   // or `stride` float4 per row: position (world),
+    int stride = 3;                 // normal (NaN x: a medium vertex), outgoing direction
+    float lo[3] = {0, 0, 0};        // position -> [0,1]^3: (p - lo) * inv
+    float inv[3] = {1, 1, 1};
+    const int* count = nullptr;     // device row count; when set it replaces the host n
+};
+
 // Device memory a GuideNetDev needs for `blocks` gradient blocks.
 size_t GuideNetBytes(int blocks);
 // Points the fields at `mem` (GuideNetBytes(blocks) bytes, 256-byte aligned).
@@ -31,15 +41,16 @@ void GuideNetBind(GuideNetDev& net, void* mem, int blocks);
 // Rebuilds the FP16 image from the FP32 master weights.
 cudaError_t GuidePack(const GuideNetDev& net, cudaStream_t st);
 
-// Raw network outputs (n x 40 FP32) for n rows of 64 FP16 features (128-byte rows).
-cudaError_t GuideForward(const GuideNetDev& net, const __half* feat, int64_t n, float* out,
+// Raw network outputs (n x 40 FP32) of n input rows.  With in.count the grid is sized for
+// up to `n` rows and the kernel reads the actual count on the device.
+cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n, float* out,
                          int sms, cudaStream_t st);
 
 // Mean over the n rows of the gradient of -weight * log q(dir) with respect to the FP32
 // weights (net.grad) and the loss sum (net.loss).  dirw: n x float4 (dir.xyz, weight);
 // weights are divided by `weightScale` first.  Per-output gradients are clipped to
 // +-kGuideGradClip before the FP16 backward pass.
-cudaError_t GuideGradient(GuideNetDev& net, const __half* feat, const float4* dirw, int64_t n,
+cudaError_t GuideGradient(GuideNetDev& net, const GuideInput& in, const float4* dirw, int64_t n,
                           float weightScale, cudaStream_t st);
 
 // Sum of the n sample weights (dirw[i].w) into net.wsum.

@@ -99,6 +99,8 @@ struct SceneDev {
     int num_media;
     int has_null_surfaces;
     CameraDev cam;
+    float guide_lo[3];       // scene bounds the guiding network's position encoding maps
+    float guide_inv[3];      // to [0,1]^3: lo and 1 / extent
 };
 
 // Error flags written by kernels (bitmask), converted to pg_status on the host.

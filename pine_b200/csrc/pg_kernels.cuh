@@ -23,6 +23,7 @@
 // its request, whose scene, film region, sample range and seed it uses.
 #pragma once
 
+#include "guide_net.cuh"
 #include "pg_shade.cuh"
 
 // Build-time register cap of the shading kernel.  Measured on B200 (volume benchmark):
@@ -46,14 +47,27 @@ enum StatIndex {
     kStatRays = 0, kStatSteps, kStatDropped, kStatPaths,
     kStatShadeItems, kStatShadeSteps, kStatShadeBricks,
     kStatShadowItems, kStatShadowSteps, kStatShadowBricks,
-    kStatTraceItems, kStatRegenItems, kStatIterations, kNumStats = 16
+    kStatTraceItems, kStatRegenItems, kStatIterations, kStatGuided, kStatRecords,
+    kStatTrainRows, kNumStats = 16
 };
 
 enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlotDead = 3 };
 
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
-                  kCntIter = 5, kNumCounts = 8 };
+                  kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kNumCounts = 8 };
+
+// Guided rendering.  A guide-queue entry (kGuideEntry float4) holds a vertex whose next
+// direction waits for the network: position + slot, normal (NaN x in a medium) +
+// material or medium, incident direction wi (towards the previous vertex) + shadow-queue
+// index of its pending shadow ray, the media on either side of a surface.
+// A training record (kRecordStride float4) holds position + the path's previous record,
+// normal, wi, the throughput before the vertex and the radiance the path had gathered
+// after the vertex (set at its next vertex; w = 1 while still unknown); rec_dirw holds the
+// sampled direction and, once the path has ended, the target weight
+// lum((L_end - L_base) / beta).
+constexpr int kGuideEntry = 4;
+constexpr int kRecordStride = 5;
 
 struct RequestDev {
     unsigned long long sample_begin;  // first global sample id of this request
@@ -96,6 +110,14 @@ struct RenderParams {
     int max_iter;
     int use_cond;                // k_swap sets the graph while-condition
     cudaGraphConditionalHandle cond;
+    // Guided rendering only.
+    float4* gq;                  // guide queue, kGuideEntry float4 per entry
+    const float* graw;           // network outputs per guide entry (kGuideOutputs floats)
+    float4* rec;                 // training records, kRecordStride float4 each
+    float4* rec_dirw;            // per record: sampled direction, target weight
+    int* rec_last;               // per slot: newest record of its path, -1 none
+    int rec_cap;
+    float rec_accept;            // probability of recording a continuing guided vertex
 };
 
 __device__ __forceinline__ int WarpAppend(int* counter, bool pred) {
@@ -254,6 +276,29 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
     }
 }
 
+// Sets the target weight of every training record of the path in slot i, whose radiance
+// ended at L (valid = false for a dropped sample: targets 0), and clears its record list.
+__device__ void FinalizeRecords(const RenderParams& P, int i, V3 L, bool valid) {
+    int r = P.rec_last[i];
+    for (int k = 0; k < 65536 && r >= 0; k++) {
+        float4 a = P.rec[kRecordStride * r], bt = P.rec[kRecordStride * r + 3],
+               b = P.rec[kRecordStride * r + 4];
+        V3 base = b.w != 0.0f ? L : v3(b.x, b.y, b.z);
+        float t = 0.0f;
+        if (valid) {
+            V3 d = L - base;
+            V3 q = v3(bt.x > 0 ? d.x / bt.x : 0.0f, bt.y > 0 ? d.y / bt.y : 0.0f,
+                      bt.z > 0 ? d.z / bt.z : 0.0f);
+            t = Max(Luminance(q), 0.0f);
+            if (!isfinite(t))
+                t = 0.0f;
+        }
+        reinterpret_cast<float*>(&P.rec_dirw[r])[3] = t;
+        r = __float_as_int(a.w);
+    }
+    P.rec_last[i] = -1;
+}
+
 // Starts camera sample `id` in slot i (RadianceIntegrator::Compute + ThinLenCamera::GenRay,
 // integrator.cpp:152-158, camera.cpp:31-41).
 template <int M, bool MULTI>
@@ -341,6 +386,7 @@ __global__ void k_swap(RenderParams P) {
     c[kCntNext] = 0;
     c[kCntFinished] = 0;
     c[kCntShadow] = 0;
+    c[kCntGuide] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
     bool more = active > 0;
@@ -557,11 +603,40 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
     return c;
 }
 
-template <int M, bool FUSED>
+// Whether a surface vertex samples its next direction with the guiding network: a single
+// diffuse layer, or a single conductor layer that is not near-specular.
+__device__ __forceinline__ bool GuideEligible(const MaterialDev& m) {
+    if (m.type != PG_MATERIAL_LAYERED || m.num_layers != 1)
+        return false;
+    const BsdfDev& b = m.layers[0];
+    return b.type == PG_BSDF_DIFFUSE || (b.type == PG_BSDF_CONDUCTOR && b.alpha >= 0.05f);
+}
+
+// Queues a vertex for the network (guide queue, see kGuideEntry).
+__device__ __forceinline__ void PushGuide(const RenderParams& P, int slot, V3 p, V3 n, bool surface,
+                                          int id, V3 wi, int shadowIdx, int medIn, int medOut) {
+    int q = WarpAppend(&P.counts[kCntGuide], true);
+    float nx = surface ? n.x : __int_as_float(0x7fc00000);
+    P.gq[kGuideEntry * q] = make_float4(p.x, p.y, p.z, __int_as_float(slot));
+    P.gq[kGuideEntry * q + 1] = make_float4(nx, n.y, n.z, __int_as_float(id));
+    P.gq[kGuideEntry * q + 2] = make_float4(wi.x, wi.y, wi.z, __int_as_float(shadowIdx));
+    P.gq[kGuideEntry * q + 3] =
+        make_float4(__int_as_float((medIn + 1) | ((medOut + 1) << 16)), 0.0f, 0.0f, 0.0f);
+}
+
+template <int M, bool FUSED, bool GUIDE>
 __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
                          uint2* stack, ShadeCounters& ct, PendingShadow& ps, bool& finished,
-                         V3& Lout) {
+                         V3& Lout, bool& deferred) {
     float4 ro = P.ray_o[i], rd = P.ray_d[i], bt = P.beta[i], Lw = P.L[i];
+    deferred = false;
+    if (GUIDE) {
+        // The radiance gathered after the previous guided vertex (its shadow ray included)
+        // is known now: the base of that vertex's training record.
+        int r = P.rec_last[i];
+        if (r >= 0 && P.rec[kRecordStride * r + 4].w != 0.0f)
+            P.rec[kRecordStride * r + 4] = make_float4(Lw.x, Lw.y, Lw.z, 0.0f);
+    }
     // Scenes without surfaces skip k_trace: every ray misses.
     float4 h = (S.has_bvh || S.num_planes) ? P.hit[i]
                                            : make_float4(kFloatMax, __int_as_float(-1), 0.0f, 0.0f);
@@ -593,14 +668,19 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             const MediumDev& m = S.media[medium];
             NextEvent<M, FUSED>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
                                 m.g, medium, medium, beta, L, stack, ct, ps);
-            float u0, u1;
-            rng.Get2D(u0, u1);
-            V3 wo;
-            bsdfPdf = PhaseSample<M>(m.g, -d, wo, u0, u1);
-            no = ev.p;
-            nd = wo;
-            nmed = medium;
-            depth++;
+            if (GUIDE) {
+                PushGuide(P, i, ev.p, v3(0.0f), false, medium, -d, ps.idx, medium, medium);
+                deferred = true;
+            } else {
+                float u0, u1;
+                rng.Get2D(u0, u1);
+                V3 wo;
+                bsdfPdf = PhaseSample<M>(m.g, -d, wo, u0, u1);
+                no = ev.p;
+                nd = wo;
+                nmed = medium;
+                depth++;
+            }
         }
     } else if (!found) {
         // Escape (path.cpp:29-40).
@@ -644,38 +724,48 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
                 fr.From(si.n);
                 NextEvent<M, FUSED>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
                                     medIn, medOut, beta, L, stack, ct, ps);
-                float u1 = rng.Get1D(), u20, u21;
-                rng.Get2D(u20, u21);
-                BsdfSample bs;
-                V3 wi = fr.ToLocal(-d);
-                bool ok = MaterialSample<M>(mat, wi, u1, u20, u21, bs);
-                if (ok) {
-                    bs.wo = fr.ToWorld(bs.wo);
-                    if (IsBlack(bs.f) || bs.pdf == 0.0f)
-                        ok = false;
-                }
-                if (!ok) {
-                    finished = true;
+                if (GUIDE && GuideEligible(mat)) {
+                    PushGuide(P, i, si.p, si.n, true, sh.material, -d, ps.idx, medIn, medOut);
+                    deferred = true;
                 } else {
-                    beta *= bs.f * (AbsDot(bs.wo, si.n) / bs.pdf);
-                    bsdfPdf = bs.pdf;
-                    no = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, bs.wo));
-                    nd = bs.wo;
-                    nmed = Dot(bs.wo, si.n) > 0 ? medOut : medIn;
-                    if (depth > 2) {  // Russian roulette (path.cpp:74-80)
-                        float qrr = Clamp(1.0f - Luminance(beta), 0.05f, 1.0f);
-                        if (rng.Get1D() < qrr)
-                            finished = true;
-                        else
-                            beta = beta / (1.0f - qrr);
+                    float u1 = rng.Get1D(), u20, u21;
+                    rng.Get2D(u20, u21);
+                    BsdfSample bs;
+                    V3 wi = fr.ToLocal(-d);
+                    bool ok = MaterialSample<M>(mat, wi, u1, u20, u21, bs);
+                    if (ok) {
+                        bs.wo = fr.ToWorld(bs.wo);
+                        if (IsBlack(bs.f) || bs.pdf == 0.0f)
+                            ok = false;
                     }
-                    depth++;
+                    if (!ok) {
+                        finished = true;
+                    } else {
+                        beta *= bs.f * (AbsDot(bs.wo, si.n) / bs.pdf);
+                        bsdfPdf = bs.pdf;
+                        no = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, bs.wo));
+                        nd = bs.wo;
+                        nmed = Dot(bs.wo, si.n) > 0 ? medOut : medIn;
+                        if (depth > 2) {  // Russian roulette (path.cpp:74-80)
+                            float qrr = Clamp(1.0f - Luminance(beta), 0.05f, 1.0f);
+                            if (rng.Get1D() < qrr)
+                                finished = true;
+                            else
+                                beta = beta / (1.0f - qrr);
+                        }
+                        depth++;
+                    }
                 }
             }
         }
     }
     P.L[i] = make_float4(L.x, L.y, L.z, __uint_as_float(rng.dim));
     Lout = L;
+    if (deferred) {
+        // k_guide_sample picks the next direction; the throughput here is the vertex's.
+        P.beta[i] = make_float4(beta.x, beta.y, beta.z, __int_as_float(depth));
+        return;
+    }
     if (finished) {
         P.state[i] = kSlotFinished;
         if (ps.idx >= 0)
@@ -687,7 +777,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     }
 }
 
-template <int M, bool MULTI, bool FUSED>
+template <int M, bool MULTI, bool FUSED, bool GUIDE = false>
 __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -703,15 +793,20 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
         bool live = q < n, finished = true;
         int i = live ? active[q] : 0;
         V3 L;
+        bool deferred = false;
         if (live)
-            ShadeOne<M, FUSED>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
-                               stack + threadIdx.x, ct, ps, finished, L);
+            ShadeOne<M, FUSED, GUIDE>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
+                                      stack + threadIdx.x, ct, ps, finished, L, deferred);
         // A path that ends here with no shadow ray in flight is flushed now and its slot
         // takes the next camera sample; one with a shadow ray pending ends in k_shadow.
-        bool endHere = live && finished && ps.idx < 0;
+        // A deferred path (guided) continues in k_guide_sample.
+        bool endHere = live && finished && !deferred && ps.idx < 0;
         uint32_t dropped = 0;
-        if (endHere)
+        if (endHere) {
             FlushPath<MULTI>(P, i, L, dropped);
+            if (GUIDE)
+                FinalizeRecords(P, i, L, Finite(L));
+        }
         unsigned long long id = BlockClaim(P, endHere, claimOff, &claimBase);
         bool spawned = id != ~0ull;
         if (spawned)
@@ -719,13 +814,15 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
         else if (endHere)
             P.state[i] = kSlotDead;
         int* const ctr[1] = {&P.counts[kCntNext]};
-        const bool pr[1] = {(live && !finished) || spawned};
+        const bool pr[1] = {(live && !finished && !deferred) || spawned};
         int sl[1];
         BlockAppend<1>(ctr, pr, sl, q1);
         if (sl[0] >= 0)
             next[sl[0]] = i;
         if (ct.err)
             atomicOr(P.err, ct.err);
+        if (GUIDE)
+            WarpAdd(&P.stats[kStatGuided], deferred ? 1u : 0u);
         WarpAdd(&P.stats[kStatSteps], ct.steps + ct.shadowSteps);
         WarpAdd(&P.stats[kStatShadeSteps], ct.steps + ct.shadowSteps);
         WarpAdd(&P.stats[kStatShadeBricks], ct.bricks + ct.shadowBricks);
@@ -736,7 +833,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     }
 }
 
-template <int M, bool MULTI>
+template <int M, bool MULTI, bool GUIDE = false>
 __global__ void k_shadow(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -761,9 +858,11 @@ __global__ void k_shadow(RenderParams P, SceneDev S0) {
                                 bricks, err, traced);
             float4 Lw = P.L[slot];
             V3 L = v3(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z);
-            if (last)
+            if (last) {
                 FlushPath<MULTI>(P, slot, L, dropped);
-            else if (!IsBlack(tr))
+                if (GUIDE)
+                    FinalizeRecords(P, slot, L, Finite(L));
+            } else if (!IsBlack(tr))
                 P.L[slot] = make_float4(L.x, L.y, L.z, Lw.w);
             if (err)
                 atomicOr(P.err, err);
@@ -787,6 +886,162 @@ __global__ void k_shadow(RenderParams P, SceneDev S0) {
         WarpAdd(&P.stats[kStatShadowBricks], bricks);
         WarpAdd(&P.stats[kStatShadowItems], q < n ? 1u : 0u);
         WarpAdd(&P.stats[kStatPaths], last ? 1u : 0u);
+        WarpAdd(&P.stats[kStatDropped], dropped);
+    }
+}
+
+// Guided direction sampling for the vertices in the guide queue, from the network's
+// mixture (graw) and the BSDF or phase function, one-sample MIS at fraction 0.5: a
+// direction w drawn from either has density pc = 0.5 pdf_bsdf(w) + 0.5 q(w) and weight
+// f(w) |cos| / pc (surfaces) or phase(w) / pc (media).  The MIS weights the path uses
+// later against light sampling stay those of the plain path tracer (functions of
+// pdf_bsdf), and directions the BSDF sampler cannot produce carry zero weight, so the
+// guided estimator has the plain one's expectation.  Continuing vertices may be recorded
+// for training (probability rec_accept).
+template <int M>
+__device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& slot, bool& cont,
+                         bool& endNow, V3& Lend, uint32_t& recorded) {
+    const float4 g0 = P.gq[kGuideEntry * q], g1 = P.gq[kGuideEntry * q + 1],
+                 g2 = P.gq[kGuideEntry * q + 2], g3 = P.gq[kGuideEntry * q + 3];
+    const int i = __float_as_int(g0.w);
+    slot = i;
+    const RequestDev& R = P.reqs[0];
+    const V3 p = v3(g0.x, g0.y, g0.z), n = v3(g1.x, g1.y, g1.z), wi = v3(g2.x, g2.y, g2.z);
+    const bool surface = !isnan(g1.x);
+    const int id = __float_as_int(g1.w), shadowIdx = __float_as_int(g2.w);
+    const int packed = __float_as_int(g3.x);
+    const int medIn = (packed & 0xffff) - 1, medOut = ((packed >> 16) & 0xffff) - 1;
+    const float4 bt = P.beta[i], Lw = P.L[i];
+    V3 beta = v3(bt.x, bt.y, bt.z);
+    int depth = __float_as_int(bt.w);
+    Rng rng{P.sample[i], R.key1, __float_as_uint(Lw.w)};
+    VmfLobe lobes[kGuideLobes];
+    GuideMixture(P.graw + (size_t)kGuideOutputs * q, lobes);
+    const float uSel = rng.Get1D();
+    V3 w = v3(0.0f, 0.0f, 1.0f), f = v3(0.0f);
+    float pdfB = 0.0f;
+    bool ok;
+    if (surface) {
+        const MaterialDev& mat = S.materials[id];
+        Frame<M> fr;
+        fr.From(n);
+        V3 wiL = fr.ToLocal(wi);
+        if (uSel < 0.5f) {
+            float u1 = rng.Get1D(), u20, u21;
+            rng.Get2D(u20, u21);
+            BsdfSample bs;
+            ok = MaterialSample<M>(mat, wiL, u1, u20, u21, bs);
+            if (ok) {
+                w = fr.ToWorld(bs.wo);
+                f = bs.f;
+                pdfB = bs.pdf;
+            }
+        } else {
+            float u0 = rng.Get1D(), u1, u2;
+            rng.Get2D(u1, u2);
+            w = GuideSample(lobes, u0, u1, u2);
+            MaterialEval<M>(mat, wiL, fr.ToLocal(w), f, pdfB);
+            ok = true;
+        }
+        ok = ok && !IsBlack(f) && pdfB > 0.0f;
+    } else {
+        const MediumDev& m = S.media[id];
+        if (uSel < 0.5f) {
+            float u0, u1;
+            rng.Get2D(u0, u1);
+            pdfB = PhaseSample<M>(m.g, wi, w, u0, u1);
+        } else {
+            float u0 = rng.Get1D(), u1, u2;
+            rng.Get2D(u1, u2);
+            w = GuideSample(lobes, u0, u1, u2);
+            pdfB = PhaseHG<M>(Dot(wi, w), m.g);
+        }
+        f = v3(pdfB);
+        ok = pdfB > 0.0f;
+    }
+    const float pc = ok ? 0.5f * pdfB + 0.5f * GuidePdf(lobes, w) : 0.0f;
+    bool finished = !(pc > 0.0f) || !isfinite(pc);
+    const V3 betaVertex = beta;
+    if (!finished) {
+        beta *= surface ? f * (AbsDot(w, n) / pc) : f / pc;
+        if (surface && depth > 2) {  // Russian roulette (path.cpp:74-80)
+            float qrr = Clamp(1.0f - Luminance(beta), 0.05f, 1.0f);
+            if (rng.Get1D() < qrr)
+                finished = true;
+            else
+                beta = beta / (1.0f - qrr);
+        }
+        depth++;
+    }
+    P.L[i] = make_float4(Lw.x, Lw.y, Lw.z, __uint_as_float(rng.dim));
+    if (!finished) {
+        V3 no = surface ? OffsetRayOrigin(p, FaceSameHemisphere(n, w)) : p;
+        int nmed = surface ? (Dot(w, n) > 0 ? medOut : medIn) : id;
+        P.ray_o[i] = make_float4(no.x, no.y, no.z, pdfB);
+        P.ray_d[i] = make_float4(w.x, w.y, w.z, __int_as_float(nmed));
+        P.beta[i] = make_float4(beta.x, beta.y, beta.z, __int_as_float(depth));
+        cont = true;
+        // Training record, with a per-vertex coin independent of the path's stream.
+        float coin = (float)(PcgHash(P.sample[i] * 0x9e3779b9u ^ PcgHash(rng.dim ^ R.key1)) >> 8) *
+                     (1.0f / 16777216.0f);
+        if (coin < P.rec_accept) {
+            int r = atomicAdd(&P.counts[kCntRecords], 1);
+            if (r < P.rec_cap) {
+                float4* rr = P.rec + (size_t)kRecordStride * r;
+                rr[0] = make_float4(p.x, p.y, p.z, __int_as_float(P.rec_last[i]));
+                rr[1] = make_float4(g1.x, n.y, n.z, 0.0f);
+                rr[2] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                rr[3] = make_float4(betaVertex.x, betaVertex.y, betaVertex.z, 0.0f);
+                rr[4] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                P.rec_dirw[r] = make_float4(w.x, w.y, w.z, 0.0f);
+                P.rec_last[i] = r;
+                recorded++;
+            }
+        }
+        return;
+    }
+    P.state[i] = kSlotFinished;
+    if (shadowIdx >= 0) {
+        reinterpret_cast<uint32_t*>(&P.sc[shadowIdx])[3] = (uint32_t)i | kFinalShadow;
+    } else {
+        endNow = true;
+        Lend = v3(Lw.x, Lw.y, Lw.z);
+    }
+}
+
+template <int M>
+__global__ void k_guide_sample(RenderParams P, SceneDev S0) {
+    __shared__ BlockQueues<1> q1;
+    __shared__ int claimOff[32];
+    __shared__ unsigned long long claimBase;
+    const int n = P.counts[kCntGuide];
+    int* next = NextList(P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
+         q += gridDim.x * blockDim.x) {
+        int slot = 0;
+        bool cont = false, endNow = false;
+        V3 Lend = v3(0.0f);
+        uint32_t recorded = 0, dropped = 0;
+        if (q < n)
+            GuideOne<M>(P, S0, q, slot, cont, endNow, Lend, recorded);
+        if (endNow) {
+            FlushPath<false>(P, slot, Lend, dropped);
+            FinalizeRecords(P, slot, Lend, Finite(Lend));
+        }
+        unsigned long long id = BlockClaim(P, endNow, claimOff, &claimBase);
+        bool spawned = id != ~0ull;
+        if (spawned)
+            SpawnPath<M, false>(P, S0, slot, id);
+        else if (endNow)
+            P.state[slot] = kSlotDead;
+        int* const ctr[1] = {&P.counts[kCntNext]};
+        const bool pr[1] = {cont || spawned};
+        int sl[1];
+        BlockAppend<1>(ctr, pr, sl, q1);
+        if (sl[0] >= 0)
+            next[sl[0]] = slot;
+        WarpAdd(&P.stats[kStatRecords], recorded);
+        WarpAdd(&P.stats[kStatPaths], endNow ? 1u : 0u);
         WarpAdd(&P.stats[kStatDropped], dropped);
     }
 }

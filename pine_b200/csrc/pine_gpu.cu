@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -125,6 +126,33 @@ struct Pool {
     }
 };
 
+// Guided rendering: the guide queue, the network outputs per entry, and the training
+// records with their per-slot lists.
+constexpr int kRecordCap = 1 << 20;     // training records per pass
+constexpr int kTrainBatch = 1 << 18;    // records per Adam step
+constexpr float kGuideLr = 1e-2f;
+
+struct GuidePool {
+    DevMem mem;
+    int slots = 0;
+    float4* gq = nullptr;
+    float* graw = nullptr;
+    int* rec_last = nullptr;
+    float4* rec = nullptr;
+    float4* rec_dirw = nullptr;
+    void Ensure(int n) {
+        if (n <= slots)
+            return;
+        mem.Free();
+        slots = n;
+        gq = mem.Alloc<float4>((size_t)kGuideEntry * n);
+        graw = mem.Alloc<float>((size_t)kGuideOutputs * n);
+        rec_last = mem.Alloc<int>(n);
+        rec = mem.Alloc<float4>((size_t)kRecordStride * kRecordCap);
+        rec_dirw = mem.Alloc<float4>(kRecordCap);
+    }
+};
+
 struct Film {
     DevMem mem;
     int64_t npix = 0;
@@ -168,6 +196,7 @@ struct pg_ctx {
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
+    pg::GuidePool guide_pool;              // guided-render queues and training records
 };
 
 namespace pg {
@@ -515,6 +544,33 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         }
     }
     Require((int64_t)boxes.size() < (1ll << 30), "too many primitives");
+    // Bounds of the guiding network's position encoding: primitives (planes excluded) and
+    // grid media; a box around the camera when there is neither.
+    {
+        float lo[3] = {kFloatMax, kFloatMax, kFloatMax}, hi[3] = {-kFloatMax, -kFloatMax, -kFloatMax};
+        auto grow = [&](V3 p) {
+            for (int k = 0; k < 3; k++)
+                lo[k] = std::min(lo[k], Comp(p, k)), hi[k] = std::max(hi[k], Comp(p, k));
+        };
+        for (const Box& b : boxes)
+            grow(v3(b.lo[0], b.lo[1], b.lo[2])), grow(v3(b.hi[0], b.hi[1], b.hi[2]));
+        for (const MediumDev& m : media)
+            if (m.type == PG_MEDIUM_GRID)
+                for (int c = 0; c < 8; c++) {
+                    float u[3] = {(float)(c & 1), (float)((c >> 1) & 1), (float)(c >> 2)}, w[3];
+                    for (int k = 0; k < 3; k++)
+                        w[k] = m.m2w[4 * k] * u[0] + m.m2w[4 * k + 1] * u[1] + m.m2w[4 * k + 2] * u[2] +
+                               m.m2w[4 * k + 3];
+                    grow(v3(w[0], w[1], w[2]));
+                }
+        if (lo[0] > hi[0])
+            for (int k = 0; k < 3; k++)
+                lo[k] = cam.from[k] - 1.0f, hi[k] = cam.from[k] + 1.0f;
+        for (int k = 0; k < 3; k++) {
+            S.guide_lo[k] = lo[k];
+            S.guide_inv[k] = 1.0f / std::max(hi[k] - lo[k], 1e-3f);
+        }
+    }
     WideBVH bvh = BuildWideBVH(boxes);
     sc->prims = (int64_t)boxes.size();
     sc->bvh_depth = bvh.max_depth;
@@ -688,7 +744,7 @@ __global__ void k_timestamp(unsigned long long* t) {
 struct Wave {
     RenderParams P{};
     SceneDev S0{};
-    bool multi = false, surfaces = false, fused = false;
+    bool multi = false, surfaces = false, fused = false, guide = false;
     int mode = PG_MATH_FAST;
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
@@ -747,8 +803,60 @@ static void LaunchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* 
         res->kernelLaunches[PG_KERNEL_REGEN]++;
 }
 
+// One guided iteration: trace, shade (guided vertices queued), network inference over the
+// queue (row count read on the device), guided sampling, shadow rays, swap.
+template <int M, bool FUSED>
+static void LaunchGuidedBody(pg_ctx* ctx, Wave& w, int n, LaunchTimer* timer, RenderResult* res) {
+    cudaStream_t st = ctx->stream;
+    const int sms = ctx->num_sms;
+    const int tb = 128;
+    auto grid = [&](int block, int perSm) { return std::max(1, std::min(Ceil(n, block), sms * perSm * 8)); };
+    auto time = [&](int k, auto&& f) {
+        if (timer)
+            timer->Time(k, f);
+        else
+            f();
+        if (res)
+            res->kernelLaunches[k]++;
+    };
+    if (w.surfaces)
+        time(PG_KERNEL_TRACE, [&]() {
+            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+    const size_t shadeSmem = FUSED ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    if (FUSED && shadeSmem > 48 * 1024)
+        PG_CUDA(cudaFuncSetAttribute(k_shade<M, false, FUSED, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shadeSmem));
+    time(PG_KERNEL_SHADE, [&]() {
+        k_shade<M, false, FUSED, true><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem,
+                                         st>>>(w.P, w.S0);
+    });
+    time(PG_KERNEL_GUIDE, [&]() {
+        GuideInput in;
+        in.vert = w.P.gq;
+        in.stride = kGuideEntry;
+        for (int k = 0; k < 3; k++)
+            in.lo[k] = w.S0.guide_lo[k], in.inv[k] = w.S0.guide_inv[k];
+        in.count = &w.P.counts[kCntGuide];
+        PG_CUDA(GuideForward(ctx->guide, in, n, const_cast<float*>(w.P.graw), sms, st));
+        k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(w.P, w.S0);
+    });
+    if (!FUSED)
+        time(PG_KERNEL_SHADOW, [&]() {
+            k_shadow<M, false, true><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
+}
+
 template <int M, bool MULTI>
 static void Body(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer, RenderResult* res) {
+    if (!MULTI && w.guide) {
+        if (w.fused)
+            LaunchGuidedBody<M, true>(ctx, w, n, timer, res);
+        else
+            LaunchGuidedBody<M, false>(ctx, w, n, timer, res);
+        return;
+    }
     if (w.fused)
         LaunchBody<M, MULTI, true>(ctx, w, n, persistent, timer, res);
     else
@@ -800,6 +908,14 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
     PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
     PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+    if (w.guide) {
+        GuidePool& gp = ctx->guide_pool;
+        gp.Ensure(slots);
+        P.gq = gp.gq, P.graw = gp.graw, P.rec = gp.rec, P.rec_dirw = gp.rec_dirw;
+        P.rec_last = gp.rec_last;
+        P.rec_cap = kRecordCap;
+        PG_CUDA(cudaMemsetAsync(gp.rec_last, 0xff, (size_t)slots * sizeof(int), st));
+    }
 }
 
 // Host-driven loop: the active count is read back after each k_swap so that every launch
@@ -926,7 +1042,7 @@ static int64_t IterationCap(uint64_t total, int slots, int maxDepth) {
 
 static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
                        int sampleOffset, int mathMode, bool accumulate, bool profile,
-                       RenderResult& res) {
+                       RenderResult& res, const float* recordAccept = nullptr) {
     Require(spp > 0 && maxDepth > 0, "spp and max depth must be positive");
     Require(mathMode == PG_MATH_PINE || mathMode == PG_MATH_FAST, "unknown math mode");
     Require(sampleOffset >= 0, "sample offset must be >= 0");
@@ -948,6 +1064,9 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
+    w.guide = recordAccept != nullptr;
+    if (w.guide)
+        w.P.rec_accept = *recordAccept;
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
     PrepareWave(ctx, w, slots, total, (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30));
     RequestDev rq{};
@@ -1129,6 +1248,98 @@ extern "C" pg_status pg_scene_info(pg_ctx* ctx, int32_t scene_id, int32_t* width
     });
 }
 
+namespace pg {
+
+static GuideNetDev& EnsureGuide(pg_ctx* ctx);
+
+// Adam steps on the records of the last guided pass, up to kTrainBatch records each, sample
+// weights normalised by their batch mean: one step per kTrainBatch records, and at least
+// kMinTrainSteps (cycling through the records) when a pass records fewer.  Returns the
+// rows trained on.
+constexpr int kMinTrainSteps = 4, kMaxTrainSteps = 16;
+
+static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec) {
+    GuideNetDev& net = ctx->guide;
+    GuidePool& gp = ctx->guide_pool;
+    cudaStream_t st = ctx->stream;
+    int64_t rows = 0;
+    if (nrec < 1024)
+        return 0;
+    int64_t steps = std::min<int64_t>(
+        kMaxTrainSteps, std::max<int64_t>(kMinTrainSteps, (nrec + kTrainBatch - 1) / kTrainBatch));
+    for (int64_t k = 0; k < steps; k++) {
+        int64_t b = (k * kTrainBatch) % nrec;
+        int64_t nb = std::min<int64_t>(kTrainBatch, nrec - b);
+        if (nb < 1024)
+            b = 0, nb = std::min<int64_t>(kTrainBatch, nrec);
+        PG_CUDA(GuideWeightSum(net, gp.rec_dirw + b, nb, st));
+        float wsum = 0.0f;
+        PG_CUDA(cudaMemcpyAsync(&wsum, net.wsum, sizeof(float), cudaMemcpyDeviceToHost, st));
+        PG_CUDA(cudaStreamSynchronize(st));
+        if (!(wsum > 0.0f) || !std::isfinite(wsum))
+            continue;
+        GuideInput in;
+        in.vert = gp.rec + (size_t)kRecordStride * b;
+        in.stride = kRecordStride;
+        for (int c = 0; c < 3; c++)
+            in.lo[c] = sc.dev.guide_lo[c], in.inv[c] = sc.dev.guide_inv[c];
+        PG_CUDA(GuideGradient(net, in, gp.rec_dirw + b, nb, wsum / (float)nb, st));
+        PG_CUDA(GuideAdam(net, kGuideLr, st));
+        rows += nb;
+    }
+    PG_CUDA(cudaStreamSynchronize(st));
+    uint32_t e = 0;
+    PG_CUDA(cudaMemcpy(&e, net.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e)
+        throw Failure{PG_ERR_DEVICE_LIMIT, "guiding network: a tensor-core wait timed out"};
+    return rows;
+}
+
+// Guided render: progressive passes of 1, 1, 2, 4, ... samples per pixel (the last one
+// truncated), each rendered with the network as trained so far and followed, except the
+// last, by training on the pass's records.  Every pass is an unbiased estimate given its
+// network, so their sum is too.  The network stays in the context for later calls.
+static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
+                         int sampleOffset, int mathMode, bool accumulate, bool profile,
+                         RenderResult& res) {
+    EnsureGuide(ctx);
+    float accept = 1.0f;
+    int done = 0, passSpp = 1;
+    while (done < spp) {
+        int sp = std::min(passSpp, spp - done);
+        RenderResult r;
+        RenderFilm(ctx, sc, sp, maxDepth, seed, sampleOffset + done, mathMode, accumulate || done > 0,
+                   profile, r, &accept);
+        res.seconds += r.seconds;
+        for (int k = 0; k < kNumStats; k++)
+            res.stats[k] += r.stats[k];
+        for (int k = 0; k < PG_NUM_KERNELS; k++) {
+            res.kernelLaunches[k] += r.kernelLaunches[k];
+            res.kernelSeconds[k] += r.kernelSeconds[k];
+        }
+        res.launches += r.launches;
+        done += sp;
+        if (done < spp) {
+            int nrec = 0;
+            PG_CUDA(cudaMemcpy(&nrec, ctx->counts + kCntRecords, sizeof(int), cudaMemcpyDeviceToHost));
+            auto t0 = std::chrono::steady_clock::now();
+            int64_t rows = TrainOnRecords(ctx, sc, std::min(nrec, kRecordCap));
+            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            res.stats[kStatTrainRows] += (unsigned long long)rows;
+            res.kernelSeconds[PG_KERNEL_TRAIN] += dt;
+            res.kernelLaunches[PG_KERNEL_TRAIN] += rows > 0 ? 4 * std::max<int64_t>(1, rows / kTrainBatch) : 0;
+            res.seconds += dt;
+            // Record about kRecordCap vertices in the next pass.
+            double perSpp = (double)r.stats[kStatGuided] / sp;
+            int next = std::min(passSpp * 2, spp - done);
+            accept = perSpp > 0 ? (float)std::min(1.0, kRecordCap / (perSpp * next)) : 1.0f;
+        }
+        passSpp *= 2;
+    }
+}
+
+}  // namespace pg
+
 extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc,
                                float* out_mean, float* out_var, uint32_t* out_count,
                                pg_render_stats* stats) {
@@ -1137,15 +1348,17 @@ extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_de
     return Guard(ctx, [&]() {
         Require(desc != nullptr, "null render description");
         Require(desc->guiding == 0 || desc->guiding == 1, "guiding must be 0 or 1");
-        Require(desc->guiding == 0, "guided rendering is not available in this build",
-                PG_ERR_UNSUPPORTED);
         PG_CUDA(cudaSetDevice(ctx->device));
         DeviceScene& sc = GetScene(ctx, scene_id);
         int spp = desc->spp > 0 ? desc->spp : sc.spp;
         int md = desc->max_depth > 0 ? desc->max_depth : sc.max_depth;
         RenderResult r;
-        RenderFilm(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
-                   desc->accumulate != 0, desc->profile != 0, r);
+        if (desc->guiding)
+            RenderGuided(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
+                         desc->accumulate != 0, desc->profile != 0, r);
+        else
+            RenderFilm(ctx, sc, spp, md, desc->seed, desc->sample_offset, desc->math_mode,
+                       desc->accumulate != 0, desc->profile != 0, r);
         ReadFilm(ctx, (int64_t)sc.width * sc.height, out_mean, out_var, out_count);
         if (stats) {
             stats->seconds = r.seconds;
@@ -1155,9 +1368,9 @@ extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_de
             stats->paths = (int64_t)r.stats[kStatPaths];
             stats->launches = r.launches;
             const int items[PG_NUM_KERNELS] = {kStatRegenItems, kStatTraceItems, kStatShadeItems,
-                                               kStatShadowItems};
-            const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps};
-            const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks};
+                                               kStatShadowItems, kStatGuided, kStatTrainRows};
+            const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps, -1, -1};
+            const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks, -1, -1};
             for (int k = 0; k < PG_NUM_KERNELS; k++) {
                 pg_kernel_stats& ks = stats->kernels[k];
                 ks.launches = r.kernelLaunches[k];
@@ -1568,7 +1781,7 @@ extern "C" pg_status pg_render_noalloc(pg_ctx* ctx, int32_t scene_id, const pg_r
         return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
     return Guard(ctx, [&]() {
         Require(desc != nullptr && mean_device != nullptr, "null render description or output");
-        Require(desc->guiding == 0, "guided rendering is not available in this build",
+        Require(desc->guiding == 0, "pg_render_noalloc does not render guided",
                 PG_ERR_UNSUPPORTED);
         Require(desc->accumulate == 0 && desc->profile == 0,
                 "pg_render_noalloc takes neither accumulate nor profile");
@@ -1653,7 +1866,8 @@ static void GuideGradientHost(pg_ctx* ctx, const float* features, const float* d
                               bool normalise, DevMem& tmp, double& loss) {
     GuideNetDev& g = EnsureGuide(ctx);
     cudaStream_t st = ctx->stream;
-    __half* feat = UploadFeatures(ctx, tmp, features, n);
+    GuideInput in;
+    in.feat = reinterpret_cast<const uint4*>(UploadFeatures(ctx, tmp, features, n));
     std::vector<float> h(dw, dw + 4 * n);
     float4* dirw = reinterpret_cast<float4*>(tmp.Upload(h, st));
     float scale = 1.0f;
@@ -1663,7 +1877,7 @@ static void GuideGradientHost(pg_ctx* ctx, const float* features, const float* d
             s += dw[4 * i + 3];
         scale = s > 0 ? (float)(s / (double)n) : 1.0f;
     }
-    PG_CUDA(GuideGradient(g, feat, dirw, n, scale, st));
+    PG_CUDA(GuideGradient(g, in, dirw, n, scale, st));
     float ls = 0;
     PG_CUDA(cudaMemcpyAsync(&ls, g.loss, sizeof(float), cudaMemcpyDeviceToHost, st));
     PG_CUDA(cudaStreamSynchronize(st));
@@ -1718,9 +1932,10 @@ extern "C" pg_status pg_guide_forward(pg_ctx* ctx, const float* features, int64_
         if (n == 0)
             return;
         DevMem tmp;
-        __half* feat = UploadFeatures(ctx, tmp, features, n);
+        GuideInput in;
+        in.feat = reinterpret_cast<const uint4*>(UploadFeatures(ctx, tmp, features, n));
         float* out = tmp.Alloc<float>((size_t)n * kGuideOutputs);
-        PG_CUDA(GuideForward(g, feat, n, out, ctx->num_sms, ctx->stream));
+        PG_CUDA(GuideForward(g, in, n, out, ctx->num_sms, ctx->stream));
         PG_CUDA(cudaStreamSynchronize(ctx->stream));
         CheckGuideErr(ctx);
         PG_CUDA(cudaMemcpy(raw, out, (size_t)n * kGuideOutputs * sizeof(float), cudaMemcpyDeviceToHost));
