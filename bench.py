@@ -68,6 +68,15 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="render the small ncu case once and print its per-kernel counters")
+    ap.add_argument("--guiding-eval", action="store_true",
+                    help="time to RMSE <= --rmse-target against a plain reference, guided vs "
+                         "plain, on --workload (one GPU; prints its own JSON line)")
+    ap.add_argument("--rmse-target", type=float, default=1e-2)
+    ap.add_argument("--ref-spp", type=int, default=65536)
+    ap.add_argument("--guide-size", type=int, nargs=2, default=None, metavar=("W", "H"),
+                    help="film size of the guiding evaluation (default: the workload's)")
+    ap.add_argument("--guide-time-limit", type=float, default=90.0,
+                    help="seconds of render time per method before extrapolating")
     return ap.parse_args()
 
 
@@ -293,6 +302,10 @@ def main():
         return reduce_max(x, dist, f"cuda:{local}")
 
     env = "constant" if cfg["kind"] != "mesh" else "none"
+    if args.guiding_eval:
+        if rank == 0:
+            print(json.dumps(guiding_eval(args, cfg, env)))
+        return 0
     if args.profile_case:
         path = scene_path(PROFILE_CASE, args.cache, "constant")
         ctx = pb.Context(local)
@@ -414,6 +427,87 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def guiding_eval(args, cfg, env):
+    """Time for the plain and the guided estimator to reach an RMSE target against a
+    high-spp plain reference (the reference is rendered once per cache directory).
+
+    Each method renders a progressive sequence (16 spp, then doubling the total) into an
+    accumulating film, and its RMSE against the reference is measured after every call.
+    Time is the render calls' device time, training included for the guided method.  The
+    reference's own noise (mean per-pixel sample variance / its spp) is a floor under the
+    measured MSE.  The time at which a method crosses the target is interpolated (or, past
+    the time limit, extrapolated) from its last two points with MSE - floor falling as
+    1 / time, so that the doubling steps do not quantise it."""
+    import pine_b200 as pb
+    size = tuple(args.guide_size) if args.guide_size else (cfg["width"], cfg["height"])
+    path = scene_path(cfg, args.cache, env, size=size)
+    ctx = pb.Context(0)
+    sid = ctx.load_scene(path)
+    info = ctx.scene_info(sid)
+    # Sample ids of one call stay below 2^32 (pg_render); longer renders accumulate calls
+    # with independent seeds.
+    npix = info["width"] * info["height"]
+    max_call = 1 << int(np.log2(max(1, ((1 << 32) - 1) // npix)))
+    ref_file = os.path.join(args.cache, f"ref_{os.path.basename(path)}_{args.ref_spp}_{args.math}.npz")
+    if os.path.exists(ref_file):
+        z = np.load(ref_file)
+        ref, ref_var = z["mean"], z["var"]
+    else:
+        done, k = 0, 0
+        while done < args.ref_spp:
+            sp = min(max_call, args.ref_spp - done)
+            r = ctx.render(sid, spp=sp, seed=7770 + k, accumulate=done > 0, math_mode=args.math)
+            done += sp
+            k += 1
+        ref, ref_var = r["mean"], r["var"]
+        np.savez(ref_file, mean=ref, var=ref_var)
+    floor = float(ref_var.mean()) / args.ref_spp
+    target2 = args.rmse_target ** 2
+    out = {"metric": f"time to RMSE <= {args.rmse_target:g} against a {args.ref_spp}-spp plain "
+                     "reference (s)",
+           "workload": f"{args.workload}: " + describe(cfg) + f" at {size[0]}x{size[1]}",
+           "math_mode": args.math,
+           "reference": {"spp": args.ref_spp, "rmse_floor": floor ** 0.5}}
+    for method in ("plain", "guided"):
+        guided = method == "guided"
+        if guided:
+            ctx.guide_reset(seed=0)
+        t, done, chunk, curve, k = 0.0, 0, 16, [], 0
+        reached = False
+        while True:
+            left = chunk
+            while left > 0:
+                sp = min(left, max_call)
+                r = ctx.render(sid, spp=sp, seed=(1100 if guided else 1200) + k,
+                               accumulate=done > 0, math_mode=args.math, guiding=guided)
+                t += r["stats"]["seconds"]
+                done += sp
+                left -= sp
+                k += 1
+            mse = float(np.mean((r["mean"] - ref) ** 2))
+            curve.append({"spp": done, "seconds": round(t, 4), "rmse": mse ** 0.5,
+                          "sample_variance": float(r["var"].mean())})
+            if mse <= target2:
+                reached = True
+                break
+            if t >= args.guide_time_limit or done >= args.ref_spp:
+                break
+            chunk = done
+        # MSE - floor falls as 1 / time: the crossing of the target is interpolated from the
+        # last two measured points (one point when the first call already reached it).
+        tail = [c for c in curve[-2:] if c["rmse"] ** 2 > floor]
+        if target2 > floor and tail:
+            cst = sum((c["rmse"] ** 2 - floor) * c["seconds"] for c in tail) / len(tail)
+            t_target = cst / (target2 - floor)
+        else:
+            t_target = t if reached else None
+        out[method] = {"seconds": t_target, "reached": reached, "curve": curve}
+    tp, tg = out["plain"]["seconds"], out["guided"]["seconds"]
+    out["guided_over_plain"] = tg / tp if tp and tg else None
+    ctx.close()
+    return out
 
 
 def reduce_max(x, dist, device):

@@ -159,7 +159,11 @@ typedef struct pg_render_desc {
     int32_t math_mode;      /* PG_MATH_PINE reproduces pine's pstd numerics
                                (src/pstd/math.h); PG_MATH_FAST uses CUDA intrinsics */
     int32_t guiding;        /* 1: MIS-combine the learned vMF proposal with BSDF/phase
-                               sampling (fraction 0.5); 0: plain path tracing */
+                               sampling (fraction 0.5) on media and single-layer diffuse
+                               surfaces, rendering in passes that double
+                               from 1 spp (continuing across calls) and training the
+                               context's network online between passes, up to 1024 Adam
+                               steps per network; 0: plain path tracing */
     int32_t accumulate;     /* 1: add to the context's film instead of clearing it */
     int32_t profile;        /* 1: time every kernel launch with CUDA events (per-kernel
                                totals in pg_render_stats.kernels) */
@@ -295,7 +299,8 @@ pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* tuning);
 #define PG_GUIDE_WEIGHTS (6 * 64 * 64)
 #define PG_GUIDE_FEATURES 32
 #define PG_GUIDE_OUTPUTS 40
-/* Glorot-uniform weights from `seed`, Adam state cleared. */
+/* Glorot-uniform weights from `seed`; Adam state, training budget and the guided pass
+ * schedule start over. */
 pg_status pg_guide_reset(pg_ctx* ctx, uint64_t seed);
 pg_status pg_guide_get_weights(pg_ctx* ctx, float* weights);
 pg_status pg_guide_set_weights(pg_ctx* ctx, const float* weights);

@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_grad(const __half* __restrict_
                                                        GuideInput in,
                                                        const float4* __restrict__ dirw, int64_t n,
                                                        float invWeightScale,
+                                                       const float* __restrict__ wsumDev,
                                                        float* __restrict__ partial,
                                                        float* __restrict__ lossSum, uint32_t* err) {
     extern __shared__ uint8_t smemRaw[];
@@ -338,6 +339,10 @@ __global__ void __launch_bounds__(128, 1) k_guide_grad(const __half* __restrict_
     const uint32_t tmem = tmemSlot;
     const uint32_t lane = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t lboZero = SmemU32(sZero) - SmemU32(sDZ);
+    if (wsumDev) {  // weights normalised by their mean over the batch
+        float ws = *wsumDev;
+        invWeightScale = ws > 0.0f && isfinite(ws) ? (float)n / ws : 0.0f;
+    }
     uint32_t phase = 0;
     int tilesDone = 0;
     float lossAcc = 0.0f;
@@ -570,7 +575,7 @@ cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n
 }
 
 cudaError_t GuideGradient(GuideNetDev& net, const GuideInput& in, const float4* dirw, int64_t n,
-                          float weightScale, cudaStream_t st) {
+                          float weightScale, cudaStream_t st, const float* wsumDev) {
     cudaError_t e = cudaFuncSetAttribute(k_guide_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kTrainSmem);
     if (e != cudaSuccess)
@@ -578,7 +583,7 @@ cudaError_t GuideGradient(GuideNetDev& net, const GuideInput& in, const float4* 
     if ((e = cudaMemsetAsync(net.loss, 0, sizeof(float), st)) != cudaSuccess)
         return e;
     k_guide_grad<<<net.blocks, 128, kTrainSmem, st>>>(net.w16, in, dirw, n, 1.0f / weightScale,
-                                                      net.partial, net.loss, net.err);
+                                                      wsumDev, net.partial, net.loss, net.err);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     k_guide_reduce<<<48, 512, 0, st>>>(net.partial, net.blocks, n > 0 ? 1.0f / (float)n : 0.0f,

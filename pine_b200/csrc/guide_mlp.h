@@ -48,10 +48,11 @@ cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n
 
 // Mean over the n rows of the gradient of -weight * log q(dir) with respect to the FP32
 // weights (net.grad) and the loss sum (net.loss).  dirw: n x float4 (dir.xyz, weight);
-// weights are divided by `weightScale` first.  Per-output gradients are clipped to
+// weights are divided by `weightScale` first, or, with wsumDev, by their mean (the sum
+// *wsumDev over n, read on the device).  Per-output gradients are clipped to
 // +-kGuideGradClip before the FP16 backward pass.
 cudaError_t GuideGradient(GuideNetDev& net, const GuideInput& in, const float4* dirw, int64_t n,
-                          float weightScale, cudaStream_t st);
+                          float weightScale, cudaStream_t st, const float* wsumDev = nullptr);
 
 // Sum of the n sample weights (dirw[i].w) into net.wsum.
 cudaError_t GuideWeightSum(GuideNetDev& net, const float4* dirw, int64_t n, cudaStream_t st);

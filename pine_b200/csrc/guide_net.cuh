@@ -128,6 +128,23 @@ PG_HD void GuideBasis(V3 n, V3& b1, V3& b2) {
     b2 = v3(b, s + n.y * n.y * a, -n.y);
 }
 
+// The frame the mixture's directions are expressed in: z is the surface normal turned to
+// the side the path arrived from, or in a medium the forward direction -wi.  Lobes that
+// follow the BSDF or the phase function (a cosine lobe, the forward peak of
+// Henyey-Greenstein) are then the same for every vertex.
+struct GuideFrameT {
+    V3 x, y, z;
+    PG_HD V3 ToLocal(V3 w) const { return v3(Dot(w, x), Dot(w, y), Dot(w, z)); }
+    PG_HD V3 ToWorld(V3 l) const { return x * l.x + y * l.y + z * l.z; }
+};
+
+PG_HD GuideFrameT GuideFrame(bool surface, V3 n, V3 wi) {
+    GuideFrameT f;
+    f.z = surface ? (Dot(n, wi) >= 0.0f ? n : -n) : -wi;
+    GuideBasis(f.z, f.x, f.y);
+    return f;
+}
+
 // Draws a direction: lobe by its weight (u0), then the vMF's cosine by inversion of its
 // CDF (Wenzel Jakob, "Numerically stable sampling of the von Mises-Fisher distribution on
 // S^2", 2012) and a uniform azimuth.
@@ -152,8 +169,8 @@ PG_HD V3 GuideSample(const VmfLobe* lobes, float u0, float u1, float u2) {
     return b1 * (s * cosf(phi)) + b2 * (s * sinf(phi)) + l.mu * w;
 }
 
-// Gradient of the training loss of one sample, -weight * log q(w), with respect to the 40
-// raw outputs (scaled by `scale`, e.g. 1/batch).  Returns the sample's loss term.  This is
+// Gradient of the training loss of one sample, -weight * log q(w) (w in the vertex's
+// frame), with respect to the 40 raw outputs (scaled by `scale`, e.g. 1/batch).  Returns the sample's loss term.  This is
 // the KL-divergence estimator of Mueller et al., "Neural Importance Sampling" (2019): the
 // target density is proportional to the sample's radiance estimate, which `weight`
 // carries divided by the density it was drawn from.

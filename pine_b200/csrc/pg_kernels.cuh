@@ -64,7 +64,8 @@ enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3
 // A training record (kRecordStride float4) holds position + the path's previous record,
 // normal, wi, the throughput before the vertex and the radiance the path had gathered
 // after the vertex (set at its next vertex; w = 1 while still unknown); rec_dirw holds the
-// sampled direction and, once the path has ended, the target weight
+// sampled direction in the vertex's guide frame and, once the path has ended, the target
+// weight
 // lum((L_end - L_base) / beta).
 constexpr int kGuideEntry = 4;
 constexpr int kRecordStride = 5;
@@ -604,12 +605,12 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
 }
 
 // Whether a surface vertex samples its next direction with the guiding network: a single
-// diffuse layer, or a single conductor layer that is not near-specular.
+// diffuse layer.  Glossy lobes follow the mirror direction of wi, which a mixture in the
+// normal's frame cannot track; with half of their samples spent on it, conductors measured
+// up to twice the plain variance, so they keep plain BSDF sampling.
 __device__ __forceinline__ bool GuideEligible(const MaterialDev& m) {
-    if (m.type != PG_MATERIAL_LAYERED || m.num_layers != 1)
-        return false;
-    const BsdfDev& b = m.layers[0];
-    return b.type == PG_BSDF_DIFFUSE || (b.type == PG_BSDF_CONDUCTOR && b.alpha >= 0.05f);
+    return m.type == PG_MATERIAL_LAYERED && m.num_layers == 1 &&
+           m.layers[0].type == PG_BSDF_DIFFUSE;
 }
 
 // Queues a vertex for the network (guide queue, see kGuideEntry).
@@ -917,6 +918,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
     Rng rng{P.sample[i], R.key1, __float_as_uint(Lw.w)};
     VmfLobe lobes[kGuideLobes];
     GuideMixture(P.graw + (size_t)kGuideOutputs * q, lobes);
+    const GuideFrameT gf = GuideFrame(surface, n, wi);  // the mixture's frame
     const float uSel = rng.Get1D();
     V3 w = v3(0.0f, 0.0f, 1.0f), f = v3(0.0f);
     float pdfB = 0.0f;
@@ -939,7 +941,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
         } else {
             float u0 = rng.Get1D(), u1, u2;
             rng.Get2D(u1, u2);
-            w = GuideSample(lobes, u0, u1, u2);
+            w = gf.ToWorld(GuideSample(lobes, u0, u1, u2));
             MaterialEval<M>(mat, wiL, fr.ToLocal(w), f, pdfB);
             ok = true;
         }
@@ -953,13 +955,14 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
         } else {
             float u0 = rng.Get1D(), u1, u2;
             rng.Get2D(u1, u2);
-            w = GuideSample(lobes, u0, u1, u2);
+            w = gf.ToWorld(GuideSample(lobes, u0, u1, u2));
             pdfB = PhaseHG<M>(Dot(wi, w), m.g);
         }
         f = v3(pdfB);
         ok = pdfB > 0.0f;
     }
-    const float pc = ok ? 0.5f * pdfB + 0.5f * GuidePdf(lobes, w) : 0.0f;
+    const V3 wl = gf.ToLocal(w);
+    const float pc = ok ? 0.5f * pdfB + 0.5f * GuidePdf(lobes, wl) : 0.0f;
     bool finished = !(pc > 0.0f) || !isfinite(pc);
     const V3 betaVertex = beta;
     if (!finished) {
@@ -993,7 +996,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
                 rr[2] = make_float4(wi.x, wi.y, wi.z, 0.0f);
                 rr[3] = make_float4(betaVertex.x, betaVertex.y, betaVertex.z, 0.0f);
                 rr[4] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-                P.rec_dirw[r] = make_float4(w.x, w.y, w.z, 0.0f);
+                P.rec_dirw[r] = make_float4(wl.x, wl.y, wl.z, 0.0f);
                 P.rec_last[i] = r;
                 recorded++;
             }

@@ -197,6 +197,8 @@ struct pg_ctx {
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
     pg::GuidePool guide_pool;              // guided-render queues and training records
+    int guide_pass = 1;                    // samples per pixel of the next guided pass
+    int64_t guide_steps = 0;               // Adam steps taken since the network was reset
 };
 
 namespace pg {
@@ -1254,58 +1256,54 @@ static GuideNetDev& EnsureGuide(pg_ctx* ctx);
 
 // Adam steps on the records of the last guided pass, up to kTrainBatch records each, sample
 // weights normalised by their batch mean: one step per kTrainBatch records, and at least
-// kMinTrainSteps (cycling through the records) when a pass records fewer.  Returns the
-// rows trained on.
-constexpr int kMinTrainSteps = 4, kMaxTrainSteps = 16;
+// kMinTrainSteps (cycling through the records) when a pass records fewer; never beyond
+// the context's training budget.  Everything is queued on the stream without host
+// synchronisation.  Returns the steps taken; *rows the rows trained on.
+constexpr int kMinTrainSteps = 16, kMaxTrainSteps = 32;
+constexpr int64_t kGuideStepBudget = 1024;  // Adam steps per network (pg_guide_reset)
 
-static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec) {
+static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec, int64_t& rows) {
     GuideNetDev& net = ctx->guide;
     GuidePool& gp = ctx->guide_pool;
     cudaStream_t st = ctx->stream;
-    int64_t rows = 0;
+    rows = 0;
     if (nrec < 1024)
         return 0;
     int64_t steps = std::min<int64_t>(
         kMaxTrainSteps, std::max<int64_t>(kMinTrainSteps, (nrec + kTrainBatch - 1) / kTrainBatch));
+    steps = std::min<int64_t>(steps, kGuideStepBudget - ctx->guide_steps);
     for (int64_t k = 0; k < steps; k++) {
         int64_t b = (k * kTrainBatch) % nrec;
         int64_t nb = std::min<int64_t>(kTrainBatch, nrec - b);
         if (nb < 1024)
             b = 0, nb = std::min<int64_t>(kTrainBatch, nrec);
         PG_CUDA(GuideWeightSum(net, gp.rec_dirw + b, nb, st));
-        float wsum = 0.0f;
-        PG_CUDA(cudaMemcpyAsync(&wsum, net.wsum, sizeof(float), cudaMemcpyDeviceToHost, st));
-        PG_CUDA(cudaStreamSynchronize(st));
-        if (!(wsum > 0.0f) || !std::isfinite(wsum))
-            continue;
         GuideInput in;
         in.vert = gp.rec + (size_t)kRecordStride * b;
         in.stride = kRecordStride;
         for (int c = 0; c < 3; c++)
             in.lo[c] = sc.dev.guide_lo[c], in.inv[c] = sc.dev.guide_inv[c];
-        PG_CUDA(GuideGradient(net, in, gp.rec_dirw + b, nb, wsum / (float)nb, st));
+        PG_CUDA(GuideGradient(net, in, gp.rec_dirw + b, nb, 1.0f, st, net.wsum));
         PG_CUDA(GuideAdam(net, kGuideLr, st));
         rows += nb;
     }
-    PG_CUDA(cudaStreamSynchronize(st));
-    uint32_t e = 0;
-    PG_CUDA(cudaMemcpy(&e, net.err, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e)
-        throw Failure{PG_ERR_DEVICE_LIMIT, "guiding network: a tensor-core wait timed out"};
-    return rows;
+    ctx->guide_steps += std::max<int64_t>(steps, 0);
+    return std::max<int64_t>(steps, 0);
 }
 
-// Guided render: progressive passes of 1, 1, 2, 4, ... samples per pixel (the last one
-// truncated), each rendered with the network as trained so far and followed, except the
-// last, by training on the pass's records.  Every pass is an unbiased estimate given its
-// network, so their sum is too.  The network stays in the context for later calls.
+// Guided render: passes whose size doubles from one sample per pixel (continuing across
+// calls on the same network: a progressive caller renders large passes after the first
+// few), each rendered with the network as trained so far and followed by training on the
+// pass's records while the network's training budget lasts.  Every pass is an unbiased
+// estimate given its network, so their sum is too.
 static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
                          int sampleOffset, int mathMode, bool accumulate, bool profile,
                          RenderResult& res) {
     EnsureGuide(ctx);
-    float accept = 1.0f;
-    int done = 0, passSpp = 1;
+    float accept = ctx->guide_steps < kGuideStepBudget ? 1.0f : 0.0f;
+    int done = 0;
     while (done < spp) {
+        int passSpp = ctx->guide_pass;
         int sp = std::min(passSpp, spp - done);
         RenderResult r;
         RenderFilm(ctx, sc, sp, maxDepth, seed, sampleOffset + done, mathMode, accumulate || done > 0,
@@ -1319,23 +1317,32 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
         }
         res.launches += r.launches;
         done += sp;
-        if (done < spp) {
+        if (sp == passSpp)
+            ctx->guide_pass = std::min(passSpp * 2, 1 << 16);
+        if (accept > 0.0f) {
             int nrec = 0;
             PG_CUDA(cudaMemcpy(&nrec, ctx->counts + kCntRecords, sizeof(int), cudaMemcpyDeviceToHost));
             auto t0 = std::chrono::steady_clock::now();
-            int64_t rows = TrainOnRecords(ctx, sc, std::min(nrec, kRecordCap));
+            int64_t rows = 0;
+            int64_t steps = TrainOnRecords(ctx, sc, std::min(nrec, kRecordCap), rows);
+            PG_CUDA(cudaStreamSynchronize(ctx->stream));
             double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             res.stats[kStatTrainRows] += (unsigned long long)rows;
             res.kernelSeconds[PG_KERNEL_TRAIN] += dt;
-            res.kernelLaunches[PG_KERNEL_TRAIN] += rows > 0 ? 4 * std::max<int64_t>(1, rows / kTrainBatch) : 0;
+            res.kernelLaunches[PG_KERNEL_TRAIN] += 4 * steps;
             res.seconds += dt;
-            // Record about kRecordCap vertices in the next pass.
+            // Record about kRecordCap vertices in the next pass, none once the budget is spent.
             double perSpp = (double)r.stats[kStatGuided] / sp;
-            int next = std::min(passSpp * 2, spp - done);
-            accept = perSpp > 0 ? (float)std::min(1.0, kRecordCap / (perSpp * next)) : 1.0f;
+            int next = ctx->guide_pass;
+            accept = ctx->guide_steps >= kGuideStepBudget ? 0.0f
+                     : perSpp > 0 ? (float)std::min(1.0, kRecordCap / (perSpp * next))
+                                  : 1.0f;
         }
-        passSpp *= 2;
     }
+    uint32_t e = 0;
+    PG_CUDA(cudaMemcpy(&e, ctx->guide.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e)
+        throw Failure{PG_ERR_DEVICE_LIMIT, "guiding network: a tensor-core wait timed out"};
 }
 
 }  // namespace pg
@@ -1833,6 +1840,8 @@ static void GuideInit(pg_ctx* ctx, uint64_t seed) {
     PG_CUDA(cudaMemsetAsync(g.err, 0, sizeof(uint32_t), st));
     PG_CUDA(GuidePack(g, st));
     g.step = 0;
+    ctx->guide_pass = 1;
+    ctx->guide_steps = 0;
 }
 
 static GuideNetDev& EnsureGuide(pg_ctx* ctx) {

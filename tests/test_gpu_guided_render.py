@@ -129,17 +129,43 @@ def test_guided_matches_plain_within_mc_error(ctx, tmp_path, name, spp):
     assert abs(d) <= 4 * se + 1e-6, (d, se)
 
 
-def test_guiding_lowers_error_on_indirect_box(ctx, tmp_path):
+def test_trained_network_lowers_variance_on_indirect_box(ctx, tmp_path):
+    """What the trained network gains: after a guided warm-up render has trained it, a
+    guided render's per-sample variance (the film's per-pixel sample variance) and its
+    error against a high-spp reference are both clearly below the plain path tracer's at
+    equal samples per pixel."""
     path = tmp_path / "box.txt"
     path.write_text(INDIRECT_BOX)
     sid = ctx.load_scene(str(path))
-    ref = ctx.render(sid, spp=8192, seed=9, math_mode="fast")["mean"]
-    plain = ctx.render(sid, spp=128, seed=1, math_mode="fast")
+    ref = ctx.render(sid, spp=16384, seed=9, math_mode="fast")["mean"]
+    plain = ctx.render(sid, spp=256, seed=1, math_mode="fast")
     ctx.guide_reset(seed=0)
-    guided = ctx.render(sid, spp=128, seed=2, math_mode="fast", guiding=True)
+    ctx.render(sid, spp=128, seed=3, math_mode="fast", guiding=True)  # warm-up: trains
+    guided = ctx.render(sid, spp=256, seed=2, math_mode="fast", guiding=True)
+    var_plain = float(plain["var"].mean())
+    var_guided = float(guided["var"].mean())
     mse_plain = float(np.mean((plain["mean"] - ref) ** 2))
     mse_guided = float(np.mean((guided["mean"] - ref) ** 2))
-    print(f"indirect box, 128 spp: MSE plain {mse_plain:.4g}, guided {mse_guided:.4g}")
-    assert mse_guided < 0.7 * mse_plain, (mse_guided, mse_plain)
-    frac, _ = _zfrac(guided, plain)
-    assert frac >= 0.97
+    print(f"indirect box, 256 spp: sample variance plain {var_plain:.4g} guided {var_guided:.4g}; "
+          f"MSE plain {mse_plain:.4g} guided {mse_guided:.4g}")
+    assert var_guided < 0.75 * var_plain, (var_guided, var_plain)
+    assert mse_guided < 0.85 * mse_plain, (mse_guided, mse_plain)
+
+
+def test_guided_matches_reference_on_indirect_box_at_high_spp(ctx, tmp_path):
+    """The indirect box's samples are heavy-tailed (rare paths find the bright patch), so
+    its agreement test runs at high spp, on 4 x 4 pixel blocks, against a plain reference."""
+    path = tmp_path / "box.txt"
+    path.write_text(INDIRECT_BOX)
+    sid = ctx.load_scene(str(path))
+    ref = ctx.render(sid, spp=32768, seed=9, math_mode="fast")
+    ctx.guide_reset(seed=0)
+    guided = ctx.render(sid, spp=4096, seed=2, math_mode="fast", guiding=True)
+    h, w = ref["mean"].shape[:2]
+    blk = lambda a: a.reshape(h // 4, 4, w // 4, 4, -1).mean(axis=(1, 3))
+    var = blk(guided["var"] / 4096 + ref["var"] / 32768) / 16
+    z = (blk(guided["mean"]) - blk(ref["mean"])) / np.sqrt(var)
+    assert np.mean(np.abs(z) < 2.576) >= 0.97, np.mean(np.abs(z) < 2.576)
+    d = guided["mean"].mean() - ref["mean"].mean()
+    se = np.sqrt(guided["var"].sum() / 4096 + ref["var"].sum() / 32768) / guided["mean"].size
+    assert abs(d) <= 4 * se, (d, se)
