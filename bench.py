@@ -68,6 +68,13 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="render the small ncu case once and print its per-kernel counters")
+    ap.add_argument("--guided", action="store_true",
+                    help="with --profile-case: render it guided (one pass, then training)")
+    ap.add_argument("--batch-eval", action="store_true",
+                    help="the 64-request batch: aggregate Mpaths/s and per-request latency "
+                         "p50/p99, one graph-captured launch vs one request at a time")
+    ap.add_argument("--batch-requests", type=int, default=64)
+    ap.add_argument("--batch-seed", type=int, default=0)
     ap.add_argument("--guiding-eval", action="store_true",
                     help="time to RMSE <= --rmse-target against a plain reference, guided vs "
                          "plain, on --workload (one GPU; prints its own JSON line)")
@@ -306,12 +313,20 @@ def main():
         if rank == 0:
             print(json.dumps(guiding_eval(args, cfg, env)))
         return 0
+    if args.batch_eval:
+        if rank == 0:
+            print(json.dumps(batch_eval(args)))
+        return 0
     if args.profile_case:
         path = scene_path(PROFILE_CASE, args.cache, "constant")
         ctx = pb.Context(local)
         sid = ctx.load_scene(path)
-        r = ctx.render(sid, seed=1, math_mode=args.math, outputs=False)
-        print(json.dumps({"profile_case": PROFILE_CASE, "stats": r["stats"]}))
+        if args.guided:
+            ctx.guide_reset(seed=0)
+        r = ctx.render(sid, seed=1, math_mode=args.math, outputs=False, guiding=args.guided,
+                       profile=args.guided)
+        print(json.dumps({"profile_case": PROFILE_CASE, "guided": args.guided,
+                          "stats": r["stats"]}))
         ctx.close()
         return 0
 
@@ -427,6 +442,51 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def batch_eval(args):
+    """The batched-requests workload: requests drawn by seed from the spheres, mesh and
+    volume generators, resolution side uniform in 128..1024 with aspect uniform in
+    1..16/9, spp log-uniform in 16..256.  The autotuner picks the tuning; then the whole
+    set renders as one graph-captured batch (latency = completion time of each request from
+    the batch start, device clock) and, for comparison, one request at a time in order
+    (latency = the running sum of the single-request device times)."""
+    import pine_b200 as pb
+    ctx = pb.Context(0)
+    kinds = ["spheres", "mesh", "volume"]
+    sids = {}
+    for k in kinds:
+        sids[k] = ctx.load_scene(scene_path(WORKLOADS[k], args.cache,
+                                            "none" if k == "mesh" else "constant"))
+    rng = np.random.default_rng(args.batch_seed)
+    reqs, mix = [], {k: 0 for k in kinds}
+    for i in range(args.batch_requests):
+        k = kinds[int(rng.integers(3))]
+        side = int(rng.uniform(128, 1024))
+        aspect = float(rng.uniform(1.0, 16.0 / 9.0))
+        w, h = side, max(1, int(round(side / aspect)))
+        spp = int(round(np.exp(rng.uniform(np.log(16), np.log(256)))))
+        reqs.append(dict(scene=sids[k], width=w, height=h, spp=spp,
+                         max_depth=WORKLOADS[k]["max_depth"], seed=1000 + i))
+        mix[k] += 1
+    paths = sum(r["width"] * r["height"] * r["spp"] for r in reqs)
+    tuning = ctx.autotune(reqs)
+    ctx.render_batch(reqs, outputs=False)  # warm-up
+    b = ctx.render_batch(reqs, outputs=False)
+    lat_b = np.array(b["request_seconds"])
+    seq, t = [], 0.0
+    for r in reqs:
+        t += ctx.render_batch([r], outputs=False)["seconds"]
+        seq.append(t)
+    lat_s = np.array(seq)
+    pct = lambda a, q: float(np.percentile(a, q))
+    ctx.close()
+    return {"metric": "Mpaths/s", "workload": f"{len(reqs)} requests (seed {args.batch_seed}): {mix}",
+            "paths": int(paths), "tuning": tuning,
+            "batch": {"seconds": b["seconds"], "value": paths / b["seconds"] / 1e6,
+                      "latency_p50_s": pct(lat_b, 50), "latency_p99_s": pct(lat_b, 99)},
+            "one_at_a_time": {"seconds": t, "value": paths / t / 1e6,
+                              "latency_p50_s": pct(lat_s, 50), "latency_p99_s": pct(lat_s, 99)}}
 
 
 def guiding_eval(args, cfg, env):

@@ -1294,7 +1294,8 @@ static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec, 
 // Guided render: passes whose size doubles from one sample per pixel (continuing across
 // calls on the same network: a progressive caller renders large passes after the first
 // few), each rendered with the network as trained so far and followed by training on the
-// pass's records while the network's training budget lasts.  Every pass is an unbiased
+// pass's records while the network's training budget lasts; until then no pass is larger
+// than what fills the record buffer.  Every pass is an unbiased
 // estimate given its network, so their sum is too.
 static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
                          int sampleOffset, int mathMode, bool accumulate, bool profile,
@@ -1319,6 +1320,11 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
         done += sp;
         if (sp == passSpp)
             ctx->guide_pass = std::min(passSpp * 2, 1 << 16);
+        // While training, a pass is at most what fills the record buffer, so that the
+        // network takes its Adam steps after every kRecordCap vertices or so.
+        const double perSpp = (double)r.stats[kStatGuided] / sp;
+        if (ctx->guide_steps < kGuideStepBudget && perSpp > 0)
+            ctx->guide_pass = std::max(1, std::min(ctx->guide_pass, (int)(kRecordCap / perSpp)));
         if (accept > 0.0f) {
             int nrec = 0;
             PG_CUDA(cudaMemcpy(&nrec, ctx->counts + kCntRecords, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1332,7 +1338,6 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
             res.kernelLaunches[PG_KERNEL_TRAIN] += 4 * steps;
             res.seconds += dt;
             // Record about kRecordCap vertices in the next pass, none once the budget is spent.
-            double perSpp = (double)r.stats[kStatGuided] / sp;
             int next = ctx->guide_pass;
             accept = ctx->guide_steps >= kGuideStepBudget ? 0.0f
                      : perSpp > 0 ? (float)std::min(1.0, kRecordCap / (perSpp * next))
@@ -1486,7 +1491,21 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     bool surfaces = false;
     int maxDepth = 1;
     const int variant = MediaVariant(tune);
+    // Shortest job first: requests take their sample ranges in increasing order of their
+    // sample count, so small requests complete early (results keep the caller's order).
+    std::vector<uint64_t> cost(n);
     for (int i = 0; i < n; i++) {
+        const pg_request& r = reqs[i];
+        DeviceScene& sc = GetScene(ctx, r.scene_id);
+        int w = r.width > 0 ? r.width : sc.width, h = r.height > 0 ? r.height : sc.height;
+        cost[i] = (uint64_t)std::max(w, 1) * std::max(h, 1) * (uint64_t)std::max(r.spp, 1);
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++)
+        order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] < cost[b]; });
+    for (int k = 0; k < n; k++) {
+        const int i = order[k];
         const pg_request& r = reqs[i];
         DeviceScene& sc = GetScene(ctx, r.scene_id);
         int w = r.width > 0 ? r.width : sc.width, h = r.height > 0 ? r.height : sc.height;
@@ -1495,7 +1514,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         int md = r.max_depth > 0 ? r.max_depth : sc.max_depth;
         uint64_t cnt = (uint64_t)w * h * spp;
         Require(cnt < (1ull << 32), "a request's width*height*spp must stay below 2^32");
-        RequestDev& d = rq[i];
+        RequestDev& d = rq[k];
         d.sample_begin = total;
         d.total = (uint32_t)cnt;
         d.npix = w * h;
@@ -1515,7 +1534,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         s.cam.width = w;
         s.cam.height = h;
         s.cam.fov2d[0] = s.cam.fov2d[1] * ((float)w / (float)h);
-        scenes[i] = s;
+        scenes[k] = s;
         surfaces = surfaces || sc.surfaces;
     }
     ClearFilm(ctx, (int64_t)pixels);
@@ -1547,13 +1566,14 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     std::vector<unsigned long long> t(n + 1);
     PG_CUDA(cudaMemcpy(t.data(), times, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     out.requestSeconds.resize(n);
-    for (int i = 0; i < n; i++)
-        out.requestSeconds[i] = t[i + 1] >= t[0] ? (double)(t[i + 1] - t[0]) * 1e-9 : -1.0;
+    for (int k = 0; k < n; k++)
+        out.requestSeconds[order[k]] = t[k + 1] >= t[0] ? (double)(t[k + 1] - t[0]) * 1e-9 : -1.0;
     if (outputs) {
-        for (int i = 0; i < n; i++) {
+        for (int k = 0; k < n; k++) {
+            const int i = order[k];
             if (!reqs[i].out_mean)
                 continue;
-            const RequestDev& d = rq[i];
+            const RequestDev& d = rq[k];
             std::vector<double> sum((size_t)d.npix * 3);
             std::vector<uint32_t> cnt(d.npix);
             PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum + d.film_base * 3, sum.size() * sizeof(double),

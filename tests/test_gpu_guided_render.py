@@ -140,7 +140,7 @@ def test_trained_network_lowers_variance_on_indirect_box(ctx, tmp_path):
     ref = ctx.render(sid, spp=16384, seed=9, math_mode="fast")["mean"]
     plain = ctx.render(sid, spp=256, seed=1, math_mode="fast")
     ctx.guide_reset(seed=0)
-    ctx.render(sid, spp=128, seed=3, math_mode="fast", guiding=True)  # warm-up: trains
+    ctx.render(sid, spp=1024, seed=3, math_mode="fast", guiding=True)  # warm-up: trains
     guided = ctx.render(sid, spp=256, seed=2, math_mode="fast", guiding=True)
     var_plain = float(plain["var"].mean())
     var_guided = float(guided["var"].mean())
@@ -148,7 +148,7 @@ def test_trained_network_lowers_variance_on_indirect_box(ctx, tmp_path):
     mse_guided = float(np.mean((guided["mean"] - ref) ** 2))
     print(f"indirect box, 256 spp: sample variance plain {var_plain:.4g} guided {var_guided:.4g}; "
           f"MSE plain {mse_plain:.4g} guided {mse_guided:.4g}")
-    assert var_guided < 0.75 * var_plain, (var_guided, var_plain)
+    assert var_guided < 0.7 * var_plain, (var_guided, var_plain)
     assert mse_guided < 0.85 * mse_plain, (mse_guided, mse_plain)
 
 
