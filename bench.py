@@ -394,12 +394,20 @@ def main():
     ctx.render(sid2, spp=1, seed=7, math_mode=args.math, into=(out_mean, out_var, out_cnt))
     ctx.release_scene(sid2)
     barrier()
+    phases = {"upload": 0.0, "render_and_readback": 0.0, "release": 0.0}
     t0 = time.perf_counter()
     for s in range(e2e_steps):
+        ta = time.perf_counter()
         sid2 = ctx.upload_scene(desc)
+        tb = time.perf_counter()
         ctx.render(sid2, seed=seed0 + 500 + s, math_mode=args.math,
                    into=(out_mean, out_var, out_cnt))
+        tc = time.perf_counter()
         ctx.release_scene(sid2)
+        td = time.perf_counter()
+        phases["upload"] += tb - ta
+        phases["render_and_readback"] += tc - tb
+        phases["release"] += td - tc
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     parsed.close()
@@ -420,7 +428,8 @@ def main():
                          if cfg["kind"] == "volume" else "scene resident; no flush"},
         "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-                "timing": "wall clock: pg_upload_scene + pg_render + film readback + release"},
+                "timing": "wall clock: pg_upload_scene + pg_render + film readback + release",
+                "phase_ms_per_step": {k: round(v / e2e_steps * 1e3, 2) for k, v in phases.items()}},
         "gpu_launches": launches,
         "mrays_per_s": stats_acc["rays"] * world / device_s_max / 1e6,
         "gsteps_per_s": stats_acc["volume_steps"] * world / device_s_max / 1e9,

@@ -58,12 +58,17 @@ struct MediumDev {
     int size[3];
     float inv_max_density;
     int interpolate;
-    const float* density;   // x fastest
+    const float* bricks;    // density in 8^3 bricks with a 1-voxel apron (9^3, x fastest,
+                            // kDensityBrickStride floats each): one brick holds every
+                            // trilinear footprint whose base voxel lies in it
+    int dnb[3];             // density bricks per axis
     const float* majorant;  // per brick of bsize^3 voxels, covering the trilinear footprint
     int nb[3];
     int bsize;              // voxels per brick edge (8, 16 or 32)
     float inv_bsize;
 };
+
+constexpr int kDensityBrickStride = 736;  // 9^3 = 729 floats, padded to 128-byte multiples
 
 struct CameraDev {
     float c2w[12];  // 3x4 row-major

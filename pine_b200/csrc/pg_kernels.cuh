@@ -1049,6 +1049,25 @@ __global__ void k_guide_sample(RenderParams P, SceneDev S0) {
     }
 }
 
+// Copies a grid (x fastest) into 8^3 bricks with a 1-voxel apron (zeros past the end).
+__global__ void k_brickify(const float* __restrict__ d, int sx, int sy, int sz, int nbx, int nby,
+                           int nbz, float* __restrict__ bricks) {
+    const int64_t nb = (int64_t)nbx * nby * nbz;
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+        float* out = bricks + b * kDensityBrickStride;
+        for (int t = threadIdx.x; t < kDensityBrickStride; t += blockDim.x) {
+            float v = 0.0f;
+            if (t < 729) {
+                int x = 8 * bx + t % 9, y = 8 * by + (t / 9) % 9, z = 8 * bz + t / 81;
+                if (x < sx && y < sy && z < sz)
+                    v = d[(size_t)x + (size_t)y * sx + (size_t)z * sx * sy];
+            }
+            out[t] = v;
+        }
+    }
+}
+
 // Brick majorants: the largest density over voxels [b*k, b*k + b] of each axis (the
 // trilinear footprint of points inside brick k of edge b voxels), one thread per brick.
 __global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int nbx, int nby,

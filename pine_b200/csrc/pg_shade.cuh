@@ -512,10 +512,28 @@ __device__ __forceinline__ bool UnitBoxHit(V3 o, V3 d, float& tmin, float& tmax)
 __device__ __forceinline__ float VoxelD(const MediumDev& m, int x, int y, int z) {
     if (x < 0 || y < 0 || z < 0 || x >= m.size[0] || y >= m.size[1] || z >= m.size[2])
         return 0.0f;
-    return __ldg(&m.density[(size_t)x + (size_t)y * m.size[0] + (size_t)z * m.size[0] * m.size[1]]);
+    return __ldg(m.bricks +
+                 ((size_t)((z >> 3) * m.dnb[1] + (y >> 3)) * m.dnb[0] + (x >> 3)) * kDensityBrickStride +
+                 ((z & 7) * 9 + (y & 7)) * 9 + (x & 7));
 }
 __device__ __forceinline__ float GridDensity(const MediumDev& m, float vx, float vy, float vz) {
     int ix = (int)vx, iy = (int)vy, iz = (int)vz;
+    if (ix >= 0 && iy >= 0 && iz >= 0 && ix < m.size[0] && iy < m.size[1] && iz < m.size[2]) {
+        // Base voxel inside the grid: all 8 voxels of the footprint are in its apron brick
+        // (the apron holds zeros past the grid's end, as VoxelD returns there).
+        const float* b = m.bricks +
+                         ((size_t)((iz >> 3) * m.dnb[1] + (iy >> 3)) * m.dnb[0] + (ix >> 3)) *
+                             kDensityBrickStride +
+                         ((iz & 7) * 9 + (iy & 7)) * 9 + (ix & 7);
+        if (!m.interpolate)
+            return __ldg(b);
+        float fx = vx - ix, fy = vy - iy, fz = vz - iz;
+        float d000 = __ldg(b), d001 = __ldg(b + 81), d010 = __ldg(b + 9), d011 = __ldg(b + 90);
+        float d100 = __ldg(b + 1), d101 = __ldg(b + 82), d110 = __ldg(b + 10), d111 = __ldg(b + 91);
+        float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+        return gx * (gy * (gz * d000 + fz * d001) + fy * (gz * d010 + fz * d011)) +
+               fx * (gy * (gz * d100 + fz * d101) + fy * (gz * d110 + fz * d111));
+    }
     if (!m.interpolate)
         return VoxelD(m, ix, iy, iz);
     float fx = vx - ix, fy = vy - iy, fz = vz - iz;

@@ -159,6 +159,7 @@ struct Film {
     double *sum = nullptr, *sq = nullptr;  // accumulated over calls (progressive passes)
     uint32_t* n = nullptr;
     float4 *acc = nullptr, *acc2 = nullptr;  // this call's samples, vector-atomic targets
+    float *rmean = nullptr, *rvar = nullptr;  // resolved mean and variance, read back
     void Ensure(int64_t np) {
         if (np <= npix)
             return;
@@ -171,6 +172,8 @@ struct Film {
         n = mem.Alloc<uint32_t>(np);
         acc = mem.Alloc<float4>(np);
         acc2 = mem.Alloc<float4>(np);
+        rmean = mem.Alloc<float>(np * 3);
+        rvar = mem.Alloc<float>(np * 3);
     }
 };
 
@@ -236,6 +239,7 @@ static void Put(float* dst, V3 v) {
 }
 
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
+    DevMem upload;  // linear density grids: inputs of the majorant and brick builds only
     Require(d != nullptr && sceneId != nullptr, "null scene description or scene id pointer");
     Require(d->num_shapes >= 0 && (d->num_shapes == 0 || d->shapes), "bad shapes array");
     Require(d->num_materials >= 0 && (d->num_materials == 0 || d->materials), "bad materials array");
@@ -432,9 +436,18 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         size_t nvox = (size_t)m.size[0] * m.size[1] * m.size[2];
         std::memcpy(o.size, m.size, sizeof(o.size));
         o.interpolate = m.interpolate;
-        float* dd = sc->mem.Alloc<float>(nvox);
+        float* dd = upload.Alloc<float>(nvox);
         PG_CUDA(cudaMemcpyAsync(dd, m.density, nvox * 4, cudaMemcpyHostToDevice, st));
-        o.density = dd;
+        for (int k = 0; k < 3; k++)
+            o.dnb[k] = (m.size[k] + 7) / 8;
+        {
+            int64_t nbd = (int64_t)o.dnb[0] * o.dnb[1] * o.dnb[2];
+            float* bk = sc->mem.Alloc<float>((size_t)nbd * kDensityBrickStride);
+            k_brickify<<<(unsigned)std::min<int64_t>(nbd, 65535), 256, 0, st>>>(
+                dd, m.size[0], m.size[1], m.size[2], o.dnb[0], o.dnb[1], o.dnb[2], bk);
+            PG_CUDA(cudaGetLastError());
+            o.bricks = bk;
+        }
         // Brick majorants are built on the device from the uploaded grid, for each brick
         // size a tuning may select; variant 0 is kept in `media`, the others below.
         for (int v = 0; v < 4; v++) {
@@ -1091,26 +1104,40 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     ctx->req_buf.Free();
 }
 
-static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_t* count) {
-    if (!mean && !var && !count)
-        return;
-    std::vector<double> sum(npix * 3), sq(npix * 3);
-    std::vector<uint32_t> n(npix);
-    PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum, npix * 3 * sizeof(double), cudaMemcpyDeviceToHost));
-    PG_CUDA(cudaMemcpy(sq.data(), ctx->film.sq, npix * 3 * sizeof(double), cudaMemcpyDeviceToHost));
-    PG_CUDA(cudaMemcpy(n.data(), ctx->film.n, npix * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < npix; i++) {
+// Per-pixel mean and unbiased sample variance of the FP64 film (FP64 arithmetic, then
+// rounded to FP32), on the device.
+__global__ void k_resolve(const double* __restrict__ sum, const double* __restrict__ sq,
+                          const uint32_t* __restrict__ n, int64_t npix, float* __restrict__ mean,
+                          float* __restrict__ var) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
+         i += (int64_t)gridDim.x * blockDim.x) {
         double k = n[i];
         for (int c = 0; c < 3; c++) {
             double m = k > 0 ? sum[3 * i + c] / k : 0.0;
-            if (mean)
-                mean[3 * i + c] = (float)m;
-            if (var)
-                var[3 * i + c] = k > 1 ? (float)std::max(0.0, (sq[3 * i + c] - k * m * m) / (k - 1)) : 0.0f;
+            mean[3 * i + c] = (float)m;
+            var[3 * i + c] = k > 1 ? (float)fmax(0.0, (sq[3 * i + c] - k * m * m) / (k - 1)) : 0.0f;
         }
-        if (count)
-            count[i] = n[i];
     }
+}
+
+// Resolves the film on the device and copies what the caller asked for straight into its
+// buffers (pinned buffers are read at full PCIe speed).
+static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_t* count) {
+    if (!mean && !var && !count)
+        return;
+    cudaStream_t st = ctx->stream;
+    Film& f = ctx->film;
+    if (mean || var) {
+        k_resolve<<<ctx->num_sms * 4, 256, 0, st>>>(f.sum, f.sq, f.n, npix, f.rmean, f.rvar);
+        PG_CUDA(cudaGetLastError());
+    }
+    if (mean)
+        PG_CUDA(cudaMemcpyAsync(mean, f.rmean, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (var)
+        PG_CUDA(cudaMemcpyAsync(var, f.rvar, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (count)
+        PG_CUDA(cudaMemcpyAsync(count, f.n, npix * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    PG_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace pg
