@@ -471,7 +471,7 @@ __device__ void Surface(const SceneDev& S, V3 o, V3 d, float4 h, SurfaceInfo& si
 // Transmittance of a shadow ray (RayIntegrator::IntersectTr, integrator.cpp:68-87):
 // zero if a surface with a material blocks it, otherwise the product of the media's
 // transmittances along the segments between null surfaces.
-template <int M>
+template <int M, bool MEDIA = true>
 __device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, Rng& rng,
                        uint2* stack, int stride, uint32_t& steps, uint32_t& bricks, uint32_t& err,
                        int& traced) {
@@ -482,7 +482,7 @@ __device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, Rn
         Hit h;
         if (surfaces && Traverse<true>(S, o, d, 0.0f, tmax, h, stack, stride, err))
             return v3(0.0f);
-        if (medium >= 0)
+        if (MEDIA && medium >= 0)
             MediumTr<M>(S.media[medium], o, d, tmax, rng, steps, bricks, err, tr);
         return tr;
     }
@@ -490,7 +490,7 @@ __device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, Rn
     for (int k = 0; k < 64; k++) {
         Hit h;
         bool hitS = Traverse<false>(S, o, d, 0.0f, tmax, h, stack, stride, err);
-        if (medium >= 0) {
+        if (MEDIA && medium >= 0) {
             V3 t3;
             MediumTr<M>(S.media[medium], o, d, hitS ? h.t : tmax, rng, steps, bricks, err, t3);
             tr *= t3;
@@ -530,7 +530,7 @@ constexpr uint32_t kFinalShadow = 0x80000000u;
 // light, samples it, evaluates the BSDF (surface) or phase function (medium) and either
 // queues a shadow ray carrying the unoccluded contribution beta * f * w * Le / pdf for
 // k_shadow or, with FUSED, traces it here and adds the result to L.
-template <int M, bool FUSED>
+template <int M, bool FUSED, bool MEDIA = true>
 __device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, uint32_t key1, Rng& rng,
                           V3 p, V3 n, V3 wiWorld, bool surface, const MaterialDev* mat,
                           const Frame<M>* frame, float g, int medIn, int medOut, V3 beta, V3& L,
@@ -573,7 +573,7 @@ __device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, ui
     if (FUSED) {
         Rng srng{P.sample[slot], key, 0};
         int traced;
-        V3 tr = ShadowTr<M>(S, o, ls.wo, tmax, med, srng, stack, blockDim.x, ct.shadowSteps,
+        V3 tr = ShadowTr<M, MEDIA>(S, o, ls.wo, tmax, med, srng, stack, blockDim.x, ct.shadowSteps,
                             ct.shadowBricks, ct.err, traced);
         L += c * tr;
         ct.shadowRays += traced;
@@ -625,7 +625,9 @@ __device__ __forceinline__ void PushGuide(const RenderParams& P, int slot, V3 p,
         make_float4(__int_as_float((medIn + 1) | ((medOut + 1) << 16)), 0.0f, 0.0f, 0.0f);
 }
 
-template <int M, bool FUSED, bool GUIDE>
+// MEDIA = false compiles the shading of scenes without participating media: the medium
+// code drops out, which frees registers for more resident warps.
+template <int M, bool FUSED, bool GUIDE, bool MEDIA = true>
 __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
                          uint2* stack, ShadeCounters& ct, PendingShadow& ps, bool& finished,
                          V3& Lout, bool& deferred) {
@@ -657,7 +659,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
 
     MediumEvent ev;
     ev.scattered = false;
-    if (medium >= 0) {
+    if (MEDIA && medium >= 0) {
         MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, ct.steps, ct.bricks, ct.err);
         beta *= ev.weight;
     }
@@ -667,7 +669,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             finished = true;
         } else {
             const MediumDev& m = S.media[medium];
-            NextEvent<M, FUSED>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
+            NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
                                 m.g, medium, medium, beta, L, stack, ct, ps);
             if (GUIDE) {
                 PushGuide(P, i, ev.p, v3(0.0f), false, medium, -d, ps.idx, medium, medium);
@@ -723,7 +725,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             } else {
                 Frame<M> fr;
                 fr.From(si.n);
-                NextEvent<M, FUSED>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
+                NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
                                     medIn, medOut, beta, L, stack, ct, ps);
                 if (GUIDE && GuideEligible(mat)) {
                     PushGuide(P, i, si.p, si.n, true, sh.material, -d, ps.idx, medIn, medOut);
@@ -778,7 +780,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     }
 }
 
-template <int M, bool MULTI, bool FUSED, bool GUIDE = false>
+template <int M, bool MULTI, bool FUSED, bool GUIDE = false, bool MEDIA = true>
 __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -796,7 +798,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
         V3 L;
         bool deferred = false;
         if (live)
-            ShadeOne<M, FUSED, GUIDE>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
+            ShadeOne<M, FUSED, GUIDE, MEDIA>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
                                       stack + threadIdx.x, ct, ps, finished, L, deferred);
         // A path that ends here with no shadow ray in flight is flushed now and its slot
         // takes the next camera sample; one with a shadow ray pending ends in k_shadow.
@@ -834,7 +836,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     }
 }
 
-template <int M, bool MULTI, bool GUIDE = false>
+template <int M, bool MULTI, bool GUIDE = false, bool MEDIA = true>
 __global__ void k_shadow(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -854,7 +856,7 @@ __global__ void k_shadow(RenderParams P, SceneDev S0) {
             last = (w & kFinalShadow) != 0;
             const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
             Rng rng{P.sample[slot], P.skey[q], 0};
-            V3 tr = ShadowTr<M>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
+            V3 tr = ShadowTr<M, MEDIA>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
                                 __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x, steps,
                                 bricks, err, traced);
             float4 Lw = P.L[slot];

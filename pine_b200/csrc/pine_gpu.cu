@@ -760,6 +760,7 @@ struct Wave {
     RenderParams P{};
     SceneDev S0{};
     bool multi = false, surfaces = false, fused = false, guide = false;
+    bool media = true;  // false: no participating media, the lean kernel variants run
     int mode = PG_MATH_FAST;
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
@@ -792,11 +793,18 @@ static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer
         PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)shadeSmem));
     time(PG_KERNEL_SHADE, [&]() {
-        k_shade<M, MULTI, FUSED><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
+        if (!FUSED && !w.media)
+            k_shade<M, MULTI, false, false, false>
+                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(w.P, w.S0);
+        else
+            k_shade<M, MULTI, FUSED><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
     });
     if (!FUSED)
         time(PG_KERNEL_SHADOW, [&]() {
-            k_shadow<M, MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+            if (!w.media)
+                k_shadow<M, MULTI, false, false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+            else
+                k_shadow<M, MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
         });
     // Queue swap; counted with the fill kernel.
     time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
@@ -1080,6 +1088,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
     w.guide = recordAccept != nullptr;
+    w.media = sc.dev.num_media > 0;
     if (w.guide)
         w.P.rec_accept = *recordAccept;
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
@@ -1515,7 +1524,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     std::vector<RequestDev> rq(n);
     std::vector<SceneDev> scenes(n);
     uint64_t total = 0, pixels = 0;
-    bool surfaces = false;
+    bool surfaces = false, media = false;
     int maxDepth = 1;
     const int variant = MediaVariant(tune);
     // Shortest job first: requests take their sample ranges in increasing order of their
@@ -1563,6 +1572,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         s.cam.fov2d[0] = s.cam.fov2d[1] * ((float)w / (float)h);
         scenes[k] = s;
         surfaces = surfaces || sc.surfaces;
+        media = media || sc.dev.num_media > 0;
     }
     ClearFilm(ctx, (int64_t)pixels);
     ClearCallFilm(ctx, (int64_t)pixels);
@@ -1577,6 +1587,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.multi = true;
     w.mode = PG_MATH_FAST;
     w.surfaces = surfaces;
+    w.media = media;
     w.fused = tune.split_shadow == 0;
     w.shadeBlock = tune.block_size;
     w.S0 = scenes[0];
