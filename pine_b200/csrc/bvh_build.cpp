@@ -1,7 +1,7 @@
 // Compressed 8-wide BVH construction (host).
 //
 // 1. Binary tree by binned SAH (32 bins per axis over centroid bounds, unit traversal and
-//    intersection costs), leaves of at most 3 primitives.
+//    intersection costs), leaves of at most 3 primitives; built on all host threads.
 // 2. Collapse to 8-wide: a wide node starts from a binary node's two children and keeps
 //    opening the internal child of largest surface area until it has 8 children.
 // 3. Children are placed in octant-ordered slots (greedy assignment on the dot product of
@@ -19,8 +19,10 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <future>
 #include <numeric>
+#include <thread>
 
 namespace pg {
 namespace {
@@ -49,11 +51,30 @@ void Grow(Box& b, const Box& o) {
     }
 }
 
+// Bins of one axis over a range of primitives.
+constexpr int kBins = 32;
+struct AxisBins {
+    Box box[kBins];
+    int count[kBins];
+    void Clear() {
+        for (int b = 0; b < kBins; b++)
+            box[b] = Empty(), count[b] = 0;
+    }
+};
+
 struct Builder {
     const std::vector<Box>& boxes;
     std::vector<float> cen;  // 3 per primitive
     std::vector<uint32_t> idx;
-    std::vector<BNode> nodes;
+    std::vector<BNode> nodes;      // preallocated: a binary tree has at most 2n - 1 nodes
+    std::atomic<int> next{0};      // next free node
+    std::atomic<int> workers{0};   // subtree threads running
+    int maxWorkers = 1;
+
+    // Large nodes are binned by several threads and large subtrees built on their own
+    // thread.  Every reduction is a min, max or count, so the tree is the same as a
+    // sequential build's.
+    static constexpr int kParallelBin = 1 << 17, kParallelTree = 1 << 14;
 
     explicit Builder(const std::vector<Box>& b) : boxes(b) {
         size_t n = b.size();
@@ -64,13 +85,26 @@ struct Builder {
                 cen[3 * i + k] = 0.5f * (b[i].lo[k] + b[i].hi[k]);
             idx[i] = (uint32_t)i;
         }
-        nodes.reserve(n / 2 + 16);
+        nodes.resize(2 * n + 1);
+        unsigned hw = std::thread::hardware_concurrency();
+        maxWorkers = (int)std::max(1u, std::min(hw, 64u)) - 1;
     }
 
-    int Build(int begin, int end) {
-        int id = (int)nodes.size();
-        nodes.emplace_back();
-        Box box = Empty(), cb = Empty();
+    // Runs f(lo, hi, part) over `parts` contiguous pieces of [begin, end) on threads.
+    template <typename F>
+    static void ForParts(int begin, int end, int parts, F&& f) {
+        std::vector<std::thread> th;
+        int n = end - begin;
+        for (int t = 1; t < parts; t++)
+            th.emplace_back([&, t]() { f(begin + (int)((int64_t)n * t / parts),
+                                         begin + (int)((int64_t)n * (t + 1) / parts), t); });
+        f(begin, begin + (int)((int64_t)n / parts), 0);
+        for (auto& x : th)
+            x.join();
+    }
+
+    void Bounds(int begin, int end, Box& box, Box& cb) const {
+        box = Empty(), cb = Empty();
         for (int i = begin; i < end; i++) {
             Grow(box, boxes[idx[i]]);
             const float* c = &cen[3 * idx[i]];
@@ -79,14 +113,66 @@ struct Builder {
                 cb.hi[k] = std::max(cb.hi[k], c[k]);
             }
         }
+    }
+
+    void Bin(int begin, int end, const Box& cb, AxisBins (&ab)[3]) const {
+        for (int k = 0; k < 3; k++)
+            ab[k].Clear();
+        for (int k = 0; k < 3; k++) {
+            float ext = cb.hi[k] - cb.lo[k];
+            if (!(ext > 0.0f))
+                continue;
+            float s = kBins / ext;
+            for (int i = begin; i < end; i++) {
+                int b = std::min(kBins - 1, (int)((cen[3 * idx[i] + k] - cb.lo[k]) * s));
+                ab[k].count[b]++;
+                Grow(ab[k].box[b], boxes[idx[i]]);
+            }
+        }
+    }
+
+    int Build(int begin, int end) {
+        int id = next.fetch_add(1);
+        int n = end - begin;
+        Box box, cb;
+        AxisBins ab[3];
+        const int parts = n >= kParallelBin ? std::max(1, std::min(16, maxWorkers + 1 - workers.load())) : 1;
+        if (parts > 1) {
+            std::vector<Box> pb(parts), pc(parts);
+            ForParts(begin, end, parts, [&](int lo, int hi, int t) { Bounds(lo, hi, pb[t], pc[t]); });
+            box = Empty(), cb = Empty();
+            for (int t = 0; t < parts; t++) {
+                Grow(box, pb[t]);
+                Grow(cb, pc[t]);
+            }
+        } else {
+            Bounds(begin, end, box, cb);
+        }
         nodes[id].box = box;
         nodes[id].begin = begin;
         nodes[id].end = end;
-        int n = end - begin;
         if (n == 1)
             return id;
+        if (parts > 1) {
+            std::vector<AxisBins> pbins(3 * (size_t)parts);
+            ForParts(begin, end, parts, [&](int lo, int hi, int t) {
+                AxisBins loc[3];
+                Bin(lo, hi, cb, loc);
+                for (int k = 0; k < 3; k++)
+                    pbins[3 * t + k] = loc[k];
+            });
+            for (int k = 0; k < 3; k++) {
+                ab[k].Clear();
+                for (int t = 0; t < parts; t++)
+                    for (int b = 0; b < kBins; b++) {
+                        ab[k].count[b] += pbins[3 * t + k].count[b];
+                        Grow(ab[k].box[b], pbins[3 * t + k].box[b]);
+                    }
+            }
+        } else {
+            Bin(begin, end, cb, ab);
+        }
 
-        const int B = 32;
         float best = FLT_MAX;
         int bestAxis = -1, bestSplit = -1;
         float parentArea = std::max(Area(box), 1e-30f);
@@ -94,27 +180,19 @@ struct Builder {
             float ext = cb.hi[k] - cb.lo[k];
             if (!(ext > 0.0f))
                 continue;
-            Box bb[B];
-            int bc[B] = {};
-            for (int b = 0; b < B; b++)
-                bb[b] = Empty();
-            float s = B / ext;
-            for (int i = begin; i < end; i++) {
-                int b = std::min(B - 1, (int)((cen[3 * idx[i] + k] - cb.lo[k]) * s));
-                bc[b]++;
-                Grow(bb[b], boxes[idx[i]]);
-            }
-            float rightCost[B];
+            const Box* bb = ab[k].box;
+            const int* bc = ab[k].count;
+            float rightCost[kBins];
             Box acc = Empty();
             int cnt = 0;
-            for (int b = B - 1; b > 0; b--) {
+            for (int b = kBins - 1; b > 0; b--) {
                 Grow(acc, bb[b]);
                 cnt += bc[b];
                 rightCost[b] = cnt ? Area(acc) * cnt : 0.0f;
             }
             acc = Empty();
             cnt = 0;
-            for (int b = 0; b < B - 1; b++) {
+            for (int b = 0; b < kBins - 1; b++) {
                 Grow(acc, bb[b]);
                 cnt += bc[b];
                 if (cnt == 0 || cnt == n)
@@ -136,16 +214,26 @@ struct Builder {
             if (n <= 3 && (float)n <= best)
                 return id;
             int k = bestAxis;
-            float ext = cb.hi[k] - cb.lo[k], s = B / ext, lo = cb.lo[k];
+            float ext = cb.hi[k] - cb.lo[k], s = kBins / ext, lo = cb.lo[k];
             auto it = std::partition(idx.begin() + begin, idx.begin() + end, [&](uint32_t p) {
-                return std::min(B - 1, (int)((cen[3 * p + k] - lo) * s)) <= bestSplit;
+                return std::min(kBins - 1, (int)((cen[3 * p + k] - lo) * s)) <= bestSplit;
             });
             mid = (int)(it - idx.begin());
             if (mid == begin || mid == end)
                 mid = begin + n / 2;
         }
-        int l = Build(begin, mid);
-        int r = Build(mid, end);
+        int l = -1, r = -1;
+        if (n >= kParallelTree && workers.fetch_add(1) < maxWorkers) {
+            std::thread t([&]() { l = Build(begin, mid); });
+            r = Build(mid, end);
+            t.join();
+            workers.fetch_sub(1);
+        } else {
+            if (n >= kParallelTree)
+                workers.fetch_sub(1);
+            l = Build(begin, mid);
+            r = Build(mid, end);
+        }
         nodes[id].left = l;
         nodes[id].right = r;
         return id;
@@ -172,7 +260,7 @@ WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
         return out;
     Builder b(boxes);
     int root = b.Build(0, (int)boxes.size());
-    out.binary_nodes = (int64_t)b.nodes.size();
+    out.binary_nodes = (int64_t)b.next.load();
     const auto& bn = b.nodes;
     auto isLeaf = [&](int i) { return bn[i].left < 0; };
 
@@ -182,22 +270,24 @@ WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
         int depth;
     };
     std::vector<Task> stack;
+    out.nodes.reserve(boxes.size() / 3 + 16);
+    out.prim_order.reserve(boxes.size());
     out.nodes.resize(1);
     stack.push_back({root, 0, 1});
     while (!stack.empty()) {
         Task t = stack.back();
         stack.pop_back();
         out.max_depth = std::max(out.max_depth, t.depth);
-        std::vector<int> ch;
+        int ch[8], nch = 0;
         if (isLeaf(t.bnode)) {
-            ch.push_back(t.bnode);
+            ch[nch++] = t.bnode;
         } else {
-            ch.push_back(bn[t.bnode].left);
-            ch.push_back(bn[t.bnode].right);
-            while (ch.size() < 8) {
+            ch[nch++] = bn[t.bnode].left;
+            ch[nch++] = bn[t.bnode].right;
+            while (nch < 8) {
                 int bi = -1;
                 float ba = -1.0f;
-                for (int i = 0; i < (int)ch.size(); i++)
+                for (int i = 0; i < nch; i++)
                     if (!isLeaf(ch[i]) && Area(bn[ch[i]].box) > ba) {
                         ba = Area(bn[ch[i]].box);
                         bi = i;
@@ -206,20 +296,20 @@ WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
                     break;
                 int c = ch[bi];
                 ch[bi] = bn[c].left;
-                ch.push_back(bn[c].right);
+                ch[nch++] = bn[c].right;
             }
         }
         // Node bounds and centre.
         Box nb = Empty();
-        for (int c : ch)
-            Grow(nb, bn[c].box);
+        for (int i = 0; i < nch; i++)
+            Grow(nb, bn[ch[i]].box);
         double pc[3];
         for (int k = 0; k < 3; k++)
             pc[k] = 0.5 * ((double)nb.lo[k] + nb.hi[k]);
         // Greedy octant slot assignment.
         int slotOf[8];
         bool usedSlot[8] = {}, placed[8] = {};
-        int nc = (int)ch.size();
+        int nc = nch;
         for (int round = 0; round < nc; round++) {
             double bestCost = 1e300;
             int bc = -1, bs = -1;
