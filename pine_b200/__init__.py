@@ -414,8 +414,8 @@ class Context:
         self._check(self._lib.pg_get_tuning(self._ctx, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
-    def set_tuning(self, queue_capacity: int = 1 << 21, block_size: int = 128,
-                   split_shadow: int = 1, majorant_brick: int = 16):
+    def set_tuning(self, queue_capacity: int = 1 << 22, block_size: int = 128,
+                   split_shadow: int = 1, majorant_brick: int = 32):
         t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))
 

@@ -53,12 +53,19 @@ static void Require(bool ok, const std::string& msg, pg_status s = PG_ERR_INVALI
 // ---------------------------------------------------------------- device memory
 struct DevMem {
     std::vector<void*> ptrs;
+    // With a stream, allocations are stream-ordered (cudaMallocAsync from the device's
+    // pool, which keeps freed memory for reuse): only work on that stream may touch them.
+    cudaStream_t stream = nullptr;
+    bool async = false;
     template <typename T>
     T* Alloc(size_t n) {
         void* p = nullptr;
         if (n == 0)
             n = 1;
-        PG_CUDA(cudaMalloc(&p, n * sizeof(T)));
+        if (async)
+            PG_CUDA(cudaMallocAsync(&p, n * sizeof(T), stream));
+        else
+            PG_CUDA(cudaMalloc(&p, n * sizeof(T)));
         ptrs.push_back(p);
         return (T*)p;
     }
@@ -71,7 +78,7 @@ struct DevMem {
     }
     void Free() {
         for (void* p : ptrs)
-            cudaFree(p);
+            async ? cudaFreeAsync(p, stream) : cudaFree(p);
         ptrs.clear();
     }
     ~DevMem() { Free(); }
@@ -195,7 +202,7 @@ struct pg_ctx {
     int* h_counts = nullptr;               // pinned
     pg::DevMem req_buf;                    // per-call request table
     std::string last_error;
-    pg_tuning tuning{1 << 21, 64, 1, 64};
+    pg_tuning tuning{1 << 22, 128, 1, 32};  // fastest on the volume benchmark (B200 sweep)
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
@@ -240,6 +247,7 @@ static void Put(float* dst, V3 v) {
 
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     DevMem upload;  // linear density grids: inputs of the majorant and brick builds only
+    upload.stream = ctx->stream, upload.async = true;
     Require(d != nullptr && sceneId != nullptr, "null scene description or scene id pointer");
     Require(d->num_shapes >= 0 && (d->num_shapes == 0 || d->shapes), "bad shapes array");
     Require(d->num_materials >= 0 && (d->num_materials == 0 || d->materials), "bad materials array");
@@ -253,6 +261,9 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         Require((int64_t)d->indices[i] < d->num_vertices, "triangle index out of range");
 
     auto sc = std::make_unique<DeviceScene>();
+    // Scene memory is stream-ordered on the context's stream, so that uploading and
+    // releasing scenes reuses the pool's memory instead of mapping and unmapping it.
+    sc->mem.stream = ctx->stream, sc->mem.async = true;
     cudaStream_t st = ctx->stream;
     SceneDev& S = sc->dev;
     const int ns = d->num_shapes;
@@ -1169,6 +1180,13 @@ extern "C" pg_status pg_create(pg_ctx** out, int device) {
         PG_CUDA(cudaSetDevice(device));
         ctx->device = device;
         PG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        // Keep freed stream-ordered memory in the device's pool for later scenes (this
+        // process only; nothing outlives it).
+        cudaMemPool_t mp;
+        if (cudaDeviceGetDefaultMemPool(&mp, device) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
         PG_CUDA(cudaEventCreate(&ctx->ev0));
         PG_CUDA(cudaEventCreate(&ctx->ev1));
         ctx->counts = ctx->small.Alloc<int>(kNumCounts);
@@ -1193,6 +1211,8 @@ extern "C" void pg_destroy(pg_ctx* ctx) {
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
     ctx->scenes.clear();
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
     ctx->pool.mem.Free();
     ctx->film.mem.Free();
     ctx->small.Free();
