@@ -40,6 +40,13 @@
 #else
 #define PG_SHADE_BOUNDS
 #endif
+// Register cap of the shadow kernel with media (128-thread blocks).  Measured on B200
+// (volume benchmark): no cap 128 registers, 1702 Mpaths/s; 6 blocks (80) 1858; 8 blocks
+// (64) 1929.  The surface-only variant keeps its natural 72 registers (7 blocks): capped at
+// 64 it lost 3 % on the mesh.
+#ifndef PG_SHADOW_MIN_BLOCKS
+#define PG_SHADOW_MIN_BLOCKS 8
+#endif
 
 namespace pg {
 
@@ -837,7 +844,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
 }
 
 template <int M, bool MULTI, bool GUIDE = false, bool MEDIA = true>
-__global__ void k_shadow(RenderParams P, SceneDev S0) {
+__global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shadow(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
     __shared__ int claimOff[32];

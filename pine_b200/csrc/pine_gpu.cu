@@ -799,7 +799,9 @@ static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer
         time(PG_KERNEL_TRACE, [&]() {
             k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
         });
-    const size_t shadeSmem = FUSED ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
+    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
+    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
     if (FUSED && shadeSmem > 48 * 1024)
         PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)shadeSmem));
@@ -813,9 +815,9 @@ static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer
     if (!FUSED)
         time(PG_KERNEL_SHADOW, [&]() {
             if (!w.media)
-                k_shadow<M, MULTI, false, false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+                k_shadow<M, MULTI, false, false><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
             else
-                k_shadow<M, MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+                k_shadow<M, MULTI><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
         });
     // Queue swap; counted with the fill kernel.
     time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
@@ -857,7 +859,9 @@ static void LaunchGuidedBody(pg_ctx* ctx, Wave& w, int n, LaunchTimer* timer, Re
         time(PG_KERNEL_TRACE, [&]() {
             k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
         });
-    const size_t shadeSmem = FUSED ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
+    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
+    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
     if (FUSED && shadeSmem > 48 * 1024)
         PG_CUDA(cudaFuncSetAttribute(k_shade<M, false, FUSED, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shadeSmem));
@@ -877,7 +881,7 @@ static void LaunchGuidedBody(pg_ctx* ctx, Wave& w, int n, LaunchTimer* timer, Re
     });
     if (!FUSED)
         time(PG_KERNEL_SHADOW, [&]() {
-            k_shadow<M, false, true><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+            k_shadow<M, false, true><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
         });
     time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
 }
