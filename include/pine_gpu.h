@@ -69,11 +69,58 @@ enum { PG_BSDF_DIFFUSE = 0, PG_BSDF_CONDUCTOR = 1, PG_BSDF_DIELECTRIC = 2 };
 enum { PG_MATERIAL_LAYERED = 0, PG_MATERIAL_EMISSIVE = 1 };
 #define PG_MAX_LAYERS 4
 
+/* ---- shader nodes (src/core/node.h:52-398, CreateNode node.cpp:33-98) ----
+ * A node-driven parameter is a program in pg_scene_desc.node_ops: postfix operations on
+ * a stack of 3-vectors, evaluated at the shading point's position p, geometric normal n and
+ * texture coordinates uv (pine's Interaction::uv per shape, geometry.cpp:95-203).  Pine
+ * evaluates a node either as a float (EvalFloat) or as a vec3 (EvalVec3), with different
+ * results for some nodes; a program is compiled for one of the two and its value is the
+ * top of the stack (a float is held in all three components).  pg_load_scene_file builds
+ * programs from pine's node syntax; a pine adapter flattens Node graphs the same way. */
+enum {
+    PG_NODE_END = 0,       /* end of program */
+    PG_NODE_CONST = 1,     /* push (c[0], c[1], c[2]) */
+    PG_NODE_POSITION = 2,  /* push p */
+    PG_NODE_NORMAL = 3,    /* push n */
+    PG_NODE_TEXCOORD = 4,  /* push (u, v, 0) */
+    PG_NODE_DECOMPOSE = 5, /* a -> (a[arg], a[arg], a[arg]) */
+    PG_NODE_COMPOSITE = 6, /* a, b, c -> (a.x, b.x, c.x) */
+    PG_NODE_ADD = 7,       /* a, b -> a + b (per component) */
+    PG_NODE_SUB = 8,
+    PG_NODE_MUL = 9,
+    PG_NODE_DIV = 10,
+    PG_NODE_MULADD = 11,   /* a, m, b -> a * m + b */
+    PG_NODE_LENGTH = 12,   /* a -> |a| in all components */
+    PG_NODE_SQR = 13,
+    PG_NODE_SQRT = 14,     /* pstd::sqrt per component */
+    PG_NODE_POW = 15,      /* a, e -> pstd::pow(a_i, e.x) */
+    PG_NODE_SIN = 16,
+    PG_NODE_COS = 17,
+    PG_NODE_TAN = 18,
+    PG_NODE_FRACT = 19,    /* pstd::fract per component */
+    PG_NODE_CHECKER = 20,  /* p, f -> Checkerboard (node.h:307-316) in all components */
+    PG_NODE_NOISE = 21,    /* p, f, o -> Turbulence(p, (int)f.x, (int)o.x) (noise.cpp) */
+    PG_NODE_NOISE3D = 22,  /* p, f, o -> Turbulence3D(p, (int)f.x, (int)o.x) */
+    PG_NODE_INVERT = 23    /* a -> 1 - a */
+};
+#define PG_NODE_MAX_OPS 256   /* longest program */
+#define PG_NODE_MAX_STACK 16  /* deepest stack */
+
+typedef struct pg_node_op {
+    int32_t op;        /* PG_NODE_* */
+    int32_t arg;       /* DECOMPOSE: component */
+    float c[3];        /* CONST: value */
+} pg_node_op;
+
 typedef struct pg_bsdf {
     int32_t type;
     float albedo[3];
     float roughness; /* alpha = clamp(roughness^2, 0.001, 1) (bxdf.cpp:37,88) */
     float eta;
+    /* Node programs replacing the constants above: 1 + the index of the program's first
+     * op in pg_scene_desc.node_ops, or 0 for none (zero-initialised records keep their
+     * constants).  albedo is a vec3 program, roughness and eta float programs. */
+    int32_t albedo_node, roughness_node, eta_node;
 } pg_bsdf;
 
 typedef struct pg_material {
@@ -81,6 +128,8 @@ typedef struct pg_material {
     int32_t num_layers;            /* layered: layers[0] is the top layer (material.cpp:33-43) */
     pg_bsdf layers[PG_MAX_LAYERS];
     float emission[3];             /* emissive: one-sided radiance (material.h:60-65) */
+    int32_t bump_node;             /* float program of Material::bumpMap (1 + first op,
+                                      0 none; BumpNormal, material.cpp:46-60) */
 } pg_material;
 
 /* ---- lights (src/core/light.h:136-187).  Area lights are not listed here: every shape
@@ -146,6 +195,8 @@ typedef struct pg_scene_desc {
     int32_t light_sampler;           /* PG_LIGHT_SAMPLER_* (lightsampler.cpp:41-51) */
     int32_t max_depth;               /* Path{maxDepth}, pine's default 4 (integrator.cpp:55) */
     int32_t samples_per_pixel;       /* Path{sampler{samplesPerPixel}} */
+    int32_t num_node_ops;            /* shader-node programs of the materials (may be 0) */
+    const pg_node_op* node_ops;
 } pg_scene_desc;
 
 /* ---- render requests ---- */
@@ -329,6 +380,16 @@ void pg_guide_sample(const float* raw, const float* u, int64_t n, float* dirs);
 /* Per-sample loss -w log q(d) and its gradient with respect to the 40 raw outputs. */
 void pg_guide_loss_grad(const float* raw, const float* dir_weight, int64_t n, float* grad,
                         float* loss);
+
+/* ---- shader nodes on the host (the device's evaluator, for tests) ----
+ * Evaluate the node program `ref` (1-based, as in pg_bsdf) of ops[0..num_ops) with
+ * PG_MATH_PINE or PG_MATH_FAST numerics.  inputs: n x 8 floats (p.xyz, n.xyz, u, v);
+ * out: n x 3.  pg_bump_normal applies the program as a bump map (BumpNormal,
+ * material.cpp:46-60) to inputs of n x 14 floats (p, n, u, v, dpdu, dpdv). */
+pg_status pg_eval_nodes(const pg_node_op* ops, int32_t num_ops, int32_t ref, int32_t math_mode,
+                        const float* inputs, int64_t n, float* out);
+pg_status pg_bump_normal(const pg_node_op* ops, int32_t num_ops, int32_t ref, int32_t math_mode,
+                         const float* inputs, int64_t n, float* out);
 
 /* ---- synthetic scene inputs (seeded) ---- */
 /* n^3 fractal-noise cloud, x fastest; ~nonzero_fraction of voxels > 0; max exactly 1. */

@@ -98,6 +98,9 @@ class Restatement:
         self._parsed = pine_b200.ParsedScene(scene_path)
         self.desc = self._parsed.desc
         self._s = lib().po_scene_new(ctypes.byref(self.desc))
+        if not self._s:
+            self._parsed.close()
+            raise ValueError("the restatement covers constant-valued materials only")
         self.width, self.height = self.desc.camera.width, self.desc.camera.height
 
     def close(self):

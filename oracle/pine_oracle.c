@@ -346,6 +346,16 @@ struct po_scene {
 };
 
 po_scene* po_scene_new(const pg_scene_desc* d) {
+    /* The restatement covers constant-valued materials; node graphs (textures, bump
+     * maps) are checked against pine's own evaluation instead. */
+    for (int i = 0; i < d->num_materials; i++) {
+        const pg_material* m = &d->materials[i];
+        if (m->bump_node)
+            return NULL;
+        for (int l = 0; l < m->num_layers; l++)
+            if (m->layers[l].albedo_node || m->layers[l].roughness_node || m->layers[l].eta_node)
+                return NULL;
+    }
     po_scene* s = (po_scene*)calloc(1, sizeof(po_scene));
     s->nshapes = d->num_shapes;
     s->shapes = (oshape*)calloc(d->num_shapes + 1, sizeof(oshape));

@@ -29,6 +29,7 @@ void po_stofs(const char* s, int64_t n, float out[3]);
 void po_bsdf(const float* in, float* out);
 
 typedef struct po_scene po_scene;
+/* NULL for scenes whose materials use shader-node programs (not restated here). */
 po_scene* po_scene_new(const pg_scene_desc* desc);
 void po_scene_free(po_scene* s);
 

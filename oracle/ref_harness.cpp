@@ -20,12 +20,19 @@
 //   density <scene.txt> <in> <out>   GridMedium::Density (src/core/medium.cpp:141-160).
 //   time   <scene.txt> [repeats] [spp]  wall time of the stock Integrator::Render() only
 //                                    (BVH build and file loading excluded), repeated.
+//   nodes  <graphs.txt> <in> <out>   CreateNode (src/core/node.cpp:33-98) of the blocks
+//                                    g0, g1, ... and their EvalFloat / EvalVec3 at rows of
+//                                    (p.xyz, n.xyz, u, v); out: per graph and row 4 floats.
+//   bump   <graphs.txt> <in> <out>   Material::BumpNormal (material.cpp:46-60) with g0 as
+//                                    the bump map at rows of (p, n, uv, dpdu, dpdv).
 #include <core/scene.h>
 #include <core/scattering.h>
 #include <util/fileio.h>
 #include <util/parser.h>
 #include <util/parallel.h>
 #include <impl/integrator/path.h>
+#include <core/material.h>
+#include <core/node.h>
 
 // BVHImpl::Intersect is a template defined in this file; it is compiled here (and left
 // out of the library objects) so that the triangle index is reachable.
@@ -356,6 +363,64 @@ int Time(const char* scenePath, int repeats, int spp) {
 
 }  // namespace
 
+std::string ReadText(const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    std::string t;
+    if (!f)
+        return t;
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0)
+        t.append(buf, k);
+    std::fclose(f);
+    return t;
+}
+
+int Nodes(const char* graphsPath, const char* inPath, const char* outPath) {
+    std::string text = ReadText(graphsPath);
+    Parameters params = Parse(text.c_str());
+    std::vector<float> in = ReadF32(inPath);
+    size_t rows = in.size() / 8;
+    std::vector<float> out;
+    for (int g = 0;; g++) {
+        std::string nm = "g" + std::to_string(g);
+        pstd::string name(nm.c_str());
+        if (!params.HasSubset(name))
+            break;
+        Node* node = CreateNode(params[name]);
+        for (size_t i = 0; i < rows; i++) {
+            const float* r = &in[i * 8];
+            NodeEvalCtx c(vec3(r[0], r[1], r[2]), vec3(r[3], r[4], r[5]), vec2(r[6], r[7]));
+            vec3 v = node->EvalVec3(c);
+            out.push_back(node->EvalFloat(c));
+            out.push_back(v.x), out.push_back(v.y), out.push_back(v.z);
+        }
+        delete node;
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+int Bump(const char* graphsPath, const char* inPath, const char* outPath) {
+    std::string text = ReadText(graphsPath);
+    std::string full = "m: Layered{\n layer0: Diffuse{\n albedo: 0.5\n }\n bumpMap: " +
+                       text.substr(text.find(':') + 1) + "\n}\n";
+    Parameters params = Parse(full.c_str());
+    Material material = CreateMaterial(params["m"]);
+    std::vector<float> in = ReadF32(inPath);
+    size_t rows = in.size() / 14;
+    std::vector<float> out(rows * 3);
+    for (size_t i = 0; i < rows; i++) {
+        const float* r = &in[i * 14];
+        MaterialEvalCtx c(vec3(r[0], r[1], r[2]), vec3(r[3], r[4], r[5]), vec2(r[6], r[7]),
+                          vec3(r[8], r[9], r[10]), vec3(r[11], r[12], r[13]), vec3(0, 0, 1));
+        vec3 n = material.BumpNormal(c);
+        out[3 * i] = n.x, out[3 * i + 1] = n.y, out[3 * i + 2] = n.z;
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::fprintf(stderr, "usage: pine_ref <mode> ...\n");
@@ -378,6 +443,10 @@ int main(int argc, char** argv) {
         return CameraRays(argv[2], argv[3], argv[4]);
     if (mode == "density" && argc == 5)
         return Density(argv[2], argv[3], argv[4]);
+    if (mode == "nodes" && argc == 5)
+        return Nodes(argv[2], argv[3], argv[4]);
+    if (mode == "bump" && argc == 5)
+        return Bump(argv[2], argv[3], argv[4]);
     if (mode == "time" && argc >= 3 && argc <= 5)
         return Time(argv[2], argc >= 4 ? std::atoi(argv[3]) : 1, argc == 5 ? std::atoi(argv[4]) : 0);
     std::fprintf(stderr, "bad arguments for mode %s\n", mode.c_str());

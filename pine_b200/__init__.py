@@ -69,14 +69,21 @@ class Shape(ctypes.Structure):
                 ("p", ctypes.c_float * 12)]
 
 
+class NodeOp(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int32), ("arg", ctypes.c_int32), ("c", ctypes.c_float * 3)]
+
+
 class Bsdf(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int32), ("albedo", ctypes.c_float * 3),
-                ("roughness", ctypes.c_float), ("eta", ctypes.c_float)]
+                ("roughness", ctypes.c_float), ("eta", ctypes.c_float),
+                ("albedo_node", ctypes.c_int32), ("roughness_node", ctypes.c_int32),
+                ("eta_node", ctypes.c_int32)]
 
 
 class Material(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int32), ("num_layers", ctypes.c_int32),
-                ("layers", Bsdf * 4), ("emission", ctypes.c_float * 3)]
+                ("layers", Bsdf * 4), ("emission", ctypes.c_float * 3),
+                ("bump_node", ctypes.c_int32)]
 
 
 class Light(ctypes.Structure):
@@ -106,7 +113,8 @@ class SceneDesc(ctypes.Structure):
                 ("num_media", ctypes.c_int32), ("media", ctypes.POINTER(Medium)),
                 ("num_lights", ctypes.c_int32), ("lights", ctypes.POINTER(Light)),
                 ("camera", Camera), ("light_sampler", ctypes.c_int32),
-                ("max_depth", ctypes.c_int32), ("samples_per_pixel", ctypes.c_int32)]
+                ("max_depth", ctypes.c_int32), ("samples_per_pixel", ctypes.c_int32),
+                ("num_node_ops", ctypes.c_int32), ("node_ops", ctypes.POINTER(NodeOp))]
 
 
 SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
@@ -193,6 +201,10 @@ def lib():
         "pg_guide_pdf": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_sample": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_loss_grad": (None, [_F, _F, ctypes.c_int64, _F, _F]),
+        "pg_eval_nodes": (st, [_P(NodeOp), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                               _F, ctypes.c_int64, _F]),
+        "pg_bump_normal": (st, [_P(NodeOp), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                _F, ctypes.c_int64, _F]),
     }
     for name, (res, args) in sig.items():
         if hasattr(L, name):
@@ -259,6 +271,27 @@ def guide_loss_grad(raw, dir_weight):
     loss = np.empty(r.shape[0], np.float32)
     lib().pg_guide_loss_grad(_fptr(r), _fptr(dw), r.shape[0], _fptr(g), _fptr(loss))
     return loss, g
+
+
+def _node_call(name, desc, ref, math_mode, inputs, cols):
+    x = _f32(inputs, cols)
+    out = np.empty((x.shape[0], 3), np.float32)
+    st = getattr(lib(), name)(desc.node_ops, desc.num_node_ops, int(ref), MATH_MODES[math_mode],
+                              _fptr(x), x.shape[0], _fptr(out))
+    if st != PG_OK:
+        raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
+    return out
+
+
+def eval_nodes(desc, ref, inputs, math_mode="pine"):
+    """Node program `ref` (1-based, from a Bsdf or Material of the SceneDesc) evaluated at
+    inputs (n x 8: p, n, u, v) on the host; n x 3."""
+    return _node_call("pg_eval_nodes", desc, ref, math_mode, inputs, 8)
+
+
+def bump_normal(desc, ref, inputs, math_mode="pine"):
+    """Shading normal of bump program `ref` at inputs (n x 14: p, n, u, v, dpdu, dpdv)."""
+    return _node_call("pg_bump_normal", desc, ref, math_mode, inputs, 14)
 
 
 class ParsedScene:

@@ -29,6 +29,9 @@ struct BsdfDev {
     float albedo[3];
     float alpha;  // clamp(roughness^2, 0.001, 1)
     float eta;
+    // Shader-node programs replacing albedo / roughness / eta: 1 + first op in
+    // SceneDev::node_ops, 0 = the constant above.
+    int albedo_prog, rough_prog, eta_prog;
 };
 
 struct MaterialDev {
@@ -36,6 +39,8 @@ struct MaterialDev {
     int num_layers;
     float emission[3];
     BsdfDev layers[4];
+    int bump_prog;  // 1 + first op of the bump map's program, 0 = none
+    int textured;   // some parameter or the normal comes from node programs
 };
 
 enum LightKind { kLightPoint = 0, kLightDirectional = 1, kLightSky = 2, kLightConstant = 3,
@@ -104,6 +109,7 @@ struct SceneDev {
     int num_media;
     int has_null_surfaces;
     CameraDev cam;
+    const pg_node_op* node_ops;  // shader-node programs of the materials
     float guide_lo[3];       // scene bounds the guiding network's position encoding maps
     float guide_inv[3];      // to [0,1]^3: lo and 1 / extent
 };

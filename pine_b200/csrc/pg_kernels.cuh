@@ -24,6 +24,7 @@
 #pragma once
 
 #include "guide_net.cuh"
+#include "pg_nodes.h"
 #include "pg_shade.cuh"
 
 // Build-time register cap of the shading kernel.  Measured on B200 (volume benchmark):
@@ -475,6 +476,73 @@ __device__ void Surface(const SceneDev& S, V3 o, V3 d, float4 h, SurfaceInfo& si
     }
 }
 
+// Interaction::uv, dpdu and dpdv of a hit, as pine's shapes set them: plane
+// (geometry.cpp:95-107), sphere (:129-147), rect (:176-194), triangles (bvh.cpp:690-708,
+// geometry.h:311-314: barycentric uv, dpdu = v1 - v0, dpdv = v2 - v0).
+template <int M>
+__device__ void SurfaceParam(const SceneDev& S, V3 o, V3 d, float4 h, const SurfaceInfo& si, float& u,
+                             float& v, V3& dpdu, V3& dpdv) {
+    const int prim = __float_as_int(h.y);
+    const ShapeDev& sh = S.shapes[si.shape];
+    if (prim <= -2) {
+        V3 pos = v3(sh.p[0], sh.p[1], sh.p[2]);
+        dpdu = v3(sh.p[6], sh.p[7], sh.p[8]);
+        dpdv = v3(sh.p[9], sh.p[10], sh.p[11]);
+        V3 p = o + h.x * d;
+        u = Dot(p - pos, dpdu);
+        v = Dot(p - pos, dpdv);
+        return;
+    }
+    if (sh.type == PG_SHAPE_SPHERE) {
+        V3 n = si.n;
+        float phi = PMath<M>::atan2(n.y, n.x);
+        if (phi < 0.0f)
+            phi = kPi * 2 + phi;  // Phi2pi (vecmath.h:1243-1246)
+        float theta = PMath<M>::acos(n.z);
+        float st = PMath<M>::sin(theta), ct = PMath<M>::cos(theta);
+        float sp = PMath<M>::sin(phi), cp = PMath<M>::cos(phi);
+        dpdu = v3(st * -sp, st * cp, 0.0f);
+        dpdv = v3(ct * cp, ct * sp, -st);
+        u = phi, v = theta;
+        return;
+    }
+    if (sh.type == PG_SHAPE_RECT) {
+        u = h.z + 0.5f, v = h.w + 0.5f;
+        dpdu = v3(sh.p[3], sh.p[4], sh.p[5]);
+        dpdv = v3(sh.p[6], sh.p[7], sh.p[8]);
+        return;
+    }
+    float4 e1 = __ldg(&S.prims[3 * prim + 1]), e2 = __ldg(&S.prims[3 * prim + 2]);
+    u = h.z, v = h.w;
+    dpdu = F3(e1);
+    dpdv = F3(e2);
+}
+
+// A textured material at a hit: the bump map tilts the normal (Material::BumpNormal,
+// path.cpp:48), then node programs give each layer's albedo, roughness and eta at
+// (p, bumped n, uv), as every BSDF call of pine evaluates them (bxdf.cpp).  Kept out of
+// line so that untextured shading does not carry the interpreter's registers.
+template <int M>
+__device__ __noinline__ void TextureMaterial(const SceneDev& S, V3 o, V3 d, float4 h, SurfaceInfo& si,
+                                             MaterialDev& m) {
+    float u, v;
+    V3 dpdu, dpdv;
+    SurfaceParam<M>(S, o, d, h, si, u, v, dpdu, dpdv);
+    if (m.bump_prog)
+        si.n = BumpNormal<M>(S.node_ops + m.bump_prog - 1, si.p, si.n, u, v, dpdu, dpdv);
+    for (int l = 0; l < m.num_layers; l++) {
+        BsdfDev& b = m.layers[l];
+        if (b.albedo_prog) {
+            V3 a = EvalNodes<M>(S.node_ops + b.albedo_prog - 1, si.p, si.n, u, v);
+            b.albedo[0] = a.x, b.albedo[1] = a.y, b.albedo[2] = a.z;
+        }
+        if (b.rough_prog)
+            b.alpha = Clamp(Sqr(EvalNodes<M>(S.node_ops + b.rough_prog - 1, si.p, si.n, u, v).x), 0.001f, 1.0f);
+        if (b.eta_prog)
+            b.eta = EvalNodes<M>(S.node_ops + b.eta_prog - 1, si.p, si.n, u, v).x;
+    }
+}
+
 // Transmittance of a shadow ray (RayIntegrator::IntersectTr, integrator.cpp:68-87):
 // zero if a surface with a material blocks it, otherwise the product of the media's
 // transmittances along the segments between null surfaces.
@@ -616,7 +684,7 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
 // normal's frame cannot track; with half of their samples spent on it, conductors measured
 // up to twice the plain variance, so they keep plain BSDF sampling.
 __device__ __forceinline__ bool GuideEligible(const MaterialDev& m) {
-    return m.type == PG_MATERIAL_LAYERED && m.num_layers == 1 &&
+    return m.type == PG_MATERIAL_LAYERED && m.num_layers == 1 && !m.textured &&
            m.layers[0].type == PG_BSDF_DIFFUSE;
 }
 
@@ -715,7 +783,14 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             no = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, d));
             nmed = Dot(d, si.n) > 0 ? medOut : medIn;
         } else {
-            const MaterialDev& mat = S.materials[sh.material];
+            const MaterialDev* mp = &S.materials[sh.material];
+            MaterialDev tmat;
+            if (mp->textured) {
+                tmat = *mp;
+                TextureMaterial<M>(S, o, d, h, si, tmat);
+                mp = &tmat;
+            }
+            const MaterialDev& mat = *mp;
             if (mat.type == PG_MATERIAL_EMISSIVE) {
                 // path.cpp:51-60; Le is one-sided (material.h:60-65).
                 V3 le = Dot(-d, si.n) > 0.0f ? v3(mat.emission[0], mat.emission[1], mat.emission[2])
@@ -1140,8 +1215,18 @@ __global__ void k_intersect(SceneDev S, const float* rays, int64_t n, int32_t* s
     if (tOut)
         tOut[i] = found ? h.t : 0.0f;
     if (uvOut) {
-        uvOut[2 * i] = found ? h.u : 0.0f;
-        uvOut[2 * i + 1] = found ? h.v : 0.0f;
+        // Interaction::uv of the hit, with pine's numerics.
+        float u = 0.0f, v = 0.0f;
+        if (found) {
+            V3 o = v3(r[0], r[1], r[2]), d = v3(r[3], r[4], r[5]);
+            float4 hh = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+            SurfaceInfo si;
+            Surface<kPine>(S, o, d, hh, si);
+            V3 dpdu, dpdv;
+            SurfaceParam<kPine>(S, o, d, hh, si, u, v, dpdu, dpdv);
+        }
+        uvOut[2 * i] = u;
+        uvOut[2 * i + 1] = v;
     }
     if (err)
         atomicOr(errOut, err);

@@ -281,6 +281,8 @@ struct PMath<kPine> {
     static PG_HD float sin(float x) { return PstdSin(x); }
     static PG_HD float acos(float x) { return PstdAcos(x); }
     static PG_HD float atan2(float y, float x) { return PstdAtan2(y, x); }
+    static PG_HD float tan(float x) { return PstdTan(x); }
+    static PG_HD float pow(float x, float e) { return PstdPow(x, e); }
     static PG_HD float pow5(float x) { return PstdPow(x, 5.0f); }
 };
 
@@ -294,6 +296,8 @@ struct PMath<kFast> {
     static __device__ __forceinline__ float sin(float x) { return __sinf(x); }
     static __device__ __forceinline__ float acos(float x) { return acosf(Clamp(x, -1.0f, 1.0f)); }
     static __device__ __forceinline__ float atan2(float y, float x) { return atan2f(y, x); }
+    static __device__ __forceinline__ float tan(float x) { return tanf(x); }
+    static __device__ __forceinline__ float pow(float x, float e) { return powf(x, e); }
 #else
     static inline float sqrt(float x) { return std::sqrt(x); }
     static inline float log(float x) { return std::log(x); }
@@ -302,6 +306,8 @@ struct PMath<kFast> {
     static inline float sin(float x) { return std::sin(x); }
     static inline float acos(float x) { return std::acos(Clamp(x, -1.0f, 1.0f)); }
     static inline float atan2(float y, float x) { return std::atan2(y, x); }
+    static inline float tan(float x) { return std::tan(x); }
+    static inline float pow(float x, float e) { return std::pow(x, e); }
 #endif
     static PG_HD float pow5(float x) { return x * x * x * x * x; }
 };

@@ -245,6 +245,31 @@ static void Put(float* dst, V3 v) {
     dst[0] = v.x, dst[1] = v.y, dst[2] = v.z;
 }
 
+// Validates the node program a material refers to (1-based, 0 = none): it must lie in
+// node_ops, end within PG_NODE_MAX_OPS ops, use known ops, never pop an empty stack or grow
+// it past PG_NODE_MAX_STACK, and leave a value.  Returns the reference.
+static int CheckNodeProgram(const pg_scene_desc* d, int32_t ref) {
+    if (ref == 0)
+        return 0;
+    Require(ref >= 1 && ref <= d->num_node_ops && d->node_ops != nullptr,
+            "node program reference out of range");
+    int depth = 0;
+    for (int k = ref - 1; k < d->num_node_ops && k - (ref - 1) < PG_NODE_MAX_OPS; k++) {
+        const pg_node_op& o = d->node_ops[k];
+        if (o.op == PG_NODE_END) {
+            Require(depth >= 1, "node program leaves no value");
+            return ref;
+        }
+        const int eff = NodeStackEffect(o.op);
+        Require(eff > -16, "unknown node op");
+        Require(depth >= NodeOperands(o.op), "node program pops an empty stack");
+        Require(o.op != PG_NODE_DECOMPOSE || (o.arg >= 0 && o.arg <= 2), "Decompose component out of range");
+        depth += eff;
+        Require(depth <= PG_NODE_MAX_STACK, "node program deeper than PG_NODE_MAX_STACK");
+    }
+    throw Failure{PG_ERR_INVALID_ARG, "node program without PG_NODE_END"};
+}
+
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     DevMem upload;  // linear density grids: inputs of the majorant and brick builds only
     upload.stream = ctx->stream, upload.async = true;
@@ -289,7 +314,13 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
             std::memcpy(o.layers[l].albedo, b.albedo, sizeof(b.albedo));
             o.layers[l].alpha = Clamp(Sqr(b.roughness), 0.001f, 1.0f);
             o.layers[l].eta = b.eta;
+            o.layers[l].albedo_prog = CheckNodeProgram(d, b.albedo_node);
+            o.layers[l].rough_prog = CheckNodeProgram(d, b.roughness_node);
+            o.layers[l].eta_prog = CheckNodeProgram(d, b.eta_node);
+            o.textured |= b.albedo_node | b.roughness_node | b.eta_node;
         }
+        o.bump_prog = m.type == PG_MATERIAL_LAYERED ? CheckNodeProgram(d, m.bump_node) : 0;
+        o.textured = (o.textured || o.bump_prog) ? 1 : 0;
     }
 
     // Shapes and their derived constants, computed with pine's numerics.
@@ -644,6 +675,9 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         S.prim_local = sc->mem.Upload(plocal, st);
         S.has_bvh = 1;
     }
+    S.node_ops = d->num_node_ops > 0
+                     ? sc->mem.Upload(std::vector<pg_node_op>(d->node_ops, d->node_ops + d->num_node_ops), st)
+                     : nullptr;
     S.shapes = sc->mem.Upload(shapes, st);
     S.num_shapes = ns;
     S.planes = sc->mem.Upload(planes, st);
@@ -2113,4 +2147,45 @@ extern "C" void pg_guide_loss_grad(const float* raw, const float* dir_weight, in
         loss[i] = GuideLossGrad(raw + kGuideOutputs * i, v3(d[0], d[1], d[2]), d[3], 1.0f,
                                 grad + kGuideOutputs * i);
     }
+}
+
+// ================================================================ shader nodes on the host
+extern "C" pg_status pg_eval_nodes(const pg_node_op* ops, int32_t num_ops, int32_t ref,
+                                   int32_t math_mode, const float* inputs, int64_t n, float* out) {
+    return Guard(nullptr, [&]() {
+        pg_scene_desc d{};
+        d.num_node_ops = num_ops;
+        d.node_ops = ops;
+        Require(ref >= 1 && CheckNodeProgram(&d, ref) == ref, "bad node program reference");
+        Require(n >= 0 && (n == 0 || (inputs && out)), "bad input or output arrays");
+        Require(math_mode == PG_MATH_PINE || math_mode == PG_MATH_FAST, "unknown math mode");
+        for (int64_t i = 0; i < n; i++) {
+            const float* r = inputs + 8 * i;
+            V3 p = v3(r[0], r[1], r[2]), nn = v3(r[3], r[4], r[5]);
+            V3 v = math_mode == PG_MATH_PINE ? EvalNodes<kPine>(ops + ref - 1, p, nn, r[6], r[7])
+                                             : EvalNodes<kFast>(ops + ref - 1, p, nn, r[6], r[7]);
+            out[3 * i] = v.x, out[3 * i + 1] = v.y, out[3 * i + 2] = v.z;
+        }
+    });
+}
+
+extern "C" pg_status pg_bump_normal(const pg_node_op* ops, int32_t num_ops, int32_t ref,
+                                    int32_t math_mode, const float* inputs, int64_t n, float* out) {
+    return Guard(nullptr, [&]() {
+        pg_scene_desc d{};
+        d.num_node_ops = num_ops;
+        d.node_ops = ops;
+        Require(ref >= 1 && CheckNodeProgram(&d, ref) == ref, "bad node program reference");
+        Require(n >= 0 && (n == 0 || (inputs && out)), "bad input or output arrays");
+        Require(math_mode == PG_MATH_PINE || math_mode == PG_MATH_FAST, "unknown math mode");
+        for (int64_t i = 0; i < n; i++) {
+            const float* r = inputs + 14 * i;
+            V3 p = v3(r[0], r[1], r[2]), nn = v3(r[3], r[4], r[5]);
+            V3 du = v3(r[8], r[9], r[10]), dv = v3(r[11], r[12], r[13]);
+            V3 v = math_mode == PG_MATH_PINE
+                       ? BumpNormal<kPine>(ops + ref - 1, p, nn, r[6], r[7], du, dv)
+                       : BumpNormal<kFast>(ops + ref - 1, p, nn, r[6], r[7], du, dv);
+            out[3 * i] = v.x, out[3 * i + 1] = v.y, out[3 * i + 2] = v.z;
+        }
+    });
 }

@@ -26,6 +26,7 @@
 #include <stdexcept>
 
 #include "pg_math.h"
+#include "pg_nodes.h"
 
 namespace pg {
 
@@ -417,7 +418,11 @@ void Warn(const std::string& msg) {
     std::fprintf(stderr, "[pine-gpu] %s\n", msg.c_str());
 }
 
-// node.cpp:33-97, restricted to constants: "k: v" literal values and Constant{float vec3}.
+int NodeStackEffectHost(int op) {
+    return NodeStackEffect(op);
+}
+
+// node.cpp:33-97 for a constant node: "k: v" literal values and Constant{float vec3}.
 struct ConstNode {
     float f;
     std::array<float, 3> v;
@@ -450,7 +455,141 @@ ConstNode CreateNode(Params& p, const std::string& what) {
     return {p.Float("float", 0.5f), p.Vec3("vec3", {0.5f, 0.5f, 0.5f})};
 }
 
-pg_bsdf CreateBSDF(Params& p) {
+// node.cpp:33-97 in full: the node graph at p, compiled into a postfix program for pine's
+// EvalVec3 (vec) or EvalFloat.  The two differ for some nodes: Position, Normal, TexCoord
+// and Composite have no float value (0, Node::EvalFloat), Constant yields its float or its
+// vec3, Noise3D is Turbulence as a float and Turbulence3D as a vec3; inputs that pine reads
+// with EvalFloat (frequency, octaves, exponents, Composite's parts) are compiled as floats.
+void EmitNode(Params& p, bool vec, std::vector<pg_node_op>& ops, const std::string& what, int depth) {
+    if (depth > 64)
+        throw SceneError(PG_ERR_UNSUPPORTED, "node graph of " + what + " nested too deeply");
+    auto op = [&](int code, int arg = 0) {
+        pg_node_op o{};
+        o.op = code;
+        o.arg = arg;
+        ops.push_back(o);
+    };
+    auto constant = [&](float f, std::array<float, 3> v) {
+        pg_node_op o{};
+        o.op = PG_NODE_CONST;
+        if (vec)
+            o.c[0] = v[0], o.c[1] = v[1], o.c[2] = v[2];
+        else
+            o.c[0] = o.c[1] = o.c[2] = f;
+        ops.push_back(o);
+    };
+    auto zero = [&]() { constant(0.0f, {0.0f, 0.0f, 0.0f}); };
+    auto emit = [&](const char* input, bool v) { EmitNode(p[input], v, ops, what, depth + 1); };
+    const std::string type = p.String("type", "");
+    struct Unary {
+        const char* name;
+        int code;
+    };
+    static const Unary kUnary[] = {{"Sqr", PG_NODE_SQR},   {"Sqrt", PG_NODE_SQRT},   {"Sin", PG_NODE_SIN},
+                                   {"Cos", PG_NODE_COS},   {"Tan", PG_NODE_TAN},     {"Fract", PG_NODE_FRACT},
+                                   {"Invert", PG_NODE_INVERT}};
+    static const Unary kBinary[] = {{"Add", PG_NODE_ADD},
+                                    {"Substract", PG_NODE_SUB},
+                                    {"Multiply", PG_NODE_MUL},
+                                    {"Divide", PG_NODE_DIV}};
+    if (type == "Constant")
+        return constant(p.Float("float"), p.Vec3("vec3"));
+    if (type == "Position")
+        return vec ? op(PG_NODE_POSITION) : zero();
+    if (type == "Normal")
+        return vec ? op(PG_NODE_NORMAL) : zero();
+    if (type == "TexCoord")
+        return vec ? op(PG_NODE_TEXCOORD) : zero();
+    if (type == "Decompose") {
+        int dim = p.Int("dimension");
+        if (dim < 0 || dim > 2)
+            throw SceneError(PG_ERR_PARSE, "Decompose dimension out of range (" + what + ")");
+        emit("input", true);
+        return op(PG_NODE_DECOMPOSE, dim);
+    }
+    if (type == "Composite") {
+        if (!vec)
+            return zero();
+        emit("inputX", false);
+        emit("inputY", false);
+        emit("inputZ", false);
+        return op(PG_NODE_COMPOSITE);
+    }
+    for (const Unary& b : kBinary)
+        if (type == b.name) {
+            emit("input", vec);
+            emit("factor", vec);
+            return op(b.code);
+        }
+    if (type == "MultiplyAdd") {
+        emit("input", vec);
+        emit("mulFactor", vec);
+        emit("addFactor", vec);
+        return op(PG_NODE_MULADD);
+    }
+    if (type == "Length") {
+        emit("input", true);
+        return op(PG_NODE_LENGTH);
+    }
+    for (const Unary& u : kUnary)
+        if (type == u.name) {
+            emit("input", vec);
+            return op(u.code);
+        }
+    if (type == "Pow") {
+        emit("input", vec);
+        emit("exp", false);
+        return op(PG_NODE_POW);
+    }
+    if (type == "Checkerboard") {
+        emit("input", true);
+        emit("frequency", false);
+        return op(PG_NODE_CHECKER);
+    }
+    if (type == "Noise" || type == "Noise3D") {
+        emit("input", true);
+        emit("frequency", false);
+        emit("octaves", false);
+        return op(type == "Noise3D" && vec ? PG_NODE_NOISE3D : PG_NODE_NOISE);
+    }
+    if (type == "Texture")
+        throw SceneError(PG_ERR_UNSUPPORTED, "Texture nodes (image files) are not supported (" + what + ")");
+    if (p.HasValue("@") && !p.values["@"].empty())
+        // The literal case (node.cpp:89-91): float from stof of the whole text, vec3 from stofs.
+        return constant(p.Float("float", p.Float("@")), p.Vec3("vec3", p.Vec3("@")));
+    if (type.empty())
+        throw SceneError(PG_ERR_PARSE, "[Parameters][GetString]cannot find \"type\" (" + what + ")");
+    Warn("[NodeInput][Create]Unknown type \"" + type + "\"");
+    return constant(p.Float("float", 0.5f), p.Vec3("vec3", {0.5f, 0.5f, 0.5f}));
+}
+
+// A BSDF or material parameter: the constant node's value (returns 0), or 1 + the first op
+// of its program in s.node_ops.
+int NodeParam(Params& p, bool vec, HostScene& s, const std::string& what, float& f,
+              std::array<float, 3>& v) {
+    std::vector<pg_node_op> prog;
+    EmitNode(p, vec, prog, what, 0);
+    if (prog.size() == 1 && prog[0].op == PG_NODE_CONST) {
+        f = prog[0].c[0];
+        v = {prog[0].c[0], prog[0].c[1], prog[0].c[2]};
+        return 0;
+    }
+    int depth = 0, maxDepth = 0;
+    for (const pg_node_op& o : prog) {
+        depth += NodeStackEffectHost(o.op);
+        maxDepth = std::max(maxDepth, depth);
+    }
+    if ((int)prog.size() + 1 > PG_NODE_MAX_OPS || maxDepth > PG_NODE_MAX_STACK)
+        throw SceneError(PG_ERR_UNSUPPORTED, "node graph of " + what + " is too large");
+    pg_node_op end{};
+    end.op = PG_NODE_END;
+    prog.push_back(end);
+    int start = (int)s.node_ops.size();
+    s.node_ops.insert(s.node_ops.end(), prog.begin(), prog.end());
+    return start + 1;
+}
+
+pg_bsdf CreateBSDF(Params& p, HostScene& s) {
     std::string type = p.String("type");
     pg_bsdf b{};
     if (type == "Conductor") {
@@ -462,24 +601,45 @@ pg_bsdf CreateBSDF(Params& p) {
             Warn("[BSDF][Create]Unknown type \"" + type + "\"");
         b.type = PG_BSDF_DIFFUSE;
     }
+    float f;
+    std::array<float, 3> v;
     if (b.type == PG_BSDF_DIELECTRIC && !p.HasSubset("albedo")) {
         b.albedo[0] = b.albedo[1] = b.albedo[2] = 1.0f;  // bxdf.cpp:176-181
     } else {
-        ConstNode a = CreateNode(p["albedo"], "albedo");
-        std::copy(a.v.begin(), a.v.end(), b.albedo);
+        b.albedo_node = NodeParam(p["albedo"], true, s, "albedo", f, v);
+        std::copy(v.begin(), v.end(), b.albedo);
     }
-    if (b.type != PG_BSDF_DIFFUSE)
-        b.roughness = CreateNode(p["roughness"], "roughness").f;
-    if (b.type == PG_BSDF_DIELECTRIC)
-        b.eta = CreateNode(p["eta"], "eta").f;
+    if (b.type != PG_BSDF_DIFFUSE) {
+        b.roughness_node = NodeParam(p["roughness"], false, s, "roughness", f, v);
+        b.roughness = f;
+    }
+    if (b.type == PG_BSDF_DIELECTRIC) {
+        b.eta_node = NodeParam(p["eta"], false, s, "eta", f, v);
+        b.eta = f;
+    }
     return b;
 }
 
-pg_material CreateMaterial(Params& p) {
+pg_material CreateMaterial(Params& p, HostScene& s) {
     std::string type = p.String("type");
     pg_material m{};
-    if (p.HasSubset("bumpMap"))
-        throw SceneError(PG_ERR_UNSUPPORTED, "bump maps are not supported");
+    if (p.HasSubset("bumpMap")) {
+        // Every bump map is a program, a constant one included: BumpNormal rebuilds the
+        // normal from dpdu x dpdv even when the map is flat (material.cpp:46-60).
+        std::vector<pg_node_op> prog;
+        EmitNode(p["bumpMap"], false, prog, "bumpMap", 0);
+        int depth = 0, maxDepth = 0;
+        for (const pg_node_op& o : prog) {
+            depth += NodeStackEffectHost(o.op);
+            maxDepth = std::max(maxDepth, depth);
+        }
+        if ((int)prog.size() + 1 > PG_NODE_MAX_OPS || maxDepth > PG_NODE_MAX_STACK)
+            throw SceneError(PG_ERR_UNSUPPORTED, "bump map node graph is too large");
+        pg_node_op end{};
+        prog.push_back(end);
+        m.bump_node = (int)s.node_ops.size() + 1;
+        s.node_ops.insert(s.node_ops.end(), prog.begin(), prog.end());
+    }
     if (type == "Emissive") {
         m.type = PG_MATERIAL_EMISSIVE;
         ConstNode c = CreateNode(p["color"], "color");
@@ -499,7 +659,7 @@ pg_material CreateMaterial(Params& p) {
     if ((int)layers.size() > PG_MAX_LAYERS)
         throw SceneError(PG_ERR_UNSUPPORTED, "more than 4 layers in a material");
     for (auto& l : layers)
-        m.layers[m.num_layers++] = CreateBSDF(*l.second);
+        m.layers[m.num_layers++] = CreateBSDF(*l.second, s);
     return m;
 }
 
@@ -516,7 +676,7 @@ void LoadSceneFile(const std::string& path, HostScene& s) {
     std::map<std::string, int> materials, media;
     for (auto& p : params.subset["Material"]) {
         materials[p.String("name")] = (int)s.materials.size();
-        s.materials.push_back(CreateMaterial(p));
+        s.materials.push_back(CreateMaterial(p, s));
     }
     for (auto& p : params.subset["Medium"]) {
         std::string type = p.String("type");
@@ -702,6 +862,8 @@ void HostScene::Describe(pg_scene_desc& d) {
     d.light_sampler = light_sampler;
     d.max_depth = max_depth;
     d.samples_per_pixel = spp;
+    d.num_node_ops = (int32_t)node_ops.size();
+    d.node_ops = node_ops.data();
 }
 
 }  // namespace pg

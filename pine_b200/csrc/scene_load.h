@@ -52,6 +52,7 @@ struct HostScene {
     std::vector<pg_medium> media;
     std::vector<std::vector<float>> densities;  // one per medium (empty if homogeneous)
     std::vector<pg_light> lights;
+    std::vector<pg_node_op> node_ops;  // shader-node programs of the materials
     pg_camera camera{};
     int light_sampler = PG_LIGHT_SAMPLER_POWER;
     int max_depth = 4;

@@ -7,6 +7,7 @@ from the seeded generators in pine_b200.scenegen; everything a test needs to rep
 not depend on the generators or on the reference being present.
 
     python tests/golden/make_golden.py           # needs oracle/_ref/pine_ref
+    python tests/golden/make_golden.py nodes pine_spheres   # only those fixtures
 """
 
 from __future__ import annotations
@@ -152,9 +153,87 @@ def image_case(name, scene, assets):
                         allow_pickle=True)
 
 
+# Shader-node graphs in pine's syntax: every node type of CreateNode (node.cpp:33-98)
+# except Texture (image files), in both evaluation modes.
+NODE_GRAPHS = [
+    "Checkerboard{\n input: TexCoord\n frequency: 4.0\n}",
+    "MultiplyAdd{\n input: Checkerboard{\n input: Position\n frequency: 2.5\n }\n"
+    " mulFactor: 0.95\n addFactor: 0.05\n}",
+    "Noise{\n input: Position\n frequency: 20\n octaves: 4.0\n}",
+    "Noise3D{\n input: Position\n frequency: 10\n octaves: 4\n}",
+    "Multiply{\n input: Noise{\n input: Position\n frequency: 20\n octaves: 4.0\n }\n"
+    " factor: 0.05\n}",
+    "Decompose{\n input: Normal\n dimension: 1\n}",
+    "Composite{\n inputX: Sin{\n input: Decompose{\n input: Position\n dimension: 0\n }\n }\n"
+    " inputY: Cos{\n input: Decompose{\n input: Position\n dimension: 2\n }\n }\n"
+    " inputZ: Tan{\n input: 0.3\n }\n}",
+    "Length{\n input: Position\n}",
+    "Sqrt{\n input: Add{\n input: Sqr{\n input: Position\n }\n factor: 1.0\n }\n}",
+    "Pow{\n input: Fract{\n input: Position\n }\n exp: 2.2\n}",
+    "Divide{\n input: Substract{\n input: TexCoord\n factor: 0.25\n }\n factor: 3.0\n}",
+    "Invert{\n input: Constant{\n float: 0.25\n vec3: 0.1 0.2 0.3\n }\n}",
+    "Add{\n input: Position\n factor: Normal\n}",
+    "Noise3D{\n input: Multiply{\n input: TexCoord\n factor: 3.0\n }\n frequency: 2.7\n"
+    " octaves: 2.9\n}",
+]
+BUMP_GRAPH = ("Multiply{\n input: Noise{\n input: Position\n frequency: 20\n octaves: 4.0\n }\n"
+              " factor: 0.05\n}")
+
+
+def nodes_kat(tmp):
+    rng = np.random.default_rng(777)
+    n = 512
+    p = np.concatenate([rng.uniform(-3, 3, (n // 2, 3)), rng.uniform(-0.2, 1.2, (n // 2, 3))])
+    nn = unit(rng.normal(size=(n, 3)))
+    uv = rng.uniform(-0.5, 1.5, (n, 2))
+    inp = np.concatenate([p, nn, uv], axis=1).astype(np.float32)
+    inp.tofile(f"{tmp}/n.in")
+    with open(f"{tmp}/graphs.txt", "w") as f:
+        for k, g in enumerate(NODE_GRAPHS):
+            f.write(f"g{k}: {g}\n")
+    run("nodes", f"{tmp}/graphs.txt", f"{tmp}/n.in", f"{tmp}/n.out")
+    out = np.fromfile(f"{tmp}/n.out", np.float32).reshape(len(NODE_GRAPHS), n, 4)
+    # Bump normals at random tangent frames.
+    du = rng.normal(size=(n, 3))
+    dv = rng.normal(size=(n, 3))
+    binp = np.concatenate([p, nn, uv, du, dv], axis=1).astype(np.float32)
+    binp.tofile(f"{tmp}/b.in")
+    with open(f"{tmp}/bump.txt", "w") as f:
+        f.write(f"g0: {BUMP_GRAPH}\n")
+    run("bump", f"{tmp}/bump.txt", f"{tmp}/b.in", f"{tmp}/b.out")
+    bout = np.fromfile(f"{tmp}/b.out", np.float32).reshape(n, 3)
+    np.savez_compressed(f"{HERE}/nodes.npz", graphs=np.array(NODE_GRAPHS, dtype=object),
+                        inputs=inp, float_out=out[:, :, 0], vec3_out=out[:, :, 1:],
+                        bump_graph=np.array(BUMP_GRAPH), bump_inputs=binp, bump_out=bout,
+                        allow_pickle=True)
+
+
+def shipped_spheres_case(tmp):
+    """pine's own scenes/spheres.txt (textures, noise, bump map, two-layer plastic) at a
+    tenth of its film size and 512 spp."""
+    src = "/root/reference/scenes/spheres.txt"
+    text = open(src).read()
+    text = text.replace("size: 1280 360", "size: 128 36").replace("samplesPerPixel: 32",
+                                                                 "samplesPerPixel: 512")
+    assert "size: 128 36" in text and "samplesPerPixel: 512" in text
+    path = f"{tmp}/pine_spheres.txt"
+    with open(path, "w") as f:
+        f.write(text)
+    image_case("pine_spheres", path, [])
+
+
 def main():
     if not os.path.exists(REF):
         sys.exit("oracle/_ref/pine_ref is missing: run `make -C oracle ref` first")
+    only = set(sys.argv[1:])
+    if only:
+        with tempfile.TemporaryDirectory() as tmp:
+            if "nodes" in only:
+                nodes_kat(tmp)
+            if "pine_spheres" in only:
+                shipped_spheres_case(tmp)
+        print("fixtures written to", HERE)
+        return
     import pine_b200
     from pine_b200 import scenegen
     L = pine_b200.lib()
@@ -196,6 +275,8 @@ def main():
         vi = scenegen.volume_scene(f"{tmp}/volume.txt", L, n=64, width=48, height=27,
                                    spp=1024, env="sky", env_radiance=1.0)
         image_case("volume", vi, ["cloud64_s0.vol"])
+        nodes_kat(tmp)
+        shipped_spheres_case(tmp)
     print("fixtures written to", HERE)
 
 

@@ -36,6 +36,11 @@ def test_hits_match_reference(ctx, tmp_path, name):
     tri = hit & (h["tri"] >= 0)
     np.testing.assert_allclose(uv[tri, 0], h["u"][tri], atol=1e-6)
     np.testing.assert_allclose(uv[tri, 1], h["v"][tri], atol=1e-6)
+    # Texture coordinates of spheres, planes and rects (Interaction::uv, which the shader
+    # nodes read through TexCoord): sphere uv goes through pstd's acos and atan2.
+    other = hit & (h["tri"] < 0)
+    np.testing.assert_allclose(uv[other, 0], h["u"][other], rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(uv[other, 1], h["v"][other], rtol=1e-5, atol=1e-5)
     ctx.release_scene(sid)
 
 

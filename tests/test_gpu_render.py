@@ -5,7 +5,9 @@ Equal-spp agreement (the acceptance test): per-pixel z-scores of the GPU image a
 pine's render, each side with its own per-pixel sample variance, pass |z| < 2.576 (the
 99% two-sided bound) for >= 98% of pixels; relative L2 of the difference must be within
 Monte Carlo error (<= 1.25x what the two variances predict), and below 1% for the volume
-scene at 1024 spp."""
+scene at 1024 spp.  `pine_spheres` is the reference's own scenes/spheres.txt (checkerboard,
+noise and 3-D noise textures, a noise bump map, a two-layer plastic) at 128 x 36 and 512
+spp, rendered by pine with its Halton sampler."""
 
 import numpy as np
 import pytest
@@ -25,7 +27,7 @@ def zfrac(a_mean, a_var, a_n, b_mean, b_var, b_n):
     return np.mean(np.abs(z[v]) < 2.576), z[v]
 
 
-@pytest.mark.parametrize("name", ["spheres", "mesh", "volume"])
+@pytest.mark.parametrize("name", ["spheres", "mesh", "volume", "pine_spheres"])
 @pytest.mark.parametrize("math_mode", ["pine", "fast"])
 def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
     z = golden(f"image_{name}.npz")

@@ -63,8 +63,8 @@ def _scene(tmp_path, body):
 
 @pytest.mark.parametrize("body,status", [
     ("Shape: Sphere{\n    position: 0 0 0\n    radius: 1\n    material: nope\n}\n", 7),
-    ("Material m: Layered{\n    layer0: Diffuse{\n        albedo: Checkerboard{\n"
-     "            input: TexCoord\n        }\n    }\n}\n", 5),
+    ("Material m: Layered{\n    layer0: Diffuse{\n        albedo: Texture{\n"
+     "            filename: wood.png\n        }\n    }\n}\n", 5),
     ("Shape: Disk{\n    position: 0 0 0\n    normal: 0 1 0\n    radius: 1\n}\n", 5),
     ("Shape: TriangleMesh{\n    file: missing.obj\n}\n", 6),
     ("Medium m: Grid{\n    file: missing.vol\n    sigma_a: 1\n    sigma_s: 1\n"
