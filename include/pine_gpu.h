@@ -178,6 +178,23 @@ typedef struct pg_camera {
 
 enum { PG_LIGHT_SAMPLER_POWER = 0, PG_LIGHT_SAMPLER_UNIFORM = 1 };
 
+/* Samplers.  PG_SAMPLER_HALTON draws pine's Halton sequence (HaltonSampler,
+ * sampler.cpp:33-96: per-pixel index, digit permutations from pine's RNG at seed 0, pine's
+ * float rounding), dimension by dimension in the order pine's PathIntegrator::Li asks for
+ * them.  Pine's Uniform, Stratified, ZeroTwoSequence and Sobol samplers map to
+ * PG_SAMPLER_INDEPENDENT, the library's counter-based stream (uniform, independent per
+ * sample and dimension). */
+enum { PG_SAMPLER_INDEPENDENT = 0, PG_SAMPLER_HALTON = 1 };
+
+/* Film reconstruction filters (filter.h:17-96, CreateFilter filter.cpp:5-21). */
+enum {
+    PG_FILTER_BOX = 0,
+    PG_FILTER_TRIANGLE = 1,
+    PG_FILTER_GAUSSIAN = 2,
+    PG_FILTER_MITCHELL = 3,
+    PG_FILTER_LANCZOS_SINC = 4
+};
+
 typedef struct pg_scene_desc {
     int32_t num_shapes;
     const pg_shape* shapes;          /* pine order; the index is the shape id */
@@ -197,6 +214,14 @@ typedef struct pg_scene_desc {
     int32_t samples_per_pixel;       /* Path{sampler{samplesPerPixel}} */
     int32_t num_node_ops;            /* shader-node programs of the materials (may be 0) */
     const pg_node_op* node_ops;
+    int32_t sampler;                 /* PG_SAMPLER_* */
+    int32_t sampler_scramble;        /* Halton randomizeStrategy: 1 permutateDigits (pine's
+                                        default), 0 none */
+    int32_t filter;                  /* PG_FILTER_* of the film; pine's default is
+                                        LanczosSinc (filter.cpp:6) */
+    float filter_radius[2];          /* a component <= 0 means pine's default 0.5; at most 16 */
+    float filter_params[2];          /* Gaussian {alpha}, Mitchell {B, C}, LanczosSinc {tau};
+                                        alpha or tau <= 0 means pine's default (1, 3) */
 } pg_scene_desc;
 
 /* ---- render requests ---- */
@@ -390,6 +415,18 @@ pg_status pg_eval_nodes(const pg_node_op* ops, int32_t num_ops, int32_t ref, int
                         const float* inputs, int64_t n, float* out);
 pg_status pg_bump_normal(const pg_node_op* ops, int32_t num_ops, int32_t ref, int32_t math_mode,
                          const float* inputs, int64_t n, float* out);
+
+/* ---- samplers and filters on the host (the device's code, for tests) ----
+ * pg_halton_sample: Halton samples for a film of width x height; rows: n x 4 int64 (pixel
+ * x, pixel y, sample index, dimension >= 2), as HaltonSampler::StartPixel(p, 0), `sample`
+ * StartNextSample calls and SampleDimension(dim) give them (sampler.cpp:62-96).
+ * scramble: 1 permuted digits, 0 none.
+ * pg_filter_table: the film's 16 x 16 table of a filter (film.cpp:20-28), row-major in y;
+ * radius and params as in pg_scene_desc. */
+pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scramble, const int64_t* rows,
+                           int64_t n, float* out);
+pg_status pg_filter_table(int32_t filter, const float* radius, const float* params,
+                          float* table);
 
 /* ---- synthetic scene inputs (seeded) ---- */
 /* n^3 fractal-noise cloud, x fastest; ~nonzero_fraction of voxels > 0; max exactly 1. */

@@ -5,10 +5,11 @@
 // vectors and its CPU integrator can be timed.  Nothing in the GPU library links this.
 //
 // Modes (all paths absolute; arrays are raw little-endian, row-major):
-//   render <scene.txt> <prefix>      per-pixel mean / sample variance / count in FP64,
+//   render <scene.txt> <prefix>      per-pixel film value / variance / count in FP64,
 //                                    replicating PixelIntegrator::Render + Compute
 //                                    (src/core/integrator.cpp:121-158) with the scene's
-//                                    own sampler and PathIntegrator::Li.
+//                                    own sampler, PathIntegrator::Li and Film::AddSample's
+//                                    filter weights (src/core/film.h:26-45).
 //   hits   <scene.txt> <rays> <out>  closest hit per ray through BVH::Intersect
 //                                    (src/impl/accel/bvh.cpp:669-709), recording the
 //                                    shape index, triangle index, t and (u, v).
@@ -20,6 +21,11 @@
 //   density <scene.txt> <in> <out>   GridMedium::Density (src/core/medium.cpp:141-160).
 //   time   <scene.txt> [repeats] [spp]  wall time of the stock Integrator::Render() only
 //                                    (BVH build and file loading excluded), repeated.
+//   halton <w> <h> <strategy> <in> <out>  HaltonSampler::StartPixel + StartNextSample +
+//                                    SampleDimension (src/core/sampler.cpp:33-96) at int64
+//                                    rows of (x, y, sample, dim) for a w x h film.
+//   filter <scene.txt> <out>         the film's filter radius and 16 x 16 table
+//                                    (src/core/film.cpp:20-28).
 //   nodes  <graphs.txt> <in> <out>   CreateNode (src/core/node.cpp:33-98) of the blocks
 //                                    g0, g1, ... and their EvalFloat / EvalVec3 at rows of
 //                                    (p.xyz, n.xyz, u, v); out: per graph and row 4 floats.
@@ -42,10 +48,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 using namespace pine;
+
+std::string ReadText(const char* path);
 
 namespace {
 
@@ -84,6 +93,31 @@ bool Finite(float x) {
     return (b & 0x7f800000u) != 0x7f800000u;
 }
 
+// The film's filter table (film.cpp:20-28) for the scene's film{filter{...}} block, built
+// with pine's CreateFilter and Filter::Evaluate, and the weight Film::AddSample gives a
+// pixel (GetFilterValue, film.h:75-78).
+struct FilterTable {
+    static constexpr int W = 16;
+    float table[W * W];
+    vec2 radius;
+    explicit FilterTable(const char* scenePath) {
+        std::string text = ReadText(scenePath);
+        Parameters params = Parse(text.c_str());
+        Filter filter = CreateFilter(params["Camera"]["film"]["filter"]);
+        radius = filter.Radius();
+        int offset = 0;
+        for (int y = 0; y < W; y++)
+            for (int x = 0; x < W; x++) {
+                vec2 p = {(x + 0.5f) / W * radius.x, (y + 0.5f) / W * radius.y};
+                table[offset++] = filter.Evaluate(p);
+            }
+    }
+    float Weight(vec2 p) const {
+        vec2i pi = W * Min(Abs(p) / radius, vec2(OneMinusEpsilon));
+        return table[pi.y * W + pi.x];
+    }
+};
+
 Scene* Load(const char* path) {
     Scene* scene = new Scene;
     LoadScene(path, scene);
@@ -100,8 +134,14 @@ int Render(const char* scenePath, const std::string& prefix) {
     vec2i size = ri->filmSize;
     int spp = ri->samplesPerPixel;
     int total = size.x * size.y;
-    std::vector<double> sum(total * 3), sumsq(total * 3);
+    const FilterTable ft(scenePath);
+    // Per pixel, over the samples Film::AddSample adds to it (film.h:26-45): sums of w,
+    // w^2, w L and w L^2, and their count.  Rows are locked because a sample can reach a
+    // neighbouring pixel.
+    std::vector<double> sum(total * 3), sumsq(total * 3), wsum(total), w2sum(total);
     std::vector<int64_t> count(total), dropped(total);
+    std::vector<std::mutex> rowLock(size.y);
+    ri->film->Clear();
 
     auto t0 = std::chrono::steady_clock::now();
     ParallelFor(total, [&](int index) {
@@ -114,11 +154,26 @@ int Render(const char* scenePath, const std::string& prefix) {
             Spectrum L = ri->Li(ray, sampler);
             vec3 rgb = L.ToRGB();
             if (Finite(rgb.x) && Finite(rgb.y) && Finite(rgb.z)) {
-                for (int c = 0; c < 3; c++) {
-                    sum[index * 3 + c] += rgb[c];
-                    sumsq[index * 3 + c] += double(rgb[c]) * rgb[c];
+                ri->film->AddSample(pFilm, L);
+                vec2 pf = pFilm;
+                pf *= size;
+                pf -= vec2(0.5f);
+                vec2i p0 = Max(vec2i(Ceil(pf - ft.radius)), vec2i(0));
+                vec2i p1 = Min(vec2i(Floor(pf + ft.radius)), size - vec2i(1));
+                for (int y = p0.y; y <= p1.y; y++) {
+                    std::lock_guard<std::mutex> lock(rowLock[y]);
+                    for (int x = p0.x; x <= p1.x; x++) {
+                        double w = ft.Weight(vec2(x, y) - pf);
+                        int j = y * size.x + x;
+                        for (int c = 0; c < 3; c++) {
+                            sum[j * 3 + c] += w * rgb[c];
+                            sumsq[j * 3 + c] += w * double(rgb[c]) * rgb[c];
+                        }
+                        wsum[j] += w;
+                        w2sum[j] += w * w;
+                        count[j]++;
+                    }
                 }
-                count[index]++;
             } else {
                 dropped[index]++;
             }
@@ -127,23 +182,40 @@ int Render(const char* scenePath, const std::string& prefix) {
     });
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 
+    // Film value sum(w L) / sum(w); per-sample variance scaled so that var / count is the
+    // variance of that value (weighted sample variance, Bessel-corrected on the effective
+    // sample size n_eff = sum(w)^2 / sum(w^2), times count / n_eff).  With unit weights
+    // these are the plain mean and unbiased sample variance.  The film's own pixels
+    // (float sums) check the restated splat.
     std::vector<double> mean(total * 3), var(total * 3);
     int64_t nDropped = 0;
+    double filmDiff = 0.0;
     for (int i = 0; i < total; i++) {
         nDropped += dropped[i];
-        double n = (double)count[i];
+        double n = (double)count[i], W = wsum[i], W2 = w2sum[i];
+        bool unit = W == n && W2 == n;
+        double neff = W2 > 0 ? W * W / W2 : 0.0;
+        Pixel& px = ri->film->GetPixel(vec2i(i % size.x, i / size.x));
         for (int c = 0; c < 3; c++) {
-            double m = n > 0 ? sum[i * 3 + c] / n : 0.0;
+            double m = W != 0 ? sum[i * 3 + c] / W : 0.0;
             mean[i * 3 + c] = m;
-            var[i * 3 + c] = n > 1 ? std::max(0.0, (sumsq[i * 3 + c] - n * m * m) / (n - 1)) : 0.0;
+            double v = 0.0;
+            if (unit)
+                v = n > 1 ? std::max(0.0, (sumsq[i * 3 + c] - n * m * m) / (n - 1)) : 0.0;
+            else if (neff > 1 && W != 0)
+                v = std::max(0.0, sumsq[i * 3 + c] / W - m * m) * neff / (neff - 1) * (n / neff);
+            var[i * 3 + c] = v;
+            float fw = (float)px.weight;
+            double fm = fw != 0 ? (float)px.rgb[c] / fw : 0.0;
+            filmDiff = std::max(filmDiff, std::abs(fm - m) / std::max(1e-3, std::abs(m)));
         }
     }
     WriteRaw((prefix + "_mean.f64").c_str(), mean.data(), mean.size() * 8);
     WriteRaw((prefix + "_var.f64").c_str(), var.data(), var.size() * 8);
     WriteRaw((prefix + "_count.i64").c_str(), count.data(), count.size() * 8);
     std::printf("{\"width\": %d, \"height\": %d, \"spp\": %d, \"seconds\": %.6f, "
-                "\"dropped\": %lld, \"threads\": %d}\n",
-                size.x, size.y, spp, secs, (long long)nDropped, NumThreads());
+                "\"dropped\": %lld, \"threads\": %d, \"film_rel_diff\": %.3g}\n",
+                size.x, size.y, spp, secs, (long long)nDropped, NumThreads(), filmDiff);
     return 0;
 }
 
@@ -376,6 +448,46 @@ std::string ReadText(const char* path) {
     return t;
 }
 
+// HaltonSampler values (sampler.cpp:33-96) for a film size and randomize strategy at rows
+// of (pixel x, pixel y, sample index, dimension), as int64; out: one float per row.
+int Halton(int w, int h, const char* strategy, const char* inPath, const char* outPath) {
+    FILE* f = std::fopen(inPath, "rb");
+    if (!f)
+        return 2;
+    std::vector<int64_t> rows;
+    int64_t buf[4];
+    while (std::fread(buf, sizeof(int64_t), 4, f) == 4)
+        rows.insert(rows.end(), buf, buf + 4);
+    std::fclose(f);
+    std::string text = std::string("sampler: Halton{\n samplesPerPixel: 1\n randomizeStrategy: ") +
+                       strategy + "\n}\n";
+    Parameters params = Parse(text.c_str());
+    Parameters sp = params["sampler"];
+    sp.Set("filmSize", vec2i(w, h));
+    Sampler sampler = CreateSampler(sp);
+    HaltonSampler& hs = sampler.Be<HaltonSampler>();
+    std::vector<float> out(rows.size() / 4);
+    for (size_t i = 0; i < out.size(); i++) {
+        // StartPixel(p, 0) then StartNextSample per sample, as the render loop advances it
+        // (64-bit index; StartPixel's own sampleIndex * stride is an int product).
+        hs.StartPixel(vec2i((int)rows[4 * i], (int)rows[4 * i + 1]), 0);
+        for (int64_t k = 0; k < rows[4 * i + 2]; k++)
+            hs.StartNextSample();
+        out[i] = hs.SampleDimension((int)rows[4 * i + 3]);
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
+// The film's filter table and radius for a scene (film.cpp:20-28); out: 2 + 256 floats.
+int FilterDump(const char* scenePath, const char* outPath) {
+    FilterTable ft(scenePath);
+    std::vector<float> out = {ft.radius.x, ft.radius.y};
+    out.insert(out.end(), ft.table, ft.table + FilterTable::W * FilterTable::W);
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
 int Nodes(const char* graphsPath, const char* inPath, const char* outPath) {
     std::string text = ReadText(graphsPath);
     Parameters params = Parse(text.c_str());
@@ -443,6 +555,10 @@ int main(int argc, char** argv) {
         return CameraRays(argv[2], argv[3], argv[4]);
     if (mode == "density" && argc == 5)
         return Density(argv[2], argv[3], argv[4]);
+    if (mode == "halton" && argc == 7)
+        return Halton(std::atoi(argv[2]), std::atoi(argv[3]), argv[4], argv[5], argv[6]);
+    if (mode == "filter" && argc == 4)
+        return FilterDump(argv[2], argv[3]);
     if (mode == "nodes" && argc == 5)
         return Nodes(argv[2], argv[3], argv[4]);
     if (mode == "bump" && argc == 5)

@@ -114,7 +114,14 @@ class SceneDesc(ctypes.Structure):
                 ("num_lights", ctypes.c_int32), ("lights", ctypes.POINTER(Light)),
                 ("camera", Camera), ("light_sampler", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("samples_per_pixel", ctypes.c_int32),
-                ("num_node_ops", ctypes.c_int32), ("node_ops", ctypes.POINTER(NodeOp))]
+                ("num_node_ops", ctypes.c_int32), ("node_ops", ctypes.POINTER(NodeOp)),
+                ("sampler", ctypes.c_int32), ("sampler_scramble", ctypes.c_int32),
+                ("filter", ctypes.c_int32), ("filter_radius", ctypes.c_float * 2),
+                ("filter_params", ctypes.c_float * 2)]
+
+
+SAMPLER_INDEPENDENT, SAMPLER_HALTON = 0, 1
+FILTERS = {"Box": 0, "Triangle": 1, "Gaussian": 2, "Mitchell": 3, "LanczosSinc": 4}
 
 
 SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
@@ -201,6 +208,9 @@ def lib():
         "pg_guide_pdf": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_sample": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_loss_grad": (None, [_F, _F, ctypes.c_int64, _F, _F]),
+        "pg_halton_sample": (st, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                  _P(ctypes.c_int64), ctypes.c_int64, _F]),
+        "pg_filter_table": (st, [ctypes.c_int32, _F, _F, _F]),
         "pg_eval_nodes": (st, [_P(NodeOp), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                _F, ctypes.c_int64, _F]),
         "pg_bump_normal": (st, [_P(NodeOp), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
@@ -278,6 +288,30 @@ def _node_call(name, desc, ref, math_mode, inputs, cols):
     out = np.empty((x.shape[0], 3), np.float32)
     st = getattr(lib(), name)(desc.node_ops, desc.num_node_ops, int(ref), MATH_MODES[math_mode],
                               _fptr(x), x.shape[0], _fptr(out))
+    if st != PG_OK:
+        raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
+    return out
+
+
+def halton_sample(width, height, rows, scramble=True):
+    """pine's Halton samples for a width x height film at rows (n x 4: pixel x, pixel y,
+    sample index, dimension); n floats."""
+    r = np.ascontiguousarray(rows, dtype=np.int64).reshape(-1, 4)
+    out = np.empty(r.shape[0], np.float32)
+    st = lib().pg_halton_sample(int(width), int(height), int(bool(scramble)),
+                                r.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), r.shape[0],
+                                _fptr(out))
+    if st != PG_OK:
+        raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
+    return out
+
+
+def filter_table(kind, radius=(0.5, 0.5), params=(0.0, 0.0)):
+    """The film's 16 x 16 table of filter `kind` (a FILTERS name)."""
+    rad = np.asarray(radius, np.float32)
+    prm = np.asarray(params, np.float32)
+    out = np.empty((16, 16), np.float32)
+    st = lib().pg_filter_table(FILTERS[kind], _fptr(rad), _fptr(prm), _fptr(out))
     if st != PG_OK:
         raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
     return out

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["pine_gpu.cu", "guide_mlp.cu", "batch.cu", "scene_load.cpp", "bvh_build.cpp",
            "scenegen.cpp"]
 HEADERS = ["pg_math.h", "pg_device.cuh", "pg_shade.cuh", "pg_kernels.cuh", "scene_load.h",
-           "bvh_build.h", "guide_net.cuh", "guide_mlp.h"]
+           "bvh_build.h", "guide_net.cuh", "guide_mlp.h", "pg_nodes.h", "pg_sampler.h"]
 
 
 def _nvcc() -> str:

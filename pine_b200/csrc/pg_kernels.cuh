@@ -86,6 +86,11 @@ struct RequestDev {
     uint32_t key1;                    // seed word of its random streams
     uint32_t key0_offset;             // sample_offset * npix (progressive passes)
     int max_depth;
+    int sampler;                      // PG_SAMPLER_*
+    HaltonDev halton;                 // tables and film parameters of a Halton render
+    int filter_splat;                 // 0: box of radius 0.5 (one pixel, weight 1)
+    float filter_radius[2];
+    const float* filter_table;        // 16 x 16 filter values (film.cpp:20-28)
 };
 
 struct RenderParams {
@@ -109,8 +114,9 @@ struct RenderParams {
     float4* sd;                  // shadow: d.xyz, medium
     float4* sc;                  // shadow: unoccluded contribution rgb, slot
     uint32_t* skey;              // shadow: random stream word
-    float4* film_acc;            // per pixel: sum r, g, b, count (this call)
-    float4* film_acc2;           // per pixel: sum of squares r, g, b (this call)
+    float4* film_acc;            // per pixel: sum w r, w g, w b, sum w (this call)
+    float4* film_acc2;           // per pixel: sum w r^2, w g^2, w b^2 (this call)
+    float2* film_acc3;           // per pixel: sum w^2, samples (filtered films; may be null)
     unsigned long long* next_sample;
     unsigned long long* stats;   // StatIndex
     uint32_t* req_done;          // completed paths per request
@@ -200,15 +206,25 @@ __device__ __forceinline__ void RedAdd4(float4* p, float a, float b, float c, fl
                  : "memory");
 }
 
-// Adds a call's float film into the FP64 film (sum, sum of squares, count).
-__global__ void k_fold(const float4* acc, const float4* acc2, size_t npix, double* sum, double* sq,
-                       uint32_t* n) {
+// Adds a call's float film into the FP64 film (weighted sums, weighted sums of squares,
+// weights, squared weights, samples).  Pixels without filtered samples (acc3 zero) were
+// written with weight 1 per sample.
+__global__ void k_fold(const float4* acc, const float4* acc2, const float2* acc3, size_t npix,
+                       double* sum, double* sq, double* wsum, double* w2sum, uint32_t* n) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
          i += (size_t)gridDim.x * blockDim.x) {
         float4 a = acc[i], b = acc2[i];
+        float2 c = acc3 ? acc3[i] : make_float2(0.0f, 0.0f);
         sum[3 * i] += a.x, sum[3 * i + 1] += a.y, sum[3 * i + 2] += a.z;
         sq[3 * i] += b.x, sq[3 * i + 1] += b.y, sq[3 * i + 2] += b.z;
-        n[i] += (uint32_t)a.w;
+        wsum[i] += a.w;
+        if (c.y > 0.0f) {
+            w2sum[i] += c.x;
+            n[i] += (uint32_t)c.y;
+        } else {
+            w2sum[i] += a.w;
+            n[i] += (uint32_t)a.w;
+        }
     }
 }
 
@@ -265,18 +281,82 @@ __device__ __forceinline__ int FindRequest(const RenderParams& P, unsigned long 
     return lo;
 }
 
-// Adds a finished path's radiance to its pixel (Film::AddSample with a box filter of
-// radius 0.5) and, in a batch, completes its request when it was the last path.
+// Halton index of camera sample key0: its pixel's first index plus sample * stride.
+__device__ __noinline__ uint64_t HaltonIndexOf(const RequestDev& R, uint32_t key0) {
+    uint32_t s = key0 / (uint32_t)R.npix, pix = key0 - s * (uint32_t)R.npix;
+    int px = (int)(pix % (uint32_t)R.width), py = (int)(pix / (uint32_t)R.width);
+    return HaltonPixelIndex(R.halton, px, py) + (uint64_t)s * R.halton.stride;
+}
+
+// The random stream of camera sample key0 from dimension `dim` on: pine's Halton sequence
+// at the sample's pixel and index for Halton renders, else the counter-based stream.
+__device__ __forceinline__ Rng PathRng(const RequestDev& R, uint32_t key0, uint32_t dim) {
+    Rng r{key0, R.key1, dim};
+    if (R.sampler == PG_SAMPLER_HALTON) {
+        uint64_t hidx = HaltonIndexOf(R, key0);
+        r.hal = &R.halton;
+        r.key0 = (uint32_t)hidx;
+        r.key1 = (uint32_t)(hidx >> 32);
+    }
+    return r;
+}
+__device__ __forceinline__ uint32_t FirstDim(const RequestDev& R) {
+    return R.sampler == PG_SAMPLER_HALTON ? 2u : 0u;  // StartPixel leaves dimension at 2
+}
+
+__device__ __forceinline__ void RedAdd2(float2* a, float x, float y) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(a), "f"(x), "f"(y) : "memory");
+}
+
+// Film::AddSample (film.h:26-45) with a filter table: the sample's film position is
+// rebuilt from its camera jitter (the first two draws of its stream) exactly as the camera
+// formed it, and the sample is added to every pixel within the filter radius with the
+// table's weight.
+__device__ __noinline__ void SplatSample(const RenderParams& P, const RequestDev& R, uint32_t key0,
+                                         uint32_t pixInImage, V3 c) {
+    float u0, u1;
+    Rng cr = PathRng(R, key0, FirstDim(R));
+    cr.Get2D(u0, u1);
+    const int W = R.width, H = R.height;
+    const int px = (int)(pixInImage % (uint32_t)W), py = (int)(pixInImage / (uint32_t)W);
+    // pFilm = (p + u) / size at the camera, then pFilm * size - 0.5 in AddSample.
+    float fx = RnAdd(RnMul(RnDiv((float)px + u0, (float)W), (float)W), -0.5f);
+    float fy = RnAdd(RnMul(RnDiv((float)py + u1, (float)H), (float)H), -0.5f);
+    const float rx = R.filter_radius[0], ry = R.filter_radius[1];
+    int x0 = max((int)ceilf(fx - rx), 0), x1 = min((int)floorf(fx + rx), W - 1);
+    int y0 = max((int)ceilf(fy - ry), 0), y1 = min((int)floorf(fy + ry), H - 1);
+    for (int y = y0; y <= y1; y++) {
+        float ty = fminf(RnDiv(fabsf((float)y - fy), ry), kOneMinusEpsilon);
+        int iy = (int)(kFilterTableWidth * ty);
+        for (int x = x0; x <= x1; x++) {
+            float tx = fminf(RnDiv(fabsf((float)x - fx), rx), kOneMinusEpsilon);
+            int ix = (int)(kFilterTableWidth * tx);
+            float w = R.filter_table[iy * kFilterTableWidth + ix];
+            size_t pix = (size_t)R.film_base + (size_t)y * W + x;
+            RedAdd4(&P.film_acc[pix], w * c.x, w * c.y, w * c.z, w);
+            RedAdd4(&P.film_acc2[pix], w * c.x * c.x, w * c.y * c.y, w * c.z * c.z, 0.0f);
+            if (P.film_acc3)
+                RedAdd2(&P.film_acc3[pix], w * w, 1.0f);
+        }
+    }
+}
+
+// Adds a finished path's radiance to the film (Film::AddSample: one pixel with weight 1
+// for a box filter of radius 0.5, else SplatSample) and, in a batch, completes its request
+// when it was the last path.
 template <bool MULTI>
 __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, uint32_t& dropped) {
     const RequestDev& R = RequestOf<MULTI>(P, i);
     uint32_t sid = P.sample[i] - R.key0_offset;
-    size_t pix = (size_t)R.film_base + sid % (uint32_t)R.npix;
-    if (Finite(c)) {
+    uint32_t pixInImage = sid % (uint32_t)R.npix;
+    size_t pix = (size_t)R.film_base + pixInImage;
+    if (!Finite(c)) {
+        dropped++;
+    } else if (R.filter_splat) {
+        SplatSample(P, R, P.sample[i], pixInImage, c);
+    } else {
         RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
         RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
-    } else {
-        dropped++;
     }
     if (MULTI) {
         int r = P.slot_req[i];
@@ -321,7 +401,7 @@ __device__ void SpawnPath(const RenderParams& P, const SceneDev& S0, int i, unsi
     int pix = (int)(sid % (uint32_t)R.npix);
     int px = pix % R.width, py = pix / R.width;
     uint32_t key0 = sid + R.key0_offset;
-    Rng rng{key0, R.key1, 0};
+    Rng rng = PathRng(R, key0, FirstDim(R));
     float u0, u1, l0, l1;
     rng.Get2D(u0, u1);
     rng.Get2D(l0, l1);
@@ -724,7 +804,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     V3 beta = v3(bt.x, bt.y, bt.z), L = v3(Lw.x, Lw.y, Lw.z);
     int depth = __float_as_int(bt.w);
     const int maxDepth = R.max_depth;
-    Rng rng{P.sample[i], R.key1, __float_as_uint(Lw.w)};
+    Rng rng = PathRng(R, P.sample[i], __float_as_uint(Lw.w));
     int prim = __float_as_int(h.y);
     bool found = prim != -1;
     float tHit = found ? h.x : kFloatMax;
@@ -999,7 +1079,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
     const float4 bt = P.beta[i], Lw = P.L[i];
     V3 beta = v3(bt.x, bt.y, bt.z);
     int depth = __float_as_int(bt.w);
-    Rng rng{P.sample[i], R.key1, __float_as_uint(Lw.w)};
+    Rng rng = PathRng(R, P.sample[i], __float_as_uint(Lw.w));
     VmfLobe lobes[kGuideLobes];
     GuideMixture(P.graw + (size_t)kGuideOutputs * q, lobes);
     const GuideFrameT gf = GuideFrame(surface, n, wi);  // the mixture's frame

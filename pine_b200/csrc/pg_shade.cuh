@@ -3,6 +3,7 @@
 #pragma once
 
 #include "pg_device.cuh"
+#include "pg_sampler.h"
 
 namespace pg {
 
@@ -14,9 +15,24 @@ __device__ __forceinline__ uint32_t PcgHash(uint32_t v) {
     uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
     return (w >> 22u) ^ w;
 }
+// Out of line, so that the Halton code adds nothing to the register allocation of the
+// kernels that only draw the counter-based stream.
+__device__ __noinline__ float HaltonDraw(const HaltonDev* h, uint32_t lo, uint32_t hi, int dim) {
+    return HaltonSample(*h, ((uint64_t)hi << 32) | lo, dim);
+}
+
+// A camera path of a Halton render draws pine's Halton sequence instead: `hal` set, the
+// sample's 64-bit Halton index in key1:key0, and `dim` pine's dimension counter, which
+// restarts at 2 after the last prime (HaltonSampler::Get1D/Get2D, sampler.cpp:76-87).
 struct Rng {
     uint32_t key0, key1, dim;
+    const HaltonDev* hal = nullptr;
     __device__ __forceinline__ float Get1D() {
+        if (hal) {
+            if (dim >= (uint32_t)kHaltonDims)
+                dim = 2;
+            return HaltonDraw(hal, key0, key1, (int)dim++);
+        }
         uint32_t h = PcgHash(dim + key1);
         h = PcgHash(h ^ key0);
         h = PcgHash(h + key1);
@@ -24,6 +40,14 @@ struct Rng {
         return (float)(h >> 8) * 0x1p-24f;
     }
     __device__ __forceinline__ void Get2D(float& a, float& b) {
+        if (hal) {
+            if (dim + 1 >= (uint32_t)kHaltonDims)
+                dim = 2;
+            a = HaltonDraw(hal, key0, key1, (int)dim);
+            b = HaltonDraw(hal, key0, key1, (int)dim + 1);
+            dim += 2;
+            return;
+        }
         a = Get1D();
         b = Get1D();
     }

@@ -92,6 +92,10 @@ struct DeviceScene {
     DevMem mem;
     const MediumDev* media_dev[4] = {nullptr, nullptr, nullptr, nullptr};  // per brick size
     int width = 0, height = 0, spp = 1, max_depth = 4;
+    int sampler = PG_SAMPLER_INDEPENDENT, scramble = 1;
+    int filter_splat = 0;                  // 0: one pixel per sample, weight 1
+    float filter_radius[2] = {0.5f, 0.5f};
+    const float* filter_table = nullptr;   // device, 16 x 16
     bool surfaces = false;
     int64_t prims = 0;
     int bvh_depth = 0;
@@ -164,8 +168,10 @@ struct Film {
     DevMem mem;
     int64_t npix = 0;
     double *sum = nullptr, *sq = nullptr;  // accumulated over calls (progressive passes)
+    double *wsum = nullptr, *w2sum = nullptr;  // filter weights and squared weights
     uint32_t* n = nullptr;
     float4 *acc = nullptr, *acc2 = nullptr;  // this call's samples, vector-atomic targets
+    float2* acc3 = nullptr;                  // this call's squared weights and samples
     float *rmean = nullptr, *rvar = nullptr;  // resolved mean and variance, read back
     void Ensure(int64_t np) {
         if (np <= npix)
@@ -176,9 +182,12 @@ struct Film {
         npix = np;
         sum = mem.Alloc<double>(np * 3);
         sq = mem.Alloc<double>(np * 3);
+        wsum = mem.Alloc<double>(np);
+        w2sum = mem.Alloc<double>(np);
         n = mem.Alloc<uint32_t>(np);
         acc = mem.Alloc<float4>(np);
         acc2 = mem.Alloc<float4>(np);
+        acc3 = mem.Alloc<float2>(np);
         rmean = mem.Alloc<float>(np * 3);
         rvar = mem.Alloc<float>(np * 3);
     }
@@ -209,6 +218,10 @@ struct pg_ctx {
     pg::GuidePool guide_pool;              // guided-render queues and training records
     int guide_pass = 1;                    // samples per pixel of the next guided pass
     int64_t guide_steps = 0;               // Adam steps taken since the network was reset
+    pg::DevMem halton_mem;                 // Halton tables (built for the first Halton scene)
+    const int* halton_primes = nullptr;
+    const int* halton_sums = nullptr;
+    const uint16_t* halton_perm = nullptr;
 };
 
 namespace pg {
@@ -270,6 +283,21 @@ static int CheckNodeProgram(const pg_scene_desc* d, int32_t ref) {
     throw Failure{PG_ERR_INVALID_ARG, "node program without PG_NODE_END"};
 }
 
+// The Halton tables of the context: primes, their prefix sums and pine's digit
+// permutations (about 7.4 MB), built once.
+static void EnsureHalton(pg_ctx* ctx) {
+    if (ctx->halton_perm)
+        return;
+    std::vector<int> primes, sums;
+    HaltonPrimes(primes, sums);
+    std::vector<uint16_t> perm = HaltonPermutations(primes);
+    ctx->halton_mem.stream = ctx->stream, ctx->halton_mem.async = true;
+    ctx->halton_primes = ctx->halton_mem.Upload(primes, ctx->stream);
+    ctx->halton_sums = ctx->halton_mem.Upload(sums, ctx->stream);
+    ctx->halton_perm = ctx->halton_mem.Upload(perm, ctx->stream);
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     DevMem upload;  // linear density grids: inputs of the majorant and brick builds only
     upload.stream = ctx->stream, upload.async = true;
@@ -284,6 +312,20 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     Require(d->camera.medium >= -1 && d->camera.medium < d->num_media, "camera medium out of range");
     for (int64_t i = 0; i < 3 * d->num_triangles; i++)
         Require((int64_t)d->indices[i] < d->num_vertices, "triangle index out of range");
+    Require(d->sampler == PG_SAMPLER_INDEPENDENT || d->sampler == PG_SAMPLER_HALTON,
+            "unknown sampler");
+    Require(d->filter >= PG_FILTER_BOX && d->filter <= PG_FILTER_LANCZOS_SINC, "unknown filter");
+    float fRadius[2], fParams[2];
+    for (int k = 0; k < 2; k++) {
+        fRadius[k] = d->filter_radius[k] > 0.0f ? d->filter_radius[k] : 0.5f;
+        fParams[k] = d->filter_params[k];
+        Require(fRadius[k] <= 16.0f, "filter radius above 16 pixels");
+        Require(std::isfinite(fParams[k]), "filter parameters must be finite");
+    }
+    if (d->filter == PG_FILTER_GAUSSIAN && !(fParams[0] > 0.0f))
+        fParams[0] = 1.0f;  // pine's default alpha
+    if (d->filter == PG_FILTER_LANCZOS_SINC && !(fParams[0] > 0.0f))
+        fParams[0] = 3.0f;  // pine's default tau
 
     auto sc = std::make_unique<DeviceScene>();
     // Scene memory is stream-ordered on the context's stream, so that uploading and
@@ -708,6 +750,24 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     S.has_null_surfaces = nullSurfaces ? 1 : 0;
     PG_CUDA(cudaStreamSynchronize(st));
 
+    // Sampler and film filter.  Halton renders always take the general splat, so that a
+    // sample on a pixel's edge reaches the neighbour as pine's film adds it; with the
+    // counter-based stream a box of radius 0.5 keeps one pixel per sample.
+    sc->sampler = d->sampler;
+    sc->scramble = d->sampler_scramble ? 1 : 0;
+    if (sc->sampler == PG_SAMPLER_HALTON)
+        EnsureHalton(ctx);
+    sc->filter_radius[0] = fRadius[0];
+    sc->filter_radius[1] = fRadius[1];
+    sc->filter_splat = sc->sampler == PG_SAMPLER_HALTON ||
+                       !(d->filter == PG_FILTER_BOX && fRadius[0] == 0.5f && fRadius[1] == 0.5f);
+    if (sc->filter_splat) {
+        std::vector<float> table(kFilterTableWidth * kFilterTableWidth);
+        FilterTable(d->filter, fRadius, fParams, table.data());
+        sc->filter_table = sc->mem.Upload(table, st);
+        PG_CUDA(cudaStreamSynchronize(st));
+    }
+
     sc->width = d->camera.width;
     sc->height = d->camera.height;
     sc->spp = std::max(1, d->samples_per_pixel);
@@ -726,6 +786,27 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
 static DeviceScene& GetScene(pg_ctx* ctx, int32_t id) {
     Require(id >= 0 && id < (int32_t)ctx->scenes.size() && ctx->scenes[id], "unknown scene id");
     return *ctx->scenes[id];
+}
+
+// A request's sampler and film filter, for a film of rq.width x rq.height.  Halton renders
+// with seed 0 draw pine's own sequence; other seeds rotate it (Cranley-Patterson, one
+// offset per dimension), which keeps its stratification and makes renders independent.
+static void SetRequestSampling(pg_ctx* ctx, const DeviceScene& sc, RequestDev& rq, uint64_t seed) {
+    rq.sampler = sc.sampler;
+    rq.halton = HaltonDev{};
+    if (sc.sampler == PG_SAMPLER_HALTON) {
+        HaltonDev& h = rq.halton;
+        h.primes = ctx->halton_primes;
+        h.prime_sums = ctx->halton_sums;
+        h.perm = ctx->halton_perm;
+        h.scramble = sc.scramble;
+        h.rotate = seed == 0 ? 0u : ((uint32_t)Hash64u(seed) | 1u);
+        HaltonFilmParams(h, rq.width, rq.height);
+    }
+    rq.filter_splat = sc.filter_splat;
+    rq.filter_radius[0] = sc.filter_radius[0];
+    rq.filter_radius[1] = sc.filter_radius[1];
+    rq.filter_table = sc.filter_table;
 }
 
 // ---------------------------------------------------------------- rendering
@@ -966,7 +1047,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.slot_req = pl.slot_req;
     P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
     P.counts = ctx->counts;
-    P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2;
+    P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2, P.film_acc3 = ctx->film.acc3;
     P.next_sample = ctx->next_sample;
     P.stats = ctx->stats;
     P.err = ctx->err;
@@ -1090,11 +1171,13 @@ static void EnsureFilm(pg_ctx* ctx, int64_t npix) {
 static void ClearCallFilm(pg_ctx* ctx, int64_t npix) {
     PG_CUDA(cudaMemsetAsync(ctx->film.acc, 0, npix * sizeof(float4), ctx->stream));
     PG_CUDA(cudaMemsetAsync(ctx->film.acc2, 0, npix * sizeof(float4), ctx->stream));
+    PG_CUDA(cudaMemsetAsync(ctx->film.acc3, 0, npix * sizeof(float2), ctx->stream));
 }
 
 static void FoldFilm(pg_ctx* ctx, int64_t npix) {
-    k_fold<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(ctx->film.acc, ctx->film.acc2, (size_t)npix,
-                                                     ctx->film.sum, ctx->film.sq, ctx->film.n);
+    Film& f = ctx->film;
+    k_fold<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(f.acc, f.acc2, f.acc3, (size_t)npix, f.sum,
+                                                     f.sq, f.wsum, f.w2sum, f.n);
     PG_CUDA(cudaGetLastError());
 }
 
@@ -1103,6 +1186,8 @@ static void ClearFilm(pg_ctx* ctx, int64_t npix) {
     cudaStream_t st = ctx->stream;
     PG_CUDA(cudaMemsetAsync(ctx->film.sum, 0, npix * 3 * sizeof(double), st));
     PG_CUDA(cudaMemsetAsync(ctx->film.sq, 0, npix * 3 * sizeof(double), st));
+    PG_CUDA(cudaMemsetAsync(ctx->film.wsum, 0, npix * sizeof(double), st));
+    PG_CUDA(cudaMemsetAsync(ctx->film.w2sum, 0, npix * sizeof(double), st));
     PG_CUDA(cudaMemsetAsync(ctx->film.n, 0, npix * sizeof(uint32_t), st));
 }
 
@@ -1152,6 +1237,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     rq.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
     rq.key0_offset = (uint32_t)sampleOffset * (uint32_t)npix;
     rq.max_depth = maxDepth;
+    SetRequestSampling(ctx, sc, rq, seed);
     RequestDev* dReq = ctx->req_buf.Alloc<RequestDev>(1);
     PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
     w.P.reqs = dReq;
@@ -1162,18 +1248,30 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     ctx->req_buf.Free();
 }
 
-// Per-pixel mean and unbiased sample variance of the FP64 film (FP64 arithmetic, then
-// rounded to FP32), on the device.
+// Per-pixel film value and variance of the FP64 film (FP64 arithmetic, then rounded to
+// FP32), on the device.  The value is the film's weighted mean sum(w L) / sum(w)
+// (film.h:26-45).  The variance is per sample, scaled so that var / count estimates the
+// variance of that mean: the weighted sample variance, Bessel-corrected on the effective
+// sample size n_eff = sum(w)^2 / sum(w^2), times count / n_eff.  With weight 1 per sample
+// these are the plain mean and the unbiased sample variance.
 __global__ void k_resolve(const double* __restrict__ sum, const double* __restrict__ sq,
+                          const double* __restrict__ wsum, const double* __restrict__ w2sum,
                           const uint32_t* __restrict__ n, int64_t npix, float* __restrict__ mean,
                           float* __restrict__ var) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
          i += (int64_t)gridDim.x * blockDim.x) {
-        double k = n[i];
+        double k = n[i], W = wsum[i], W2 = w2sum[i];
+        bool unit = W == k && W2 == k;
+        double neff = W2 > 0 ? W * W / W2 : 0.0;
         for (int c = 0; c < 3; c++) {
-            double m = k > 0 ? sum[3 * i + c] / k : 0.0;
+            double m = W != 0 ? sum[3 * i + c] / W : 0.0;
             mean[3 * i + c] = (float)m;
-            var[3 * i + c] = k > 1 ? (float)fmax(0.0, (sq[3 * i + c] - k * m * m) / (k - 1)) : 0.0f;
+            double v = 0.0;
+            if (unit)
+                v = k > 1 ? fmax(0.0, (sq[3 * i + c] - k * m * m) / (k - 1)) : 0.0;
+            else if (neff > 1 && W != 0)
+                v = fmax(0.0, sq[3 * i + c] / W - m * m) * neff / (neff - 1) * (k / neff);
+            var[3 * i + c] = (float)v;
         }
     }
 }
@@ -1186,7 +1284,8 @@ static void ReadFilm(pg_ctx* ctx, int64_t npix, float* mean, float* var, uint32_
     cudaStream_t st = ctx->stream;
     Film& f = ctx->film;
     if (mean || var) {
-        k_resolve<<<ctx->num_sms * 4, 256, 0, st>>>(f.sum, f.sq, f.n, npix, f.rmean, f.rvar);
+        k_resolve<<<ctx->num_sms * 4, 256, 0, st>>>(f.sum, f.sq, f.wsum, f.w2sum, f.n, npix,
+                                                    f.rmean, f.rvar);
         PG_CUDA(cudaGetLastError());
     }
     if (mean)
@@ -1619,6 +1718,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
                  (uint32_t)(r.seed >> 32);
         d.key0_offset = 0;
         d.max_depth = md;
+        SetRequestSampling(ctx, sc, d, r.seed);
         total += cnt;
         pixels += (uint64_t)w * h;
         maxDepth = std::max(maxDepth, md);
@@ -1670,15 +1770,14 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
             if (!reqs[i].out_mean)
                 continue;
             const RequestDev& d = rq[k];
-            std::vector<double> sum((size_t)d.npix * 3);
-            std::vector<uint32_t> cnt(d.npix);
+            std::vector<double> sum((size_t)d.npix * 3), wsum(d.npix);
             PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum + d.film_base * 3, sum.size() * sizeof(double),
                                cudaMemcpyDeviceToHost));
-            PG_CUDA(cudaMemcpy(cnt.data(), ctx->film.n + d.film_base, cnt.size() * sizeof(uint32_t),
+            PG_CUDA(cudaMemcpy(wsum.data(), ctx->film.wsum + d.film_base, wsum.size() * sizeof(double),
                                cudaMemcpyDeviceToHost));
             for (int p = 0; p < d.npix; p++)
                 for (int c = 0; c < 3; c++)
-                    reqs[i].out_mean[3 * p + c] = cnt[p] ? (float)(sum[3 * p + c] / cnt[p]) : 0.0f;
+                    reqs[i].out_mean[3 * p + c] = wsum[p] != 0 ? (float)(sum[3 * p + c] / wsum[p]) : 0.0f;
         }
     }
     ctx->req_buf.Free();
@@ -1815,14 +1914,15 @@ static unsigned char* NoAllocScratch(int device) {
     return static_cast<unsigned char*>(g_noalloc_addr[device]);
 }
 
+// sum(w L) / sum(w) per pixel (weight 1 per sample for a box filter of radius 0.5).
 __global__ void k_noalloc_mean(const float4* acc, int64_t npix, float* mean) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
          i += (int64_t)gridDim.x * blockDim.x) {
         float4 a = acc[i];
         float k = a.w;
-        mean[3 * i] = k > 0.0f ? a.x / k : 0.0f;
-        mean[3 * i + 1] = k > 0.0f ? a.y / k : 0.0f;
-        mean[3 * i + 2] = k > 0.0f ? a.z / k : 0.0f;
+        mean[3 * i] = k != 0.0f ? a.x / k : 0.0f;
+        mean[3 * i + 1] = k != 0.0f ? a.y / k : 0.0f;
+        mean[3 * i + 2] = k != 0.0f ? a.z / k : 0.0f;
     }
 }
 
@@ -1862,7 +1962,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     P.skey = reinterpret_cast<uint32_t*>(i32(1));
     P.state = i32(2), P.finished = i32(3), P.slot_req = i32(4), P.lists = i32(5);
     P.counts = ctx->counts;
-    P.film_acc = acc, P.film_acc2 = acc2;
+    P.film_acc = acc, P.film_acc2 = acc2, P.film_acc3 = nullptr;  // the mean needs no more
     P.next_sample = ctx->next_sample;
     P.stats = ctx->stats;
     P.err = ctx->err;
@@ -1889,6 +1989,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     rq.key1 = PcgHashHost((uint32_t)seed ^ 0x2545f491u) ^ (uint32_t)(seed >> 32);
     rq.key0_offset = (uint32_t)sampleOffset * (uint32_t)npix;
     rq.max_depth = maxDepth;
+    SetRequestSampling(ctx, sc, rq, seed);
     PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
     RunHostLoop(ctx, w, false, res);
     k_noalloc_mean<<<ctx->num_sms * 4, 256, 0, st>>>(acc, npix, meanDevice);
@@ -2187,5 +2288,42 @@ extern "C" pg_status pg_bump_normal(const pg_node_op* ops, int32_t num_ops, int3
                        : BumpNormal<kFast>(ops + ref - 1, p, nn, r[6], r[7], du, dv);
             out[3 * i] = v.x, out[3 * i + 1] = v.y, out[3 * i + 2] = v.z;
         }
+    });
+}
+
+// ================================================================ samplers and filters on the host
+extern "C" pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scramble,
+                                      const int64_t* rows, int64_t n, float* out) {
+    return Guard(nullptr, [&]() {
+        Require(width > 0 && height > 0, "film size must be positive");
+        Require(n >= 0 && (n == 0 || (rows && out)), "bad input or output arrays");
+        static std::vector<int> primes, sums;
+        static std::vector<uint16_t> perm;
+        static std::once_flag once;
+        std::call_once(once, [] {
+            HaltonPrimes(primes, sums);
+            perm = HaltonPermutations(primes);
+        });
+        HaltonDev h{};
+        h.primes = primes.data();
+        h.prime_sums = sums.data();
+        h.perm = perm.data();
+        h.scramble = scramble ? 1 : 0;
+        HaltonFilmParams(h, width, height);
+        for (int64_t i = 0; i < n; i++) {
+            const int64_t* r = rows + 4 * i;
+            Require(r[2] >= 0 && r[3] >= 2 && r[3] < kHaltonDims, "bad sample index or dimension");
+            uint64_t a = HaltonPixelIndex(h, (int)r[0], (int)r[1]) + (uint64_t)r[2] * h.stride;
+            out[i] = HaltonSample(h, a, (int)r[3]);
+        }
+    });
+}
+
+extern "C" pg_status pg_filter_table(int32_t filter, const float* radius, const float* params,
+                                     float* table) {
+    return Guard(nullptr, [&]() {
+        Require(radius && params && table, "null argument");
+        Require(filter >= PG_FILTER_BOX && filter <= PG_FILTER_LANCZOS_SINC, "unknown filter");
+        FilterTable(filter, radius, params, table);
     });
 }

@@ -218,6 +218,15 @@ std::array<int, 2> Params::Vec2i(const std::string& name, std::array<int, 2> fb)
     return r;
 }
 
+std::array<float, 2> Params::Vec2(const std::string& name, std::array<float, 2> fb) const {
+    auto v = Value(name);
+    if (!v)
+        return fb;
+    std::array<float, 2> r;
+    Stofs(*v, r.data(), 2);
+    return r;
+}
+
 // ---------------------------------------------------------------- parser
 namespace {
 
@@ -837,7 +846,53 @@ void LoadSceneFile(const std::string& path, HostScene& s) {
     if (itype != "Path" && itype != "GpuPath")
         Warn("[Integrator][Create]Integrator \"" + itype + "\" is rendered as GpuPath");
     s.max_depth = integ.Int("maxDepth", 4);
-    s.spp = integ["sampler"].Int("samplesPerPixel", 1);
+    // Sampler (CreateSampler, sampler.cpp:281-293) and its samples per pixel.
+    Params& smp = integ["sampler"];
+    std::string stype = smp.String("type", "Uniform");
+    s.sampler = PG_SAMPLER_INDEPENDENT;
+    if (stype == "Stratified") {
+        s.spp = smp.Int("xPixelSamples", 1) * smp.Int("yPixelSamples", 1);
+    } else if (stype == "ZeroTwoSequence") {
+        int n = smp.Int("samplesPerPixel", 1), r = 1;
+        while (r < n)
+            r <<= 1;  // pstd::roundup2 (sampler.cpp:98-99)
+        s.spp = r;
+    } else {
+        if (stype == "Halton") {
+            s.sampler = PG_SAMPLER_HALTON;
+            // randomizeStrategy: "none" or "permutateDigits"; anything else keeps the
+            // default (sampler.cpp:252-259).
+            s.sampler_scramble = smp.String("randomizeStrategy", "permutateDigits") != "none";
+        } else if (stype != "Uniform" && stype != "Sobol") {
+            Warn("[Sampler][Create]Unknown type \"" + stype + "\"");
+        }
+        s.spp = smp.Int("samplesPerPixel", 1);
+    }
+    // Film filter (CreateFilter, filter.cpp:5-21): LanczosSinc of radius 0.5 by default.
+    Params& flt = film["filter"];
+    std::string ftype = flt.String("type", "LanczosSinc");
+    auto radius = flt.Vec2("radius", {0.5f, 0.5f});
+    s.filter_radius[0] = radius[0];
+    s.filter_radius[1] = radius[1];
+    s.filter_params[0] = s.filter_params[1] = 0.0f;
+    if (ftype == "Box") {
+        s.filter = PG_FILTER_BOX;
+    } else if (ftype == "Triangle") {
+        s.filter = PG_FILTER_TRIANGLE;
+    } else if (ftype == "Gaussian") {
+        s.filter = PG_FILTER_GAUSSIAN;
+        s.filter_params[0] = flt.Float("alpha", 1.0f);
+    } else if (ftype == "Mitchell") {
+        s.filter = PG_FILTER_MITCHELL;
+        s.filter_params[0] = flt.Float("B", 1 / 3.0f);
+        s.filter_params[1] = flt.Float("C", 1.0f / 3.0f);
+    } else if (ftype == "LanczosSinc") {
+        s.filter = PG_FILTER_LANCZOS_SINC;
+        s.filter_params[0] = flt.Float("tau", 3.0f);
+    } else {
+        Warn("[Filter][Create]Unknown type \"" + ftype + "\"");
+        s.filter = PG_FILTER_BOX;
+    }
     std::string ls = integ["lightSampler"].String("type", "Power");
     s.light_sampler = ls == "Uniform" ? PG_LIGHT_SAMPLER_UNIFORM : PG_LIGHT_SAMPLER_POWER;
 }
@@ -864,6 +919,13 @@ void HostScene::Describe(pg_scene_desc& d) {
     d.samples_per_pixel = spp;
     d.num_node_ops = (int32_t)node_ops.size();
     d.node_ops = node_ops.data();
+    d.sampler = sampler;
+    d.sampler_scramble = sampler_scramble;
+    d.filter = filter;
+    for (int k = 0; k < 2; k++) {
+        d.filter_radius[k] = filter_radius[k];
+        d.filter_params[k] = filter_params[k];
+    }
 }
 
 }  // namespace pg

@@ -42,6 +42,7 @@ struct Params {
     std::array<float, 3> Vec3(const std::string& name) const;
     std::array<float, 3> Vec3(const std::string& name, std::array<float, 3> fallback) const;
     std::array<int, 2> Vec2i(const std::string& name, std::array<int, 2> fallback) const;
+    std::array<float, 2> Vec2(const std::string& name, std::array<float, 2> fallback) const;
 };
 
 struct HostScene {
@@ -57,6 +58,11 @@ struct HostScene {
     int light_sampler = PG_LIGHT_SAMPLER_POWER;
     int max_depth = 4;
     int spp = 1;
+    int sampler = PG_SAMPLER_INDEPENDENT;
+    int sampler_scramble = 1;
+    int filter = PG_FILTER_LANCZOS_SINC;
+    float filter_radius[2] = {0.5f, 0.5f};
+    float filter_params[2] = {3.0f, 0.0f};
 
     // Fills d with pointers into this scene (valid while it lives).
     void Describe(pg_scene_desc& d);

@@ -7,7 +7,7 @@ from the seeded generators in pine_b200.scenegen; everything a test needs to rep
 not depend on the generators or on the reference being present.
 
     python tests/golden/make_golden.py           # needs oracle/_ref/pine_ref
-    python tests/golden/make_golden.py nodes pine_spheres   # only those fixtures
+    python tests/golden/make_golden.py nodes pine_spheres sampler filtered   # only those
 """
 
 from __future__ import annotations
@@ -208,6 +208,67 @@ def nodes_kat(tmp):
                         allow_pickle=True)
 
 
+HALTON_FILMS = [(48, 27), (128, 36), (1280, 360), (7, 5), (1, 1), (300, 200)]
+FILTER_BLOCKS = [
+    "",  # no filter block: pine's default LanczosSinc of radius 0.5
+    "filter: Box{\n radius: 0.5\n}",
+    "filter: Box{\n radius: 1.5 0.75\n}",
+    "filter: Triangle{\n radius: 1 0.7\n}",
+    "filter: Gaussian{\n radius: 1.5\n alpha: 2\n}",
+    "filter: Mitchell{\n radius: 2\n}",
+    "filter: Mitchell{\n radius: 1.5 1.25\n B: 0\n C: 0.5\n}",
+    "filter: LanczosSinc{\n radius: 0.5\n}",
+    "filter: LanczosSinc{\n radius: 2 1.5\n tau: 2\n}",
+]
+
+
+def sampler_filter_kat(tmp):
+    """pine's HaltonSampler values at random (pixel, sample, dimension) rows for several
+    film sizes and both randomize strategies, and the film's filter tables."""
+    rng = np.random.default_rng(4242)
+    rows_all, vals_all, meta = [], [], []
+    for (w, h) in HALTON_FILMS:
+        for strat in ("permutateDigits", "none"):
+            n = 768
+            rows = np.stack([rng.integers(0, w, n), rng.integers(0, h, n),
+                             rng.integers(0, 4096, n), rng.integers(2, 1000, n)], 1)
+            rows[:64, 3] = np.arange(2, 66)
+            rows[64:80, 2] = rng.integers(150000, 300000, 16)  # indices above 2^32
+            rows[80:84, 3] = 999
+            rows = rows.astype(np.int64)
+            rows.tofile(f"{tmp}/h.in")
+            run("halton", str(w), str(h), strat, f"{tmp}/h.in", f"{tmp}/h.out")
+            rows_all.append(rows)
+            vals_all.append(np.fromfile(f"{tmp}/h.out", np.float32))
+            meta.append((w, h, 1 if strat == "permutateDigits" else 0))
+    tables = []
+    for block in FILTER_BLOCKS:
+        with open(f"{tmp}/f.txt", "w") as f:
+            f.write("Camera: ThinLen{\n film{\n size: 8 8\n " + block + "\n }\n}\n")
+        run("filter", f"{tmp}/f.txt", f"{tmp}/f.out")
+        tables.append(np.fromfile(f"{tmp}/f.out", np.float32))
+    np.savez_compressed(f"{HERE}/sampler_filter.npz", halton_meta=np.array(meta, np.int32),
+                        halton_rows=np.stack(rows_all), halton_values=np.stack(vals_all),
+                        filter_blocks=np.array(FILTER_BLOCKS, dtype=object),
+                        filter_tables=np.stack(tables), allow_pickle=True)
+
+
+def filtered_case(tmp):
+    """The spheres fixture's scene with a wide Gaussian filter (samples reach up to four
+    pixels) at 256 spp."""
+    z = np.load(f"{HERE}/image_spheres.npz", allow_pickle=True)
+    text = str(z["scene_text"])
+    old = "filter: Box{\n            radius: 0.5\n        }"
+    assert old in text
+    text = text.replace(old, "filter: Gaussian{\n            radius: 1.5\n            alpha: 2\n        }")
+    text = text.replace("samplesPerPixel: 1024", "samplesPerPixel: 256")
+    assert "samplesPerPixel: 256" in text
+    path = f"{tmp}/filtered.txt"
+    with open(path, "w") as f:
+        f.write(text)
+    image_case("filtered", path, [])
+
+
 def shipped_spheres_case(tmp):
     """pine's own scenes/spheres.txt (textures, noise, bump map, two-layer plastic) at a
     tenth of its film size and 512 spp."""
@@ -230,6 +291,10 @@ def main():
         with tempfile.TemporaryDirectory() as tmp:
             if "nodes" in only:
                 nodes_kat(tmp)
+            if "sampler" in only:
+                sampler_filter_kat(tmp)
+            if "filtered" in only:
+                filtered_case(tmp)
             if "pine_spheres" in only:
                 shipped_spheres_case(tmp)
         print("fixtures written to", HERE)
@@ -277,6 +342,8 @@ def main():
         image_case("volume", vi, ["cloud64_s0.vol"])
         nodes_kat(tmp)
         shipped_spheres_case(tmp)
+        sampler_filter_kat(tmp)
+        filtered_case(tmp)
     print("fixtures written to", HERE)
 
 

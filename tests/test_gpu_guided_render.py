@@ -120,7 +120,7 @@ def test_guided_matches_plain_within_mc_error(ctx, tmp_path, name, spp):
     st = guided["stats"]
     assert st["kernels"]["guide"]["items"] > 0 and st["kernels"]["train"]["items"] > 0
     assert st["dropped"] == 0 and st["paths"] == plain["stats"]["paths"]
-    assert np.all(guided["count"] == spp)
+    assert np.all(guided["count"] >= spp)  # edge samples may also reach a neighbour
     frac, z = _zfrac(guided, plain)
     assert frac >= 0.97, (frac, np.abs(z).max())
     # Whole-image mean within four standard errors.
