@@ -209,7 +209,7 @@ __device__ __forceinline__ void RedAdd4(float4* p, float a, float b, float c, fl
 // Adds a call's float film into the FP64 film (weighted sums, weighted sums of squares,
 // weights, squared weights, samples).  Pixels without filtered samples (acc3 zero) were
 // written with weight 1 per sample.
-__global__ void k_fold(const float4* acc, const float4* acc2, const float2* acc3, size_t npix,
+static __global__ void k_fold(const float4* acc, const float4* acc2, const float2* acc3, size_t npix,
                        double* sum, double* sq, double* wsum, double* w2sum, uint32_t* n) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
          i += (size_t)gridDim.x * blockDim.x) {
@@ -282,17 +282,20 @@ __device__ __forceinline__ int FindRequest(const RenderParams& P, unsigned long 
 }
 
 // Halton index of camera sample key0: its pixel's first index plus sample * stride.
-__device__ __noinline__ uint64_t HaltonIndexOf(const RequestDev& R, uint32_t key0) {
+static __device__ __noinline__ uint64_t HaltonIndexOf(const RequestDev& R, uint32_t key0) {
     uint32_t s = key0 / (uint32_t)R.npix, pix = key0 - s * (uint32_t)R.npix;
     int px = (int)(pix % (uint32_t)R.width), py = (int)(pix / (uint32_t)R.width);
     return HaltonPixelIndex(R.halton, px, py) + (uint64_t)s * R.halton.stride;
 }
 
 // The random stream of camera sample key0 from dimension `dim` on: pine's Halton sequence
-// at the sample's pixel and index for Halton renders, else the counter-based stream.
+// at the sample's pixel and index for Halton renders, else the counter-based stream.  GEN
+// (general) kernel variants serve scenes with Halton sampling, filter splats or shader-node
+// materials; the others compile none of that code.
+template <bool GEN>
 __device__ __forceinline__ Rng PathRng(const RequestDev& R, uint32_t key0, uint32_t dim) {
     Rng r{key0, R.key1, dim};
-    if (R.sampler == PG_SAMPLER_HALTON) {
+    if (GEN && R.sampler == PG_SAMPLER_HALTON) {
         uint64_t hidx = HaltonIndexOf(R, key0);
         r.hal = &R.halton;
         r.key0 = (uint32_t)hidx;
@@ -300,8 +303,9 @@ __device__ __forceinline__ Rng PathRng(const RequestDev& R, uint32_t key0, uint3
     }
     return r;
 }
+template <bool GEN>
 __device__ __forceinline__ uint32_t FirstDim(const RequestDev& R) {
-    return R.sampler == PG_SAMPLER_HALTON ? 2u : 0u;  // StartPixel leaves dimension at 2
+    return GEN && R.sampler == PG_SAMPLER_HALTON ? 2u : 0u;  // StartPixel leaves it at 2
 }
 
 __device__ __forceinline__ void RedAdd2(float2* a, float x, float y) {
@@ -312,10 +316,10 @@ __device__ __forceinline__ void RedAdd2(float2* a, float x, float y) {
 // rebuilt from its camera jitter (the first two draws of its stream) exactly as the camera
 // formed it, and the sample is added to every pixel within the filter radius with the
 // table's weight.
-__device__ __noinline__ void SplatSample(const RenderParams& P, const RequestDev& R, uint32_t key0,
+static __device__ __noinline__ void SplatSample(const RenderParams& P, const RequestDev& R, uint32_t key0,
                                          uint32_t pixInImage, V3 c) {
     float u0, u1;
-    Rng cr = PathRng(R, key0, FirstDim(R));
+    Rng cr = PathRng<true>(R, key0, FirstDim<true>(R));
     cr.Get2D(u0, u1);
     const int W = R.width, H = R.height;
     const int px = (int)(pixInImage % (uint32_t)W), py = (int)(pixInImage / (uint32_t)W);
@@ -344,7 +348,7 @@ __device__ __noinline__ void SplatSample(const RenderParams& P, const RequestDev
 // Adds a finished path's radiance to the film (Film::AddSample: one pixel with weight 1
 // for a box filter of radius 0.5, else SplatSample) and, in a batch, completes its request
 // when it was the last path.
-template <bool MULTI>
+template <bool MULTI, bool GEN>
 __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, uint32_t& dropped) {
     const RequestDev& R = RequestOf<MULTI>(P, i);
     uint32_t sid = P.sample[i] - R.key0_offset;
@@ -352,7 +356,7 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
     size_t pix = (size_t)R.film_base + pixInImage;
     if (!Finite(c)) {
         dropped++;
-    } else if (R.filter_splat) {
+    } else if (GEN && R.filter_splat) {
         SplatSample(P, R, P.sample[i], pixInImage, c);
     } else {
         RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
@@ -367,7 +371,7 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
 
 // Sets the target weight of every training record of the path in slot i, whose radiance
 // ended at L (valid = false for a dropped sample: targets 0), and clears its record list.
-__device__ void FinalizeRecords(const RenderParams& P, int i, V3 L, bool valid) {
+static __device__ void FinalizeRecords(const RenderParams& P, int i, V3 L, bool valid) {
     int r = P.rec_last[i];
     for (int k = 0; k < 65536 && r >= 0; k++) {
         float4 a = P.rec[kRecordStride * r], bt = P.rec[kRecordStride * r + 3],
@@ -390,7 +394,7 @@ __device__ void FinalizeRecords(const RenderParams& P, int i, V3 L, bool valid) 
 
 // Starts camera sample `id` in slot i (RadianceIntegrator::Compute + ThinLenCamera::GenRay,
 // integrator.cpp:152-158, camera.cpp:31-41).
-template <int M, bool MULTI>
+template <int M, bool MULTI, bool GEN>
 __device__ void SpawnPath(const RenderParams& P, const SceneDev& S0, int i, unsigned long long id) {
     int r = MULTI ? FindRequest(P, id) : 0;
     const RequestDev& R = P.reqs[r];
@@ -401,7 +405,7 @@ __device__ void SpawnPath(const RenderParams& P, const SceneDev& S0, int i, unsi
     int pix = (int)(sid % (uint32_t)R.npix);
     int px = pix % R.width, py = pix / R.width;
     uint32_t key0 = sid + R.key0_offset;
-    Rng rng = PathRng(R, key0, FirstDim(R));
+    Rng rng = PathRng<GEN>(R, key0, FirstDim<GEN>(R));
     float u0, u1, l0, l1;
     rng.Get2D(u0, u1);
     rng.Get2D(l0, l1);
@@ -440,7 +444,7 @@ __device__ __forceinline__ unsigned long long BlockClaim(const RenderParams& P, 
 
 // Fills the slots listed in the finished queue with new camera samples (the start of a
 // render; afterwards shading and shadow kernels refill slots themselves).
-template <int M, bool MULTI>
+template <int M, bool MULTI, bool GEN>
 __global__ void k_regen(RenderParams P, SceneDev S0) {
     __shared__ int claimOff[32];
     __shared__ unsigned long long claimBase;
@@ -454,7 +458,7 @@ __global__ void k_regen(RenderParams P, SceneDev S0) {
         unsigned long long id = BlockClaim(P, live, claimOff, &claimBase);
         bool spawned = id != ~0ull;
         if (spawned)
-            SpawnPath<M, MULTI>(P, S0, i, id);
+            SpawnPath<M, MULTI, GEN>(P, S0, i, id);
         if (live)
             P.state[i] = spawned ? kSlotActive : kSlotDead;
         int* const ctr[1] = {&P.counts[kCntNext]};
@@ -468,7 +472,7 @@ __global__ void k_regen(RenderParams P, SceneDev S0) {
 }
 
 // Makes the next queue the active one and decides whether the loop continues.
-__global__ void k_swap(RenderParams P) {
+static __global__ void k_swap(RenderParams P) {
     int* c = P.counts;
     int active = c[kCntNext];
     c[kCntActive] = active;
@@ -627,7 +631,7 @@ __device__ __noinline__ void TextureMaterial(const SceneDev& S, V3 o, V3 d, floa
 // zero if a surface with a material blocks it, otherwise the product of the media's
 // transmittances along the segments between null surfaces.
 template <int M, bool MEDIA = true>
-__device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, Rng& rng,
+__device__ V3 ShadowTr(const SceneDev& S, V3 o, V3 d, float tmax, int medium, HashRng& rng,
                        uint2* stack, int stride, uint32_t& steps, uint32_t& bricks, uint32_t& err,
                        int& traced) {
     V3 tr = v3(1.0f);
@@ -726,7 +730,7 @@ __device__ void NextEvent(const RenderParams& P, const SceneDev& S, int slot, ui
     float tmax = ls.distance * (1.0f - 1e-3f);
     uint32_t key = PcgHash(rng.dim ^ 0x68bc21ebu) ^ key1;
     if (FUSED) {
-        Rng srng{P.sample[slot], key, 0};
+        HashRng srng{P.sample[slot], key, 0};
         int traced;
         V3 tr = ShadowTr<M, MEDIA>(S, o, ls.wo, tmax, med, srng, stack, blockDim.x, ct.shadowSteps,
                             ct.shadowBricks, ct.err, traced);
@@ -782,7 +786,7 @@ __device__ __forceinline__ void PushGuide(const RenderParams& P, int slot, V3 p,
 
 // MEDIA = false compiles the shading of scenes without participating media: the medium
 // code drops out, which frees registers for more resident warps.
-template <int M, bool FUSED, bool GUIDE, bool MEDIA = true>
+template <int M, bool FUSED, bool GUIDE, bool MEDIA, bool GEN>
 __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
                          uint2* stack, ShadeCounters& ct, PendingShadow& ps, bool& finished,
                          V3& Lout, bool& deferred) {
@@ -804,7 +808,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     V3 beta = v3(bt.x, bt.y, bt.z), L = v3(Lw.x, Lw.y, Lw.z);
     int depth = __float_as_int(bt.w);
     const int maxDepth = R.max_depth;
-    Rng rng = PathRng(R, P.sample[i], __float_as_uint(Lw.w));
+    Rng rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(Lw.w));
     int prim = __float_as_int(h.y);
     bool found = prim != -1;
     float tHit = found ? h.x : kFloatMax;
@@ -815,7 +819,9 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     MediumEvent ev;
     ev.scattered = false;
     if (MEDIA && medium >= 0) {
-        MediumSampleEvent<M>(S.media[medium], o, d, tHit, rng, ev, ct.steps, ct.bricks, ct.err);
+        HashRng trk = rng.Tracking();
+        MediumSampleEvent<M>(S.media[medium], o, d, tHit, trk, ev, ct.steps, ct.bricks, ct.err);
+        rng.EndTracking(trk);
         beta *= ev.weight;
     }
     if (ev.scattered) {
@@ -865,7 +871,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
         } else {
             const MaterialDev* mp = &S.materials[sh.material];
             MaterialDev tmat;
-            if (mp->textured) {
+            if (GEN && mp->textured) {
                 tmat = *mp;
                 TextureMaterial<M>(S, o, d, h, si, tmat);
                 mp = &tmat;
@@ -942,7 +948,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     }
 }
 
-template <int M, bool MULTI, bool FUSED, bool GUIDE = false, bool MEDIA = true>
+template <int M, bool MULTI, bool FUSED, bool GUIDE, bool MEDIA, bool GEN>
 __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -960,7 +966,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
         V3 L;
         bool deferred = false;
         if (live)
-            ShadeOne<M, FUSED, GUIDE, MEDIA>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
+            ShadeOne<M, FUSED, GUIDE, MEDIA, GEN>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
                                       stack + threadIdx.x, ct, ps, finished, L, deferred);
         // A path that ends here with no shadow ray in flight is flushed now and its slot
         // takes the next camera sample; one with a shadow ray pending ends in k_shadow.
@@ -968,14 +974,14 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
         bool endHere = live && finished && !deferred && ps.idx < 0;
         uint32_t dropped = 0;
         if (endHere) {
-            FlushPath<MULTI>(P, i, L, dropped);
+            FlushPath<MULTI, GEN>(P, i, L, dropped);
             if (GUIDE)
                 FinalizeRecords(P, i, L, Finite(L));
         }
         unsigned long long id = BlockClaim(P, endHere, claimOff, &claimBase);
         bool spawned = id != ~0ull;
         if (spawned)
-            SpawnPath<M, MULTI>(P, S0, i, id);
+            SpawnPath<M, MULTI, GEN>(P, S0, i, id);
         else if (endHere)
             P.state[i] = kSlotDead;
         int* const ctr[1] = {&P.counts[kCntNext]};
@@ -998,7 +1004,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
     }
 }
 
-template <int M, bool MULTI, bool GUIDE = false, bool MEDIA = true>
+template <int M, bool MULTI, bool GUIDE, bool MEDIA, bool GEN>
 __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shadow(RenderParams P, SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -1017,14 +1023,14 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
             slot = (int)(w & ~kFinalShadow);
             last = (w & kFinalShadow) != 0;
             const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
-            Rng rng{P.sample[slot], P.skey[q], 0};
+            HashRng rng{P.sample[slot], P.skey[q], 0};
             V3 tr = ShadowTr<M, MEDIA>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
                                 __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x, steps,
                                 bricks, err, traced);
             float4 Lw = P.L[slot];
             V3 L = v3(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z);
             if (last) {
-                FlushPath<MULTI>(P, slot, L, dropped);
+                FlushPath<MULTI, GEN>(P, slot, L, dropped);
                 if (GUIDE)
                     FinalizeRecords(P, slot, L, Finite(L));
             } else if (!IsBlack(tr))
@@ -1036,7 +1042,7 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
         unsigned long long id = BlockClaim(P, last, claimOff, &claimBase);
         bool spawned = id != ~0ull;
         if (spawned)
-            SpawnPath<M, MULTI>(P, S0, slot, id);
+            SpawnPath<M, MULTI, GEN>(P, S0, slot, id);
         else if (last)
             P.state[slot] = kSlotDead;
         int* const ctr[1] = {&P.counts[kCntNext]};
@@ -1079,7 +1085,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
     const float4 bt = P.beta[i], Lw = P.L[i];
     V3 beta = v3(bt.x, bt.y, bt.z);
     int depth = __float_as_int(bt.w);
-    Rng rng = PathRng(R, P.sample[i], __float_as_uint(Lw.w));
+    Rng rng = PathRng<true>(R, P.sample[i], __float_as_uint(Lw.w));
     VmfLobe lobes[kGuideLobes];
     GuideMixture(P.graw + (size_t)kGuideOutputs * q, lobes);
     const GuideFrameT gf = GuideFrame(surface, n, wi);  // the mixture's frame
@@ -1192,13 +1198,13 @@ __global__ void k_guide_sample(RenderParams P, SceneDev S0) {
         if (q < n)
             GuideOne<M>(P, S0, q, slot, cont, endNow, Lend, recorded);
         if (endNow) {
-            FlushPath<false>(P, slot, Lend, dropped);
+            FlushPath<false, true>(P, slot, Lend, dropped);
             FinalizeRecords(P, slot, Lend, Finite(Lend));
         }
         unsigned long long id = BlockClaim(P, endNow, claimOff, &claimBase);
         bool spawned = id != ~0ull;
         if (spawned)
-            SpawnPath<M, false>(P, S0, slot, id);
+            SpawnPath<M, false, true>(P, S0, slot, id);
         else if (endNow)
             P.state[slot] = kSlotDead;
         int* const ctr[1] = {&P.counts[kCntNext]};
@@ -1214,7 +1220,7 @@ __global__ void k_guide_sample(RenderParams P, SceneDev S0) {
 }
 
 // Copies a grid (x fastest) into 8^3 bricks with a 1-voxel apron (zeros past the end).
-__global__ void k_brickify(const float* __restrict__ d, int sx, int sy, int sz, int nbx, int nby,
+static __global__ void k_brickify(const float* __restrict__ d, int sx, int sy, int sz, int nbx, int nby,
                            int nbz, float* __restrict__ bricks) {
     const int64_t nb = (int64_t)nbx * nby * nbz;
     for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
@@ -1234,7 +1240,7 @@ __global__ void k_brickify(const float* __restrict__ d, int sx, int sy, int sz, 
 
 // Brick majorants: the largest density over voxels [b*k, b*k + b] of each axis (the
 // trilinear footprint of points inside brick k of edge b voxels), one thread per brick.
-__global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int nbx, int nby,
+static __global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int nbx, int nby,
                            int nbz, float* maj) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (int64_t)nbx * nby * nbz)
@@ -1253,7 +1259,7 @@ __global__ void k_majorant(const float* dens, int sx, int sy, int sz, int b, int
 // Majorants of bricks of edge 2s from those of edge s: the footprint of brick b
 // ([2s*b, 2s*b + 2s] per axis) is the union of its children's (2b and 2b+1), so the
 // maximum over the existing children is exact.
-__global__ void k_majorant_coarsen(const float* fine, int fx, int fy, int fz, int nbx, int nby,
+static __global__ void k_majorant_coarsen(const float* fine, int fx, int fy, int fz, int nbx, int nby,
                                    int nbz, float* maj) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (int64_t)nbx * nby * nbz)
@@ -1268,7 +1274,7 @@ __global__ void k_majorant_coarsen(const float* fine, int fx, int fy, int fz, in
 }
 
 // pg_intersect: closest hit per ray with pine's shape index and triangle index.
-__global__ void k_intersect(SceneDev S, const float* rays, int64_t n, int32_t* shapeId,
+static __global__ void k_intersect(SceneDev S, const float* rays, int64_t n, int32_t* shapeId,
                             int32_t* primId, float* tOut, float* uvOut, uint32_t* errOut) {
     extern __shared__ uint2 stack[];
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,0 +1,238 @@
+// The wavefront's launch sequences (trace, shade, shadow, swap; the initial fill; the
+// guided iteration), shared by the translation units that compile the kernels of each math
+// mode (pg_kernels_pine.cu, pg_kernels_fast.cu) and called from pine_gpu.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <utility>
+#include <vector>
+
+#include "guide_mlp.h"
+#include "pg_error.h"
+#include "pg_kernels.cuh"
+
+namespace pg {
+
+template <typename T>
+static T Ceil(T a, T b) {
+    return (a + b - 1) / b;
+}
+
+// What the launches need from the context.
+struct LaunchEnv {
+    cudaStream_t stream;
+    int num_sms;
+    const GuideNetDev* guide;
+};
+
+struct RenderResult {
+    double seconds = 0;
+    unsigned long long stats[kNumStats] = {};
+    int64_t launches = 0;
+    int64_t kernelLaunches[PG_NUM_KERNELS] = {};
+    double kernelSeconds[PG_NUM_KERNELS] = {};
+};
+
+// Optional per-launch timing: a start/stop event pair around each kernel launch.
+struct LaunchTimer {
+    std::vector<cudaEvent_t>* events;  // the context's events, reused
+    cudaStream_t stream;
+    bool on;
+    size_t used = 0;
+    std::vector<std::pair<int, size_t>> marks;  // kernel, index of its start event
+    cudaEvent_t Next() {
+        if (used == events->size()) {
+            cudaEvent_t e;
+            PG_CUDA(cudaEventCreate(&e));
+            events->push_back(e);
+        }
+        return (*events)[used++];
+    }
+    template <typename F>
+    void Time(int kernel, F&& launch) {
+        if (!on) {
+            launch();
+            return;
+        }
+        size_t first = used;
+        PG_CUDA(cudaEventRecord(Next(), stream));
+        launch();
+        PG_CUDA(cudaEventRecord(Next(), stream));
+        marks.push_back({kernel, first});
+    }
+    void Collect(RenderResult& r) {
+        for (auto& m : marks) {
+            float ms = 0.0f;
+            PG_CUDA(cudaEventElapsedTime(&ms, (*events)[m.second], (*events)[m.second + 1]));
+            r.kernelSeconds[m.first] += ms * 1e-3;
+        }
+    }
+};
+
+// One wavefront: its parameters, kernels and launch shapes.
+struct Wave {
+    RenderParams P{};
+    SceneDev S0{};
+    bool multi = false, surfaces = false, fused = false, guide = false;
+    bool media = true;  // false: no participating media, the lean kernel variants run
+    bool general = false;  // Halton sampling, filter splats or shader nodes: GEN variants
+    int mode = PG_MATH_FAST;
+    int shadeBlock = 128;
+    size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
+};
+
+template <int M, bool MULTI, bool FUSED, bool GEN>
+static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                       RenderResult* res) {
+    cudaStream_t st = env.stream;
+    const int sms = env.num_sms;
+    const int tb = 128;
+    auto grid = [&](int block, int perSm) {
+        int cap = sms * perSm;
+        return persistent ? cap : std::max(1, std::min(Ceil(n, block), cap * 8));
+    };
+    auto time = [&](int k, auto&& f) {
+        if (timer)
+            timer->Time(k, f);
+        else
+            f();
+        if (res)
+            res->kernelLaunches[k]++;
+    };
+    if (w.surfaces)
+        time(PG_KERNEL_TRACE, [&]() {
+            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
+    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
+    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    if (FUSED && shadeSmem > 48 * 1024)
+        PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED, false, true, GEN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)shadeSmem));
+    time(PG_KERNEL_SHADE, [&]() {
+        if (!FUSED && !w.media)
+            k_shade<M, MULTI, false, false, false, GEN>
+                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(w.P, w.S0);
+        else
+            k_shade<M, MULTI, FUSED, false, true, GEN><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
+    });
+    if (!FUSED)
+        time(PG_KERNEL_SHADOW, [&]() {
+            if (!w.media)
+                k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+            else
+                k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+        });
+    // Queue swap; counted with the fill kernel.
+    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
+}
+
+// The initial fill of every slot and the first swap.  Later refills happen inside k_shade
+// and k_shadow as paths end.
+template <int M, bool MULTI, bool GEN>
+static void LaunchRegen(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res) {
+    auto f = [&]() {
+        k_regen<M, MULTI, GEN><<<env.num_sms * 8, 256, 0, env.stream>>>(w.P, w.S0);
+        k_swap<<<1, 1, 0, env.stream>>>(w.P);
+    };
+    if (timer)
+        timer->Time(PG_KERNEL_REGEN, f);
+    else
+        f();
+    if (res)
+        res->kernelLaunches[PG_KERNEL_REGEN]++;
+}
+
+// One guided iteration: trace, shade (guided vertices queued), network inference over the
+// queue (row count read on the device), guided sampling, shadow rays, swap.
+template <int M, bool FUSED>
+static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* timer, RenderResult* res) {
+    cudaStream_t st = env.stream;
+    const int sms = env.num_sms;
+    const int tb = 128;
+    auto grid = [&](int block, int perSm) { return std::max(1, std::min(Ceil(n, block), sms * perSm * 8)); };
+    auto time = [&](int k, auto&& f) {
+        if (timer)
+            timer->Time(k, f);
+        else
+            f();
+        if (res)
+            res->kernelLaunches[k]++;
+    };
+    if (w.surfaces)
+        time(PG_KERNEL_TRACE, [&]() {
+            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+        });
+    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
+    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
+    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
+    if (FUSED && shadeSmem > 48 * 1024)
+        PG_CUDA(cudaFuncSetAttribute(k_shade<M, false, FUSED, true, true, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shadeSmem));
+    time(PG_KERNEL_SHADE, [&]() {
+        k_shade<M, false, FUSED, true, true, true><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem,
+                                         st>>>(w.P, w.S0);
+    });
+    time(PG_KERNEL_GUIDE, [&]() {
+        GuideInput in;
+        in.vert = w.P.gq;
+        in.stride = kGuideEntry;
+        for (int k = 0; k < 3; k++)
+            in.lo[k] = w.S0.guide_lo[k], in.inv[k] = w.S0.guide_inv[k];
+        in.count = &w.P.counts[kCntGuide];
+        PG_CUDA(GuideForward(*env.guide, in, n, const_cast<float*>(w.P.graw), sms, st));
+        k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(w.P, w.S0);
+    });
+    if (!FUSED)
+        time(PG_KERNEL_SHADOW, [&]() {
+            k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+        });
+    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
+}
+
+template <int M, bool MULTI>
+static void Body(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer, RenderResult* res) {
+    if (!MULTI && w.guide) {
+        if (w.fused)
+            LaunchGuidedBody<M, true>(env, w, n, timer, res);
+        else
+            LaunchGuidedBody<M, false>(env, w, n, timer, res);
+        return;
+    }
+    if (w.general)
+        w.fused ? LaunchBody<M, MULTI, true, true>(env, w, n, persistent, timer, res)
+                : LaunchBody<M, MULTI, false, true>(env, w, n, persistent, timer, res);
+    else
+        w.fused ? LaunchBody<M, MULTI, true, false>(env, w, n, persistent, timer, res)
+                : LaunchBody<M, MULTI, false, false>(env, w, n, persistent, timer, res);
+}
+
+// Regen and body launches of one math mode (M is kPine or kFast); each mode's kernels are
+// compiled in their own translation unit.
+template <int M>
+static void DispatchRegenM(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res) {
+    const bool gen = w.general || w.guide;
+    if (w.multi)
+        gen ? LaunchRegen<M, true, true>(env, w, timer, res) : LaunchRegen<M, true, false>(env, w, timer, res);
+    else
+        gen ? LaunchRegen<M, false, true>(env, w, timer, res) : LaunchRegen<M, false, false>(env, w, timer, res);
+}
+
+template <int M>
+static void DispatchBodyM(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                          RenderResult* res) {
+    w.multi ? Body<M, true>(env, w, n, persistent, timer, res)
+            : Body<M, false>(env, w, n, persistent, timer, res);
+}
+
+void DispatchRegenPine(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res);
+void DispatchRegenFast(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res);
+void DispatchBodyPine(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                      RenderResult* res);
+void DispatchBodyFast(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
+                      RenderResult* res);
+
+}  // namespace pg

@@ -15,9 +15,22 @@ __device__ __forceinline__ uint32_t PcgHash(uint32_t v) {
     uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
     return (w >> 22u) ^ w;
 }
+// The counter-based stream alone: what the distance-sampling and tracking loops draw, so
+// that those loops carry no Halton code.
+struct HashRng {
+    uint32_t key0, key1, dim;
+    __device__ __forceinline__ float Get1D() {
+        uint32_t h = PcgHash(dim + key1);
+        h = PcgHash(h ^ key0);
+        h = PcgHash(h + key1);
+        dim++;
+        return (float)(h >> 8) * 0x1p-24f;
+    }
+};
+
 // Out of line, so that the Halton code adds nothing to the register allocation of the
 // kernels that only draw the counter-based stream.
-__device__ __noinline__ float HaltonDraw(const HaltonDev* h, uint32_t lo, uint32_t hi, int dim) {
+static __device__ __noinline__ float HaltonDraw(const HaltonDev* h, uint32_t lo, uint32_t hi, int dim) {
     return HaltonSample(*h, ((uint64_t)hi << 32) | lo, dim);
 }
 
@@ -38,6 +51,19 @@ struct Rng {
         h = PcgHash(h + key1);
         dim++;
         return (float)(h >> 8) * 0x1p-24f;
+    }
+    // The stream of this vertex's tracking loops: the path's own counter-based stream
+    // (continued afterwards through EndTracking), or for a Halton path a counter-based
+    // stream keyed by its sample and this vertex's dimension, which leaves the Halton
+    // dimensions to the vertex draws pine makes.
+    __device__ __forceinline__ HashRng Tracking() const {
+        if (hal)
+            return HashRng{key0 ^ PcgHash(dim ^ 0x3c6ef372u), key1 ^ 0xa54ff53au, 0};
+        return HashRng{key0, key1, dim};
+    }
+    __device__ __forceinline__ void EndTracking(const HashRng& t) {
+        if (!hal)
+            dim = t.dim;
     }
     __device__ __forceinline__ void Get2D(float& a, float& b) {
         if (hal) {
@@ -637,7 +663,7 @@ struct MediumEvent {
 // HomogeneousMedium::Sample (medium.cpp:38-53).  `tmax` is the world-space hit distance,
 // used as the bound in medium space as pine does (medium.cpp:99-101).
 template <int M>
-__device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng,
+__device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& rng,
                                   MediumEvent& ev, uint32_t& steps, uint32_t& bricks,
                                   uint32_t& err) {
     ev.scattered = false;
@@ -701,7 +727,7 @@ __device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, Rn
 // GridMedium::Tr (medium.cpp:55-80): ratio tracking with pine's Russian roulette once the
 // transmittance estimate drops below 0.1.  HomogeneousMedium::Tr (medium.cpp:33-36).
 template <int M>
-__device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, Rng& rng, uint32_t& steps,
+__device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& rng, uint32_t& steps,
                           uint32_t& bricks, uint32_t& err, V3& trRGB) {
     if (m.type == PG_MEDIUM_HOMOGENEOUS) {
         trRGB = v3(PMath<M>::exp(-tmax * (m.sigma_a[0] + m.sigma_s[0])),

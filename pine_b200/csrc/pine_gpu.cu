@@ -17,17 +17,15 @@
 #include "bvh_build.h"
 #include "guide_mlp.h"
 #include "guide_net.cuh"
+#include "pg_error.h"
 #include "pg_kernels.cuh"
+#include "pg_launch.cuh"
 #include "pine_gpu.h"
 #include "scene_load.h"
 
 namespace pg {
 
 // ---------------------------------------------------------------- errors
-struct Failure {
-    pg_status status;
-    std::string msg;
-};
 
 static std::mutex g_errMutex;
 static std::string g_err;
@@ -37,13 +35,6 @@ static void SetGlobalError(const std::string& m) {
     g_err = m;
 }
 
-#define PG_CUDA(call)                                                                       \
-    do {                                                                                    \
-        cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess)                                                              \
-            throw Failure{e_ == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_CUDA,       \
-                          std::string(#call) + ": " + cudaGetErrorString(e_)};              \
-    } while (0)
 
 static void Require(bool ok, const std::string& msg, pg_status s = PG_ERR_INVALID_ARG) {
     if (!ok)
@@ -96,15 +87,12 @@ struct DeviceScene {
     int filter_splat = 0;                  // 0: one pixel per sample, weight 1
     float filter_radius[2] = {0.5f, 0.5f};
     const float* filter_table = nullptr;   // device, 16 x 16
+    bool general = false;                  // needs the GEN kernel variants
     bool surfaces = false;
     int64_t prims = 0;
     int bvh_depth = 0;
 };
 
-template <typename T>
-static T Ceil(T a, T b) {
-    return (a + b - 1) / b;
-}
 
 // ---------------------------------------------------------------- path pool
 struct Pool {
@@ -761,6 +749,7 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     sc->filter_radius[1] = fRadius[1];
     sc->filter_splat = sc->sampler == PG_SAMPLER_HALTON ||
                        !(d->filter == PG_FILTER_BOX && fRadius[0] == 0.5f && fRadius[1] == 0.5f);
+    sc->general = sc->filter_splat || d->num_node_ops > 0;
     if (sc->filter_splat) {
         std::vector<float> table(kFilterTableWidth * kFilterTableWidth);
         FilterTable(d->filter, fRadius, fParams, table.data());
@@ -830,49 +819,6 @@ static uint32_t PcgHashHost(uint32_t v) {
 }
 
 
-struct RenderResult {
-    double seconds = 0;
-    unsigned long long stats[kNumStats] = {};
-    int64_t launches = 0;
-    int64_t kernelLaunches[PG_NUM_KERNELS] = {};
-    double kernelSeconds[PG_NUM_KERNELS] = {};
-};
-
-// Optional per-launch timing: a start/stop event pair around each kernel launch.
-struct LaunchTimer {
-    pg_ctx* ctx;
-    bool on;
-    size_t used = 0;
-    std::vector<std::pair<int, size_t>> marks;  // kernel, index of its start event
-    cudaEvent_t Next() {
-        if (used == ctx->events.size()) {
-            cudaEvent_t e;
-            PG_CUDA(cudaEventCreate(&e));
-            ctx->events.push_back(e);
-        }
-        return ctx->events[used++];
-    }
-    template <typename F>
-    void Time(int kernel, F&& launch) {
-        if (!on) {
-            launch();
-            return;
-        }
-        size_t first = used;
-        PG_CUDA(cudaEventRecord(Next(), ctx->stream));
-        launch();
-        PG_CUDA(cudaEventRecord(Next(), ctx->stream));
-        marks.push_back({kernel, first});
-    }
-    void Collect(RenderResult& r) {
-        for (auto& m : marks) {
-            float ms = 0.0f;
-            PG_CUDA(cudaEventElapsedTime(&ms, ctx->events[m.second], ctx->events[m.second + 1]));
-            r.kernelSeconds[m.first] += ms * 1e-3;
-        }
-    }
-};
-
 __global__ void k_iota(int* a, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         a[i] = i;
@@ -881,156 +827,21 @@ __global__ void k_timestamp(unsigned long long* t) {
     *t = GlobalTimer();
 }
 
-// One wavefront: its parameters, kernels and launch shapes.
-struct Wave {
-    RenderParams P{};
-    SceneDev S0{};
-    bool multi = false, surfaces = false, fused = false, guide = false;
-    bool media = true;  // false: no participating media, the lean kernel variants run
-    int mode = PG_MATH_FAST;
-    int shadeBlock = 128;
-    size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
-};
-
-template <int M, bool MULTI, bool FUSED>
-static void LaunchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer,
-                       RenderResult* res) {
-    cudaStream_t st = ctx->stream;
-    const int sms = ctx->num_sms;
-    const int tb = 128;
-    auto grid = [&](int block, int perSm) {
-        int cap = sms * perSm;
-        return persistent ? cap : std::max(1, std::min(Ceil(n, block), cap * 8));
-    };
-    auto time = [&](int k, auto&& f) {
-        if (timer)
-            timer->Time(k, f);
-        else
-            f();
-        if (res)
-            res->kernelLaunches[k]++;
-    };
-    if (w.surfaces)
-        time(PG_KERNEL_TRACE, [&]() {
-            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
-        });
-    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
-    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
-    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
-    if (FUSED && shadeSmem > 48 * 1024)
-        PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)shadeSmem));
-    time(PG_KERNEL_SHADE, [&]() {
-        if (!FUSED && !w.media)
-            k_shade<M, MULTI, false, false, false>
-                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(w.P, w.S0);
-        else
-            k_shade<M, MULTI, FUSED><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
-    });
-    if (!FUSED)
-        time(PG_KERNEL_SHADOW, [&]() {
-            if (!w.media)
-                k_shadow<M, MULTI, false, false><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
-            else
-                k_shadow<M, MULTI><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
-        });
-    // Queue swap; counted with the fill kernel.
-    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
-}
-
-// The initial fill of every slot and the first swap.  Later refills happen inside k_shade
-// and k_shadow as paths end.
-template <int M, bool MULTI>
-static void LaunchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
-    auto f = [&]() {
-        k_regen<M, MULTI><<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(w.P, w.S0);
-        k_swap<<<1, 1, 0, ctx->stream>>>(w.P);
-    };
-    if (timer)
-        timer->Time(PG_KERNEL_REGEN, f);
-    else
-        f();
-    if (res)
-        res->kernelLaunches[PG_KERNEL_REGEN]++;
-}
-
-// One guided iteration: trace, shade (guided vertices queued), network inference over the
-// queue (row count read on the device), guided sampling, shadow rays, swap.
-template <int M, bool FUSED>
-static void LaunchGuidedBody(pg_ctx* ctx, Wave& w, int n, LaunchTimer* timer, RenderResult* res) {
-    cudaStream_t st = ctx->stream;
-    const int sms = ctx->num_sms;
-    const int tb = 128;
-    auto grid = [&](int block, int perSm) { return std::max(1, std::min(Ceil(n, block), sms * perSm * 8)); };
-    auto time = [&](int k, auto&& f) {
-        if (timer)
-            timer->Time(k, f);
-        else
-            f();
-        if (res)
-            res->kernelLaunches[k]++;
-    };
-    if (w.surfaces)
-        time(PG_KERNEL_TRACE, [&]() {
-            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
-        });
-    // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
-    const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
-    const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
-    if (FUSED && shadeSmem > 48 * 1024)
-        PG_CUDA(cudaFuncSetAttribute(k_shade<M, false, FUSED, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shadeSmem));
-    time(PG_KERNEL_SHADE, [&]() {
-        k_shade<M, false, FUSED, true><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem,
-                                         st>>>(w.P, w.S0);
-    });
-    time(PG_KERNEL_GUIDE, [&]() {
-        GuideInput in;
-        in.vert = w.P.gq;
-        in.stride = kGuideEntry;
-        for (int k = 0; k < 3; k++)
-            in.lo[k] = w.S0.guide_lo[k], in.inv[k] = w.S0.guide_inv[k];
-        in.count = &w.P.counts[kCntGuide];
-        PG_CUDA(GuideForward(ctx->guide, in, n, const_cast<float*>(w.P.graw), sms, st));
-        k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(w.P, w.S0);
-    });
-    if (!FUSED)
-        time(PG_KERNEL_SHADOW, [&]() {
-            k_shadow<M, false, true><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
-        });
-    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
-}
-
-template <int M, bool MULTI>
-static void Body(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer, RenderResult* res) {
-    if (!MULTI && w.guide) {
-        if (w.fused)
-            LaunchGuidedBody<M, true>(ctx, w, n, timer, res);
-        else
-            LaunchGuidedBody<M, false>(ctx, w, n, timer, res);
-        return;
-    }
-    if (w.fused)
-        LaunchBody<M, MULTI, true>(ctx, w, n, persistent, timer, res);
-    else
-        LaunchBody<M, MULTI, false>(ctx, w, n, persistent, timer, res);
-}
-
 static void DispatchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
+    LaunchEnv env{ctx->stream, ctx->num_sms, &ctx->guide};
     if (w.mode == PG_MATH_PINE)
-        w.multi ? LaunchRegen<kPine, true>(ctx, w, timer, res) : LaunchRegen<kPine, false>(ctx, w, timer, res);
+        DispatchRegenPine(env, w, timer, res);
     else
-        w.multi ? LaunchRegen<kFast, true>(ctx, w, timer, res) : LaunchRegen<kFast, false>(ctx, w, timer, res);
+        DispatchRegenFast(env, w, timer, res);
 }
 
 static void DispatchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTimer* timer,
                          RenderResult* res) {
+    LaunchEnv env{ctx->stream, ctx->num_sms, &ctx->guide};
     if (w.mode == PG_MATH_PINE)
-        w.multi ? Body<kPine, true>(ctx, w, n, persistent, timer, res)
-                : Body<kPine, false>(ctx, w, n, persistent, timer, res);
+        DispatchBodyPine(env, w, n, persistent, timer, res);
     else
-        w.multi ? Body<kFast, true>(ctx, w, n, persistent, timer, res)
-                : Body<kFast, false>(ctx, w, n, persistent, timer, res);
+        DispatchBodyFast(env, w, n, persistent, timer, res);
 }
 
 // Fills the pool pointers of a wave and resets its queues: every slot starts empty and
@@ -1075,7 +886,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
 // is sized to its queue (and can be timed per kernel).
 static void RunHostLoop(pg_ctx* ctx, Wave& w, bool profile, RenderResult& res) {
     cudaStream_t st = ctx->stream;
-    LaunchTimer timer{ctx, profile};
+    LaunchTimer timer{&ctx->events, ctx->stream, profile};
     PG_CUDA(cudaEventRecord(ctx->ev0, st));
     DispatchRegen(ctx, w, &timer, &res);
     for (int64_t iter = 0;; iter++) {
@@ -1223,6 +1034,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
     w.guide = recordAccept != nullptr;
     w.media = sc.dev.num_media > 0;
+    w.general = sc.general;
     if (w.guide)
         w.P.rec_accept = *recordAccept;
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
@@ -1353,6 +1165,7 @@ extern "C" void pg_destroy(pg_ctx* ctx) {
     ctx->pool.mem.Free();
     ctx->film.mem.Free();
     ctx->small.Free();
+    ctx->halton_mem.Free();  // stream-ordered: freed while the stream still exists
     if (ctx->h_counts)
         cudaFreeHost(ctx->h_counts);
     if (ctx->ev0)
@@ -1681,7 +1494,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     std::vector<RequestDev> rq(n);
     std::vector<SceneDev> scenes(n);
     uint64_t total = 0, pixels = 0;
-    bool surfaces = false, media = false;
+    bool surfaces = false, media = false, general = false;
     int maxDepth = 1;
     const int variant = MediaVariant(tune);
     // Shortest job first: requests take their sample ranges in increasing order of their
@@ -1731,6 +1544,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         scenes[k] = s;
         surfaces = surfaces || sc.surfaces;
         media = media || sc.dev.num_media > 0;
+        general = general || sc.general;
     }
     ClearFilm(ctx, (int64_t)pixels);
     ClearCallFilm(ctx, (int64_t)pixels);
@@ -1746,6 +1560,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.mode = PG_MATH_FAST;
     w.surfaces = surfaces;
     w.media = media;
+    w.general = general;
     w.fused = tune.split_shadow == 0;
     w.shadeBlock = tune.block_size;
     w.S0 = scenes[0];
@@ -1948,6 +1763,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     Wave w;
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
+    w.general = sc.general;
     w.fused = ctx->tuning.split_shadow == 0;
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;

@@ -120,7 +120,8 @@ def test_guided_matches_plain_within_mc_error(ctx, tmp_path, name, spp):
     st = guided["stats"]
     assert st["kernels"]["guide"]["items"] > 0 and st["kernels"]["train"]["items"] > 0
     assert st["dropped"] == 0 and st["paths"] == plain["stats"]["paths"]
-    assert np.all(guided["count"] >= spp)  # edge samples may also reach a neighbour
+    # Samples on a pixel edge may reach a neighbour (Halton scene, pine's film splat).
+    assert abs(int(guided["count"].sum()) - guided["count"].size * spp) <= guided["count"].size
     frac, z = _zfrac(guided, plain)
     assert frac >= 0.97, (frac, np.abs(z).max())
     # Whole-image mean within four standard errors.
