@@ -18,10 +18,36 @@ namespace pg {
 constexpr int kHaltonDims = 1000;       // PrimeTableSize (util/primes.h:8)
 constexpr int kHaltonMaxRes = 128;      // HaltonSampler::MaxHaltonResolution (sampler.h:102)
 
+// Division of a 32-bit unsigned integer by a fixed prime through a multiply-high (Granlund
+// and Montgomery, "Division by invariant integers using multiplication", 1994):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, and n / d = (t + ((n - t) >> 1))
+// >> (l - 1) with t = mulhi(n, m), exact for every 32-bit n and every d >= 2.
+struct DivMagic {
+    uint32_t m, l;
+    float inv_base;  // 1.0f / base, rounded as pine's float division rounds it
+    float series;    // perm[0] / (base + 1.0f), the scrambled tail term of pine's formula
+};
+PG_HD uint32_t DivByMagic(uint32_t n, DivMagic g) {
+#ifdef __CUDA_ARCH__
+    uint32_t t = __umulhi(n, g.m);
+#else
+    uint32_t t = (uint32_t)(((uint64_t)n * g.m) >> 32);
+#endif
+    return (t + ((n - t) >> 1)) >> (g.l - 1);
+}
+inline DivMagic MakeDivMagic(uint32_t d) {
+    uint32_t l = 0;
+    while ((1ull << l) < d)
+        l++;
+    uint64_t m = (((uint64_t)1 << 32) * ((1ull << l) - d)) / d + 1;
+    return DivMagic{(uint32_t)m, l, 1.0f / (float)d, 0.0f};
+}
+
 // Everything a path needs to draw its Halton samples; lives in device memory next to the
 // request it belongs to.
 struct HaltonDev {
     const int* primes;          // the first 1000 primes
+    const DivMagic* magic;      // division by each prime and its float constants
     const int* prime_sums;      // exclusive prefix sums: start of each prime's permutation
     const uint16_t* perm;       // digit permutations, concatenated in prime order
     int scramble;               // 1: permuted digits (pine's default), 0: plain radical inverse
@@ -100,7 +126,8 @@ PG_HD float U64ToFloat(uint64_t v) {
 PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
     const int base = h.primes[dim];
     const uint16_t* perm = h.scramble ? h.perm + h.prime_sums[dim] : nullptr;
-    const float invBase = RnDiv(1.0f, (float)base);
+    const DivMagic mg = h.magic[dim];
+    const float invBase = mg.inv_base;
     float invBaseN = 1.0f;
     uint64_t rev = 0;
     while (a >> 32) {
@@ -113,7 +140,7 @@ PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
     uint32_t a32 = (uint32_t)a;
     const uint32_t b32 = (uint32_t)base;
     while (a32) {
-        uint32_t next = a32 / b32;
+        uint32_t next = DivByMagic(a32, mg);
         uint32_t digit = a32 - next * b32;
         rev = rev * (uint64_t)base + (perm ? perm[digit] : digit);
         invBaseN = RnMul(invBaseN, invBase);
@@ -121,8 +148,7 @@ PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
     }
     float v;
     if (perm) {
-        float series = RnDiv((float)perm[0], (float)base + 1.0f);
-        v = RnMul(RnAdd(U64ToFloat(rev), series), invBaseN);
+        v = RnMul(RnAdd(U64ToFloat(rev), mg.series), invBaseN);
     } else {
         v = RnMul(U64ToFloat(rev), invBaseN);
     }
@@ -164,6 +190,19 @@ inline void HaltonPrimes(std::vector<int>& primes, std::vector<int>& sums) {
     sums.assign(kHaltonDims, 0);
     for (int i = 1; i < kHaltonDims; i++)
         sums[i] = sums[i - 1] + primes[i - 1];
+}
+
+// Per prime: the division magic, 1/base and the scrambled tail perm[0] / (base + 1).
+inline std::vector<DivMagic> HaltonMagics(const std::vector<int>& primes,
+                                          const std::vector<int>& sums,
+                                          const std::vector<uint16_t>& perm) {
+    std::vector<DivMagic> m;
+    for (size_t i = 0; i < primes.size(); i++) {
+        DivMagic g = MakeDivMagic((uint32_t)primes[i]);
+        g.series = (float)perm[sums[i]] / ((float)primes[i] + 1.0f);
+        m.push_back(g);
+    }
+    return m;
 }
 
 // ComputeRadicalInversePermutations (lowdiscrepancy.cpp:5-20) with pine's RNG at its

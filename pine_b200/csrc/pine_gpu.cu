@@ -208,6 +208,7 @@ struct pg_ctx {
     int64_t guide_steps = 0;               // Adam steps taken since the network was reset
     pg::DevMem halton_mem;                 // Halton tables (built for the first Halton scene)
     const int* halton_primes = nullptr;
+    const pg::DivMagic* halton_magic = nullptr;
     const int* halton_sums = nullptr;
     const uint16_t* halton_perm = nullptr;
 };
@@ -281,6 +282,7 @@ static void EnsureHalton(pg_ctx* ctx) {
     std::vector<uint16_t> perm = HaltonPermutations(primes);
     ctx->halton_mem.stream = ctx->stream, ctx->halton_mem.async = true;
     ctx->halton_primes = ctx->halton_mem.Upload(primes, ctx->stream);
+    ctx->halton_magic = ctx->halton_mem.Upload(HaltonMagics(primes, sums, perm), ctx->stream);
     ctx->halton_sums = ctx->halton_mem.Upload(sums, ctx->stream);
     ctx->halton_perm = ctx->halton_mem.Upload(perm, ctx->stream);
     PG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -786,6 +788,7 @@ static void SetRequestSampling(pg_ctx* ctx, const DeviceScene& sc, RequestDev& r
     if (sc.sampler == PG_SAMPLER_HALTON) {
         HaltonDev& h = rq.halton;
         h.primes = ctx->halton_primes;
+        h.magic = ctx->halton_magic;
         h.prime_sums = ctx->halton_sums;
         h.perm = ctx->halton_perm;
         h.scramble = sc.scramble;
@@ -2115,13 +2118,16 @@ extern "C" pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scr
         Require(n >= 0 && (n == 0 || (rows && out)), "bad input or output arrays");
         static std::vector<int> primes, sums;
         static std::vector<uint16_t> perm;
+        static std::vector<DivMagic> magic;
         static std::once_flag once;
         std::call_once(once, [] {
             HaltonPrimes(primes, sums);
             perm = HaltonPermutations(primes);
+            magic = HaltonMagics(primes, sums, perm);
         });
         HaltonDev h{};
         h.primes = primes.data();
+        h.magic = magic.data();
         h.prime_sums = sums.data();
         h.perm = perm.data();
         h.scramble = scramble ? 1 : 0;
