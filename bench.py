@@ -94,7 +94,9 @@ def scene_path(cfg, cache, env, spp=None, size=None):
     w, h = size or (cfg["width"], cfg["height"])
     spp = cfg["spp"] if spp is None else spp
     kind = cfg["kind"]
-    name = f"{kind}_{env}_{w}x{h}_{spp}.txt"
+    # Every workload uses the Uniform sampler (the library's independent stream, no Halton
+    # draws) and a box filter of radius 0.5; the reference arm renders the same file.
+    name = f"{kind}_{env}_{w}x{h}_{spp}_uniform.txt"
     path = os.path.join(cache, name)
     if kind == "volume":
         scenegen.volume_scene(path, lib(), n=cfg["n"], width=w, height=h, spp=spp,
@@ -102,10 +104,11 @@ def scene_path(cfg, cache, env, spp=None, size=None):
                               env_radiance=0.3 if env == "constant" else 1.0)
     elif kind == "spheres":
         scenegen.spheres_scene(path, width=w, height=h, spp=spp, max_depth=cfg["max_depth"],
-                               env=env, env_radiance=0.2 if env == "constant" else 0.5)
+                               env=env, env_radiance=0.2 if env == "constant" else 0.5,
+                               sampler="Uniform")
     else:
         scenegen.mesh_scene(path, lib(), subdiv=cfg["subdiv"], width=w, height=h, spp=spp,
-                            max_depth=cfg["max_depth"], env="none")
+                            max_depth=cfg["max_depth"], env="none", sampler="Uniform")
     return path
 
 

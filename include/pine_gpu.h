@@ -186,6 +186,12 @@ enum { PG_LIGHT_SAMPLER_POWER = 0, PG_LIGHT_SAMPLER_UNIFORM = 1 };
  * sample and dimension). */
 enum { PG_SAMPLER_INDEPENDENT = 0, PG_SAMPLER_HALTON = 1 };
 
+/* Integrators.  PG_INTEGRATOR_PATH: PathIntegrator::Li (path.cpp:6-86), next-event
+ * estimation with MIS and Russian roulette.  PG_INTEGRATOR_RANDOM_WALK:
+ * RandomWalkIntegrator::Li (randomwalk.cpp:6-64), BSDF and phase sampling only, emission
+ * added where paths hit it, no roulette: a second unbiased estimator of the same image. */
+enum { PG_INTEGRATOR_PATH = 0, PG_INTEGRATOR_RANDOM_WALK = 1 };
+
 /* Film reconstruction filters (filter.h:17-96, CreateFilter filter.cpp:5-21). */
 enum {
     PG_FILTER_BOX = 0,
@@ -222,6 +228,7 @@ typedef struct pg_scene_desc {
     float filter_radius[2];          /* a component <= 0 means pine's default 0.5; at most 16 */
     float filter_params[2];          /* Gaussian {alpha}, Mitchell {B, C}, LanczosSinc {tau};
                                         alpha or tau <= 0 means pine's default (1, 3) */
+    int32_t integrator;              /* PG_INTEGRATOR_* */
 } pg_scene_desc;
 
 /* ---- render requests ---- */

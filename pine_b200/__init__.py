@@ -117,7 +117,7 @@ class SceneDesc(ctypes.Structure):
                 ("num_node_ops", ctypes.c_int32), ("node_ops", ctypes.POINTER(NodeOp)),
                 ("sampler", ctypes.c_int32), ("sampler_scramble", ctypes.c_int32),
                 ("filter", ctypes.c_int32), ("filter_radius", ctypes.c_float * 2),
-                ("filter_params", ctypes.c_float * 2)]
+                ("filter_params", ctypes.c_float * 2), ("integrator", ctypes.c_int32)]
 
 
 SAMPLER_INDEPENDENT, SAMPLER_HALTON = 0, 1

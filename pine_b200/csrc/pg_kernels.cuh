@@ -91,6 +91,7 @@ struct RequestDev {
     int filter_splat;                 // 0: box of radius 0.5 (one pixel, weight 1)
     float filter_radius[2];
     const float* filter_table;        // 16 x 16 filter values (film.cpp:20-28)
+    int random_walk;                  // RandomWalkIntegrator::Li instead of PathIntegrator::Li
 };
 
 struct RenderParams {
@@ -445,7 +446,7 @@ __device__ __forceinline__ unsigned long long BlockClaim(const RenderParams& P, 
 // Fills the slots listed in the finished queue with new camera samples (the start of a
 // render; afterwards shading and shadow kernels refill slots themselves).
 template <int M, bool MULTI, bool GEN>
-__global__ void k_regen(RenderParams P, SceneDev S0) {
+__global__ void k_regen(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     __shared__ int claimOff[32];
     __shared__ unsigned long long claimBase;
     __shared__ BlockQueues<1> q1;
@@ -472,7 +473,7 @@ __global__ void k_regen(RenderParams P, SceneDev S0) {
 }
 
 // Makes the next queue the active one and decides whether the loop continues.
-static __global__ void k_swap(RenderParams P) {
+static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     int* c = P.counts;
     int active = c[kCntNext];
     c[kCntActive] = active;
@@ -494,7 +495,7 @@ static __global__ void k_swap(RenderParams P) {
 }
 
 template <bool MULTI>
-__global__ void k_trace(RenderParams P, SceneDev S0) {
+__global__ void k_trace(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];
     const int n = P.counts[kCntActive];
     const int* active = ActiveList(P);
@@ -808,6 +809,9 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     V3 beta = v3(bt.x, bt.y, bt.z), L = v3(Lw.x, Lw.y, Lw.z);
     int depth = __float_as_int(bt.w);
     const int maxDepth = R.max_depth;
+    // RandomWalkIntegrator::Li (randomwalk.cpp:6-64): no next-event estimation, emission
+    // counted in full where a path meets it, no Russian roulette.
+    const bool walk = GEN && R.random_walk;
     Rng rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(Lw.w));
     int prim = __float_as_int(h.y);
     bool found = prim != -1;
@@ -830,8 +834,9 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             finished = true;
         } else {
             const MediumDev& m = S.media[medium];
-            NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr, nullptr,
-                                m.g, medium, medium, beta, L, stack, ct, ps);
+            if (!walk)
+                NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr,
+                                           nullptr, m.g, medium, medium, beta, L, stack, ct, ps);
             if (GUIDE) {
                 PushGuide(P, i, ev.p, v3(0.0f), false, medium, -d, ps.idx, medium, medium);
                 deferred = true;
@@ -851,7 +856,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
         if (S.env_light >= 0) {
             float lpdf;
             V3 le = EnvColor<M>(S, d, lpdf);
-            if (depth == 0)
+            if (depth == 0 || walk)
                 L += beta * le;
             else
                 L += beta * le * PowerHeuristic(bsdfPdf, lpdf);
@@ -881,7 +886,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
                 // path.cpp:51-60; Le is one-sided (material.h:60-65).
                 V3 le = Dot(-d, si.n) > 0.0f ? v3(mat.emission[0], mat.emission[1], mat.emission[2])
                                               : v3(0.0f);
-                if (depth == 0) {
+                if (depth == 0 || walk) {
                     L += beta * le;
                 } else {
                     float lightPdf = Sqr(tHit) / (AbsDot(-d, si.n) * sh.area);  // Shape::Pdf
@@ -893,8 +898,9 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             } else {
                 Frame<M> fr;
                 fr.From(si.n);
-                NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr, 0.0f,
-                                    medIn, medOut, beta, L, stack, ct, ps);
+                if (!walk)
+                    NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr,
+                                               0.0f, medIn, medOut, beta, L, stack, ct, ps);
                 if (GUIDE && GuideEligible(mat)) {
                     PushGuide(P, i, si.p, si.n, true, sh.material, -d, ps.idx, medIn, medOut);
                     deferred = true;
@@ -917,7 +923,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
                         no = OffsetRayOrigin(si.p, FaceSameHemisphere(si.n, bs.wo));
                         nd = bs.wo;
                         nmed = Dot(bs.wo, si.n) > 0 ? medOut : medIn;
-                        if (depth > 2) {  // Russian roulette (path.cpp:74-80)
+                        if (depth > 2 && !walk) {  // Russian roulette (path.cpp:74-80)
                             float qrr = Clamp(1.0f - Luminance(beta), 0.05f, 1.0f);
                             if (rng.Get1D() < qrr)
                                 finished = true;
@@ -949,7 +955,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
 }
 
 template <int M, bool MULTI, bool FUSED, bool GUIDE, bool MEDIA, bool GEN>
-__global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
+__global__ void PG_SHADE_BOUNDS k_shade(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
     __shared__ int claimOff[32];
@@ -1005,7 +1011,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(RenderParams P, SceneDev S0) {
 }
 
 template <int M, bool MULTI, bool GUIDE, bool MEDIA, bool GEN>
-__global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shadow(RenderParams P, SceneDev S0) {
+__global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shadow(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
     __shared__ int claimOff[32];
@@ -1183,7 +1189,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
 }
 
 template <int M>
-__global__ void k_guide_sample(RenderParams P, SceneDev S0) {
+__global__ void k_guide_sample(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     __shared__ BlockQueues<1> q1;
     __shared__ int claimOff[32];
     __shared__ unsigned long long claimBase;

@@ -4,6 +4,10 @@
 
 namespace pg {
 
+cudaError_t ConfigureKernelsFast() {
+    return ConfigureKernelsM<kFast>();
+}
+
 void DispatchRegenFast(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res) {
     DispatchRegenM<kFast>(env, w, timer, res);
 }

@@ -4,6 +4,10 @@
 
 namespace pg {
 
+cudaError_t ConfigureKernelsPine() {
+    return ConfigureKernelsM<kPine>();
+}
+
 void DispatchRegenPine(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res) {
     DispatchRegenM<kPine>(env, w, timer, res);
 }

@@ -108,10 +108,6 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
     // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
     const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
     const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
-    if (FUSED && shadeSmem > 48 * 1024)
-        PG_CUDA(cudaFuncSetAttribute(k_shade<M, MULTI, FUSED, false, true, GEN>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)shadeSmem));
     time(PG_KERNEL_SHADE, [&]() {
         if (!FUSED && !w.media)
             k_shade<M, MULTI, false, false, false, GEN>
@@ -169,9 +165,6 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
     // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
     const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
     const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
-    if (FUSED && shadeSmem > 48 * 1024)
-        PG_CUDA(cudaFuncSetAttribute(k_shade<M, false, FUSED, true, true, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shadeSmem));
     time(PG_KERNEL_SHADE, [&]() {
         k_shade<M, false, FUSED, true, true, true><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem,
                                          st>>>(w.P, w.S0);
@@ -210,6 +203,26 @@ static void Body(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTi
                 : LaunchBody<M, MULTI, false, false>(env, w, n, persistent, timer, res);
 }
 
+// The fused shading kernels keep traversal stacks in dynamic shared memory; the opt-in for
+// their largest size is set once per device, before any launch or stream capture.
+template <int M>
+static cudaError_t ConfigureKernelsM() {
+    const int smem = PG_SHADE_MAX_THREADS * kStackSize * (int)sizeof(uint2);
+    const void* fused[] = {
+        (const void*)k_shade<M, false, true, false, true, false>,
+        (const void*)k_shade<M, false, true, false, true, true>,
+        (const void*)k_shade<M, true, true, false, true, false>,
+        (const void*)k_shade<M, true, true, false, true, true>,
+        (const void*)k_shade<M, false, true, true, true, true>,
+    };
+    for (const void* f : fused) {
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
 // Regen and body launches of one math mode (M is kPine or kFast); each mode's kernels are
 // compiled in their own translation unit.
 template <int M>
@@ -228,6 +241,8 @@ static void DispatchBodyM(const LaunchEnv& env, Wave& w, int n, bool persistent,
             : Body<M, false>(env, w, n, persistent, timer, res);
 }
 
+cudaError_t ConfigureKernelsPine();
+cudaError_t ConfigureKernelsFast();
 void DispatchRegenPine(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res);
 void DispatchRegenFast(const LaunchEnv& env, Wave& w, LaunchTimer* timer, RenderResult* res);
 void DispatchBodyPine(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,

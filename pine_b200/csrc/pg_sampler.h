@@ -139,12 +139,28 @@ PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
     }
     uint32_t a32 = (uint32_t)a;
     const uint32_t b32 = (uint32_t)base;
+    // Four digits at a time: the divisions first, then the four permutation loads issued
+    // together, so that their latencies overlap; then the digits in pine's order.
     while (a32) {
-        uint32_t next = DivByMagic(a32, mg);
-        uint32_t digit = a32 - next * b32;
-        rev = rev * (uint64_t)base + (perm ? perm[digit] : digit);
-        invBaseN = RnMul(invBaseN, invBase);
-        a32 = next;
+        uint32_t dg[4];
+        int k = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            uint32_t next = DivByMagic(a32, mg);
+            dg[j] = a32 - next * b32;
+            k += a32 != 0;
+            a32 = next;
+        }
+        uint32_t pd[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            pd[j] = j < k ? (perm ? perm[dg[j]] : dg[j]) : 0u;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (j < k) {
+                rev = rev * (uint64_t)base + pd[j];
+                invBaseN = RnMul(invBaseN, invBase);
+            }
     }
     float v;
     if (perm) {

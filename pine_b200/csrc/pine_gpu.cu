@@ -88,6 +88,7 @@ struct DeviceScene {
     float filter_radius[2] = {0.5f, 0.5f};
     const float* filter_table = nullptr;   // device, 16 x 16
     bool general = false;                  // needs the GEN kernel variants
+    int random_walk = 0;                   // PG_INTEGRATOR_RANDOM_WALK
     bool surfaces = false;
     int64_t prims = 0;
     int bvh_depth = 0;
@@ -305,6 +306,8 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     Require(d->sampler == PG_SAMPLER_INDEPENDENT || d->sampler == PG_SAMPLER_HALTON,
             "unknown sampler");
     Require(d->filter >= PG_FILTER_BOX && d->filter <= PG_FILTER_LANCZOS_SINC, "unknown filter");
+    Require(d->integrator == PG_INTEGRATOR_PATH || d->integrator == PG_INTEGRATOR_RANDOM_WALK,
+            "unknown integrator");
     float fRadius[2], fParams[2];
     for (int k = 0; k < 2; k++) {
         fRadius[k] = d->filter_radius[k] > 0.0f ? d->filter_radius[k] : 0.5f;
@@ -751,7 +754,8 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     sc->filter_radius[1] = fRadius[1];
     sc->filter_splat = sc->sampler == PG_SAMPLER_HALTON ||
                        !(d->filter == PG_FILTER_BOX && fRadius[0] == 0.5f && fRadius[1] == 0.5f);
-    sc->general = sc->filter_splat || d->num_node_ops > 0;
+    sc->random_walk = d->integrator == PG_INTEGRATOR_RANDOM_WALK;
+    sc->general = sc->filter_splat || d->num_node_ops > 0 || sc->random_walk;
     if (sc->filter_splat) {
         std::vector<float> table(kFilterTableWidth * kFilterTableWidth);
         FilterTable(d->filter, fRadius, fParams, table.data());
@@ -799,6 +803,7 @@ static void SetRequestSampling(pg_ctx* ctx, const DeviceScene& sc, RequestDev& r
     rq.filter_radius[0] = sc.filter_radius[0];
     rq.filter_radius[1] = sc.filter_radius[1];
     rq.filter_table = sc.filter_table;
+    rq.random_walk = sc.random_walk;
 }
 
 // ---------------------------------------------------------------- rendering
@@ -937,9 +942,18 @@ static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res, unsigned long long
     w.P.use_cond = 1;
     w.P.cond = cond;
     PG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    DispatchBody(ctx, w, w.P.slots, true, nullptr, nullptr);
+    cudaError_t le = cudaSuccess;
+    try {
+        DispatchBody(ctx, w, w.P.slots, true, nullptr, nullptr);
+    } catch (const Failure&) {
+        le = cudaErrorUnknown;
+    }
+    if (le == cudaSuccess)
+        le = cudaGetLastError();  // a launch the capture refused
     cudaGraph_t captured = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(st, &captured);
+    cudaError_t ce = cudaStreamEndCapture(st, &captured);  // always ends the capture
+    if (le != cudaSuccess)
+        throw Failure{PG_ERR_CUDA, std::string("graph capture launch: ") + cudaGetErrorString(le)};
     if (ce != cudaSuccess)
         throw Failure{PG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)};
     PG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -1131,6 +1145,8 @@ extern "C" pg_status pg_create(pg_ctx** out, int device) {
         Require(device >= 0 && device < count, "device index out of range");
         PG_CUDA(cudaSetDevice(device));
         ctx->device = device;
+        PG_CUDA(ConfigureKernelsPine());
+        PG_CUDA(ConfigureKernelsFast());
         PG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         // Keep freed stream-ordered memory in the device's pool for later scenes (this
         // process only; nothing outlives it).
@@ -1309,6 +1325,7 @@ static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec, 
 static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
                          int sampleOffset, int mathMode, bool accumulate, bool profile,
                          RenderResult& res) {
+    Require(!sc.random_walk, "guided rendering needs the Path integrator");
     EnsureGuide(ctx);
     float accept = ctx->guide_steps < kGuideStepBudget ? 1.0f : 0.0f;
     int done = 0;

@@ -843,7 +843,8 @@ void LoadSceneFile(const std::string& path, HostScene& s) {
     // Integrator (integrator.cpp:20-56): maxDepth default 4, sampler spp, light sampler.
     Params& integ = params["Integrator"];
     std::string itype = integ.String("type", "Path");
-    if (itype != "Path" && itype != "GpuPath")
+    s.integrator = itype == "RandomWalk" ? PG_INTEGRATOR_RANDOM_WALK : PG_INTEGRATOR_PATH;
+    if (itype != "Path" && itype != "GpuPath" && itype != "RandomWalk")
         Warn("[Integrator][Create]Integrator \"" + itype + "\" is rendered as GpuPath");
     s.max_depth = integ.Int("maxDepth", 4);
     // Sampler (CreateSampler, sampler.cpp:281-293) and its samples per pixel.
@@ -922,6 +923,7 @@ void HostScene::Describe(pg_scene_desc& d) {
     d.sampler = sampler;
     d.sampler_scramble = sampler_scramble;
     d.filter = filter;
+    d.integrator = integrator;
     for (int k = 0; k < 2; k++) {
         d.filter_radius[k] = filter_radius[k];
         d.filter_params[k] = filter_params[k];

@@ -61,6 +61,7 @@ struct HostScene {
     int sampler = PG_SAMPLER_INDEPENDENT;
     int sampler_scramble = 1;
     int filter = PG_FILTER_LANCZOS_SINC;
+    int integrator = PG_INTEGRATOR_PATH;
     float filter_radius[2] = {0.5f, 0.5f};
     float filter_params[2] = {3.0f, 0.0f};
 

@@ -7,7 +7,7 @@ from the seeded generators in pine_b200.scenegen; everything a test needs to rep
 not depend on the generators or on the reference being present.
 
     python tests/golden/make_golden.py           # needs oracle/_ref/pine_ref
-    python tests/golden/make_golden.py nodes pine_spheres sampler filtered   # only those
+    python tests/golden/make_golden.py nodes pine_spheres sampler filtered randomwalk
 """
 
 from __future__ import annotations
@@ -269,6 +269,20 @@ def filtered_case(tmp):
     image_case("filtered", path, [])
 
 
+def randomwalk_case(tmp):
+    """The spheres fixture's scene rendered by pine's RandomWalk integrator at 512 spp."""
+    z = np.load(f"{HERE}/image_spheres.npz", allow_pickle=True)
+    text = str(z["scene_text"])
+    assert text.startswith("Integrator: Path{")
+    text = text.replace("Integrator: Path{", "Integrator: RandomWalk{", 1)
+    text = text.replace("samplesPerPixel: 1024", "samplesPerPixel: 512")
+    assert "samplesPerPixel: 512" in text
+    path = f"{tmp}/randomwalk.txt"
+    with open(path, "w") as f:
+        f.write(text)
+    image_case("randomwalk", path, [])
+
+
 def shipped_spheres_case(tmp):
     """pine's own scenes/spheres.txt (textures, noise, bump map, two-layer plastic) at a
     tenth of its film size and 512 spp."""
@@ -295,6 +309,8 @@ def main():
                 sampler_filter_kat(tmp)
             if "filtered" in only:
                 filtered_case(tmp)
+            if "randomwalk" in only:
+                randomwalk_case(tmp)
             if "pine_spheres" in only:
                 shipped_spheres_case(tmp)
         print("fixtures written to", HERE)
@@ -344,6 +360,7 @@ def main():
         shipped_spheres_case(tmp)
         sampler_filter_kat(tmp)
         filtered_case(tmp)
+        randomwalk_case(tmp)
     print("fixtures written to", HERE)
 
 

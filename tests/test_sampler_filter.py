@@ -95,3 +95,16 @@ def test_loader_reads_filters(pglib, tmp_path, k):
     np.testing.assert_allclose(list(d.filter_radius), radius)
     np.testing.assert_allclose(list(d.filter_params), params, rtol=1e-6)
     ps.close()
+
+
+@pytest.mark.parametrize("itype,kind", [("Path", 0), ("RandomWalk", 1), ("GpuPath", 0)])
+def test_loader_reads_integrators(pglib, tmp_path, itype, kind):
+    import pine_b200 as pb
+    path = _scene(tmp_path, "Uniform{\n samplesPerPixel: 2\n }", "")
+    with open(path) as f:
+        text = f.read().replace("Integrator: Path{", "Integrator: " + itype + "{")
+    with open(path, "w") as f:
+        f.write(text)
+    ps = pb.ParsedScene(path)
+    assert ps.desc.integrator == kind
+    ps.close()
