@@ -83,23 +83,6 @@ def test_halton_renders_follow_pine_sample_by_sample(ctx, tmp_path, name):
     ctx.release_scene(sid)
 
 
-def test_random_walk_and_path_estimate_the_same_image(ctx, tmp_path):
-    """RandomWalkIntegrator (no light sampling) and PathIntegrator are two unbiased
-    estimators of one image: the GPU's random walk agrees with its path tracer within
-    their combined Monte Carlo error."""
-    zr, zp = golden("image_randomwalk.npz"), golden("image_spheres.npz")
-    walk = ctx.load_scene(write_fixture_scene(zr, str(tmp_path / "w")))
-    path = ctx.load_scene(write_fixture_scene(zp, str(tmp_path / "p")))
-    a = ctx.render(walk, spp=2048, seed=5, math_mode="fast")
-    b = ctx.render(path, spp=256, seed=6, math_mode="fast")
-    frac, zs = zfrac(a["mean"].astype(float), a["var"].astype(float), a["count"].astype(float),
-                     b["mean"].astype(float), b["var"].astype(float), b["count"].astype(float))
-    assert frac >= 0.98, frac
-    assert abs(zs.mean()) < 0.1
-    ctx.release_scene(walk)
-    ctx.release_scene(path)
-
-
 def test_against_restatement_other_seeds(ctx, tmp_path):
     """The C restatement at 256 spp vs the GPU on the spheres scene, new seeds."""
     z = golden("image_spheres.npz")
