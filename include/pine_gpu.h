@@ -312,7 +312,7 @@ pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc, f
  * or a thread that cannot take the device-wide synchronisation cudaMalloc and cudaFree
  * may cause.  No counterpart in the reference (pine renders on the host).
  * Path state and the film accumulators live in one fixed array inside the library,
- * about 26 MiB on every GPU that loads it, held until the process exits: at most 65536
+ * about 27 MiB on every GPU that loads it, held until the process exits: at most 65536
  * path slots and films of at most 524288 pixels (larger films: PG_ERR_INVALID_ARG).
  * mean_device: caller-owned DEVICE memory of width*height*3 floats on the context's
  * GPU; it receives the per-pixel mean as pg_render's out_mean does.  desc->accumulate

@@ -63,7 +63,7 @@ enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlot
 
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
-                  kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kNumCounts = 8 };
+                  kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kNumCounts = 9 };
 
 // Guided rendering.  A guide-queue entry (kGuideEntry float4) holds a vertex whose next
 // direction waits for the network: position + slot, normal (NaN x in a medium) +
@@ -118,6 +118,8 @@ struct RenderParams {
     float4* film_acc;            // per pixel: sum w r, w g, w b, sum w (this call)
     float4* film_acc2;           // per pixel: sum w r^2, w g^2, w b^2 (this call)
     float2* film_acc3;           // per pixel: sum w^2, samples (filtered films; may be null)
+    float4* splat;               // finished samples of filtered films: L.rgb, sample key
+    int* splat_req;              // their requests (batched renders)
     unsigned long long* next_sample;
     unsigned long long* stats;   // StatIndex
     uint32_t* req_done;          // completed paths per request
@@ -316,8 +318,8 @@ __device__ __forceinline__ void RedAdd2(float2* a, float x, float y) {
 // Film::AddSample (film.h:26-45) with a filter table: the sample's film position is
 // rebuilt from its camera jitter (the first two draws of its stream) exactly as the camera
 // formed it, and the sample is added to every pixel within the filter radius with the
-// table's weight.
-static __device__ __noinline__ void SplatSample(const RenderParams& P, const RequestDev& R, uint32_t key0,
+// table's weight.  Runs in k_splat, over the samples the shading kernels queued.
+__device__ __forceinline__ void SplatSample(const RenderParams& P, const RequestDev& R, uint32_t key0,
                                          uint32_t pixInImage, V3 c) {
     float u0, u1;
     Rng cr = PathRng<true>(R, key0, FirstDim<true>(R));
@@ -358,7 +360,11 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
     if (!Finite(c)) {
         dropped++;
     } else if (GEN && R.filter_splat) {
-        SplatSample(P, R, P.sample[i], pixInImage, c);
+        // Queued for k_splat, which keeps the filter's work out of the shading kernels.
+        int q = WarpAppend(&P.counts[kCntSplat], true);
+        P.splat[q] = make_float4(c.x, c.y, c.z, __uint_as_float(P.sample[i]));
+        if (MULTI)
+            P.splat_req[q] = P.slot_req[i];
     } else {
         RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
         RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
@@ -472,6 +478,20 @@ __global__ void k_regen(const __grid_constant__ RenderParams P, const __grid_con
     }
 }
 
+// Adds the queued samples of filtered films to the film (at most one per path slot and
+// iteration: a slot refilled in an iteration starts its new path in the next one).
+template <bool MULTI>
+__global__ void k_splat(const __grid_constant__ RenderParams P) {
+    const int n = P.counts[kCntSplat];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const float4 e = P.splat[q];
+        const RequestDev& R = P.reqs[MULTI ? P.splat_req[q] : 0];
+        const uint32_t key0 = __float_as_uint(e.w);
+        const uint32_t pix = (key0 - R.key0_offset) % (uint32_t)R.npix;
+        SplatSample(P, R, key0, pix, v3(e.x, e.y, e.z));
+    }
+}
+
 // Makes the next queue the active one and decides whether the loop continues.
 static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     int* c = P.counts;
@@ -481,6 +501,7 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     c[kCntFinished] = 0;
     c[kCntShadow] = 0;
     c[kCntGuide] = 0;
+    c[kCntSplat] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
     bool more = active > 0;

@@ -78,6 +78,7 @@ struct Wave {
     bool multi = false, surfaces = false, fused = false, guide = false;
     bool media = true;  // false: no participating media, the lean kernel variants run
     bool general = false;  // Halton sampling, filter splats or shader nodes: GEN variants
+    bool splat = false;    // some film splats through a filter table: k_splat runs
     int mode = PG_MATH_FAST;
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
@@ -122,8 +123,12 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
             else
                 k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
         });
-    // Queue swap; counted with the fill kernel.
-    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
+    // Filtered films' splats and the queue swap; counted with the fill kernel.
+    time(PG_KERNEL_REGEN, [&]() {
+        if (w.splat)
+            k_splat<MULTI><<<grid(tb, 12), tb, 0, st>>>(w.P);
+        k_swap<<<1, 1, 0, st>>>(w.P);
+    });
 }
 
 // The initial fill of every slot and the first swap.  Later refills happen inside k_shade
@@ -183,7 +188,11 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
         time(PG_KERNEL_SHADOW, [&]() {
             k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
         });
-    time(PG_KERNEL_REGEN, [&]() { k_swap<<<1, 1, 0, st>>>(w.P); });
+    time(PG_KERNEL_REGEN, [&]() {
+        if (w.splat)
+            k_splat<false><<<grid(tb, 12), tb, 0, st>>>(w.P);
+        k_swap<<<1, 1, 0, st>>>(w.P);
+    });
 }
 
 template <int M, bool MULTI>

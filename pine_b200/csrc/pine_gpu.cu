@@ -104,6 +104,8 @@ struct Pool {
     int *state = nullptr, *lists = nullptr, *finished = nullptr, *slot_req = nullptr;
     float4 *so = nullptr, *sd = nullptr, *sc = nullptr;
     uint32_t* skey = nullptr;
+    float4* splat = nullptr;   // queued samples of filtered films
+    int* splat_req = nullptr;
     void Ensure(int n) {
         if (n <= slots)
             return;
@@ -123,6 +125,8 @@ struct Pool {
         sd = mem.Alloc<float4>(n);
         sc = mem.Alloc<float4>(n);
         skey = mem.Alloc<uint32_t>(n);
+        splat = mem.Alloc<float4>(n);
+        splat_req = mem.Alloc<int>(n);
     }
 };
 
@@ -865,6 +869,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.sample = pl.sample, P.state = pl.state, P.lists = pl.lists, P.finished = pl.finished;
     P.slot_req = pl.slot_req;
     P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
+    P.splat = pl.splat, P.splat_req = pl.splat_req;
     P.counts = ctx->counts;
     P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2, P.film_acc3 = ctx->film.acc3;
     P.next_sample = ctx->next_sample;
@@ -1052,6 +1057,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.guide = recordAccept != nullptr;
     w.media = sc.dev.num_media > 0;
     w.general = sc.general;
+    w.splat = sc.filter_splat != 0;
     if (w.guide)
         w.P.rec_accept = *recordAccept;
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
@@ -1514,7 +1520,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     std::vector<RequestDev> rq(n);
     std::vector<SceneDev> scenes(n);
     uint64_t total = 0, pixels = 0;
-    bool surfaces = false, media = false, general = false;
+    bool surfaces = false, media = false, general = false, splat = false;
     int maxDepth = 1;
     const int variant = MediaVariant(tune);
     // Shortest job first: requests take their sample ranges in increasing order of their
@@ -1565,6 +1571,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         surfaces = surfaces || sc.surfaces;
         media = media || sc.dev.num_media > 0;
         general = general || sc.general;
+        splat = splat || sc.filter_splat != 0;
     }
     ClearFilm(ctx, (int64_t)pixels);
     ClearCallFilm(ctx, (int64_t)pixels);
@@ -1581,6 +1588,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.surfaces = surfaces;
     w.media = media;
     w.general = general;
+    w.splat = splat;
     w.fused = tune.split_shadow == 0;
     w.shadeBlock = tune.block_size;
     w.S0 = scenes[0];
@@ -1718,17 +1726,17 @@ constexpr size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct NoAllocLayout {
     static constexpr size_t kF4 = (size_t)kNoAllocSlots * sizeof(float4);
     static constexpr size_t kI = (size_t)kNoAllocSlots * sizeof(int);
-    // ray_o, ray_d, beta, L, hit, so, sd, sc
+    // ray_o, ray_d, beta, L, hit, so, sd, sc, splat
     static constexpr size_t float4s = 0;
-    // sample, skey, state, finished, slot_req, lists (2 x slots)
-    static constexpr size_t ints = float4s + 8 * Align256(kF4);
-    static constexpr size_t film = ints + 7 * Align256(kI);
+    // sample, skey, state, finished, slot_req, lists (2 x slots), splat_req
+    static constexpr size_t ints = float4s + 9 * Align256(kF4);
+    static constexpr size_t film = ints + 8 * Align256(kI);
     static constexpr size_t filmBytes = Align256((size_t)kNoAllocPixels * sizeof(float4));
     static constexpr size_t request = film + 2 * filmBytes;
     static constexpr size_t total = request + Align256(sizeof(RequestDev));
 };
 
-// The array: about 26 MiB on every GPU that loads the library, held until the process
+// The array: about 27 MiB on every GPU that loads the library, held until the process
 // exits.  All calls on a device share it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
 
@@ -1784,6 +1792,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
     w.general = sc.general;
+    w.splat = sc.filter_splat != 0;
     w.fused = ctx->tuning.split_shadow == 0;
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
@@ -1797,6 +1806,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     P.sample = reinterpret_cast<uint32_t*>(i32(0));
     P.skey = reinterpret_cast<uint32_t*>(i32(1));
     P.state = i32(2), P.finished = i32(3), P.slot_req = i32(4), P.lists = i32(5);
+    P.splat = f4(8), P.splat_req = i32(7);
     P.counts = ctx->counts;
     P.film_acc = acc, P.film_acc2 = acc2, P.film_acc3 = nullptr;  // the mean needs no more
     P.next_sample = ctx->next_sample;
