@@ -335,6 +335,19 @@ pg_status pg_intersect_device(pg_ctx* ctx, int32_t scene_id, const float* d_rays
                               int32_t* d_shape_id, int32_t* d_prim_id, float* d_t,
                               float* d_uv);
 
+/* ---- BVH construction ----
+ * PG_BVH_HOST: binned SAH on the host threads (pine builds its binary BVH on one host
+ * thread with a full SAH sweep, src/impl/accel/bvh.cpp:145-284).  PG_BVH_GPU: a linear BVH
+ * built on the GPU (Morton order, radix tree, bottom-up boxes), faster to build and
+ * slower to traverse.  Both collapse to the same 8-wide compressed format; closest hits do
+ * not depend on the tree.  The choice applies to later pg_upload_scene calls. */
+enum { PG_BVH_HOST = 0, PG_BVH_GPU = 1 };
+pg_status pg_set_bvh_builder(pg_ctx* ctx, int32_t builder);
+/* The BVH of a loaded scene: build time (host clock, seconds), depth and node count of the
+ * 8-wide tree.  Any output may be NULL. */
+pg_status pg_scene_bvh_info(pg_ctx* ctx, int32_t scene_id, double* build_seconds,
+                            int32_t* wide_depth, int64_t* wide_nodes);
+
 /* ---- batched requests (many renders in one persistent, graph-captured launch) ---- */
 typedef struct pg_request {
     int32_t scene_id;

@@ -208,6 +208,9 @@ def lib():
         "pg_guide_pdf": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_sample": (None, [_F, _F, ctypes.c_int64, _F]),
         "pg_guide_loss_grad": (None, [_F, _F, ctypes.c_int64, _F, _F]),
+        "pg_set_bvh_builder": (st, [ctypes.c_void_p, ctypes.c_int32]),
+        "pg_scene_bvh_info": (st, [ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_double),
+                                   _P(ctypes.c_int32), _P(ctypes.c_int64)]),
         "pg_halton_sample": (st, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                   _P(ctypes.c_int64), ctypes.c_int64, _F]),
         "pg_filter_table": (st, [ctypes.c_int32, _F, _F, _F]),
@@ -403,6 +406,17 @@ class Context:
         self._check(self._lib.pg_scene_info(self._ctx, int(scene), ctypes.byref(w),
                                             ctypes.byref(h), ctypes.byref(s), ctypes.byref(d)))
         return {"width": w.value, "height": h.value, "spp": s.value, "max_depth": d.value}
+
+    def set_bvh_builder(self, builder: str):
+        """"host" (binned SAH on the host threads) or "gpu" (linear BVH on the GPU) for
+        later load_scene calls."""
+        self._check(self._lib.pg_set_bvh_builder(self._ctx, {"host": 0, "gpu": 1}[builder]))
+
+    def bvh_info(self, scene: int):
+        sec, depth, nodes = ctypes.c_double(), ctypes.c_int32(), ctypes.c_int64()
+        self._check(self._lib.pg_scene_bvh_info(self._ctx, int(scene), ctypes.byref(sec),
+                                                ctypes.byref(depth), ctypes.byref(nodes)))
+        return {"build_seconds": sec.value, "depth": depth.value, "nodes": nodes.value}
 
     # ---- rendering
     def render(self, scene: int, spp: int = 0, max_depth: int = 0, seed: int = 0,

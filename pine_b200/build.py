@@ -21,7 +21,7 @@ CLI = os.path.join(HERE, "pine-gpu")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["pine_gpu.cu", "pg_kernels_pine.cu", "pg_kernels_fast.cu", "guide_mlp.cu", "batch.cu",
-           "scene_load.cpp", "bvh_build.cpp", "scenegen.cpp"]
+           "scene_load.cpp", "bvh_build.cpp", "bvh_gpu.cu", "scenegen.cpp"]
 HEADERS = ["pg_math.h", "pg_device.cuh", "pg_shade.cuh", "pg_kernels.cuh", "scene_load.h",
            "bvh_build.h", "guide_net.cuh", "guide_mlp.h", "pg_nodes.h", "pg_sampler.h",
            "pg_launch.cuh", "pg_error.h"]

@@ -27,12 +27,6 @@
 namespace pg {
 namespace {
 
-struct BNode {
-    Box box;
-    int left = -1, right = -1;
-    int begin = 0, end = 0;
-};
-
 float Area(const Box& b) {
     float dx = std::max(0.0f, b.hi[0] - b.lo[0]), dy = std::max(0.0f, b.hi[1] - b.lo[1]),
           dz = std::max(0.0f, b.hi[2] - b.lo[2]);
@@ -255,13 +249,17 @@ uint8_t ExpByte(double ext) {
 }  // namespace
 
 WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
-    WideBVH out;
     if (boxes.empty())
-        return out;
+        return WideBVH{};
     Builder b(boxes);
     int root = b.Build(0, (int)boxes.size());
+    WideBVH out = CollapseToWide(b.nodes, root, b.idx);
     out.binary_nodes = (int64_t)b.next.load();
-    const auto& bn = b.nodes;
+    return out;
+}
+
+WideBVH CollapseToWide(const std::vector<BNode>& bn, int root, const std::vector<uint32_t>& idx) {
+    WideBVH out;
     auto isLeaf = [&](int i) { return bn[i].left < 0; };
 
     struct Task {
@@ -270,8 +268,8 @@ WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
         int depth;
     };
     std::vector<Task> stack;
-    out.nodes.reserve(boxes.size() / 3 + 16);
-    out.prim_order.reserve(boxes.size());
+    out.nodes.reserve(idx.size() / 3 + 16);
+    out.prim_order.reserve(idx.size());
     out.nodes.resize(1);
     stack.push_back({root, 0, 1});
     while (!stack.empty()) {
@@ -391,7 +389,7 @@ WideBVH BuildWideBVH(const std::vector<Box>& boxes) {
                 int cnt = bn[c].end - bn[c].begin;
                 node.meta[s] = (uint8_t)((cnt << 5) | primOffset);
                 for (int i = bn[c].begin; i < bn[c].end; i++)
-                    out.prim_order.push_back(b.idx[i]);
+                    out.prim_order.push_back(idx[i]);
                 primOffset += (uint32_t)cnt;
             } else {
                 node.imask |= (uint8_t)(1u << s);

@@ -39,8 +39,27 @@ struct WideBVH {
     int64_t binary_nodes = 0;
 };
 
-// Builds over boxes[i] (i = caller's primitive index).  Leaves hold at most 3 primitives.
-// An empty input gives an empty BVH.
+// Binary tree node: an internal node has both children (node indices); a leaf (left < 0)
+// covers the primitives idx[begin .. end) of the build's primitive order.
+struct BNode {
+    Box box;
+    int left = -1, right = -1;
+    int begin = 0, end = 0;
+};
+
+// Builds over boxes[i] (i = caller's primitive index) by binned SAH on the host threads.
+// Leaves hold at most 3 primitives.  An empty input gives an empty BVH.
 WideBVH BuildWideBVH(const std::vector<Box>& boxes);
+
+// The 8-wide compressed tree of a binary tree (collapse, octant slots, quantised boxes).
+// Leaves must hold at most 3 primitives.
+WideBVH CollapseToWide(const std::vector<BNode>& nodes, int root,
+                       const std::vector<uint32_t>& idx);
+
+// The binary tree as a linear BVH on the GPU (Morton order, Karras's radix-tree
+// construction, bottom-up boxes; subtrees of at most 3 primitives become leaves), then
+// CollapseToWide on the host.  stream: the CUDA stream to build on (device memory is
+// stream-ordered and released before returning).
+WideBVH BuildWideBVHGpu(const std::vector<Box>& boxes, void* stream);
 
 }  // namespace pg

@@ -92,6 +92,8 @@ struct DeviceScene {
     bool surfaces = false;
     int64_t prims = 0;
     int bvh_depth = 0;
+    int64_t bvh_nodes = 0;
+    double bvh_seconds = 0.0;  // build time, host clock (GPU builds include their copies)
 };
 
 
@@ -216,6 +218,7 @@ struct pg_ctx {
     const pg::DivMagic* halton_magic = nullptr;
     const int* halton_sums = nullptr;
     const uint16_t* halton_perm = nullptr;
+    int bvh_builder = PG_BVH_HOST;         // PG_BVH_*: how later scene uploads build their BVH
 };
 
 namespace pg {
@@ -667,7 +670,11 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
             S.guide_inv[k] = 1.0f / std::max(hi[k] - lo[k], 1e-3f);
         }
     }
-    WideBVH bvh = BuildWideBVH(boxes);
+    auto tb0 = std::chrono::steady_clock::now();
+    WideBVH bvh = ctx->bvh_builder == PG_BVH_GPU ? BuildWideBVHGpu(boxes, (void*)st)
+                                                 : BuildWideBVH(boxes);
+    sc->bvh_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb0).count();
+    sc->bvh_nodes = (int64_t)bvh.nodes.size();
     sc->prims = (int64_t)boxes.size();
     sc->bvh_depth = bvh.max_depth;
     if (!boxes.empty()) {
@@ -2174,5 +2181,30 @@ extern "C" pg_status pg_filter_table(int32_t filter, const float* radius, const 
         Require(radius && params && table, "null argument");
         Require(filter >= PG_FILTER_BOX && filter <= PG_FILTER_LANCZOS_SINC, "unknown filter");
         FilterTable(filter, radius, params, table);
+    });
+}
+
+// ================================================================ BVH builder choice
+extern "C" pg_status pg_set_bvh_builder(pg_ctx* ctx, int32_t builder) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        Require(builder == PG_BVH_HOST || builder == PG_BVH_GPU, "unknown BVH builder");
+        ctx->bvh_builder = builder;
+    });
+}
+
+extern "C" pg_status pg_scene_bvh_info(pg_ctx* ctx, int32_t scene_id, double* build_seconds,
+                                       int32_t* wide_depth, int64_t* wide_nodes) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        DeviceScene& sc = GetScene(ctx, scene_id);
+        if (build_seconds)
+            *build_seconds = sc.bvh_seconds;
+        if (wide_depth)
+            *wide_depth = sc.bvh_depth;
+        if (wide_nodes)
+            *wide_nodes = sc.bvh_nodes;
     });
 }

@@ -85,3 +85,54 @@ def test_full_size_mesh_hits(ctx, tmp_path):
     assert hit.sum() > n * 0.9
     assert np.array_equal(t[hit].view(np.uint32), rt[hit].view(np.uint32))
     assert (rs == 0).sum() > n // 3  # most rays were aimed at the sphere
+
+
+@pytest.mark.parametrize("name", ["spheres", "mesh"])
+def test_gpu_built_bvh_gives_the_same_hits(pglib, tmp_path, name):
+    """The linear BVH built on the GPU: closest hits do not depend on the tree, so they
+    match pine's exactly, as the host-built tree's do."""
+    z = golden(f"hits_{name}.npz")
+    path = write_fixture_scene(z, str(tmp_path))
+    with pb.Context(0) as ctx:
+        ctx.set_bvh_builder("gpu")
+        sid = ctx.load_scene(path)
+        info = ctx.bvh_info(sid)
+        assert info["nodes"] > 0 and info["depth"] > 0
+        shape, prim, t, uv = ctx.intersect(sid, z["rays"])
+    h = z["hits"]
+    ref = oracle.Restatement(path)
+    _, _, _, amb = ref.intersect(z["rays"])
+    ref.close()
+    same = (shape == h["shape"]) & (prim == h["tri"])
+    assert same[~amb].all(), f"{np.count_nonzero(~same & ~amb)} rays differ"
+    hit = (h["shape"] >= 0) & same
+    assert np.array_equal(t[hit].view(np.uint32), h["t"][hit].view(np.uint32))
+
+
+def test_gpu_built_bvh_on_the_full_mesh(pglib, tmp_path):
+    """The benchmark mesh (about 1.3M triangles): both builders' trees give the same
+    closest hits on 65536 random rays, and the GPU build is faster."""
+    from pine_b200 import scenegen
+    path = scenegen.mesh_scene(str(tmp_path / "m.txt"), pb.lib(), width=64, height=36, spp=1,
+                               sampler="Uniform")
+    rng = np.random.default_rng(9)
+    o = rng.uniform(-3, 3, (65536, 3))
+    d = rng.normal(size=(65536, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d, np.zeros((65536, 1)), np.full((65536, 1), 3.4e38)], 1)
+    out = {}
+    with pb.Context(0) as ctx:
+        for builder in ("host", "gpu"):
+            ctx.set_bvh_builder(builder)
+            sid = ctx.load_scene(path)
+            out[builder] = ctx.intersect(sid, rays), ctx.bvh_info(sid)
+            ctx.release_scene(sid)
+    (hs, hp, ht, _), hi = out["host"]
+    (gs, gp, gt, _), gi = out["gpu"]
+    same = (hs == gs) & (hp == gp)
+    # Ties between two triangles at the same distance may go either way.
+    assert same.mean() > 0.9999
+    assert np.array_equal(ht[same].view(np.uint32), gt[same].view(np.uint32))
+    print(f"host build {hi['build_seconds']:.3f} s, GPU build {gi['build_seconds']:.3f} s; "
+          f"depth {hi['depth']} / {gi['depth']}, nodes {hi['nodes']} / {gi['nodes']}")
+    assert gi["build_seconds"] < hi["build_seconds"]
