@@ -57,9 +57,9 @@ WideBVH CollapseToWide(const std::vector<BNode>& nodes, int root,
                        const std::vector<uint32_t>& idx);
 
 // The binary tree as a linear BVH on the GPU (Morton order, Karras's radix-tree
-// construction, bottom-up boxes; subtrees of at most 3 primitives become leaves), then
-// CollapseToWide on the host.  stream: the CUDA stream to build on (device memory is
-// stream-ordered and released before returning).
+// construction, bottom-up boxes; subtrees of at most 3 primitives become leaves), then the
+// steps of CollapseToWide on the GPU as well, level by level.  stream: the CUDA stream to
+// build on (device memory is stream-ordered and released before returning).
 WideBVH BuildWideBVHGpu(const std::vector<Box>& boxes, void* stream);
 
 }  // namespace pg

@@ -2,7 +2,7 @@
 // their centroids, the radix tree over the sorted keys built with one thread per internal
 // node (Karras, "Maximizing parallelism in the construction of BVHs, octrees, and k-d
 // trees", HPG 2012), and node boxes reduced bottom-up with one thread per leaf.  The tree
-// then goes through the same 8-wide collapse and quantisation as the host build.
+// then goes through the 8-wide collapse and quantisation of the host build, on the GPU.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
@@ -12,6 +12,9 @@
 
 #include "bvh_build.h"
 #include "pg_error.h"
+
+#include <algorithm>
+#include <string>
 
 namespace pg {
 namespace {
@@ -150,6 +153,182 @@ __global__ void k_node_boxes(const Box* __restrict__ boxes, const unsigned long 
     }
 }
 
+// ---------------------------------------------------------------- collapse on the GPU
+// The same steps as the host's CollapseToWide, one thread per 8-wide node, level by level:
+// open the largest-area internal child until 8 children, octant slots, quantised boxes.
+struct BinTree {
+    int n;                       // primitives; nodes 0 .. n-2 internal, n-1 + k leaf k
+    const int *left, *right, *first, *last;
+    const Box* box;
+    const unsigned long long* keys;  // sorted; low 32 bits: primitive index
+};
+__device__ __forceinline__ bool IsLeafB(const BinTree& t, int b) {
+    return b >= t.n - 1 || t.last[b] - t.first[b] + 1 <= 3;
+}
+__device__ __forceinline__ void RangeB(const BinTree& t, int b, int& begin, int& end) {
+    if (b >= t.n - 1)
+        begin = b - (t.n - 1), end = begin + 1;
+    else
+        begin = t.first[b], end = t.last[b] + 1;
+}
+__device__ __forceinline__ float AreaB(const Box& b) {
+    float dx = fmaxf(0.0f, b.hi[0] - b.lo[0]), dy = fmaxf(0.0f, b.hi[1] - b.lo[1]),
+          dz = fmaxf(0.0f, b.hi[2] - b.lo[2]);
+    return 2.0f * (dx * dy + dx * dz + dy * dz);
+}
+__device__ __forceinline__ uint8_t ExpByteD(double ext) {
+    int e = -126;
+    if (ext > 0.0) {
+        e = (int)ceil(log2(ext / 254.0));
+        while (ldexp(254.0, e) < ext)
+            e++;
+        e = max(-126, min(127, e));
+    }
+    return (uint8_t)(e + 127);
+}
+
+__global__ void k_collapse(BinTree t, const int2* tasks, int ntasks, int2* next, int* counters,
+                           WideNode* nodes, uint32_t* primOrder) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ntasks; q += gridDim.x * blockDim.x) {
+        const int bnode = tasks[q].x, windex = tasks[q].y;
+        int ch[8], nch = 0;
+        if (IsLeafB(t, bnode)) {
+            ch[nch++] = bnode;
+        } else {
+            ch[nch++] = t.left[bnode];
+            ch[nch++] = t.right[bnode];
+            while (nch < 8) {
+                int bi = -1;
+                float ba = -1.0f;
+                for (int i = 0; i < nch; i++)
+                    if (!IsLeafB(t, ch[i]) && AreaB(t.box[ch[i]]) > ba) {
+                        ba = AreaB(t.box[ch[i]]);
+                        bi = i;
+                    }
+                if (bi < 0)
+                    break;
+                int c = ch[bi];
+                ch[bi] = t.left[c];
+                ch[nch++] = t.right[c];
+            }
+        }
+        Box nb;
+        for (int k = 0; k < 3; k++)
+            nb.lo[k] = FLT_MAX, nb.hi[k] = -FLT_MAX;
+        for (int i = 0; i < nch; i++)
+            for (int k = 0; k < 3; k++) {
+                nb.lo[k] = fminf(nb.lo[k], t.box[ch[i]].lo[k]);
+                nb.hi[k] = fmaxf(nb.hi[k], t.box[ch[i]].hi[k]);
+            }
+        double pc[3];
+        for (int k = 0; k < 3; k++)
+            pc[k] = 0.5 * ((double)nb.lo[k] + nb.hi[k]);
+        int slotOf[8];
+        bool usedSlot[8] = {}, placed[8] = {};
+        for (int round = 0; round < nch; round++) {
+            double bestCost = 1e300;
+            int bc = -1, bs = -1;
+            for (int c = 0; c < nch; c++) {
+                if (placed[c])
+                    continue;
+                double off[3];
+                for (int k = 0; k < 3; k++)
+                    off[k] = 0.5 * ((double)t.box[ch[c]].lo[k] + t.box[ch[c]].hi[k]) - pc[k];
+                for (int sl = 0; sl < 8; sl++) {
+                    if (usedSlot[sl])
+                        continue;
+                    double cost = 0.0;
+                    for (int k = 0; k < 3; k++)
+                        cost -= off[k] * ((sl >> k) & 1 ? -1.0 : 1.0);
+                    if (cost < bestCost) {
+                        bestCost = cost;
+                        bc = c;
+                        bs = sl;
+                    }
+                }
+            }
+            placed[bc] = true;
+            usedSlot[bs] = true;
+            slotOf[bc] = bs;
+        }
+        int childAt[8];
+        for (int sl = 0; sl < 8; sl++)
+            childAt[sl] = -1;
+        for (int c = 0; c < nch; c++)
+            childAt[slotOf[c]] = ch[c];
+
+        WideNode node;
+        memset(&node, 0, sizeof(node));
+        double pp[3], scale[3];
+        for (int k = 0; k < 3; k++) {
+            double lo = nb.lo[k], hi = nb.hi[k];
+            double ext = hi - lo;
+            double pad = fmax(fmax(ext / 512.0, fabs(lo) * 1e-6), 1e-30);
+            float pf = (float)(lo - pad);
+            while ((double)pf >= lo)
+                pf = nextafterf(pf, -FLT_MAX);
+            pp[k] = pf;
+            node.e[k] = ExpByteD(hi - (double)pf);
+            scale[k] = ldexp(1.0, (int)node.e[k] - 127);
+        }
+        node.px = (float)pp[0], node.py = (float)pp[1], node.pz = (float)pp[2];
+        int internal = 0, prims = 0;
+        for (int sl = 0; sl < 8; sl++) {
+            int c = childAt[sl];
+            if (c < 0)
+                continue;
+            if (IsLeafB(t, c)) {
+                int b0, b1;
+                RangeB(t, c, b0, b1);
+                prims += b1 - b0;
+            } else {
+                internal++;
+            }
+        }
+        node.child_base = internal ? (uint32_t)atomicAdd(&counters[0], internal) : 0u;
+        node.prim_base = prims ? (uint32_t)atomicAdd(&counters[1], prims) : 0u;
+        uint32_t nextChild = node.child_base, primOffset = 0;
+        for (int sl = 0; sl < 8; sl++) {
+            int c = childAt[sl];
+            if (c < 0)
+                continue;
+            const Box cbx = t.box[c];
+            for (int k = 0; k < 3; k++) {
+                double ql = floor(((double)cbx.lo[k] - pp[k]) / scale[k]) - 1.0;
+                double qh = ceil(((double)cbx.hi[k] - pp[k]) / scale[k]) + 1.0;
+                int qlo = (int)fmax(0.0, fmin(255.0, ql));
+                int qhi = (int)fmax(0.0, fmin(255.0, qh));
+                const float fp = (float)pp[k], fs = (float)scale[k];
+                while (qlo > 0 && __fadd_rn(fp, __fmul_rn((float)qlo, fs)) > cbx.lo[k])
+                    qlo--;
+                while (qhi < 255 && __fadd_rn(fp, __fmul_rn((float)qhi, fs)) < cbx.hi[k])
+                    qhi++;
+                node.qlo[k][sl] = (uint8_t)qlo;
+                node.qhi[k][sl] = (uint8_t)qhi;
+            }
+            if (IsLeafB(t, c)) {
+                int b0, b1;
+                RangeB(t, c, b0, b1);
+                node.meta[sl] = (uint8_t)(((b1 - b0) << 5) | primOffset);
+                for (int i = b0; i < b1; i++)
+                    primOrder[node.prim_base + primOffset + (i - b0)] = (uint32_t)t.keys[i];
+                primOffset += (uint32_t)(b1 - b0);
+            } else {
+                node.imask |= (uint8_t)(1u << sl);
+                node.meta[sl] = 0x80;
+                int o = atomicAdd(&counters[2], 1);
+                next[o] = make_int2(c, (int)nextChild++);
+            }
+        }
+        nodes[windex] = node;
+    }
+}
+
+void Require(bool ok, const char* msg) {
+    if (!ok)
+        throw Failure{PG_ERR_DEVICE_LIMIT, msg};
+}
+
 template <typename T>
 T* DevAlloc(size_t n, cudaStream_t st, std::vector<void*>& owned) {
     void* p = nullptr;
@@ -214,40 +393,42 @@ WideBVH BuildWideBVHGpu(const std::vector<Box>& boxes, void* streamPtr) {
     k_node_boxes<<<grid, block, 0, st>>>(dBoxes, sorted, n, left, right, parent, visits, nodeBox);
     PG_CUDA(cudaGetLastError());
 
-    std::vector<unsigned long long> hKeys(n);
-    std::vector<int> hl(n - 1), hr(n - 1), hf(n - 1), hla(n - 1);
-    std::vector<Box> hBox(nodes);
-    PG_CUDA(cudaMemcpyAsync(hKeys.data(), sorted, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(hl.data(), left, (size_t)(n - 1) * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(hr.data(), right, (size_t)(n - 1) * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(hf.data(), first, (size_t)(n - 1) * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(hla.data(), last, (size_t)(n - 1) * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(hBox.data(), nodeBox, (size_t)nodes * sizeof(Box), cudaMemcpyDeviceToHost, st));
+    // Collapse level by level: the tasks of one level (binary node, wide node index) make
+    // the next level's.  A wide node holds at least two binary nodes' worth of children, so
+    // n wide nodes and n queue entries are enough.
+    BinTree t{n, left, right, first, last, nodeBox, sorted};
+    WideNode* wnodes = DevAlloc<WideNode>(n, st, owned);
+    uint32_t* primOrder = DevAlloc<uint32_t>(n, st, owned);
+    int2* q0 = DevAlloc<int2>(n, st, owned);
+    int2* q1 = DevAlloc<int2>(n, st, owned);
+    int* counters = DevAlloc<int>(3, st, owned);  // wide nodes, primitives, next level
+    const int2 root = make_int2(0, 0);
+    const int init3[3] = {1, 0, 0};
+    PG_CUDA(cudaMemcpyAsync(q0, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaMemcpyAsync(counters, init3, sizeof(init3), cudaMemcpyHostToDevice, st));
+    int ntasks = 1, levels = 0, hc[3] = {1, 0, 0};
+    while (ntasks > 0) {
+        Require(levels < 64, "BVH collapse deeper than 64 levels");
+        k_collapse<<<std::min((ntasks + 127) / 128, 148 * 16), 128, 0, st>>>(t, q0, ntasks, q1,
+                                                                            counters, wnodes, primOrder);
+        PG_CUDA(cudaGetLastError());
+        PG_CUDA(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        PG_CUDA(cudaStreamSynchronize(st));
+        ntasks = hc[2];
+        Require(hc[0] <= n && hc[1] <= n && ntasks <= n, "BVH collapse overflowed its buffers");
+        PG_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(int), st));
+        std::swap(q0, q1);
+        levels++;
+    }
+    WideBVH out;
+    out.nodes.resize(hc[0]);
+    out.prim_order.resize(hc[1]);
+    PG_CUDA(cudaMemcpyAsync(out.nodes.data(), wnodes, (size_t)hc[0] * sizeof(WideNode),
+                            cudaMemcpyDeviceToHost, st));
+    PG_CUDA(cudaMemcpyAsync(out.prim_order.data(), primOrder, (size_t)hc[1] * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, st));
     PG_CUDA(cudaStreamSynchronize(st));
-
-    // Host tree for the collapse: subtrees of at most 3 primitives become leaves over
-    // their contiguous range of the sorted order.
-    std::vector<uint32_t> idx(n);
-    for (int k = 0; k < n; k++)
-        idx[k] = (uint32_t)hKeys[k];
-    std::vector<BNode> bn(nodes);
-    for (int i = 0; i < n - 1; i++) {
-        bn[i].box = hBox[i];
-        if (hla[i] - hf[i] + 1 <= 3) {
-            bn[i].begin = hf[i];
-            bn[i].end = hla[i] + 1;
-        } else {
-            bn[i].left = hl[i];
-            bn[i].right = hr[i];
-        }
-    }
-    for (int k = 0; k < n; k++) {
-        BNode& leaf = bn[n - 1 + k];
-        leaf.box = hBox[n - 1 + k];
-        leaf.begin = k;
-        leaf.end = k + 1;
-    }
-    WideBVH out = CollapseToWide(bn, 0, idx);
+    out.max_depth = levels;
     out.binary_nodes = nodes;
     return out;
 }
