@@ -66,6 +66,13 @@ def parse_args():
                                                       os.path.join(tempfile.gettempdir(),
                                                                    "pine_b200_scenes")))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sampler", choices=["Uniform", "Halton"], default="Uniform",
+                    help="the scene file's sampler (both arms render the same file)")
+    ap.add_argument("--filter", choices=["Box", "Triangle", "Gaussian", "Mitchell",
+                                         "LanczosSinc"], default="Box",
+                    help="the scene file's film filter (radius 0.5)")
+    ap.add_argument("--bvh", choices=["host", "gpu"], default="host",
+                    help="BVH builder for the scene upload")
     ap.add_argument("--profile-case", action="store_true",
                     help="render the small ncu case once and print its per-kernel counters")
     ap.add_argument("--guided", action="store_true",
@@ -88,15 +95,20 @@ def parse_args():
 
 
 # ---------------------------------------------------------------- scenes
+SCENE_OPTS = {"sampler": "Uniform", "filter": "Box"}
+
+
 def scene_path(cfg, cache, env, spp=None, size=None):
     from pine_b200 import lib, scenegen
     os.makedirs(cache, exist_ok=True)
     w, h = size or (cfg["width"], cfg["height"])
     spp = cfg["spp"] if spp is None else spp
     kind = cfg["kind"]
-    # Every workload uses the Uniform sampler (the library's independent stream, no Halton
-    # draws) and a box filter of radius 0.5; the reference arm renders the same file.
-    name = f"{kind}_{env}_{w}x{h}_{spp}_uniform.txt"
+    # By default every workload uses the Uniform sampler (the library's independent stream,
+    # no Halton draws) and a box filter of radius 0.5; the reference arm renders the same
+    # file.
+    smp, flt = SCENE_OPTS["sampler"], SCENE_OPTS["filter"]
+    name = f"{kind}_{env}_{w}x{h}_{spp}_{smp.lower()}_{flt.lower()}.txt"
     path = os.path.join(cache, name)
     if kind == "volume":
         scenegen.volume_scene(path, lib(), n=cfg["n"], width=w, height=h, spp=spp,
@@ -105,10 +117,16 @@ def scene_path(cfg, cache, env, spp=None, size=None):
     elif kind == "spheres":
         scenegen.spheres_scene(path, width=w, height=h, spp=spp, max_depth=cfg["max_depth"],
                                env=env, env_radiance=0.2 if env == "constant" else 0.5,
-                               sampler="Uniform")
+                               sampler=smp)
     else:
         scenegen.mesh_scene(path, lib(), subdiv=cfg["subdiv"], width=w, height=h, spp=spp,
-                            max_depth=cfg["max_depth"], env="none", sampler="Uniform")
+                            max_depth=cfg["max_depth"], env="none", sampler=smp)
+    if flt != "Box":
+        with open(path) as f:
+            text = f.read()
+        assert "filter: Box{" in text
+        with open(path, "w") as f:
+            f.write(text.replace("filter: Box{", "filter: " + flt + "{"))
     return path
 
 
@@ -286,6 +304,7 @@ def reference_arm(args, cfg, rank):
 # ---------------------------------------------------------------- our arm
 def main():
     args = parse_args()
+    SCENE_OPTS["sampler"], SCENE_OPTS["filter"] = args.sampler, args.filter
     cfg = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -341,8 +360,10 @@ def main():
         path = scene_path(cfg, args.cache, env)
 
     ctx = pb.Context(local)
+    ctx.set_bvh_builder(args.bvh)
     sid = ctx.load_scene(path)
     info = ctx.scene_info(sid)
+    bvh = ctx.bvh_info(sid)
     paths_per_step = info["width"] * info["height"] * cfg["spp"]
     seed0 = 1000 * rank
 
@@ -427,6 +448,8 @@ def main():
         "config": {"workload": f"{args.workload}: " + describe(cfg), "width": info["width"],
                    "height": info["height"], "spp": cfg["spp"], "max_depth": cfg["max_depth"],
                    "math_mode": args.math, "parallelism": f"replicas x{world}",
+                   "sampler": args.sampler, "filter": args.filter,
+                   "bvh": dict(builder=args.bvh, **bvh),
                    "l2": "inputs larger than L2 (512 MiB density grid vs 126 MB L2)"
                          if cfg["kind"] == "volume" else "scene resident; no flush"},
         "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
