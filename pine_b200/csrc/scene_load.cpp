@@ -18,6 +18,7 @@
 #include "scene_load.h"
 
 #include <algorithm>
+#include <iterator>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -404,7 +405,112 @@ void LoadObj(const std::string& path, std::vector<float>& verts, std::vector<uin
 }
 
 // fileio.cpp:194-202: int32 sx, sy, sz then sx*sy*sz floats, x fastest.
+// Huffman-compressed 16-bit volume (the format of pine's CompressVolume /
+// LoadCompressedVolume, fileio.cpp:204-249, and HuffmanEncode/HuffmanDecode,
+// util/huffman.h:87-190; pine itself ships the reader commented out).  Layout:
+//   int32 size[3]; uint64 treeBytes, encodedBytes;
+//   tree: the raw bytes of the writer's hash map object (56 bytes; its element count at
+//         byte 24), then per entry a uint16 value and its uint32 code;
+//   encoded: the raw bytes of the writer's byte vector (24 bytes: begin, end, capacity
+//         pointers; its length is end - begin), the bytes, uint32 bit count, uint64 count.
+// A code is its bits under a leading 1 (the tree path); the stream holds each code's bits
+// below that 1, least significant first, packed from bit 0 of each byte.  A voxel is its
+// 16-bit value / 2047 (the writer clamped densities to 32 and scaled by 65535 / 32 in int).
+void LoadCompressedVolume(const std::string& path, std::vector<float>& density, int size[3]) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw SceneError(PG_ERR_IO, "cannot open volume \"" + path + "\"");
+    std::vector<char> all((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    auto fail = [&](const char* what) {
+        throw SceneError(PG_ERR_PARSE, std::string("compressed volume \"") + path + "\": " + what);
+    };
+    size_t pos = 0;
+    auto take = [&](void* dst, size_t n) {
+        if (pos + n > all.size())
+            fail("truncated");
+        std::memcpy(dst, all.data() + pos, n);
+        pos += n;
+    };
+    int32_t hdr[3];
+    uint64_t treeBytes, encBytes;
+    take(hdr, 12);
+    take(&treeBytes, 8);
+    take(&encBytes, 8);
+    if (hdr[0] <= 0 || hdr[1] <= 0 || hdr[2] <= 0 || (int64_t)hdr[0] * hdr[1] * hdr[2] > (1ll << 33))
+        fail("bad size");
+    if (treeBytes < 56 || (treeBytes - 56) % 6 != 0 || pos + treeBytes + encBytes != all.size())
+        fail("section sizes do not add up");
+    const size_t treeStart = pos;
+    uint64_t entries;
+    std::memcpy(&entries, all.data() + treeStart + 24, 8);
+    if (entries != (treeBytes - 56) / 6 || entries == 0)
+        fail("code table size");
+    pos = treeStart + 56;
+    std::vector<uint16_t> values(entries);
+    std::vector<uint32_t> codes(entries);
+    for (uint64_t i = 0; i < entries; i++) {
+        take(&values[i], 2);
+        take(&codes[i], 4);
+        if (codes[i] == 0)
+            fail("empty code");
+    }
+    uint64_t vb[3];
+    take(vb, 24);
+    const uint64_t nbytes = vb[1] - vb[0];
+    if (vb[1] < vb[0] || 24 + nbytes + 12 != encBytes)
+        fail("encoded section size");
+    const unsigned char* bits = reinterpret_cast<const unsigned char*>(all.data() + pos);
+    pos += nbytes;
+    uint32_t nbits;
+    uint64_t count;
+    take(&nbits, 4);
+    take(&count, 8);
+    if (count != (uint64_t)hdr[0] * hdr[1] * hdr[2] || nbits > nbytes * 8)
+        fail("element or bit count");
+    density.resize(count);
+    if (entries == 1) {  // a single value needs no bits (huffman.h:129-134)
+        std::fill(density.begin(), density.end(), values[0] / 2047.0f);
+    } else {
+        // Decoding trie over the codes' bits, least significant first: node 0 is the root,
+        // node k's children are 2k + 1 (bit 0) and 2k + 2 (bit 1); leaf[k] = 1 + value index.
+        std::vector<uint32_t> leaf(2);
+        for (uint64_t i = 0; i < entries; i++) {
+            uint32_t c = codes[i];
+            int h = 31 - __builtin_clz(c);
+            if (h == 0)
+                fail("code without bits");
+            size_t node = 0;
+            for (int b = 0; b < h; b++) {
+                node = node * 2 + ((c >> b) & 1 ? 2 : 1);
+                if (node >= (size_t)1 << 26)
+                    fail("code too long");
+            }
+            if (node >= leaf.size())
+                leaf.resize(std::max(node + 1, leaf.size() * 2));
+            leaf[node] = (uint32_t)i + 1;
+        }
+        size_t node = 0, out = 0;
+        for (uint32_t b = 0; b < nbits; b++) {
+            node = node * 2 + (((bits[b >> 3] >> (b & 7)) & 1) ? 2 : 1);
+            if (node >= leaf.size())
+                fail("bit stream leaves the code table");
+            if (uint32_t v = leaf[node]) {
+                if (out == count)
+                    fail("more voxels than the header holds");
+                density[out++] = values[v - 1] / 2047.0f;
+                node = 0;
+            }
+        }
+        if (out != count || node != 0)
+            fail("bit stream ends inside the volume");
+    }
+    size[0] = hdr[0], size[1] = hdr[1], size[2] = hdr[2];
+}
+
 void LoadVolume(const std::string& path, std::vector<float>& density, int size[3]) {
+    const std::string ext = ".compressed";
+    if (path.size() > ext.size() && path.compare(path.size() - ext.size(), ext.size(), ext) == 0)
+        return LoadCompressedVolume(path, density, size);
     std::ifstream f(path, std::ios::binary);
     if (!f)
         throw SceneError(PG_ERR_IO, "cannot open volume \"" + path + "\"");

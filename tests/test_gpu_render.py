@@ -10,6 +10,7 @@ noise and 3-D noise textures, a noise bump map, a two-layer plastic) at 128 x 36
 spp, rendered by pine with its Halton sampler."""
 
 import json
+import os
 
 import numpy as np
 import pytest
@@ -145,3 +146,26 @@ def test_full_size_spheres_counts(ctx, tmp_path):
     assert abs(int(r["count"].sum()) - 640 * 360 * 8) < 640 * 360 * 8 * 1e-3
     assert r["stats"]["paths"] == 640 * 360 * 8
     ctx.release_scene(sid)
+
+
+def test_compressed_volume_renders_like_its_float_grid(ctx, tmp_path):
+    """A `.compressed` grid and the float grid it decodes to give the same image."""
+    import struct
+    from test_compressed_volume import _scene, write_compressed
+    rng = np.random.default_rng(8)
+    size = (24, 16, 20)
+    dens = np.where(rng.uniform(size=size[::-1]) < 0.5, 0.0,
+                    rng.gamma(2.0, 2.0, size[::-1])).astype(np.float32)
+    grid = write_compressed(tmp_path / "v.compressed", dens, size)
+    with open(tmp_path / "v.vol", "wb") as f:
+        f.write(struct.pack("<3i", *size) + grid.astype(np.float32).tobytes())
+    images = []
+    for name in ("v.compressed", "v.vol"):
+        d = tmp_path / name.replace(".", "_")
+        d.mkdir()
+        os.symlink(tmp_path / name, d / name)
+        sid = ctx.load_scene(_scene(d, name))
+        images.append(ctx.render(sid, spp=64, seed=3, math_mode="fast")["mean"])
+        ctx.release_scene(sid)
+    assert np.abs(images[0]).sum() > 0
+    np.testing.assert_allclose(images[0], images[1], rtol=1e-5, atol=1e-7)
