@@ -44,6 +44,7 @@ static void Require(bool ok, const std::string& msg, pg_status s = PG_ERR_INVALI
 // ---------------------------------------------------------------- device memory
 struct DevMem {
     std::vector<void*> ptrs;
+    std::vector<size_t> sizes;  // bytes of each allocation
     // With a stream, allocations are stream-ordered (cudaMallocAsync from the device's
     // pool, which keeps freed memory for reuse): only work on that stream may touch them.
     cudaStream_t stream = nullptr;
@@ -58,6 +59,7 @@ struct DevMem {
         else
             PG_CUDA(cudaMalloc(&p, n * sizeof(T)));
         ptrs.push_back(p);
+        sizes.push_back(n * sizeof(T));
         return (T*)p;
     }
     template <typename T>
@@ -71,9 +73,20 @@ struct DevMem {
         for (void* p : ptrs)
             async ? cudaFreeAsync(p, stream) : cudaFree(p);
         ptrs.clear();
+        sizes.clear();
     }
     ~DevMem() { Free(); }
 };
+
+static void ZeroAll(DevMem& mem) {
+    for (size_t i = 0; i < mem.ptrs.size(); i++)
+        PG_CUDA(mem.async ? cudaMemsetAsync(mem.ptrs[i], 0, mem.sizes[i], mem.stream)
+                          : cudaMemset(mem.ptrs[i], 0, mem.sizes[i]));
+    // Plain allocations are zeroed on the legacy stream, which the context's non-blocking
+    // stream does not wait for: finish before any kernel uses them.
+    if (!mem.async)
+        PG_CUDA(cudaDeviceSynchronize());
+}
 
 // Majorant brick edges a grid medium is prepared for (selected by pg_tuning).
 constexpr int kBrickSizes[4] = {8, 16, 32, 64};
@@ -138,6 +151,9 @@ constexpr int kRecordCap = 1 << 20;     // training records per pass
 constexpr int kTrainBatch = 1 << 18;    // records per Adam step
 constexpr float kGuideLr = 1e-2f;
 
+// Zeroes every allocation of mem (on its stream when it is stream-ordered).
+static void ZeroAll(DevMem& mem);
+
 struct GuidePool {
     DevMem mem;
     int slots = 0;
@@ -156,6 +172,8 @@ struct GuidePool {
         rec_last = mem.Alloc<int>(n);
         rec = mem.Alloc<float4>((size_t)kRecordStride * kRecordCap);
         rec_dirw = mem.Alloc<float4>(kRecordCap);
+        // Start from zeros, not from whatever the device's memory held before.
+        ZeroAll(mem);
     }
 };
 
@@ -1917,6 +1935,7 @@ static void GuideInit(pg_ctx* ctx, uint64_t seed) {
 static GuideNetDev& EnsureGuide(pg_ctx* ctx) {
     if (!ctx->guide.w16) {
         void* mem = ctx->guide_mem.Alloc<uint8_t>(GuideNetBytes(ctx->num_sms));
+        ZeroAll(ctx->guide_mem);
         GuideNetBind(ctx->guide, mem, ctx->num_sms);
         GuideInit(ctx, 0);
     }
