@@ -74,20 +74,30 @@ PG_HD int64_t PstdMod(int64_t a, int64_t b) {
     return r < 0 ? r + b : r;
 }
 
-// HaltonSampler::StartPixel(p, 0) (sampler.cpp:62-75): the index of the pixel's first
-// sample; sample s of the pixel is this + s * stride.
-PG_HD uint64_t HaltonPixelIndex(const HaltonDev& h, int px, int py) {
-    int64_t index = 0;
-    if (h.stride > 1) {
-        int pm[2] = {(int)PstdMod(px, kHaltonMaxRes), (int)PstdMod(py, kHaltonMaxRes)};
-        for (int i = 0; i < 2; i++) {
-            uint64_t off = InverseRadicalInverse((uint64_t)pm[i], i == 0 ? 2 : 3, h.exps[i]);
-            index += (int64_t)(off * (uint64_t)(int64_t)h.scale[1 - i] *
-                               (uint64_t)(int64_t)h.inv[1 - i]);
-        }
-        index %= (int64_t)h.stride;
+// InverseRadicalInverse of a value below 128 in base 2 or 3 (at most 7 or 5 digits).
+template <uint32_t B>
+PG_HD uint32_t InverseRadicalInverseSmall(uint32_t inverse, int nDigits) {
+    uint32_t index = 0;
+    for (int i = 0; i < nDigits; i++) {
+        uint32_t digit = inverse % B;
+        inverse /= B;
+        index = index * B + digit;
     }
-    return (uint64_t)index;
+    return index;
+}
+
+// HaltonSampler::StartPixel(p, 0) (sampler.cpp:62-75): the index of the pixel's first
+// sample; sample s of the pixel is this + s * stride.  pine sums in 64 bits; every term
+// here is below 128 * 243 * 243 < 2^23, so 32-bit arithmetic gives the same index.
+PG_HD uint64_t HaltonPixelIndex(const HaltonDev& h, int px, int py) {
+    if (h.stride <= 1)
+        return 0;
+    const uint32_t mx = (uint32_t)PstdMod(px, kHaltonMaxRes), my = (uint32_t)PstdMod(py, kHaltonMaxRes);
+    uint32_t index = InverseRadicalInverseSmall<2>(mx, h.exps[0]) * (uint32_t)h.scale[1] *
+                     (uint32_t)h.inv[1];
+    index += InverseRadicalInverseSmall<3>(my, h.exps[1]) * (uint32_t)h.scale[0] *
+             (uint32_t)h.inv[0];
+    return index % h.stride;
 }
 
 PG_HD float RnMul(float a, float b) {
