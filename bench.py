@@ -12,9 +12,12 @@ Arms:
   scene resident in HBM; ``e2e`` is wall time through the public C ABI with host buffers:
   each step uploads the scene from pinned host memory (pg_upload_scene), renders and reads
   the film back (mean, variance, count) into pinned host memory.
-* ``--impl reference``: pine's own CPU integrator (the reference compiled from source into
-  oracle/_ref) on the same scene, with pine's Sky standing in for the constant sky, which
-  pine cannot express; all host threads, one bounded sample of the image per step.
+* ``--impl reference``: pine's own CPU integrator (the reference compiled from its sources
+  into oracle/_ref) on the same scene file.  Scenes with the constant sky render with
+  oracle/_ref/pine_ref_const, pine plus a `Constant{ color }` environment light
+  (oracle/constant_env.py), since pine's own environment set cannot express it; all host
+  threads, one bounded sample of the image per step.  This arm loads no part of this
+  repository's renderer (the scene inputs come from the separate pine-scenegen tool).
 
 Multi-GPU (``torchrun --nproc-per-node N bench.py --gpus N``): independent replicas, each
 rank renders the full workload with its own seed (weak scaling); times are the max over
@@ -27,6 +30,7 @@ import argparse
 import csv
 import io
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -42,7 +46,8 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "pine_ref")
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "volume_traffic.md")
+REF_BIN_CONST = os.path.join(ROOT, "oracle", "_ref", "pine_ref_const")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "volume_traffic.json")
 FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
@@ -50,8 +55,13 @@ WORKLOADS = {
     "spheres": dict(kind="spheres", width=640, height=360, spp=64, max_depth=8),
     "mesh": dict(kind="mesh", width=1920, height=1080, spp=256, max_depth=16, subdiv=8),
 }
-# ncu case: the same 512^3 grid (larger than L2) with one sample per pixel.
-PROFILE_CASE = dict(kind="volume", width=1280, height=720, spp=1, max_depth=128, n=512)
+# ncu cases (--profile-case): each workload's scene with one sample per pixel (the 512^3
+# grid and the 1.31M-triangle mesh are larger than L2 either way).
+PROFILE_CASES = {
+    "volume": dict(WORKLOADS["volume"], spp=1),
+    "spheres": dict(WORKLOADS["spheres"], spp=1),
+    "mesh": dict(WORKLOADS["mesh"], width=480, height=270, spp=1),
+}
 
 
 def parse_args():
@@ -99,7 +109,7 @@ SCENE_OPTS = {"sampler": "Uniform", "filter": "Box"}
 
 
 def scene_path(cfg, cache, env, spp=None, size=None):
-    from pine_b200 import lib, scenegen
+    from pine_b200 import scenegen
     os.makedirs(cache, exist_ok=True)
     w, h = size or (cfg["width"], cfg["height"])
     spp = cfg["spp"] if spp is None else spp
@@ -111,7 +121,7 @@ def scene_path(cfg, cache, env, spp=None, size=None):
     name = f"{kind}_{env}_{w}x{h}_{spp}_{smp.lower()}_{flt.lower()}.txt"
     path = os.path.join(cache, name)
     if kind == "volume":
-        scenegen.volume_scene(path, lib(), n=cfg["n"], width=w, height=h, spp=spp,
+        scenegen.volume_scene(path, n=cfg["n"], width=w, height=h, spp=spp,
                               max_depth=cfg["max_depth"], env=env,
                               env_radiance=0.3 if env == "constant" else 1.0)
     elif kind == "spheres":
@@ -119,7 +129,7 @@ def scene_path(cfg, cache, env, spp=None, size=None):
                                env=env, env_radiance=0.2 if env == "constant" else 0.5,
                                sampler=smp)
     else:
-        scenegen.mesh_scene(path, lib(), subdiv=cfg["subdiv"], width=w, height=h, spp=spp,
+        scenegen.mesh_scene(path, subdiv=cfg["subdiv"], width=w, height=h, spp=spp,
                             max_depth=cfg["max_depth"], env="none", sampler=smp)
     if flt != "Box":
         with open(path) as f:
@@ -190,49 +200,75 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-# Algorithmic bytes: per path iteration of k_shade 128 B of path state (64 B read, 64 B
-# written); per shadow ray of k_shadow 64 B (48 B ray read, 16 B radiance update); per
-# volume tracking step 32 B (the 8 voxels of a trilinear lookup); 4 B per majorant brick.
-STATE_BYTES = {"shade": 128, "shadow": 64, "trace": 48, "regen": 16}
+# Algorithmic bytes (a fixed model):
+# * a traced ray (k_trace, and shadow rays through a BVH): B_ray = 32 B ray read + 16 B hit
+#   write + 80 B per level of the 8-wide BVH (one compressed node, ceil(log8 N) levels for
+#   N primitives) + one leaf primitive (48 B triangle, 16 B sphere);
+# * a path iteration of k_shade: 128 B of path state (64 B read, 64 B written);
+# * a shadow ray of k_shadow without a BVH (volume-only scenes): 64 B (48 B ray read, 16 B
+#   radiance update);
+# * a ray walked by k_track (delta tracking of an extension ray): 32 B ray read + 16 B result
+#   written; by k_transmit (ratio tracking of a shadow ray): 48 B ray read + 16 B
+#   contribution read and written;
+# * per volume tracking step 32 B (the 8 voxels of a trilinear lookup), 4 B per majorant
+#   brick entered.
+STATE_BYTES = {"shade": 128, "shadow": 64, "regen": 16, "track": 48, "transmit": 80}
 
 
-def algorithmic_bytes(name, k):
-    return STATE_BYTES[name] * k["items"] + 32 * k["volume_steps"] + 4 * k["bricks"]
+def ray_bytes(prims, triangles):
+    """B_ray for a scene of `prims` BVH primitives (0: no BVH)."""
+    if prims <= 0:
+        return 0
+    levels = max(1, math.ceil(math.log(prims, 8) - 1e-12))
+    return 32 + 16 + 80 * levels + (48 if triangles else 16)
+
+
+def algorithmic_bytes(name, k, b_ray):
+    if name == "trace":
+        per_item = b_ray
+    elif name == "shadow" and b_ray:
+        per_item = b_ray
+    else:
+        per_item = STATE_BYTES[name]
+    return per_item * k["items"] + 32 * k["volume_steps"] + 4 * k["bricks"]
 
 
 def read_traffic():
-    """DRAM bytes per algorithmic byte of each kernel, from the committed ncu summary."""
-    out = {}
+    """DRAM bytes per algorithmic byte of each kernel, measured by ncu on the small case and
+    committed beside its summary (profiles/volume_traffic.json)."""
     try:
-        for line in open(TRAFFIC_FILE):
-            if line.startswith("dram_bytes_per_algorithmic_byte"):
-                _, rest = line.split(":", 1)
-                for kv in rest.split():
-                    k, v = kv.split("=")
-                    out[k] = float(v)
-    except OSError:
-        pass
-    return out
+        with open(TRAFFIC_FILE) as f:
+            return {k: float(v) for k, v in json.load(f)["dram_bytes_per_algorithmic_byte"].items()}
+    except (OSError, KeyError, ValueError):
+        return {}
 
 
-def roofline(kernels, peak, peak_kind):
+def roofline(kernels, peak, peak_kind, b_ray, workload):
     timed = {n: k for n, k in kernels.items() if k["seconds"] > 0 and k["launches"] > 0}
     if not timed:
         return None
     name = max(timed, key=lambda n: timed[n]["seconds"])
     k = timed[name]
-    per_launch_bytes = algorithmic_bytes(name, k) / k["launches"]
+    per_launch_bytes = algorithmic_bytes(name, k, b_ray) / k["launches"]
     launch_s = k["seconds"] / k["launches"]
     achieved = per_launch_bytes / launch_s / 1e9
-    traffic = None
-    tr = read_traffic()
+    traffic, traffic_note = None, None
+    tr = read_traffic() if workload == "volume" else {}
     if name in tr:
         traffic = tr[name] * per_launch_bytes
-    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-            "kernel": "k_" + name, "algorithmic_bytes_per_launch": per_launch_bytes,
-            "avg_launch_ms": launch_s * 1e3, "launches": k["launches"],
-            "share_of_device_time": k["seconds"] / sum(v["seconds"] for v in timed.values())}
+        traffic_note = ("scaled from the 1-spp case: ncu DRAM bytes per algorithmic byte of the "
+                        "kernel (profiles/volume_traffic.json) x this run's algorithmic bytes "
+                        "per launch")
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+           "kernel": "k_" + name, "algorithmic_bytes_per_launch": per_launch_bytes,
+           "avg_launch_ms": launch_s * 1e3, "launches": k["launches"],
+           "share_of_device_time": k["seconds"] / sum(v["seconds"] for v in timed.values())}
+    if b_ray:
+        out["bytes_per_traced_ray"] = b_ray
+    if traffic_note:
+        out["traffic_note"] = traffic_note
+    return out
 
 
 def add_kernels(acc, k):
@@ -243,60 +279,82 @@ def add_kernels(acc, k):
 
 
 # ---------------------------------------------------------------- CPU baseline (pine)
-def run_pine(scene, repeats, spp):
-    p = subprocess.run([REF_BIN, "time", scene, str(repeats), str(spp)], capture_output=True,
+def scene_env(cfg):
+    """The environment of a workload's scene: the constant sky, or none for the mesh."""
+    return "none" if cfg["kind"] == "mesh" else "constant"
+
+
+def ref_binary(env):
+    """pine built from its sources; scenes with the constant sky need the build that adds
+    pine's missing `Constant` environment (oracle/constant_env.py)."""
+    return REF_BIN_CONST if env == "constant" else REF_BIN
+
+
+def run_pine(binary, scene, repeats, spp):
+    p = subprocess.run([binary, "time", scene, str(repeats), str(spp)], capture_output=True,
                        text=True, cwd=os.path.dirname(scene))
     lines = [json.loads(l) for l in p.stdout.splitlines() if l.startswith("{")]
     if p.returncode != 0 or not lines:
-        raise RuntimeError(f"pine_ref failed ({p.returncode}): {p.stderr[-500:]}")
+        raise RuntimeError(f"{os.path.basename(binary)} failed ({p.returncode}): "
+                           f"{p.stderr[-500:]}")
     return lines
 
 
 def cpu_baseline(cfg, cache):
-    """pine's Path integrator on the host cores: a 1-spp calibration run sizes a sample of
-    about 10 s, which is then timed (scene loading and BVH build excluded)."""
-    if not os.path.exists(REF_BIN):
+    """pine's Path integrator on the host cores, on the scene file our arm renders: a 1-spp
+    calibration run sizes a sample of about 10 s, which is then timed (scene loading and
+    BVH build excluded)."""
+    env = scene_env(cfg)
+    binary = ref_binary(env)
+    if not os.path.exists(binary):
         return None
-    scene = scene_path(cfg, cache, "sky", spp=1)
-    cal = run_pine(scene, 1, 1)[0]
+    scene = scene_path(cfg, cache, env)
+    runs = run_pine(binary, scene, 2, 1)
+    cal = runs[-1]
     spp = int(max(1, min(cfg["spp"], 10.0 / max(cal["seconds"], 1e-3))))
-    run = run_pine(scene, 1, spp)[0]
+    run = run_pine(binary, scene, 1, spp)[0]
     return {"value": run["mpaths_per_s"], "unit": "Mpaths/s", "cores": run["threads"],
             "kind": "reference",
-            "sample": f"{cfg['width']}x{cfg['height']} at {spp} spp of the same scene with "
-                      f"pine's Sky in place of the constant sky ({run['paths']:.0f} paths, "
-                      f"{run['seconds']:.2f} s)"}
+            "sample": f"{cfg['width']}x{cfg['height']} at {spp} of the file's {cfg['spp']} spp "
+                      f"({run['paths']:.0f} paths, {run['seconds']:.2f} s), the same scene file "
+                      f"({os.path.basename(binary)})"}
 
 
 def reference_arm(args, cfg, rank):
     if rank != 0:
         return 0
+    env = scene_env(cfg)
+    binary = ref_binary(env)
     line = {"metric": "Mpaths/s", "unit": "Mpaths/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: pine Path integrator (CPU), scene as "
-                                   "ours with Sky for the constant sky"}}
-    if not os.path.exists(REF_BIN):
-        line["unavailable"] = "oracle/_ref/pine_ref is not built (needs the pine sources)"
+            "config": {"workload": f"{args.workload}: " + describe(cfg) + "; pine's Path "
+                                   "integrator on the host cores, the same scene file",
+                       "binary": os.path.relpath(binary, ROOT)}}
+    if not os.path.exists(binary):
+        line["unavailable"] = (f"{os.path.relpath(binary, ROOT)} is not built (it needs the "
+                               "pine sources at build time)")
         print(json.dumps(line))
         return 0
-    scene = scene_path(cfg, args.cache, "sky", spp=1)
-    cal = run_pine(scene, 1, 1)[0]
+    scene = scene_path(cfg, args.cache, env)
+    cal = run_pine(binary, scene, 2, 1)[-1]
     # Steps sized so that warmup + steps finish in about two minutes.
     per_step = 120.0 / max(1, args.steps + args.warmup)
     spp = int(max(1, min(cfg["spp"], per_step / max(cal["seconds"], 1e-3))))
-    runs = run_pine(scene, args.warmup + args.steps, spp)[args.warmup:]
+    runs = run_pine(binary, scene, args.warmup + args.steps, spp)[args.warmup:]
     secs = sum(r["seconds"] for r in runs)
     paths = sum(r["paths"] for r in runs)
     value = paths / secs / 1e6
     line.update({"value": value, "ms_per_step": secs / len(runs) * 1e3,
                  "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": runs[0]["threads"],
                                   "kind": "reference",
-                                  "sample": f"{cfg['width']}x{cfg['height']} at {spp} spp per step"},
+                                  "sample": f"{cfg['width']}x{cfg['height']} at {spp} of the "
+                                            f"file's {cfg['spp']} spp per step"},
                  "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                          "d2h_bytes_per_step": 0}})
-    line["config"].update({"width": cfg["width"], "height": cfg["height"], "spp_per_step": spp,
-                           "max_depth": cfg["max_depth"]})
+    line["config"].update({"width": cfg["width"], "height": cfg["height"], "spp": cfg["spp"],
+                           "spp_per_step": spp, "max_depth": cfg["max_depth"],
+                           "scene_file": os.path.basename(scene)})
     print(json.dumps(line))
     return 0
 
@@ -330,7 +388,7 @@ def main():
     def max_over_ranks(x):
         return reduce_max(x, dist, f"cuda:{local}")
 
-    env = "constant" if cfg["kind"] != "mesh" else "none"
+    env = scene_env(cfg)
     if args.guiding_eval:
         if rank == 0:
             print(json.dumps(guiding_eval(args, cfg, env)))
@@ -340,14 +398,15 @@ def main():
             print(json.dumps(batch_eval(args)))
         return 0
     if args.profile_case:
-        path = scene_path(PROFILE_CASE, args.cache, "constant")
+        case = PROFILE_CASES[args.workload]
+        path = scene_path(case, args.cache, env)
         ctx = pb.Context(local)
         sid = ctx.load_scene(path)
         if args.guided:
             ctx.guide_reset(seed=0)
         r = ctx.render(sid, seed=1, math_mode=args.math, outputs=False, guiding=args.guided,
                        profile=args.guided)
-        print(json.dumps({"profile_case": PROFILE_CASE, "guided": args.guided,
+        print(json.dumps({"profile_case": case, "guided": args.guided,
                           "stats": r["stats"]}))
         ctx.close()
         return 0
@@ -434,6 +493,12 @@ def main():
         phases["release"] += td - tc
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
+    # BVH primitives for the traced-ray bytes: triangles plus the analytic shapes (planes are
+    # tested outside the BVH).
+    shapes = [desc.shapes[i].type for i in range(desc.num_shapes)]
+    prims = int(desc.num_triangles) + sum(t in (pb.SHAPE_SPHERE, pb.SHAPE_RECT,
+                                                pb.SHAPE_TRIANGLE) for t in shapes)
+    b_ray = ray_bytes(prims, desc.num_triangles > 0) if bvh["nodes"] > 0 else 0
     parsed.close()
 
     value = aggregate(paths_per_step, args.steps, world, device_s_max)
@@ -460,7 +525,7 @@ def main():
         "mrays_per_s": stats_acc["rays"] * world / device_s_max / 1e6,
         "gsteps_per_s": stats_acc["volume_steps"] * world / device_s_max / 1e9,
         "dropped_samples": stats_acc["dropped"],
-        "roofline": roofline(kernels, peak, peak_kind),
+        "roofline": roofline(kernels, peak, peak_kind, b_ray, args.workload),
         "kernels": {n: {"launches": k["launches"], "seconds": k["seconds"],
                         "items": k["items"], "volume_steps": k["volume_steps"]}
                     for n, k in kernels.items()},

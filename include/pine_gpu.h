@@ -10,7 +10,7 @@
  *     -> pg_intersect (batched; the per-ray synchronous Accel API cannot amortise a launch)
  *   LoadScene + Create* factories     src/util/fileio.cpp:251-281       -> pg_load_scene_file
  *   Scene (flattened)                 src/core/scene.h:18-27             -> pg_scene_desc
- *   LoadVolume (.vol)                 src/util/fileio.cpp:194-202       -> pg_write_volume
+ *   LoadVolume (.vol)                 src/util/fileio.cpp:194-202       -> pg_load_scene_file
  *
  * Conventions: plain pointers and sizes only.  The caller owns every host buffer; the
  * library copies inputs during the call and fills caller-allocated outputs before it
@@ -254,9 +254,12 @@ typedef struct pg_render_desc {
 
 /* Kernels of the wavefront loop, in pg_render_stats.kernels order.  GUIDE (network
  * inference and guided direction sampling) and TRAIN (gradient and Adam between passes)
- * run only in guided renders. */
+ * run only in guided renders.  TRACK (delta tracking of the extension rays through grid
+ * media) runs in scenes with media; TRANSMIT (ratio tracking of the shadow rays) in scenes
+ * with media and no surfaces, when shadow rays have their own kernel. */
 enum { PG_KERNEL_REGEN = 0, PG_KERNEL_TRACE = 1, PG_KERNEL_SHADE = 2, PG_KERNEL_SHADOW = 3,
-       PG_KERNEL_GUIDE = 4, PG_KERNEL_TRAIN = 5, PG_NUM_KERNELS = 6 };
+       PG_KERNEL_GUIDE = 4, PG_KERNEL_TRAIN = 5, PG_KERNEL_TRACK = 6, PG_KERNEL_TRANSMIT = 7,
+       PG_NUM_KERNELS = 8 };
 
 typedef struct pg_kernel_stats {
     int64_t launches;
@@ -312,7 +315,7 @@ pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_desc* desc, f
  * or a thread that cannot take the device-wide synchronisation cudaMalloc and cudaFree
  * may cause.  No counterpart in the reference (pine renders on the host).
  * Path state and the film accumulators live in one fixed array inside the library,
- * about 27 MiB on every GPU that loads it, held until the process exits: at most 65536
+ * about 20 MiB on every GPU that loads it, held until the process exits: at most 65536
  * path slots and films of at most 524288 pixels (larger films: PG_ERR_INVALID_ARG).
  * mean_device: caller-owned DEVICE memory of width*height*3 floats on the context's
  * GPU; it receives the per-pixel mean as pg_render's out_mean does.  desc->accumulate
@@ -447,17 +450,6 @@ pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scramble, cons
                            int64_t n, float* out);
 pg_status pg_filter_table(int32_t filter, const float* radius, const float* params,
                           float* table);
-
-/* ---- synthetic scene inputs (seeded) ---- */
-/* n^3 fractal-noise cloud, x fastest; ~nonzero_fraction of voxels > 0; max exactly 1. */
-pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fraction, float* density);
-/* Pine's uncompressed volume file: int32 sx, sy, sz then floats (fileio.cpp:194-202). */
-pg_status pg_write_volume(const char* path, int sx, int sy, int sz, const float* density);
-/* Icosphere with 20*4^subdiv triangles, displaced along its normals by 4-octave noise of
- * amplitude*radius, written as OBJ with plain decimals (pine's parser has no exponents). */
-pg_status pg_gen_icosphere_obj(const char* path, int subdiv, float radius, float cx, float cy,
-                               float cz, float amplitude, uint64_t seed,
-                               int64_t* out_triangles);
 
 /* ---- host restatements exposed for tests ---- */
 /* pstd::stof (src/pstd/string.cpp:50-68), bit-exact. */

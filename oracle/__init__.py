@@ -3,7 +3,11 @@
 * ``Restatement`` -- the plain-C restatement of pine's hot path (oracle/pine_oracle.c),
   built into oracle/_build/libpine_oracle.so by oracle/Makefile.
 * ``REF_BIN`` -- pine itself, built from the reference sources into oracle/_ref/pine_ref
-  (present only where the reference sources were available at build time).
+  (present only where the reference sources were available at build time);
+  ``REF_BIN_CONST`` the same with the added `Constant` environment light
+  (oracle/constant_env.py).
+* ``REFERENCE_SRC`` -- where the pine sources are ($PINE_REFERENCE, else the Makefile's
+  default), for the scripts that read them at build time.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
 """
@@ -19,6 +23,24 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libpine_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "pine_ref")
+REF_BIN_CONST = os.path.join(HERE, "_ref", "pine_ref_const")
+
+
+def _reference_src() -> str:
+    """The pine source tree: $PINE_REFERENCE, else the default of oracle/Makefile's REF."""
+    env = os.environ.get("PINE_REFERENCE")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
+# Only present where the pine sources are (the build machine); nothing run on the GPU
+# machine reads it.
+REFERENCE_SRC = _reference_src()
 MATH_NAMES = ["sqrt", "log2", "log", "exp", "cos", "sin", "tan", "acos", "asin", "atan",
               "atan2", "pow"]
 

@@ -1046,12 +1046,6 @@ typedef struct {
     int delta;
 } lsample;
 
-static float env_select(const po_scene* s) {
-    if (s->uniform || s->func_int == 0)
-        return 1.0f / s->nlights;
-    return s->lights[s->env].power / s->nlights;
-}
-
 static void sample_light(const po_scene* s, const olight* l, v3 p, float u0, float u1, lsample* ls) {
     ls->dist = 1.0f;
     ls->pdf = 1.0f;
@@ -1071,10 +1065,11 @@ static void sample_light(const po_scene* s, const olight* l, v3 p, float u0, flo
         ls->Le = sky_color(l->a, l->a, l->c);
         return;
     case PG_LIGHT_CONSTANT_ENV:
-        ls->dist = 1e+10f;
-        ls->wo = uniform_sphere(u0, u1);
-        ls->pdf = 1.0f / (4 * kPi);
-        ls->Le = l->c;
+        /* The constant environment of the oracle's pine build (constant_env.py): like the
+         * gradient part of Sky it is gathered only by escaping paths; next-event estimation
+         * finds a zero-radiance delta sample here and contributes nothing. */
+        ls->dist = 0.0f, ls->delta = 1, ls->wo = V(0.0f, 0.0f, 1.0f);
+        ls->Le = V(0.0f, 0.0f, 0.0f);
         return;
     default: { /* AreaLight -> Shape::Sample (geometry.h:432-442) */
         const oshape* sh = &s->shapes[l->shape];
@@ -1267,13 +1262,9 @@ static v3 Li(const po_scene* s, v3 o, v3 d, int medium, int max_depth, orng* r) 
                 const olight* e = &s->lights[s->env];
                 v3 le;
                 float lp;
-                if (e->type == PG_LIGHT_SKY) {
-                    le = sky_color(d, e->a, e->c);
-                    lp = 0.0f;
-                } else {
-                    le = e->c;
-                    lp = env_select(s) / (4 * kPi);
-                }
+                /* Sky::Pdf and the constant environment's Pdf are 0 (light.cpp:77-79). */
+                le = e->type == PG_LIGHT_SKY ? sky_color(d, e->a, e->c) : e->c;
+                lp = 0.0f;
                 L = add(L, mul(beta, depth == 0 ? le : muls(le, power_heuristic(bsdf_pdf, lp))));
             }
             break;

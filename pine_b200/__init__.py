@@ -39,7 +39,7 @@ class RenderDesc(ctypes.Structure):
                 ("accumulate", ctypes.c_int32), ("profile", ctypes.c_int32)]
 
 
-KERNELS = ["regen", "trace", "shade", "shadow", "guide", "train"]
+KERNELS = ["regen", "trace", "shade", "shadow", "guide", "train", "track", "transmit"]
 
 
 class KernelStats(ctypes.Structure):
@@ -52,7 +52,7 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("seconds", ctypes.c_double), ("paths", ctypes.c_int64),
                 ("rays", ctypes.c_int64), ("volume_steps", ctypes.c_int64),
                 ("dropped", ctypes.c_int64), ("launches", ctypes.c_int64),
-                ("kernels", KernelStats * 6)]
+                ("kernels", KernelStats * len(KERNELS))]
 
     def to_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "kernels"}
@@ -187,11 +187,6 @@ def lib():
                                      ctypes.c_void_p, ctypes.c_void_p]),
         "pg_set_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
         "pg_get_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
-        "pg_gen_cloud_volume": (st, [ctypes.c_int, ctypes.c_uint64, ctypes.c_float, _F]),
-        "pg_write_volume": (st, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]),
-        "pg_gen_icosphere_obj": (st, [ctypes.c_char_p, ctypes.c_int, ctypes.c_float,
-                                      ctypes.c_float, ctypes.c_float, ctypes.c_float,
-                                      ctypes.c_float, ctypes.c_uint64, _P(ctypes.c_int64)]),
         "pg_pstd_stof": (ctypes.c_float, [ctypes.c_char_p, ctypes.c_int64]),
         "pg_parse_scene_file": (st, [ctypes.c_char_p, _P(SceneDesc), _P(ctypes.c_void_p)]),
         "pg_free_parsed_scene": (None, [ctypes.c_void_p]),

@@ -56,14 +56,21 @@ enum StatIndex {
     kStatShadeItems, kStatShadeSteps, kStatShadeBricks,
     kStatShadowItems, kStatShadowSteps, kStatShadowBricks,
     kStatTraceItems, kStatRegenItems, kStatIterations, kStatGuided, kStatRecords,
-    kStatTrainRows, kNumStats = 16
+    kStatTrainRows, kStatTrackItems, kStatTrackSteps, kStatTrackBricks, kStatTransmitItems,
+    kStatTransmitSteps, kStatTransmitBricks, kNumStats = 22
 };
 
 enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlotDead = 3 };
 
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
-                  kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kNumCounts = 9 };
+                  kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kCntTrackNext = 9,
+                  kCntTransmitNext = 10, kNumCounts = 11 };
+
+// k_track's result per slot (RenderParams::trk): the scattering position (world space) and,
+// in w, the tracking stream's next dimension with kTrackScattered set when the walk ended in
+// a real collision.
+constexpr uint32_t kTrackScattered = 0x80000000u;
 
 // Guided rendering.  A guide-queue entry (kGuideEntry float4) holds a vertex whose next
 // direction waits for the network: position + slot, normal (NaN x in a medium) +
@@ -116,7 +123,7 @@ struct RenderParams {
     float4* sc;                  // shadow: unoccluded contribution rgb, slot
     uint32_t* skey;              // shadow: random stream word
     float4* film_acc;            // per pixel: sum w r, w g, w b, sum w (this call)
-    float4* film_acc2;           // per pixel: sum w r^2, w g^2, w b^2 (this call)
+    float4* film_acc2;           // per pixel: sum w r^2, w g^2, w b^2 (this call; may be null)
     float2* film_acc3;           // per pixel: sum w^2, samples (filtered films; may be null)
     float4* splat;               // finished samples of filtered films: L.rgb, sample key
     int* splat_req;              // their requests (batched renders)
@@ -125,6 +132,8 @@ struct RenderParams {
     uint32_t* req_done;          // completed paths per request
     unsigned long long* req_time;  // globaltimer (ns) at each request's completion
     uint32_t* err;
+    float4* trk;                 // k_track's result per slot (scenes with media)
+    int transmitted;             // 1: k_transmit scaled sc by each shadow ray's transmittance
     int max_iter;
     int use_cond;                // k_swap sets the graph while-condition
     cudaGraphConditionalHandle cond;
@@ -341,7 +350,8 @@ __device__ __forceinline__ void SplatSample(const RenderParams& P, const Request
             float w = R.filter_table[iy * kFilterTableWidth + ix];
             size_t pix = (size_t)R.film_base + (size_t)y * W + x;
             RedAdd4(&P.film_acc[pix], w * c.x, w * c.y, w * c.z, w);
-            RedAdd4(&P.film_acc2[pix], w * c.x * c.x, w * c.y * c.y, w * c.z * c.z, 0.0f);
+            if (P.film_acc2)
+                RedAdd4(&P.film_acc2[pix], w * c.x * c.x, w * c.y * c.y, w * c.z * c.z, 0.0f);
             if (P.film_acc3)
                 RedAdd2(&P.film_acc3[pix], w * w, 1.0f);
         }
@@ -367,7 +377,8 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
             P.splat_req[q] = P.slot_req[i];
     } else {
         RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
-        RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
+        if (P.film_acc2)
+            RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
     }
     if (MULTI) {
         int r = P.slot_req[i];
@@ -502,6 +513,8 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     c[kCntShadow] = 0;
     c[kCntGuide] = 0;
     c[kCntSplat] = 0;
+    c[kCntTrackNext] = 0;
+    c[kCntTransmitNext] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
     bool more = active > 0;
@@ -779,9 +792,9 @@ __device__ V3 EnvColor(const SceneDev& S, V3 d, float& pdf) {
         pdf = 0.0f;  // Sky::Pdf (light.cpp:77-79)
         return SkyColor<M>(d, v3(l.p[0], l.p[1], l.p[2]), c);
     }
-    // Constant environment: the pdf of reaching d through next-event estimation, light
-    // selection included, so that the two strategies' MIS weights sum to one.
-    pdf = l.p[0] / (4 * kPi);
+    // Constant environment: reached only by escaping paths (next-event estimation never
+    // samples it), so the escape carries the full weight.
+    pdf = 0.0f;
     return c;
 }
 
@@ -844,9 +857,26 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     MediumEvent ev;
     ev.scattered = false;
     if (MEDIA && medium >= 0) {
-        HashRng trk = rng.Tracking();
-        MediumSampleEvent<M>(S.media[medium], o, d, tHit, trk, ev, ct.steps, ct.bricks, ct.err);
-        rng.EndTracking(trk);
+        const MediumDev& med = S.media[medium];
+        if (med.type == PG_MEDIUM_GRID) {
+            // GridMedium::Sample (medium.cpp:98-116): delta tracking ran in k_track, which
+            // every launch sequence runs before this kernel in scenes with media.  Read as
+            // integers: the w word is a counter and a flag, not a float.
+            const uint4 e = reinterpret_cast<const uint4*>(P.trk)[i];
+            const uint32_t wd = e.w;
+            ev.weight = v3(1.0f);
+            if (wd & kTrackScattered) {
+                ev.scattered = true;
+                ev.p = v3(__uint_as_float(e.x), __uint_as_float(e.y), __uint_as_float(e.z));
+                ev.weight = v3(med.sigma_s[0], med.sigma_s[1], med.sigma_s[2]) / med.sigma_t;
+            }
+            if (!rng.hal)
+                rng.dim = wd & ~kTrackScattered;  // the path's stream continues after the walk
+        } else {
+            HashRng trk = rng.Tracking();
+            HomogeneousSampleEvent<M>(med, o, d, tHit, trk, ev);
+            rng.EndTracking(trk);
+        }
         beta *= ev.weight;
     }
     if (ev.scattered) {
@@ -1050,18 +1080,26 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
             slot = (int)(w & ~kFinalShadow);
             last = (w & kFinalShadow) != 0;
             const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
-            HashRng rng{P.sample[slot], P.skey[q], 0};
-            V3 tr = ShadowTr<M, MEDIA>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
-                                __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x, steps,
-                                bricks, err, traced);
-            float4 Lw = P.L[slot];
-            V3 L = v3(Lw.x + sc.x * tr.x, Lw.y + sc.y * tr.y, Lw.z + sc.z * tr.z);
+            V3 tr = v3(1.0f);
+            if (P.transmitted) {
+                traced = 1;  // k_transmit already applied the transmittance to sc
+            } else {
+                HashRng rng{P.sample[slot], P.skey[q], 0};
+                tr = ShadowTr<M, MEDIA>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
+                                        __float_as_int(sd.w), rng, stack + threadIdx.x, blockDim.x,
+                                        steps, bricks, err, traced);
+            }
+            const V3 c = v3(sc.x * tr.x, sc.y * tr.y, sc.z * tr.z);
             if (last) {
+                float4 Lw = P.L[slot];
+                V3 L = v3(Lw.x + c.x, Lw.y + c.y, Lw.z + c.z);
                 FlushPath<MULTI, GEN>(P, slot, L, dropped);
                 if (GUIDE)
                     FinalizeRecords(P, slot, L, Finite(L));
-            } else if (!IsBlack(tr))
-                P.L[slot] = make_float4(L.x, L.y, L.z, Lw.w);
+            } else if (!IsBlack(c)) {
+                float4 Lw = P.L[slot];
+                P.L[slot] = make_float4(Lw.x + c.x, Lw.y + c.y, Lw.z + c.z, Lw.w);
+            }
             if (err)
                 atomicOr(P.err, err);
         }
@@ -1086,6 +1124,198 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
         WarpAdd(&P.stats[kStatPaths], last ? 1u : 0u);
         WarpAdd(&P.stats[kStatDropped], dropped);
     }
+}
+
+// ---------------------------------------------------------------- tracking kernels
+// Delta tracking of the extension rays (k_track) and ratio tracking of the shadow rays
+// (k_transmit) run in persistent warps: each lane walks one ray through the majorant bricks
+// a step at a time (GridWalk), and a warp takes new queue entries for its idle lanes once
+// kRefillLanes of them are idle (or all are), with one atomic on the queue's work counter.
+// A long walk then holds up one lane instead of its whole warp, and every iteration of the
+// loop is one short step with one memory lookup.
+#ifndef PG_REFILL_LANES
+#define PG_REFILL_LANES 8
+#endif
+constexpr int kRefillLanes = PG_REFILL_LANES;
+constexpr int kTrackThreads = 128;
+#ifndef PG_TRACK_MIN_BLOCKS
+#define PG_TRACK_MIN_BLOCKS 8
+#endif
+
+// Starts slot i's delta-tracking walk when its ray is in a grid medium: false when there is
+// nothing to walk (no grid medium: the shading kernel tracks inline; or the ray misses the
+// grid: the result, no collision, is written here).
+template <int M, bool MULTI, bool GEN>
+__device__ __forceinline__ bool TrackBegin(const RenderParams& P, const SceneDev& S0, int i, GridWalk& w,
+                                           HashRng& rng, const MediumDev*& med, uint32_t& bricks) {
+    const float4 rd = P.ray_d[i];
+    const int medium = __float_as_int(rd.w);
+    if (medium < 0)
+        return false;
+    const SceneDev& S = SceneOf<MULTI>(P, S0, i);
+    med = &S.media[medium];
+    if (med->type != PG_MEDIUM_GRID)
+        return false;
+    const float4 ro = P.ray_o[i];
+    // The segment ends at the surface k_trace found (path.cpp:13-17).
+    float tHit = kFloatMax;
+    if (S.has_bvh || S.num_planes) {
+        const float4 h = P.hit[i];
+        if (__float_as_int(h.y) != -1)
+            tHit = h.x;
+    }
+    const RequestDev& R = RequestOf<MULTI>(P, i);
+    rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(P.L[i].w)).Tracking();
+    if (GridWalkBegin<M>(*med, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), tHit, w, bricks))
+        return true;
+    reinterpret_cast<uint4*>(P.trk)[i] = make_uint4(0u, 0u, 0u, rng.dim);
+    return false;
+}
+
+template <int M, bool MULTI, bool GEN>
+__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
+    k_track(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    const int n = P.counts[kCntActive];
+    const int* active = ActiveList(P);
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    int slot = -1;
+    const MediumDev* med = nullptr;
+    GridWalk w;
+    HashRng rng{0u, 0u, 0u};
+    uint32_t items = 0, steps = 0, bricks = 0, err = 0;
+    bool more = true;
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, slot < 0);
+        if (more && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            int base = 0;
+            if (lane == 0)
+                base = atomicAdd(&P.counts[kCntTrackNext], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            more = base + __popc(idle) < n;
+            if (slot < 0) {
+                const int q = base + __popc(idle & below);
+                if (q < n) {
+                    const int i = active[q];
+                    items++;
+                    if (TrackBegin<M, MULTI, GEN>(P, S0, i, w, rng, med, bricks))
+                        slot = i;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, slot >= 0) == 0) {
+            if (!more)
+                break;
+            continue;
+        }
+        if (slot >= 0) {
+            const int r = DeltaTrackStep<M>(*med, w, rng, bricks, err);
+            if (r != kWalkGoing) {
+                V3 p = v3(0.0f);
+                uint32_t wd = rng.dim;
+                if (r == kWalkCollided) {
+                    p = Affine(med->m2w, w.mo + w.t * w.md);
+                    wd |= kTrackScattered;
+                }
+                reinterpret_cast<uint4*>(P.trk)[slot] =
+                    make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), __float_as_uint(p.z), wd);
+                steps += w.n;
+                slot = -1;
+            }
+        }
+    }
+    if (err)
+        atomicOr(P.err, err);
+    WarpAdd(&P.stats[kStatTrackItems], items);
+    WarpAdd(&P.stats[kStatTrackSteps], steps);
+    WarpAdd(&P.stats[kStatTrackBricks], bricks);
+    WarpAdd(&P.stats[kStatSteps], steps);
+}
+
+// Starts the ratio-tracking walk of shadow-queue entry q (scenes without surfaces: the
+// transmittance is the medium's alone, RayIntegrator::IntersectTr, integrator.cpp:68-87);
+// false when there is nothing to walk, with the entry's contribution already final.
+template <int M, bool MULTI>
+__device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const SceneDev& S0, int q, GridWalk& w,
+                                              HashRng& rng, const MediumDev*& med, uint32_t& bricks) {
+    const float4 sd = P.sd[q];
+    const int medium = __float_as_int(sd.w);
+    if (medium < 0)
+        return false;
+    const float4 so = P.so[q], sc = P.sc[q];
+    const int slot = (int)(__float_as_uint(sc.w) & ~kFinalShadow);
+    const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
+    med = &S.media[medium];
+    if (med->type != PG_MEDIUM_GRID) {
+        // HomogeneousMedium::Tr (medium.cpp:33-36): closed form.
+        const MediumDev& m = *med;
+        const float t = so.w;
+        P.sc[q] = make_float4(sc.x * PMath<M>::exp(-t * (m.sigma_a[0] + m.sigma_s[0])),
+                              sc.y * PMath<M>::exp(-t * (m.sigma_a[1] + m.sigma_s[1])),
+                              sc.z * PMath<M>::exp(-t * (m.sigma_a[2] + m.sigma_s[2])), sc.w);
+        return false;
+    }
+    rng = HashRng{P.sample[slot], P.skey[q], 0};
+    return GridWalkBegin<M>(*med, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w, w, bricks);
+}
+
+// Ratio tracking of the shadow queue (the media-only scenes' k_shadow work): scales each
+// entry's unoccluded contribution by its transmittance; k_shadow then adds it to the path.
+template <int M, bool MULTI>
+__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
+    k_transmit(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    const int n = P.counts[kCntShadow];
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    int entry = -1;
+    const MediumDev* med = nullptr;
+    GridWalk w;
+    HashRng rng{0u, 0u, 0u};
+    float tr = 1.0f;
+    uint32_t items = 0, steps = 0, bricks = 0, err = 0;
+    bool more = true;
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, entry < 0);
+        if (more && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            int base = 0;
+            if (lane == 0)
+                base = atomicAdd(&P.counts[kCntTransmitNext], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            more = base + __popc(idle) < n;
+            if (entry < 0) {
+                const int q = base + __popc(idle & below);
+                if (q < n) {
+                    items++;
+                    if (TransmitBegin<M, MULTI>(P, S0, q, w, rng, med, bricks)) {
+                        entry = q;
+                        tr = 1.0f;
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, entry >= 0) == 0) {
+            if (!more)
+                break;
+            continue;
+        }
+        if (entry >= 0) {
+            if (RatioTrackStep<M>(*med, w, rng, tr, bricks, err) != kWalkGoing) {
+                if (tr != 1.0f) {
+                    float4* c = &P.sc[entry];
+                    const float4 v = *c;
+                    *c = make_float4(v.x * tr, v.y * tr, v.z * tr, v.w);
+                }
+                steps += w.n;
+                entry = -1;
+            }
+        }
+    }
+    if (err)
+        atomicOr(P.err, err);
+    WarpAdd(&P.stats[kStatTransmitItems], items);
+    WarpAdd(&P.stats[kStatTransmitSteps], steps);
+    WarpAdd(&P.stats[kStatTransmitBricks], bricks);
+    WarpAdd(&P.stats[kStatSteps], steps);
 }
 
 // Guided direction sampling for the vertices in the guide queue, from the network's

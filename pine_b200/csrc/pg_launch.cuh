@@ -82,7 +82,20 @@ struct Wave {
     int mode = PG_MATH_FAST;
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
+    float4* trk = nullptr;  // per-slot results of k_track (required in scenes with media)
 };
+
+// The parameters of one iteration's launches: k_track's results when it runs (scenes with
+// media), and whether k_transmit applies the shadow rays' transmittance (media without
+// surfaces, shadow rays in their own kernel).
+static RenderParams IterationParams(const Wave& w, bool fused) {
+    if (w.media && !w.trk)
+        throw Failure{PG_ERR_CUDA, "wavefront with media but no tracking buffer"};
+    RenderParams P = w.P;
+    P.trk = w.media ? w.trk : nullptr;
+    P.transmitted = (P.trk && !fused && !w.surfaces) ? 1 : 0;
+    return P;
+}
 
 template <int M, bool MULTI, bool FUSED, bool GEN>
 static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
@@ -102,9 +115,16 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
         if (res)
             res->kernelLaunches[k]++;
     };
+    const RenderParams P = IterationParams(w, FUSED);
+    // The tracking kernels are persistent: one full wave of resident blocks.
+    const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
-            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(P, w.S0);
+        });
+    if (P.trk)
+        time(PG_KERNEL_TRACK, [&]() {
+            k_track<M, MULTI, GEN><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
         });
     // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
     const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
@@ -112,22 +132,27 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
     time(PG_KERNEL_SHADE, [&]() {
         if (!FUSED && !w.media)
             k_shade<M, MULTI, false, false, false, GEN>
-                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(w.P, w.S0);
+                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(P, w.S0);
         else
-            k_shade<M, MULTI, FUSED, false, true, GEN><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(w.P, w.S0);
+            k_shade<M, MULTI, FUSED, false, true, GEN><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(P, w.S0);
     });
-    if (!FUSED)
+    if (!FUSED) {
+        if (P.transmitted)
+            time(PG_KERNEL_TRANSMIT, [&]() {
+                k_transmit<M, MULTI><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
+            });
         time(PG_KERNEL_SHADOW, [&]() {
             if (!w.media)
-                k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+                k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
             else
-                k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+                k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
         });
+    }
     // Filtered films' splats and the queue swap; counted with the fill kernel.
     time(PG_KERNEL_REGEN, [&]() {
         if (w.splat)
-            k_splat<MULTI><<<grid(tb, 12), tb, 0, st>>>(w.P);
-        k_swap<<<1, 1, 0, st>>>(w.P);
+            k_splat<MULTI><<<grid(tb, 12), tb, 0, st>>>(P);
+        k_swap<<<1, 1, 0, st>>>(P);
     });
 }
 
@@ -163,35 +188,46 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
         if (res)
             res->kernelLaunches[k]++;
     };
+    const RenderParams P = IterationParams(w, FUSED);
+    const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
-            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(w.P, w.S0);
+            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(P, w.S0);
+        });
+    if (P.trk)
+        time(PG_KERNEL_TRACK, [&]() {
+            k_track<M, false, true><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
         });
     // Traversal stacks only where rays meet surfaces: a scene of media alone never traverses.
     const size_t stackBytes = w.surfaces ? w.stackBytes : 0;
     const size_t shadeSmem = FUSED && w.surfaces ? (size_t)w.shadeBlock * kStackSize * sizeof(uint2) : 0;
     time(PG_KERNEL_SHADE, [&]() {
         k_shade<M, false, FUSED, true, true, true><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem,
-                                         st>>>(w.P, w.S0);
+                                         st>>>(P, w.S0);
     });
     time(PG_KERNEL_GUIDE, [&]() {
         GuideInput in;
-        in.vert = w.P.gq;
+        in.vert = P.gq;
         in.stride = kGuideEntry;
         for (int k = 0; k < 3; k++)
             in.lo[k] = w.S0.guide_lo[k], in.inv[k] = w.S0.guide_inv[k];
-        in.count = &w.P.counts[kCntGuide];
-        PG_CUDA(GuideForward(*env.guide, in, n, const_cast<float*>(w.P.graw), sms, st));
-        k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(w.P, w.S0);
+        in.count = &P.counts[kCntGuide];
+        PG_CUDA(GuideForward(*env.guide, in, n, const_cast<float*>(P.graw), sms, st));
+        k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(P, w.S0);
     });
-    if (!FUSED)
+    if (!FUSED) {
+        if (P.transmitted)
+            time(PG_KERNEL_TRANSMIT, [&]() {
+                k_transmit<M, false><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
+            });
         time(PG_KERNEL_SHADOW, [&]() {
-            k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(w.P, w.S0);
+            k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
         });
+    }
     time(PG_KERNEL_REGEN, [&]() {
         if (w.splat)
-            k_splat<false><<<grid(tb, 12), tb, 0, st>>>(w.P);
-        k_swap<<<1, 1, 0, st>>>(w.P);
+            k_splat<false><<<grid(tb, 12), tb, 0, st>>>(P);
+        k_swap<<<1, 1, 0, st>>>(P);
     });
 }
 

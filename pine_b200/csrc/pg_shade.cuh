@@ -457,10 +457,13 @@ __device__ void SampleLight(const SceneDev& S, const LightDev& l, V3 p, float u0
         ls.Le = SkyColor<M>(a, a, c);
         return;
     case kLightConstant:
-        ls.distance = 1e+10f;
-        ls.wo = UniformSphereSampling<M>(u0, u1);
-        ls.pdf = 1.0f / (4 * kPi);
-        ls.Le = c;
+        // Constant{color}: like the gradient part of pine's Sky (Pdf 0, light.cpp:77-79) it
+        // is gathered only by escaping paths, so next-event estimation finds a zero-radiance
+        // delta sample and queues no shadow ray.
+        ls.distance = 0.0f;
+        ls.isDelta = true;
+        ls.wo = v3(0.0f, 0.0f, 1.0f);
+        ls.Le = v3(0.0f);
         return;
     default: {
         const ShapeDev& sh = S.shapes[l.shape];
@@ -596,136 +599,204 @@ __device__ __forceinline__ float GridDensity(const MediumDev& m, float vx, float
            fx * (gy * (gz * d100 + fz * d101) + fy * (gz * d110 + fz * d111));
 }
 
-// Walks the majorant bricks (m.bsize^3 voxels each) crossed by the medium-space ray
-// o + t d, t in [t0, t1], in order (3D DDA), calling f(tEnter, tExit, majorant) for bricks
-// whose majorant is > 0.  f returns true to stop the walk.
-template <typename F>
-__device__ __forceinline__ void WalkBricks(const MediumDev& m, V3 o, V3 d, float t0, float t1,
-                                           uint32_t& bricks, F&& f) {
-    // Voxel-index space: v = (o + t d) * size; bricks are bsize voxels wide.
-    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
-    V3 vo = v3(o.x * sx, o.y * sy, o.z * sz), vd = v3(d.x * sx, d.y * sy, d.z * sz);
-    float px = vo.x + t0 * vd.x, py = vo.y + t0 * vd.y, pz = vo.z + t0 * vd.z;
-    const float inb = m.inv_bsize, bs = (float)m.bsize;
-    int bx = min(max((int)floorf(px * inb), 0), m.nb[0] - 1);
-    int by = min(max((int)floorf(py * inb), 0), m.nb[1] - 1);
-    int bz = min(max((int)floorf(pz * inb), 0), m.nb[2] - 1);
-    int stx = vd.x > 0.0f ? 1 : -1, sty = vd.y > 0.0f ? 1 : -1, stz = vd.z > 0.0f ? 1 : -1;
-    float inx = vd.x != 0.0f ? 1.0f / vd.x : 0.0f, iny = vd.y != 0.0f ? 1.0f / vd.y : 0.0f,
-          inz = vd.z != 0.0f ? 1.0f / vd.z : 0.0f;
-    auto nextT = [&](int b, int st, float vo_, float in) {
-        if (in == 0.0f)
-            return kFloatMax;
-        float plane = (float)(b + (st > 0 ? 1 : 0)) * bs;
-        return (plane - vo_) * in;
-    };
-    float tx = nextT(bx, stx, vo.x, inx), ty = nextT(by, sty, vo.y, iny), tz = nextT(bz, stz, vo.z, inz);
-    float dtx = inx != 0.0f ? bs * Fabs(inx) : kFloatMax, dty = iny != 0.0f ? bs * Fabs(iny) : kFloatMax,
-          dtz = inz != 0.0f ? bs * Fabs(inz) : kFloatMax;
-    float t = t0;
-    const int maxSteps = m.nb[0] + m.nb[1] + m.nb[2] + 4;
-    for (int i = 0; i < maxSteps && t < t1; i++) {
-        float tn = Min(Min(tx, ty), Min(tz, t1));
-        float maj = __ldg(&m.majorant[bx + m.nb[0] * (by + m.nb[1] * bz)]);
-        if (maj > 0.0f && tn > t) {
-            bricks++;
-            if (f(t, tn, maj))
-                return;
-        }
-        t = tn;
-        if (tx <= ty && tx <= tz) {
-            bx += stx;
-            tx += dtx;
-            if (bx < 0 || bx >= m.nb[0])
-                return;
-        } else if (ty <= tz) {
-            by += sty;
-            ty += dty;
-            if (by < 0 || by >= m.nb[1])
-                return;
-        } else {
-            bz += stz;
-            tz += dtz;
-            if (bz < 0 || bz >= m.nb[2])
-                return;
-        }
-    }
-}
-
 struct MediumEvent {
     bool scattered;
     V3 p;       // world position of the scattering event
     V3 weight;  // beta multiplier (medium.cpp:98-139 returns sigma_s/sigma_t or 1)
 };
 
-// GridMedium::Sample (medium.cpp:98-116) with per-brick majorants instead of the global
-// one; delta tracking is unbiased for any majorant that bounds the density it samples.
-// HomogeneousMedium::Sample (medium.cpp:38-53).  `tmax` is the world-space hit distance,
-// used as the bound in medium space as pine does (medium.cpp:99-101).
+// HomogeneousMedium::Sample (medium.cpp:38-53).  (Grid media are delta-tracked by k_track,
+// GridWalk below.)
 template <int M>
-__device__ void MediumSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& rng,
-                                  MediumEvent& ev, uint32_t& steps, uint32_t& bricks,
-                                  uint32_t& err) {
+__device__ void HomogeneousSampleEvent(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& rng,
+                                       MediumEvent& ev) {
     ev.scattered = false;
-    ev.weight = v3(1.0f);
-    if (m.type == PG_MEDIUM_HOMOGENEOUS) {
-        V3 st = v3(m.sigma_a[0] + m.sigma_s[0], m.sigma_a[1] + m.sigma_s[1], m.sigma_a[2] + m.sigma_s[2]);
-        int ch = (int)(rng.Get1D() * 3);
-        ch = min(ch, 2);
-        float dist = -PMath<M>::log(1.0f - rng.Get1D()) / Comp(st, ch);
-        bool sampled = dist < tmax;
-        float t = Min(dist, tmax);
-        V3 tr = v3(PMath<M>::exp(-st.x * t), PMath<M>::exp(-st.y * t), PMath<M>::exp(-st.z * t));
-        if (sampled) {
-            ev.scattered = true;
-            ev.p = o + t * d;
-            float pdf = (st.x * tr.x + st.y * tr.y + st.z * tr.z) / 3.0f;
-            ev.weight = v3(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]) * tr / pdf;
-        } else {
-            float pdf = (tr.x + tr.y + tr.z) / 3.0f;
-            ev.weight = tr / pdf;
-        }
-        return;
-    }
-    V3 mo = Affine(m.w2m, o);
-    V3 md = Normalize<M>(Linear(m.w2m, d));
-    float t0 = 0.0f, t1 = tmax;
-    if (!FiniteRay(mo, md) || !UnitBoxHit(mo, md, t0, t1))
-        return;
-    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
-    float ts = 0.0f;
-    uint32_t n = 0;
-    bool hit = false;
-    WalkBricks(m, mo, md, t0, t1, bricks, [&](float ta, float tb, float maj) {
-        float inv = 1.0f / (m.sigma_t * maj);
-        float t = ta;
-        while (true) {
-            t -= PMath<M>::log(1.0f - rng.Get1D()) * inv;
-            if (t >= tb)
-                return false;
-            if (++n > (uint32_t)kTrackingCap) {
-                err |= kErrTrackingCap;
-                return true;
-            }
-            float dens = GridDensity(m, (mo.x + t * md.x) * sx, (mo.y + t * md.y) * sy,
-                                     (mo.z + t * md.z) * sz);
-            if (dens / maj > rng.Get1D()) {
-                ts = t;
-                hit = true;
-                return true;
-            }
-        }
-    });
-    steps += n;
-    if (hit) {
+    V3 st = v3(m.sigma_a[0] + m.sigma_s[0], m.sigma_a[1] + m.sigma_s[1], m.sigma_a[2] + m.sigma_s[2]);
+    int ch = (int)(rng.Get1D() * 3);
+    ch = min(ch, 2);
+    float dist = -PMath<M>::log(1.0f - rng.Get1D()) / Comp(st, ch);
+    bool sampled = dist < tmax;
+    float t = Min(dist, tmax);
+    V3 tr = v3(PMath<M>::exp(-st.x * t), PMath<M>::exp(-st.y * t), PMath<M>::exp(-st.z * t));
+    if (sampled) {
         ev.scattered = true;
-        ev.p = Affine(m.m2w, mo + ts * md);
-        ev.weight = v3(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]) / m.sigma_t;
+        ev.p = o + t * d;
+        float pdf = (st.x * tr.x + st.y * tr.y + st.z * tr.z) / 3.0f;
+        ev.weight = v3(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]) * tr / pdf;
+    } else {
+        float pdf = (tr.x + tr.y + tr.z) / 3.0f;
+        ev.weight = tr / pdf;
     }
 }
 
+// ---------------------------------------------------------------- stepped grid walks
+// The walk of WalkBricks with delta tracking (MediumSampleEvent) or ratio tracking
+// (MediumTr) inside each brick, as a state machine advanced by one step per call: one
+// tentative collision, or one brick.  The tracking kernels run it in loops in which every
+// lane of a warp takes a step per iteration and a lane whose walk has ended takes the next
+// ray, so that the lanes stay busy while walks differ in length.  It makes the same random
+// draws in the same order as the nested loops above, so the results are the same.
+struct GridWalk {
+    V3 mo, md;             // medium-space ray (direction normalised)
+    float t;               // position along the ray
+    float tb;              // exit of the current brick
+    float t1;              // end of the segment (box exit or the ray's bound)
+    float maj, inv;        // the current brick's majorant (0: moving on), 1 / (sigma_t maj)
+    float tx, ty, tz;      // next brick-boundary crossings
+    float dtx, dty, dtz;   // distance between crossings per axis
+    int bx, by, bz;
+    int left;              // brick moves before the walk gives up (WalkBricks' maxSteps)
+    int stepSigns;         // bit k set: the walk moves towards +k on axis k
+    uint32_t n;            // tentative collisions taken (kTrackingCap)
+};
+
+// Enters the brick the walk is in: its majorant and exit, or maj = 0 when it holds no
+// density or is passed at zero length (WalkBricks' loop head).  Returns false when the walk
+// is over (the brick budget spent or the segment's end reached).
+__device__ __forceinline__ bool GridWalkEnter(const MediumDev& m, GridWalk& w, uint32_t& bricks) {
+    if (w.left <= 0 || !(w.t < w.t1))
+        return false;
+    w.left--;
+    float tn = Min(Min(w.tx, w.ty), Min(w.tz, w.t1));
+    float maj = __ldg(&m.majorant[w.bx + m.nb[0] * (w.by + m.nb[1] * w.bz)]);
+    w.tb = tn;
+    w.maj = 0.0f;
+    if (maj > 0.0f && tn > w.t) {
+        bricks++;
+        w.maj = maj;
+        w.inv = 1.0f / (m.sigma_t * maj);
+    }
+    return true;
+}
+
+// Leaves the current brick at its exit for the next one along the ray (WalkBricks' loop
+// tail) and enters it; false when the walk is over.
+__device__ __forceinline__ bool GridWalkNext(const MediumDev& m, GridWalk& w, uint32_t& bricks) {
+    w.t = w.tb;
+    if (w.tx <= w.ty && w.tx <= w.tz) {
+        w.bx += (w.stepSigns & 1) ? 1 : -1;
+        w.tx += w.dtx;
+        if (w.bx < 0 || w.bx >= m.nb[0])
+            return false;
+    } else if (w.ty <= w.tz) {
+        w.by += (w.stepSigns & 2) ? 1 : -1;
+        w.ty += w.dty;
+        if (w.by < 0 || w.by >= m.nb[1])
+            return false;
+    } else {
+        w.bz += (w.stepSigns & 4) ? 1 : -1;
+        w.tz += w.dtz;
+        if (w.bz < 0 || w.bz >= m.nb[2])
+            return false;
+    }
+    return GridWalkEnter(m, w, bricks);
+}
+
+// Starts the walk of the world-space ray o + t d, t in [0, tmax], through grid medium m
+// (MediumSampleEvent / MediumTr up to WalkBricks' first brick); false when the ray misses
+// the grid's box.
+template <int M>
+__device__ __forceinline__ bool GridWalkBegin(const MediumDev& m, V3 o, V3 d, float tmax, GridWalk& w,
+                                              uint32_t& bricks) {
+    w.mo = Affine(m.w2m, o);
+    w.md = Normalize<M>(Linear(m.w2m, d));
+    float t0 = 0.0f, t1 = tmax;
+    if (!FiniteRay(w.mo, w.md) || !UnitBoxHit(w.mo, w.md, t0, t1))
+        return false;
+    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
+    V3 vo = v3(w.mo.x * sx, w.mo.y * sy, w.mo.z * sz), vd = v3(w.md.x * sx, w.md.y * sy, w.md.z * sz);
+    float px = vo.x + t0 * vd.x, py = vo.y + t0 * vd.y, pz = vo.z + t0 * vd.z;
+    const float inb = m.inv_bsize, bs = (float)m.bsize;
+    w.bx = min(max((int)floorf(px * inb), 0), m.nb[0] - 1);
+    w.by = min(max((int)floorf(py * inb), 0), m.nb[1] - 1);
+    w.bz = min(max((int)floorf(pz * inb), 0), m.nb[2] - 1);
+    w.stepSigns = (vd.x > 0.0f ? 1 : 0) | (vd.y > 0.0f ? 2 : 0) | (vd.z > 0.0f ? 4 : 0);
+    float inx = vd.x != 0.0f ? 1.0f / vd.x : 0.0f, iny = vd.y != 0.0f ? 1.0f / vd.y : 0.0f,
+          inz = vd.z != 0.0f ? 1.0f / vd.z : 0.0f;
+    auto nextT = [&](int b, bool pos, float vo_, float in) {
+        if (in == 0.0f)
+            return kFloatMax;
+        float plane = (float)(b + (pos ? 1 : 0)) * bs;
+        return (plane - vo_) * in;
+    };
+    w.tx = nextT(w.bx, vd.x > 0.0f, vo.x, inx);
+    w.ty = nextT(w.by, vd.y > 0.0f, vo.y, iny);
+    w.tz = nextT(w.bz, vd.z > 0.0f, vo.z, inz);
+    w.dtx = inx != 0.0f ? bs * Fabs(inx) : kFloatMax;
+    w.dty = iny != 0.0f ? bs * Fabs(iny) : kFloatMax;
+    w.dtz = inz != 0.0f ? bs * Fabs(inz) : kFloatMax;
+    w.t = t0;
+    w.t1 = t1;
+    w.left = m.nb[0] + m.nb[1] + m.nb[2] + 4;
+    w.n = 0;
+    w.maj = 0.0f;
+    return GridWalkEnter(m, w, bricks);
+}
+
+// Outcome of a walk step.
+enum WalkStep : int { kWalkGoing = 0, kWalkEnded = 1, kWalkCollided = 2 };
+
+// One step of delta tracking (GridMedium::Sample, medium.cpp:98-116, per brick): a
+// tentative collision in the current brick, accepted with probability density / majorant
+// (kWalkCollided: the walk stops at w.t), or the move to the next brick.  kWalkEnded: the
+// ray left the segment without a real collision (or hit the tracking cap, flagged in err).
+template <int M>
+__device__ __forceinline__ int DeltaTrackStep(const MediumDev& m, GridWalk& w, HashRng& rng,
+                                              uint32_t& bricks, uint32_t& err) {
+    if (w.maj > 0.0f) {
+        float t = w.t - PMath<M>::log(1.0f - rng.Get1D()) * w.inv;
+        if (t < w.tb) {
+            w.t = t;
+            if (++w.n > (uint32_t)kTrackingCap) {
+                err |= kErrTrackingCap;
+                return kWalkEnded;
+            }
+            float dens = GridDensity(m, (w.mo.x + t * w.md.x) * (float)m.size[0],
+                                     (w.mo.y + t * w.md.y) * (float)m.size[1],
+                                     (w.mo.z + t * w.md.z) * (float)m.size[2]);
+            return dens / w.maj > rng.Get1D() ? kWalkCollided : kWalkGoing;
+        }
+    }
+    return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+}
+
+// One step of ratio tracking with pine's Russian roulette (GridMedium::Tr, medium.cpp:55-80,
+// per brick), multiplying the transmittance estimate tr; kWalkEnded when the walk is over
+// (tr = 0 when the roulette or the tracking cap ended it).
+template <int M>
+__device__ __forceinline__ int RatioTrackStep(const MediumDev& m, GridWalk& w, HashRng& rng, float& tr,
+                                              uint32_t& bricks, uint32_t& err) {
+    if (w.maj > 0.0f) {
+        float t = w.t - PMath<M>::log(1.0f - rng.Get1D()) * w.inv;
+        if (t < w.tb) {
+            w.t = t;
+            if (++w.n > (uint32_t)kTrackingCap) {
+                err |= kErrTrackingCap;
+                tr = 0.0f;
+                return kWalkEnded;
+            }
+            float dens = GridDensity(m, (w.mo.x + t * w.md.x) * (float)m.size[0],
+                                     (w.mo.y + t * w.md.y) * (float)m.size[1],
+                                     (w.mo.z + t * w.md.z) * (float)m.size[2]);
+            tr *= 1.0f - Max(0.0f, dens / w.maj);
+            if (tr < 0.1f) {
+                float q = Max(0.05f, 1.0f - tr);
+                if (rng.Get1D() < q) {
+                    tr = 0.0f;
+                    return kWalkEnded;
+                }
+                tr /= 1.0f - q;
+            }
+            return kWalkGoing;
+        }
+    }
+    return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+}
+
 // GridMedium::Tr (medium.cpp:55-80): ratio tracking with pine's Russian roulette once the
-// transmittance estimate drops below 0.1.  HomogeneousMedium::Tr (medium.cpp:33-36).
+// transmittance estimate drops below 0.1, per majorant brick.  HomogeneousMedium::Tr
+// (medium.cpp:33-36).  For the shadow rays traced inside the shading or shadow kernels
+// (scenes with surfaces, or shadows fused into shading); k_transmit runs the same walk.
 template <int M>
 __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& rng, uint32_t& steps,
                           uint32_t& bricks, uint32_t& err, V3& trRGB) {
@@ -735,41 +806,13 @@ __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& r
                    PMath<M>::exp(-tmax * (m.sigma_a[2] + m.sigma_s[2])));
         return 1.0f;
     }
-    trRGB = v3(1.0f);
-    V3 mo = Affine(m.w2m, o);
-    V3 md = Normalize<M>(Linear(m.w2m, d));
-    float t0 = 0.0f, t1 = tmax;
-    if (!FiniteRay(mo, md) || !UnitBoxHit(mo, md, t0, t1))
-        return 1.0f;
-    float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     float tr = 1.0f;
-    uint32_t n = 0;
-    WalkBricks(m, mo, md, t0, t1, bricks, [&](float ta, float tb, float maj) {
-        float inv = 1.0f / (m.sigma_t * maj);
-        float t = ta;
-        while (true) {
-            t -= PMath<M>::log(1.0f - rng.Get1D()) * inv;
-            if (t >= tb)
-                return false;
-            if (++n > (uint32_t)kTrackingCap) {
-                err |= kErrTrackingCap;
-                tr = 0.0f;
-                return true;
-            }
-            float dens = GridDensity(m, (mo.x + t * md.x) * sx, (mo.y + t * md.y) * sy,
-                                     (mo.z + t * md.z) * sz);
-            tr *= 1.0f - Max(0.0f, dens / maj);
-            if (tr < 0.1f) {
-                float q = Max(0.05f, 1.0f - tr);
-                if (rng.Get1D() < q) {
-                    tr = 0.0f;
-                    return true;
-                }
-                tr /= 1.0f - q;
-            }
+    GridWalk w;
+    if (GridWalkBegin<M>(m, o, d, tmax, w, bricks)) {
+        while (RatioTrackStep<M>(m, w, rng, tr, bricks, err) == kWalkGoing) {
         }
-    });
-    steps += n;
+        steps += w.n;
+    }
     trRGB = v3(tr);
     return tr;
 }

@@ -121,6 +121,7 @@ struct Pool {
     uint32_t* skey = nullptr;
     float4* splat = nullptr;   // queued samples of filtered films
     int* splat_req = nullptr;
+    float4* trk = nullptr;     // k_track's result per slot
     void Ensure(int n) {
         if (n <= slots)
             return;
@@ -142,6 +143,7 @@ struct Pool {
         skey = mem.Alloc<uint32_t>(n);
         splat = mem.Alloc<float4>(n);
         splat_req = mem.Alloc<int>(n);
+        trk = mem.Alloc<float4>(n);
     }
 };
 
@@ -515,8 +517,6 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         for (auto& c : cdf)
             c /= funcInt;
     bool uniform = d->light_sampler == PG_LIGHT_SAMPLER_UNIFORM;
-    if (env >= 0 && lights[env].type == kLightConstant)
-        lights[env].p[0] = (uniform || funcInt == 0.0f) ? 1.0f / nl : power[env] / nl;
 
     // Media.
     std::vector<MediumDev> media(d->num_media);
@@ -895,6 +895,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.slot_req = pl.slot_req;
     P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
     P.splat = pl.splat, P.splat_req = pl.splat_req;
+    w.trk = pl.trk;
     P.counts = ctx->counts;
     P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2, P.film_acc3 = ctx->film.acc3;
     P.next_sample = ctx->next_sample;
@@ -1437,9 +1438,12 @@ extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_de
             stats->paths = (int64_t)r.stats[kStatPaths];
             stats->launches = r.launches;
             const int items[PG_NUM_KERNELS] = {kStatRegenItems, kStatTraceItems, kStatShadeItems,
-                                               kStatShadowItems, kStatGuided, kStatTrainRows};
-            const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps, -1, -1};
-            const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks, -1, -1};
+                                               kStatShadowItems, kStatGuided, kStatTrainRows,
+                                               kStatTrackItems, kStatTransmitItems};
+            const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps, -1, -1,
+                                               kStatTrackSteps, kStatTransmitSteps};
+            const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks, -1, -1,
+                                                kStatTrackBricks, kStatTransmitBricks};
             for (int k = 0; k < PG_NUM_KERNELS; k++) {
                 pg_kernel_stats& ks = stats->kernels[k];
                 ks.launches = r.kernelLaunches[k];
@@ -1751,17 +1755,17 @@ constexpr size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct NoAllocLayout {
     static constexpr size_t kF4 = (size_t)kNoAllocSlots * sizeof(float4);
     static constexpr size_t kI = (size_t)kNoAllocSlots * sizeof(int);
-    // ray_o, ray_d, beta, L, hit, so, sd, sc, splat
+    // ray_o, ray_d, beta, L, hit, so, sd, sc, splat, trk
     static constexpr size_t float4s = 0;
     // sample, skey, state, finished, slot_req, lists (2 x slots), splat_req
-    static constexpr size_t ints = float4s + 9 * Align256(kF4);
+    static constexpr size_t ints = float4s + 10 * Align256(kF4);
     static constexpr size_t film = ints + 8 * Align256(kI);
     static constexpr size_t filmBytes = Align256((size_t)kNoAllocPixels * sizeof(float4));
-    static constexpr size_t request = film + 2 * filmBytes;
+    static constexpr size_t request = film + filmBytes;  // the mean needs no squared sums
     static constexpr size_t total = request + Align256(sizeof(RequestDev));
 };
 
-// The array: about 27 MiB on every GPU that loads the library, held until the process
+// The array: about 20 MiB on every GPU that loads the library, held until the process
 // exits.  All calls on a device share it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
 
@@ -1810,12 +1814,12 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     auto f4 = [&](int k) { return reinterpret_cast<float4*>(base + L::float4s + k * Align256(L::kF4)); };
     auto i32 = [&](int k) { return reinterpret_cast<int*>(base + L::ints + k * Align256(L::kI)); };
     float4* acc = reinterpret_cast<float4*>(base + L::film);
-    float4* acc2 = reinterpret_cast<float4*>(base + L::film + L::filmBytes);
     RequestDev* dReq = reinterpret_cast<RequestDev*>(base + L::request);
 
     Wave w;
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
+    w.media = sc.dev.num_media > 0;
     w.general = sc.general;
     w.splat = sc.filter_splat != 0;
     w.fused = ctx->tuning.split_shadow == 0;
@@ -1832,8 +1836,9 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     P.skey = reinterpret_cast<uint32_t*>(i32(1));
     P.state = i32(2), P.finished = i32(3), P.slot_req = i32(4), P.lists = i32(5);
     P.splat = f4(8), P.splat_req = i32(7);
+    w.trk = f4(9);
     P.counts = ctx->counts;
-    P.film_acc = acc, P.film_acc2 = acc2, P.film_acc3 = nullptr;  // the mean needs no more
+    P.film_acc = acc, P.film_acc2 = nullptr, P.film_acc3 = nullptr;  // the mean needs no more
     P.next_sample = ctx->next_sample;
     P.stats = ctx->stats;
     P.err = ctx->err;
@@ -1843,7 +1848,6 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     // What must start at zero: slot states, the film accumulators of this film, counters.
     PG_CUDA(cudaMemsetAsync(P.state, 0, (size_t)slots * sizeof(int), st));
     PG_CUDA(cudaMemsetAsync(acc, 0, (size_t)npix * sizeof(float4), st));
-    PG_CUDA(cudaMemsetAsync(acc2, 0, (size_t)npix * sizeof(float4), st));
     k_iota<<<ctx->num_sms * 4, 256, 0, st>>>(P.finished, slots);
     PG_CUDA(cudaGetLastError());
     int c[kNumCounts] = {};

@@ -438,7 +438,11 @@ void LoadCompressedVolume(const std::string& path, std::vector<float>& density, 
     take(&encBytes, 8);
     if (hdr[0] <= 0 || hdr[1] <= 0 || hdr[2] <= 0 || (int64_t)hdr[0] * hdr[1] * hdr[2] > (1ll << 33))
         fail("bad size");
-    if (treeBytes < 56 || (treeBytes - 56) % 6 != 0 || pos + treeBytes + encBytes != all.size())
+    // Every size is checked against the bytes that remain before any arithmetic on it, so
+    // no sum below can wrap around.
+    const uint64_t rest = all.size() - pos;
+    if (treeBytes < 56 || treeBytes > rest || (treeBytes - 56) % 6 != 0 ||
+        encBytes != rest - treeBytes || encBytes < 36)
         fail("section sizes do not add up");
     const size_t treeStart = pos;
     uint64_t entries;
@@ -456,9 +460,9 @@ void LoadCompressedVolume(const std::string& path, std::vector<float>& density, 
     }
     uint64_t vb[3];
     take(vb, 24);
-    const uint64_t nbytes = vb[1] - vb[0];
-    if (vb[1] < vb[0] || 24 + nbytes + 12 != encBytes)
+    if (vb[1] < vb[0] || vb[1] - vb[0] != encBytes - 36)
         fail("encoded section size");
+    const uint64_t nbytes = encBytes - 36;  // bounded by the file size
     const unsigned char* bits = reinterpret_cast<const unsigned char*>(all.data() + pos);
     pos += nbytes;
     uint32_t nbits;

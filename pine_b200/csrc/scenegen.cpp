@@ -1,17 +1,26 @@
-// Seeded synthetic inputs for the benchmark scenes: a fractal-noise cloud density grid
-// (written as pine's uncompressed .vol format, src/util/fileio.cpp:194-202) and a
-// noise-displaced subdivided icosphere (written as OBJ for src/util/objloader.cpp).
+// pine-scenegen: seeded synthetic inputs for the benchmark and test scenes, a standalone
+// tool kept out of libpinegpu.so so that generating a scene loads none of the renderer.
+//
+//   pine-scenegen cloud <n> <seed> <nonzero_fraction> <out.vol>
+//       an n^3 fractal-noise cloud density grid, written as pine's uncompressed .vol
+//       (src/util/fileio.cpp:194-202: int32 sx, sy, sz, then float32, x fastest)
+//   pine-scenegen icosphere <subdiv> <radius> <cx> <cy> <cz> <amplitude> <seed> <out.obj>
+//       a noise-displaced subdivided icosphere (20 * 4^subdiv triangles), written as OBJ
+//       for src/util/objloader.cpp with plain decimals (pine's stof has no exponents)
+//
+// Each prints one JSON line on success and exits 0; on bad arguments or an I/O error it
+// prints the reason on stderr and exits 1.  The output is a fixed function of the
+// arguments (no fast-math, per-element work independent of the thread schedule).
 //
 // The noise is gradient noise in the style of Perlin's improved noise (quintic fade,
 // 12 edge gradients), with the permutation table replaced by an integer hash of the
 // lattice point and the seed so that any seed gives an independent field.
-#include "pine_gpu.h"
-
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -110,12 +119,10 @@ void ParallelRange(int64_t n, F&& f) {
         th.join();
 }
 
-}  // namespace
-
-extern "C" pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fraction,
-                                         float* density) {
+// Fills density[n^3] (x fastest); false on invalid arguments.
+bool GenCloudVolume(int n, uint64_t seed, float nonzero_fraction, float* density) {
     if (n <= 1 || !density || nonzero_fraction <= 0.0f || nonzero_fraction > 1.0f)
-        return PG_ERR_INVALID_ARG;
+        return false;
     const uint32_t s = (uint32_t)(seed ^ (seed >> 32));
     const int64_t total = (int64_t)n * n * n;
     // Raw field: 6-octave fractal noise mapped to [0, 1], shaped by a smooth ellipsoidal
@@ -135,7 +142,7 @@ extern "C" pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fra
     for (int64_t i = 0; i < total; i++)
         vmax = std::max(vmax, density[i]);
     if (vmax <= 0.0f)
-        return PG_ERR_INVALID_ARG;
+        return false;
     const int bins = 4096;
     std::vector<int64_t> hist(bins, 0);
     for (int64_t i = 0; i < total; i++)
@@ -151,24 +158,19 @@ extern "C" pg_status pg_gen_cloud_volume(int n, uint64_t seed, float nonzero_fra
         float d = density[i] - tau;
         density[i] = d > 0.0f ? std::min(1.0f, d * scale) : 0.0f;
     });
-    return PG_OK;
+    return true;
 }
 
-extern "C" pg_status pg_write_volume(const char* path, int sx, int sy, int sz,
-                                     const float* density) {
-    if (!path || !density || sx <= 0 || sy <= 0 || sz <= 0)
-        return PG_ERR_INVALID_ARG;
+bool WriteVolume(const char* path, int sx, int sy, int sz, const float* density) {
     FILE* f = std::fopen(path, "wb");
     if (!f)
-        return PG_ERR_IO;
+        return false;
     int32_t hdr[3] = {sx, sy, sz};
     size_t total = (size_t)sx * sy * sz;
     bool ok = std::fwrite(hdr, 4, 3, f) == 3 && std::fwrite(density, 4, total, f) == total;
-    std::fclose(f);
-    return ok ? PG_OK : PG_ERR_IO;
+    ok = std::fclose(f) == 0 && ok;
+    return ok;
 }
-
-namespace {
 
 struct IcoMesh {
     std::vector<float> v;      // xyz per vertex (unit sphere before displacement)
@@ -219,13 +221,11 @@ IcoMesh Icosphere(int subdiv) {
     return m;
 }
 
-}  // namespace
-
-extern "C" pg_status pg_gen_icosphere_obj(const char* path, int subdiv, float radius, float cx,
-                                          float cy, float cz, float amplitude, uint64_t seed,
-                                          int64_t* out_triangles) {
+// Writes the displaced icosphere as OBJ; returns the triangle count, or -1 on an error.
+int64_t GenIcosphereObj(const char* path, int subdiv, float radius, float cx, float cy, float cz,
+                        float amplitude, uint64_t seed) {
     if (!path || subdiv < 0 || subdiv > 9 || radius <= 0.0f)
-        return PG_ERR_INVALID_ARG;
+        return -1;
     IcoMesh m = Icosphere(subdiv);
     const uint32_t s = (uint32_t)(seed ^ (seed >> 32));
     size_t nv = m.v.size() / 3;
@@ -241,7 +241,7 @@ extern "C" pg_status pg_gen_icosphere_obj(const char* path, int subdiv, float ra
     });
     FILE* f = std::fopen(path, "wb");
     if (!f)
-        return PG_ERR_IO;
+        return -1;
     // Plain decimals only: pine's number parser has no exponent support.
     std::vector<char> buf(1 << 20);
     std::setvbuf(f, buf.data(), _IOFBF, buf.size());
@@ -250,8 +250,74 @@ extern "C" pg_status pg_gen_icosphere_obj(const char* path, int subdiv, float ra
     for (size_t i = 0; i < m.idx.size(); i += 3)
         std::fprintf(f, "f %d %d %d\n", m.idx[i] + 1, m.idx[i + 1] + 1, m.idx[i + 2] + 1);
     bool ok = std::fflush(f) == 0;
-    std::fclose(f);
-    if (out_triangles)
-        *out_triangles = (int64_t)(m.idx.size() / 3);
-    return ok ? PG_OK : PG_ERR_IO;
+    ok = std::fclose(f) == 0 && ok;
+    return ok ? (int64_t)(m.idx.size() / 3) : -1;
+}
+
+bool ParseInt(const char* s, long long lo, long long hi, long long& out) {
+    char* end = nullptr;
+    long long v = std::strtoll(s, &end, 10);
+    if (!end || *end || end == s || v < lo || v > hi)
+        return false;
+    out = v;
+    return true;
+}
+
+bool ParseFloat(const char* s, float& out) {
+    char* end = nullptr;
+    float v = std::strtof(s, &end);
+    if (!end || *end || end == s || !std::isfinite(v))
+        return false;
+    out = v;
+    return true;
+}
+
+int Usage() {
+    std::fprintf(stderr,
+                 "usage: pine-scenegen cloud <n> <seed> <nonzero_fraction> <out.vol>\n"
+                 "       pine-scenegen icosphere <subdiv> <radius> <cx> <cy> <cz> <amplitude> "
+                 "<seed> <out.obj>\n");
+    return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2)
+        return Usage();
+    std::string cmd = argv[1];
+    if (cmd == "cloud" && argc == 6) {
+        long long n, seed;
+        float frac;
+        if (!ParseInt(argv[2], 2, 2048, n) || !ParseInt(argv[3], 0, INT64_MAX, seed) ||
+            !ParseFloat(argv[4], frac))
+            return Usage();
+        std::vector<float> dens((size_t)n * n * n);
+        if (!GenCloudVolume((int)n, (uint64_t)seed, frac, dens.data())) {
+            std::fprintf(stderr, "pine-scenegen: invalid cloud parameters\n");
+            return 1;
+        }
+        if (!WriteVolume(argv[5], (int)n, (int)n, (int)n, dens.data())) {
+            std::fprintf(stderr, "pine-scenegen: cannot write %s\n", argv[5]);
+            return 1;
+        }
+        std::printf("{\"voxels\": %lld}\n", n * n * n);
+        return 0;
+    }
+    if (cmd == "icosphere" && argc == 10) {
+        long long subdiv, seed;
+        float radius, cx, cy, cz, amp;
+        if (!ParseInt(argv[2], 0, 9, subdiv) || !ParseFloat(argv[3], radius) ||
+            !ParseFloat(argv[4], cx) || !ParseFloat(argv[5], cy) || !ParseFloat(argv[6], cz) ||
+            !ParseFloat(argv[7], amp) || !ParseInt(argv[8], 0, INT64_MAX, seed))
+            return Usage();
+        int64_t nt = GenIcosphereObj(argv[9], (int)subdiv, radius, cx, cy, cz, amp, (uint64_t)seed);
+        if (nt < 0) {
+            std::fprintf(stderr, "pine-scenegen: cannot write %s\n", argv[9]);
+            return 1;
+        }
+        std::printf("{\"triangles\": %lld}\n", (long long)nt);
+        return 0;
+    }
+    return Usage();
 }

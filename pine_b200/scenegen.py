@@ -13,18 +13,50 @@ Scenes (sizes are the defaults; tests shrink them):
   Cornell-style box with a ceiling area light; diffuse and GGX conductor materials.
 * ``volume``: an n^3 fractal-noise cloud (about 30% of voxels non-zero, max density 1,
   sigma_a 0.2 + sigma_s 19.8 = sigma_t 20), HG g = 0.8, lit by a directional sun
-  (irradiance 5) plus an environment, camera inside the medium as in pine's cloud scene.
+  (irradiance 5) plus an environment; the camera is attached to the medium as in pine's
+  cloud scene and frames the cloud (about 80% of the pixels see non-zero density).
 
-The environment is ``constant`` (uniform radiance, this library's extension),
-``sky`` (pine's ``Sky``, for scenes that pine itself must render) or ``none``.
+The environment is ``constant`` (uniform radiance, ``Environment{ environment:
+Constant{ color } }``), ``sky`` (pine's ``Sky``) or ``none``.
+
+The grids and meshes come from the ``pine-scenegen`` tool (csrc/scenegen.cpp, built by
+:func:`pine_b200.build.build`), a separate executable, so generating a scene loads no part
+of the renderer library.
 """
 
 from __future__ import annotations
 
-import ctypes
+import json
 import os
+import subprocess
 
 import numpy as np
+
+from . import build as _build
+
+
+def _scenegen(*args) -> dict:
+    exe = _build.SCENEGEN
+    if not os.path.exists(exe):
+        exe = _build.build_scenegen()
+    p = subprocess.run([exe, *[str(a) for a in args]], capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"pine-scenegen {args[0]} failed: {p.stderr.strip()}")
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
+def gen_cloud_volume(path: str, n: int, seed: int = 0, nonzero_fraction: float = 0.3) -> str:
+    """Writes the seeded n^3 fractal-noise cloud (pine's .vol format) to `path`."""
+    _scenegen("cloud", int(n), int(seed), repr(float(nonzero_fraction)), path)
+    return path
+
+
+def gen_icosphere_obj(path: str, subdiv: int, radius=1.2, center=(0.0, 1.6, 0.5),
+                      amplitude=0.1, seed: int = 0) -> int:
+    """Writes the seeded noise-displaced icosphere as OBJ; returns its triangle count."""
+    r = _scenegen("icosphere", int(subdiv), repr(float(radius)), *[repr(float(c)) for c in center],
+                  repr(float(amplitude)), int(seed), path)
+    return int(r["triangles"])
 
 
 def _f(x: float) -> str:
@@ -131,20 +163,15 @@ def cornell_box_obj(path: str, half=3.0, height=6.0) -> str:
     return path
 
 
-def mesh_scene(path: str, lib, *, subdiv=8, width=1920, height=1080, spp=256, max_depth=16,
+def mesh_scene(path: str, *, subdiv=8, width=1920, height=1080, spp=256, max_depth=16,
                seed=0, env="none", env_radiance=0.2, sampler="Halton",
                obj_name=None) -> str:
     d = os.path.dirname(os.path.abspath(path))
     obj = obj_name or f"ico{subdiv}_s{seed}.obj"
     obj_path = os.path.join(d, obj)
     if not os.path.exists(obj_path):
-        ntri = ctypes.c_int64(0)
-        st = lib.pg_gen_icosphere_obj(obj_path.encode(), int(subdiv), ctypes.c_float(1.2),
-                                      ctypes.c_float(0.0), ctypes.c_float(1.6),
-                                      ctypes.c_float(0.5), ctypes.c_float(0.1),
-                                      ctypes.c_uint64(seed), ctypes.byref(ntri))
-        if st != 0:
-            raise RuntimeError(f"pg_gen_icosphere_obj failed with status {st}")
+        gen_icosphere_obj(obj_path + ".tmp", subdiv, seed=seed)
+        os.replace(obj_path + ".tmp", obj_path)
     cornell_box_obj(os.path.join(d, "cornell.obj"))
     rng = np.random.default_rng(seed + 1)
     rough_obj = rng.uniform(0.1, 0.6)
@@ -165,25 +192,19 @@ def mesh_scene(path: str, lib, *, subdiv=8, width=1920, height=1080, spp=256, ma
     return path
 
 
-def volume_scene(path: str, lib, *, n=512, width=1280, height=720, spp=256, max_depth=128,
+def volume_scene(path: str, *, n=512, width=1280, height=720, spp=256, max_depth=128,
                  seed=0, env="constant", env_radiance=0.3, sun_irradiance=5.0,
                  sampler="Uniform", vol_name=None, sigma_a=0.2, sigma_s=19.8, g=0.8) -> str:
     d = os.path.dirname(os.path.abspath(path))
     vol = vol_name or f"cloud{n}_s{seed}.vol"
     vol_path = os.path.join(d, vol)
     if not os.path.exists(vol_path):
-        dens = np.empty(n * n * n, dtype=np.float32)
-        st = lib.pg_gen_cloud_volume(int(n), ctypes.c_uint64(seed), ctypes.c_float(0.3),
-                                     dens.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-        if st != 0:
-            raise RuntimeError(f"pg_gen_cloud_volume failed with status {st}")
-        st = lib.pg_write_volume(vol_path.encode(), n, n, n,
-                                 dens.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-        if st != 0:
-            raise RuntimeError(f"pg_write_volume failed with status {st}")
-        del dens
+        gen_cloud_volume(vol_path + ".tmp", n, seed)
+        os.replace(vol_path + ".tmp", vol_path)
     sun = (-0.4, 0.8, 0.45)
-    out = [_header(max_depth, spp, sampler, width, height, (0.0, 0.05, -1.6),
+    # The camera sits just outside the grid's box and frames the cloud: about 80% of the
+    # pixels of a 16:9 film look through non-zero density.
+    out = [_header(max_depth, spp, sampler, width, height, (0.0, 0.05, -0.8),
                    (0.0, 0.0, 0.0), 0.75, camera_medium="cloud")]
     out.append("Medium cloud: Grid{\n"
                f"    file: {vol}\n    sigma_a: {_f(sigma_a)}\n    sigma_s: {_f(sigma_s)}\n"

@@ -8,6 +8,7 @@ not depend on the generators or on the reference being present.
 
     python tests/golden/make_golden.py           # needs oracle/_ref/pine_ref
     python tests/golden/make_golden.py nodes pine_spheres sampler filtered randomwalk
+    python tests/golden/make_golden.py volume512 mesh_full spheres_c0   # benchmark scenes
 """
 
 from __future__ import annotations
@@ -24,6 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 REF = os.path.join(ROOT, "oracle", "_ref", "pine_ref")
+REF_CONST = os.path.join(ROOT, "oracle", "_ref", "pine_ref_const")
+from oracle import REFERENCE_SRC  # noqa: E402
 
 HIT_DTYPE = np.dtype([("shape", "<i4"), ("tri", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
 
@@ -286,7 +289,7 @@ def randomwalk_case(tmp):
 def shipped_spheres_case(tmp):
     """pine's own scenes/spheres.txt (textures, noise, bump map, two-layer plastic) at a
     tenth of its film size and 512 spp."""
-    src = "/root/reference/scenes/spheres.txt"
+    src = os.path.join(REFERENCE_SRC, "scenes", "spheres.txt")
     text = open(src).read()
     text = text.replace("size: 1280 360", "size: 128 36").replace("samplesPerPixel: 32",
                                                                  "samplesPerPixel: 512")
@@ -295,6 +298,75 @@ def shipped_spheres_case(tmp):
     with open(path, "w") as f:
         f.write(text)
     image_case("pine_spheres", path, [])
+
+
+def sha256(path):
+    import hashlib
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 22), b""):
+            h.update(chunk)
+    return h.hexdigest()
+
+
+def image_case_generated(name, scene, assets, generated, binary=REF):
+    """image_case for scenes whose large assets are too big to store: the fixture keeps the
+    generator's arguments and each file's SHA-256 (`generated`: {file: [args...]}), and
+    tests/conftest.py regenerates and checks them."""
+    d = os.path.dirname(scene)
+    p = subprocess.run([binary, "render", scene, f"{d}/{name}"], capture_output=True, text=True,
+                       cwd=d)
+    if p.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(binary)} render failed: {p.stderr[-2000:]}")
+    info = json.loads(p.stdout.strip().splitlines()[-1])
+    h, w = info["height"], info["width"]
+    mean = np.fromfile(f"{d}/{name}_mean.f64").reshape(h, w, 3)
+    var = np.fromfile(f"{d}/{name}_var.f64").reshape(h, w, 3)
+    cnt = np.fromfile(f"{d}/{name}_count.i64", np.int64).reshape(h, w)
+    gen = {f: {"args": a, "sha256": sha256(os.path.join(d, f))} for f, a in generated.items()}
+    info["reference_binary"] = os.path.basename(binary)
+    np.savez_compressed(f"{HERE}/image_{name}.npz", mean=mean.astype(np.float32),
+                        var=var.astype(np.float32), count=cnt.astype(np.int32),
+                        info=np.array(json.dumps(info)), generated=np.array(json.dumps(gen)),
+                        **pack_scene(scene, assets), allow_pickle=True)
+
+
+def volume512_case(tmp):
+    """The volume benchmark scene itself (512^3 cloud, constant sky 0.3, sun 5, max 128
+    events) at 128 x 72 and 1024 spp, rendered by pine with the added Constant environment
+    (oracle/_ref/pine_ref_const).  The 512 MiB grid is stored as its generator arguments
+    and hash."""
+    from pine_b200 import scenegen
+    vs = scenegen.volume_scene(f"{tmp}/volume512.txt", n=512, width=128, height=72, spp=1024,
+                               env="constant", env_radiance=0.3)
+    image_case_generated("volume512", vs, [], {"cloud512_s0.vol": ["cloud", 512, 0, "0.3"]},
+                         binary=REF_CONST)
+
+
+def mesh_full_case(tmp, spp=16384):
+    """The mesh benchmark scene itself (1,310,720-triangle displaced icosphere in the
+    12-triangle box, max depth 16, independent sampler) at 48 x 27, rendered by pine (its
+    full-sweep SAH build of this mesh takes about 13 minutes on one host thread).  16384 spp
+    bring the Monte Carlo error of the image to about 0.6% (relative L2).  The OBJ is
+    stored as its generator arguments and hash."""
+    from pine_b200 import scenegen
+    ms = scenegen.mesh_scene(f"{tmp}/mesh_full.txt", subdiv=8, width=48, height=27, spp=spp,
+                             max_depth=16, sampler="Uniform")
+    image_case_generated("mesh_full", ms, ["cornell.obj"],
+                         {"ico8_s0.obj": ["icosphere", 8, "1.2", "0.0", "1.6", "0.5", "0.1", 0,
+                                          ]})
+
+
+def spheres_c0_case(tmp, spp=131072):
+    """The spheres benchmark scene itself (64 seeded spheres, plane, rect light, constant
+    environment 0.2, max depth 8, independent sampler) at 48 x 27, rendered by pine with the
+    added Constant environment.  The dielectric spheres' caustics make the image noisy:
+    131072 spp bring its Monte Carlo error to about 0.7% (relative L2)."""
+    from pine_b200 import scenegen
+    sp = scenegen.spheres_scene(f"{tmp}/spheres_c0.txt", width=48, height=27, spp=spp,
+                                max_depth=8, env="constant", env_radiance=0.2,
+                                sampler="Uniform")
+    image_case_generated("spheres_c0", sp, [], {}, binary=REF_CONST)
 
 
 def main():
@@ -313,11 +385,15 @@ def main():
                 randomwalk_case(tmp)
             if "pine_spheres" in only:
                 shipped_spheres_case(tmp)
+            if "volume512" in only:
+                volume512_case(tmp)
+            if "mesh_full" in only:
+                mesh_full_case(tmp)
+            if "spheres_c0" in only:
+                spheres_c0_case(tmp)
         print("fixtures written to", HERE)
         return
-    import pine_b200
     from pine_b200 import scenegen
-    L = pine_b200.lib()
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as tmp:
         math_kat(tmp, rng)
@@ -334,7 +410,7 @@ def main():
         image_case("spheres", sp, [])
 
         # Mesh: 5120-triangle displaced icosphere in the 12-triangle box.
-        ms = scenegen.mesh_scene(f"{tmp}/mesh.txt", L, subdiv=4, width=48, height=27,
+        ms = scenegen.mesh_scene(f"{tmp}/mesh.txt", subdiv=4, width=48, height=27,
                                  spp=512, max_depth=16)
         mesh_assets = ["ico4_s0.obj", "cornell.obj"]
         # Rays from inside the box toward the sphere and walls, and from the camera side.
@@ -344,7 +420,7 @@ def main():
         image_case("mesh", ms, mesh_assets)
 
         # Volume: 32^3 cloud for density lookups, 64^3 for the image.
-        vs = scenegen.volume_scene(f"{tmp}/vol32.txt", L, n=32, width=16, height=9, spp=1,
+        vs = scenegen.volume_scene(f"{tmp}/vol32.txt", n=32, width=16, height=9, spp=1,
                                    env="sky", env_radiance=1.0)
         pts = np.concatenate([rng.uniform(-0.05, 1.05, (3000, 3)),
                               rng.integers(0, 33, (200, 3)) / 32.0]).astype(np.float32)
@@ -353,7 +429,7 @@ def main():
         dens = np.fromfile(f"{tmp}/p.out", np.float32)
         np.savez_compressed(f"{HERE}/density.npz", points=pts, density=dens,
                             **pack_scene(vs, ["cloud32_s0.vol"]), allow_pickle=True)
-        vi = scenegen.volume_scene(f"{tmp}/volume.txt", L, n=64, width=48, height=27,
+        vi = scenegen.volume_scene(f"{tmp}/volume.txt", n=64, width=48, height=27,
                                    spp=1024, env="sky", env_radiance=1.0)
         image_case("volume", vi, ["cloud64_s0.vol"])
         nodes_kat(tmp)

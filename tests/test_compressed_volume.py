@@ -9,6 +9,8 @@ import struct
 import numpy as np
 import pytest
 
+import oracle
+
 
 def _codes(values):
     """Prefix-free codes (Huffman) as pine stores them: the path bits, least significant
@@ -97,27 +99,41 @@ def test_single_value_volume(pglib, tmp_path):
     np.testing.assert_array_equal(got, want.ravel())
 
 
-@pytest.mark.parametrize("damage", ["truncate", "count", "bits"])
+@pytest.mark.parametrize("damage", ["truncate", "count", "bits", "wrapped_vector",
+                                    "wrapped_tree"])
 def test_damaged_files_are_rejected(pglib, tmp_path, damage):
     import pine_b200 as pb
     rng = np.random.default_rng(4)
     write_compressed(tmp_path / "v.compressed", rng.uniform(0, 5, (4, 4, 4)).astype(np.float32),
                      (4, 4, 4))
     raw = bytearray((tmp_path / "v.compressed").read_bytes())
+    tree_bytes = struct.unpack_from("<Q", raw, 12)[0]
     if damage == "truncate":
         raw = raw[:-5]
     elif damage == "count":
         raw[-8:] = struct.pack("<Q", 65)
-    else:
+    elif damage == "bits":
         nb = struct.unpack_from("<I", raw, len(raw) - 12)[0]
         struct.pack_into("<I", raw, len(raw) - 12, nb - 3)
+    elif damage == "wrapped_vector":
+        # A 30-byte encoded section whose vector claims 2^64 - 6 bytes: 24 + that + 12
+        # wraps around to 30.
+        enc = 28 + tree_bytes
+        raw = raw[:enc + 30]
+        struct.pack_into("<Q", raw, 20, 30)
+        struct.pack_into("<QQ", raw, enc, 0, (1 << 64) - 6)
+    else:
+        # A tree size that makes the three section sizes wrap around to the file size.
+        enc_bytes = struct.unpack_from("<Q", raw, 20)[0]
+        struct.pack_into("<Q", raw, 12, (1 << 64) - 8)
+        struct.pack_into("<Q", raw, 20, (len(raw) - 28 + 8 + enc_bytes) - enc_bytes)
     (tmp_path / "v.compressed").write_bytes(bytes(raw))
     with pytest.raises(pb.PgError) as e:
         pb.ParsedScene(_scene(tmp_path, "v.compressed"))
     assert e.value.status == 7  # PG_ERR_PARSE
 
 
-SHIPPED = "/root/reference/scenes/wdas_cloud.compressed"
+SHIPPED = os.path.join(oracle.REFERENCE_SRC, "scenes", "wdas_cloud.compressed")
 
 
 @pytest.mark.skipif(not os.path.exists(SHIPPED), reason="the reference tree is not present")

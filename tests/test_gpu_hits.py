@@ -64,7 +64,7 @@ def test_full_size_mesh_hits(ctx, tmp_path):
     """1.31M-triangle displaced icosphere (20 * 4^8) in the Cornell box, 3000 seeded rays:
     GPU vs exhaustive search."""
     from pine_b200 import scenegen
-    path = scenegen.mesh_scene(str(tmp_path / "mesh.txt"), pb.lib(), subdiv=8, width=64,
+    path = scenegen.mesh_scene(str(tmp_path / "mesh.txt"), subdiv=8, width=64,
                                height=36, spp=1)
     sid = ctx.load_scene(path)
     rng = np.random.default_rng(3)
@@ -113,7 +113,7 @@ def test_gpu_built_bvh_on_the_full_mesh(pglib, tmp_path):
     """The benchmark mesh (about 1.3M triangles): both builders' trees give the same
     closest hits on 65536 random rays, and the GPU build is faster."""
     from pine_b200 import scenegen
-    path = scenegen.mesh_scene(str(tmp_path / "m.txt"), pb.lib(), width=64, height=36, spp=1,
+    path = scenegen.mesh_scene(str(tmp_path / "m.txt"), width=64, height=36, spp=1,
                                sampler="Uniform")
     rng = np.random.default_rng(9)
     o = rng.uniform(-3, 3, (65536, 3))

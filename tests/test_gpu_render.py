@@ -4,10 +4,23 @@ full-size renders.
 Equal-spp agreement (the acceptance test): per-pixel z-scores of the GPU image against
 pine's render, each side with its own per-pixel sample variance, pass |z| < 2.576 (the
 99% two-sided bound) for >= 98% of pixels; relative L2 of the difference must be within
-Monte Carlo error (<= 1.25x what the two variances predict), and below 1% for the volume
-scene at 1024 spp.  `pine_spheres` is the reference's own scenes/spheres.txt (checkerboard,
-noise and 3-D noise textures, a noise bump map, a two-layer plastic) at 128 x 36 and 512
-spp, rendered by pine with its Halton sampler."""
+Monte Carlo error (<= 1.25x what the two variances predict).
+
+The three benchmark scenes are fixtures themselves, at a reduced film with everything
+else as benchmarked: `volume512` (the 512^3 cloud with the constant sky, 1024 spp),
+`mesh_full` (the 1.31M-triangle icosphere, 16384 spp) and `spheres_c0` (64 spheres with
+the constant environment, 131072 spp).  At those sample counts the Monte Carlo error of
+the first two is below 0.7%, and the GPU image must agree with pine's to relative L2 < 1%;
+so must the 64^3 `volume` fixture at 1024 spp.  In the spheres scene pine's near-specular
+dielectrics (roughness 0, so GGX alpha 0.001) give rare samples of 1e9-1e11, and NaN/Inf
+ones that pine drops (32 of its 170M): the pixels such a sample lands in do not converge
+like 1/sqrt(spp), in pine's image or the GPU's.  `spheres_c0` is held to relative
+L2 < 1% over the pixels that no single sample dominates (relative standard error below 5%
+in both images; 3 of pine's 1296 pixels are out).  The other fixtures' noise at their
+sample counts is 2-24% (dielectric caustics, random walks), so they are held to the
+z-score and MC-error bounds only.  `pine_spheres` is the reference's own scenes/spheres.txt
+(checkerboard, noise and 3-D noise textures, a noise bump map, a two-layer plastic) at
+128 x 36 and 512 spp, rendered by pine with its Halton sampler."""
 
 import json
 import os
@@ -34,17 +47,28 @@ def _spp(z):
     return json.loads(str(z["info"]))["spp"]
 
 
+# Fixtures whose Monte Carlo error is below 1% (relative L2 of the image).
+CONVERGED = {"volume", "volume512", "mesh_full"}
+# Fixtures with rare samples so large that a few pixels never converge (see above).
+HEAVY_TAILED = {"spheres_c0"}
+# Independent sampler with a box filter of radius 0.5: every sample lands in its own pixel.
+ONE_PIXEL = {"volume", "volume512", "spheres_c0", "mesh_full"}
+
+
 @pytest.mark.parametrize("name", ["spheres", "mesh", "volume", "pine_spheres", "filtered",
-                                  "randomwalk"])
+                                  "randomwalk", "volume512", "spheres_c0", "mesh_full"])
 @pytest.mark.parametrize("math_mode", ["pine", "fast"])
 def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
     z = golden(f"image_{name}.npz")
     sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
     spp = _spp(z)
     r = ctx.render(sid, spp=spp, seed=17, math_mode=math_mode)
-    assert r["stats"]["dropped"] == 0
-    if name == "volume":  # independent stream, box filter of radius 0.5: one pixel a sample
-        assert (r["count"] == spp).all()
+    dropped = r["stats"]["dropped"]
+    total = spp * r["count"].size
+    # NaN/Inf samples are dropped and not counted (integrator.cpp:156-157), as pine does.
+    assert dropped <= (1e-6 * total if name in HEAVY_TAILED else 0)
+    if name in ONE_PIXEL:
+        assert (r["count"] <= spp).all() and r["count"].sum() == total - dropped
     else:  # Film::AddSample moves a sample that rounding puts on a pixel edge
         assert abs(r["count"].sum() / z["count"].sum() - 1) < 2e-3
     g, gv = r["mean"].astype(np.float64), r["var"].astype(np.float64)
@@ -55,8 +79,18 @@ def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
     rel = np.linalg.norm(g - rm) / np.linalg.norm(rm)
     expected = np.sqrt(np.sum(gv / spp + rv / z["count"][..., None])) / np.linalg.norm(rm)
     assert rel <= 1.25 * expected, (rel, expected)
-    if name == "volume":
-        assert rel < 0.01
+    if name in CONVERGED:
+        assert expected < 0.01 and rel < 0.01, (rel, expected)
+    if name in HEAVY_TAILED:
+        rse_g = np.sqrt(gv / r["count"][..., None]) / np.maximum(np.abs(g), 1e-30)
+        rse_r = np.sqrt(rv / z["count"][..., None]) / np.maximum(np.abs(rm), 1e-30)
+        ok = np.all((rse_g < 0.05) & (rse_r < 0.05), axis=-1)
+        assert ok.mean() > 0.99, ok.mean()
+        d, ref = (g - rm)[ok], rm[ok]
+        rel_ok = np.linalg.norm(d) / np.linalg.norm(ref)
+        exp_ok = np.sqrt(np.sum((gv / r["count"][..., None] + rv / z["count"][..., None])[ok])) / \
+            np.linalg.norm(ref)
+        assert exp_ok < 0.01 and rel_ok < 0.01, (rel_ok, exp_ok, ok.mean())
     ctx.release_scene(sid)
 
 
@@ -120,7 +154,7 @@ def test_full_size_volume_properties(ctx, tmp_path):
     sample, no NaN/Inf, radiance bounded by the brightest light path, and two seeds agree
     within their variance."""
     from pine_b200 import scenegen
-    path = scenegen.volume_scene(str(tmp_path / "v.txt"), pb.lib(), n=512, spp=4)
+    path = scenegen.volume_scene(str(tmp_path / "v.txt"), n=512, spp=4)
     sid = ctx.load_scene(path)
     a = ctx.render(sid, seed=1)
     b = ctx.render(sid, seed=2)

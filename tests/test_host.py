@@ -106,25 +106,38 @@ def test_context_without_gpu_reports_cuda_error(pglib):
     assert e.value.status == 3
 
 
-def test_cloud_generator(pglib):
+def test_cloud_generator(tmp_path):
+    """pine-scenegen's cloud: ~30% of voxels non-zero, max exactly 1, and the same file for
+    the same seed (the benchmark fixtures identify grids by their hash)."""
+    from pine_b200 import scenegen
     n = 48
-    d = np.empty(n ** 3, np.float32)
-    st = pglib.pg_gen_cloud_volume(n, ctypes.c_uint64(7), ctypes.c_float(0.3),
-                                   d.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-    assert st == 0
+    a, b, c = (str(tmp_path / f"{k}.vol") for k in "abc")
+    scenegen.gen_cloud_volume(a, n, seed=7)
+    scenegen.gen_cloud_volume(b, n, seed=7)
+    scenegen.gen_cloud_volume(c, n, seed=8)
+    hdr = np.fromfile(a, np.int32, 3)
+    assert list(hdr) == [n, n, n]
+    d = np.fromfile(a, np.float32)[3:]
+    assert d.size == n ** 3
     assert abs((d > 0).mean() - 0.3) < 0.02 and d.max() == 1.0 and d.min() == 0.0
-    d2 = np.empty_like(d)
-    pglib.pg_gen_cloud_volume(n, ctypes.c_uint64(7), ctypes.c_float(0.3),
-                              d2.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-    assert np.array_equal(d, d2)
+    assert open(a, "rb").read() == open(b, "rb").read()
+    assert open(a, "rb").read() != open(c, "rb").read()
 
 
-def test_icosphere_generator(pglib, tmp_path):
+def test_scenegen_rejects_bad_arguments(tmp_path):
+    from pine_b200 import scenegen
+    with pytest.raises(RuntimeError):
+        scenegen.gen_cloud_volume(str(tmp_path / "x.vol"), 1)
+    with pytest.raises(RuntimeError):
+        scenegen.gen_icosphere_obj(str(tmp_path / "x.obj"), 12)
+    with pytest.raises(RuntimeError):
+        scenegen.gen_cloud_volume(str(tmp_path / "no" / "such" / "dir.vol"), 8)
+
+
+def test_icosphere_generator(tmp_path):
+    from pine_b200 import scenegen
     p = str(tmp_path / "ico.obj")
-    nt = ctypes.c_int64()
-    assert pglib.pg_gen_icosphere_obj(p.encode(), 3, ctypes.c_float(1), ctypes.c_float(0),
-                                      ctypes.c_float(0), ctypes.c_float(0), ctypes.c_float(0.1),
-                                      ctypes.c_uint64(0), ctypes.byref(nt)) == 0
-    assert nt.value == 20 * 4 ** 3
+    nt = scenegen.gen_icosphere_obj(p, 3, radius=1.0, center=(0.0, 0.0, 0.0), amplitude=0.1)
+    assert nt == 20 * 4 ** 3
     text = open(p).read()
     assert "e" not in text.replace("\n", " ").split("f ")[0]  # no exponents anywhere

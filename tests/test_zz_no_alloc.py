@@ -40,9 +40,12 @@ def test_noalloc_matches_pg_render(pglib, tmp_path, name, math, spp):
         for call in range(2):  # two calls in a row reuse the same scratch array
             out.fill_(-1.0)
             torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info(0)[0]
             status, stats = _noalloc(ctx, sid, out, spp, 11, math)
             assert status == 0, ctx._lib.pg_last_error(ctx._ctx)
             torch.cuda.synchronize()
+            if call == 1:  # after the first call: no device memory taken or given back
+                assert torch.cuda.mem_get_info(0)[0] == free_before
             got = out.cpu().numpy()
             assert stats.paths == h * w * spp
             np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-6 * scale,
