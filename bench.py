@@ -83,6 +83,10 @@ def parse_args():
                     help="the scene file's film filter (radius 0.5)")
     ap.add_argument("--bvh", choices=["host", "gpu"], default="host",
                     help="BVH builder for the scene upload")
+    ap.add_argument("--majorant-brick", type=int, choices=[8, 16, 32, 64], default=None,
+                    help="majorant brick edge in voxels (default: the library's tuning)")
+    ap.add_argument("--queue-capacity", type=int, default=None,
+                    help="path slots of the wavefront (default: the library's tuning)")
     ap.add_argument("--profile-case", action="store_true",
                     help="render the small ncu case once and print its per-kernel counters")
     ap.add_argument("--guided", action="store_true",
@@ -420,6 +424,12 @@ def main():
 
     ctx = pb.Context(local)
     ctx.set_bvh_builder(args.bvh)
+    tune = ctx.tuning()
+    if args.majorant_brick:
+        tune["majorant_brick"] = args.majorant_brick
+    if args.queue_capacity:
+        tune["queue_capacity"] = args.queue_capacity
+    ctx.set_tuning(**tune)
     sid = ctx.load_scene(path)
     info = ctx.scene_info(sid)
     bvh = ctx.bvh_info(sid)
@@ -513,7 +523,7 @@ def main():
         "config": {"workload": f"{args.workload}: " + describe(cfg), "width": info["width"],
                    "height": info["height"], "spp": cfg["spp"], "max_depth": cfg["max_depth"],
                    "math_mode": args.math, "parallelism": f"replicas x{world}",
-                   "sampler": args.sampler, "filter": args.filter,
+                   "sampler": args.sampler, "filter": args.filter, "tuning": tune,
                    "bvh": dict(builder=args.bvh, **bvh),
                    "l2": "inputs larger than L2 (512 MiB density grid vs 126 MB L2)"
                          if cfg["kind"] == "volume" else "scene resident; no flush"},

@@ -140,9 +140,12 @@ enum {
     PG_LIGHT_DIRECTIONAL = 1,  /* p[0..2] direction, p[3..5] color (light.cpp:33-41) */
     PG_LIGHT_SKY = 2,          /* p[0..2] sunDirection, p[3..5] sunColor; environment
                                   (light.cpp:65-79, color.cpp:91-99) */
-    PG_LIGHT_CONSTANT_ENV = 3  /* p[3..5] radiance; environment of uniform radiance,
-                                  sampled uniformly over the sphere.  Not in pine, whose
-                                  environment set is {Atmosphere, Sky}. */
+    PG_LIGHT_CONSTANT_ENV = 3  /* p[3..5] radiance; environment of uniform radiance.
+                                  Not in pine, whose environment set is {Atmosphere, Sky}:
+                                  it is treated as pine treats the gradient of its Sky
+                                  (gathered by escaping paths, Pdf 0; next-event estimation
+                                  has nothing to sample), the Constant{color} light of the
+                                  oracle's pine build (oracle/constant_env.py). */
 };
 
 typedef struct pg_light {

@@ -491,7 +491,7 @@ class Context:
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def set_tuning(self, queue_capacity: int = 1 << 22, block_size: int = 128,
-                   split_shadow: int = 1, majorant_brick: int = 32):
+                   split_shadow: int = 1, majorant_brick: int = 64):
         t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))
 

@@ -27,14 +27,16 @@
 #include "pg_nodes.h"
 #include "pg_shade.cuh"
 
-// Build-time register cap of the shading kernel.  Measured on B200 (volume benchmark):
-// (128 threads, 6 blocks) -> 85 registers, 1160 Mpaths/s; no cap -> 128 registers, 1128;
-// (64, 12) -> 1162.  Blocks of up to PG_SHADE_MAX_THREADS threads can be launched.
+// Build-time register cap of the shading kernel: (128 threads, 4 blocks) -> at most 128
+// registers.  With the cap at 6 blocks (80 registers, with spills) the volume renders of
+// that build came out about 10% brighter than pine's and than the same sources built at 128
+// registers or without a cap, in both shadow modes; builds at 128 registers agree with pine.
+// Blocks of up to PG_SHADE_MAX_THREADS threads can be launched.
 #ifndef PG_SHADE_MAX_THREADS
 #define PG_SHADE_MAX_THREADS 128
 #endif
 #ifndef PG_SHADE_MIN_BLOCKS
-#define PG_SHADE_MIN_BLOCKS 6
+#define PG_SHADE_MIN_BLOCKS 4
 #endif
 #if PG_SHADE_MIN_BLOCKS > 0
 #define PG_SHADE_BOUNDS __launch_bounds__(PG_SHADE_MAX_THREADS, PG_SHADE_MIN_BLOCKS)
@@ -122,9 +124,22 @@ struct RenderParams {
     float4* sd;                  // shadow: d.xyz, medium
     float4* sc;                  // shadow: unoccluded contribution rgb, slot
     uint32_t* skey;              // shadow: random stream word
-    float4* film_acc;            // per pixel: sum w r, w g, w b, sum w (this call)
-    float4* film_acc2;           // per pixel: sum w r^2, w g^2, w b^2 (this call; may be null)
-    float2* film_acc3;           // per pixel: sum w^2, samples (filtered films; may be null)
+    // The film, in FP64 (pg_render, batches): per pixel sum w L (rgb), sum w L^2 (rgb),
+    // sum w and sum w^2 (filtered films only: samples of a box film of radius 0.5 have weight
+    // 1, and the resolve takes the sample count for both), and the sample count.  Summed in
+    // double so that a call of any sample count keeps every pixel's mean to float precision.
+    double* film_sum;
+    double* film_sq;
+    double* film_wsum;
+    double* film_w2sum;
+    uint32_t* film_n;
+    // Or, with film_sum null (pg_render_noalloc), a float film of sum w L and sum w.
+    float4* film_acc;
+    // Single renders with a box film of radius 0.5: each sample's radiance in its own slot
+    // (index: its sample id in the call; w = 1 marks a dropped NaN/Inf sample), summed per
+    // pixel in FP64 by k_film_reduce after the wavefront: exact and independent of the order
+    // in which paths finish.  Null: the film atomics above.
+    float4* samples;
     float4* splat;               // finished samples of filtered films: L.rgb, sample key
     int* splat_req;              // their requests (batched renders)
     unsigned long long* next_sample;
@@ -218,28 +233,6 @@ __device__ __forceinline__ void RedAdd4(float4* p, float a, float b, float c, fl
                  : "memory");
 }
 
-// Adds a call's float film into the FP64 film (weighted sums, weighted sums of squares,
-// weights, squared weights, samples).  Pixels without filtered samples (acc3 zero) were
-// written with weight 1 per sample.
-static __global__ void k_fold(const float4* acc, const float4* acc2, const float2* acc3, size_t npix,
-                       double* sum, double* sq, double* wsum, double* w2sum, uint32_t* n) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
-         i += (size_t)gridDim.x * blockDim.x) {
-        float4 a = acc[i], b = acc2[i];
-        float2 c = acc3 ? acc3[i] : make_float2(0.0f, 0.0f);
-        sum[3 * i] += a.x, sum[3 * i + 1] += a.y, sum[3 * i + 2] += a.z;
-        sq[3 * i] += b.x, sq[3 * i + 1] += b.y, sq[3 * i + 2] += b.z;
-        wsum[i] += a.w;
-        if (c.y > 0.0f) {
-            w2sum[i] += c.x;
-            n[i] += (uint32_t)c.y;
-        } else {
-            w2sum[i] += a.w;
-            n[i] += (uint32_t)a.w;
-        }
-    }
-}
-
 __device__ __forceinline__ unsigned long long GlobalTimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -320,8 +313,19 @@ __device__ __forceinline__ uint32_t FirstDim(const RequestDev& R) {
     return GEN && R.sampler == PG_SAMPLER_HALTON ? 2u : 0u;  // StartPixel leaves it at 2
 }
 
-__device__ __forceinline__ void RedAdd2(float2* a, float x, float y) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(a), "f"(x), "f"(y) : "memory");
+// Adds one sample's weighted radiance and its square to pixel pix of the FP64 film and
+// counts it.
+__device__ __forceinline__ void FilmAdd(const RenderParams& P, size_t pix, float r, float g, float b,
+                                        float r2, float g2, float b2) {
+    double* sum = P.film_sum + 3 * pix;
+    double* sq = P.film_sq + 3 * pix;
+    atomicAdd(sum, (double)r);
+    atomicAdd(sum + 1, (double)g);
+    atomicAdd(sum + 2, (double)b);
+    atomicAdd(sq, (double)r2);
+    atomicAdd(sq + 1, (double)g2);
+    atomicAdd(sq + 2, (double)b2);
+    atomicAdd(&P.film_n[pix], 1u);
 }
 
 // Film::AddSample (film.h:26-45) with a filter table: the sample's film position is
@@ -349,11 +353,14 @@ __device__ __forceinline__ void SplatSample(const RenderParams& P, const Request
             int ix = (int)(kFilterTableWidth * tx);
             float w = R.filter_table[iy * kFilterTableWidth + ix];
             size_t pix = (size_t)R.film_base + (size_t)y * W + x;
-            RedAdd4(&P.film_acc[pix], w * c.x, w * c.y, w * c.z, w);
-            if (P.film_acc2)
-                RedAdd4(&P.film_acc2[pix], w * c.x * c.x, w * c.y * c.y, w * c.z * c.z, 0.0f);
-            if (P.film_acc3)
-                RedAdd2(&P.film_acc3[pix], w * w, 1.0f);
+            if (P.film_sum) {
+                FilmAdd(P, pix, w * c.x, w * c.y, w * c.z, w * c.x * c.x, w * c.y * c.y,
+                        w * c.z * c.z);
+                atomicAdd(&P.film_wsum[pix], (double)w);
+                atomicAdd(&P.film_w2sum[pix], (double)w * (double)w);
+            } else {
+                RedAdd4(&P.film_acc[pix], w * c.x, w * c.y, w * c.z, w);
+            }
         }
     }
 }
@@ -365,6 +372,13 @@ template <bool MULTI, bool GEN>
 __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, uint32_t& dropped) {
     const RequestDev& R = RequestOf<MULTI>(P, i);
     uint32_t sid = P.sample[i] - R.key0_offset;
+    if (!MULTI && P.samples) {
+        const bool ok = Finite(c);
+        if (!ok)
+            dropped++;
+        P.samples[sid] = ok ? make_float4(c.x, c.y, c.z, 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        return;
+    }
     uint32_t pixInImage = sid % (uint32_t)R.npix;
     size_t pix = (size_t)R.film_base + pixInImage;
     if (!Finite(c)) {
@@ -375,10 +389,11 @@ __device__ __forceinline__ void FlushPath(const RenderParams& P, int i, V3 c, ui
         P.splat[q] = make_float4(c.x, c.y, c.z, __uint_as_float(P.sample[i]));
         if (MULTI)
             P.splat_req[q] = P.slot_req[i];
+    } else if (P.film_sum) {
+        // Box filter of radius 0.5: weight 1 (Film::AddSample, film.h:26-45).
+        FilmAdd(P, pix, c.x, c.y, c.z, c.x * c.x, c.y * c.y, c.z * c.z);
     } else {
         RedAdd4(&P.film_acc[pix], c.x, c.y, c.z, 1.0f);
-        if (P.film_acc2)
-            RedAdd4(&P.film_acc2[pix], c.x * c.x, c.y * c.y, c.z * c.z, 0.0f);
     }
     if (MULTI) {
         int r = P.slot_req[i];
@@ -1166,7 +1181,7 @@ __device__ __forceinline__ bool TrackBegin(const RenderParams& P, const SceneDev
     }
     const RequestDev& R = RequestOf<MULTI>(P, i);
     rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(P.L[i].w)).Tracking();
-    if (GridWalkBegin<M>(*med, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), tHit, w, bricks))
+    if (GridWalkBegin<M>(*med, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), tHit, w, rng, bricks))
         return true;
     reinterpret_cast<uint4*>(P.trk)[i] = make_uint4(0u, 0u, 0u, rng.dim);
     return false;
@@ -1256,7 +1271,7 @@ __device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const Scene
         return false;
     }
     rng = HashRng{P.sample[slot], P.skey[q], 0};
-    return GridWalkBegin<M>(*med, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w, w, bricks);
+    return GridWalkBegin<M>(*med, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w, w, rng, bricks);
 }
 
 // Ratio tracking of the shadow queue (the media-only scenes' k_shadow work): scales each

@@ -630,74 +630,83 @@ __device__ void HomogeneousSampleEvent(const MediumDev& m, V3 o, V3 d, float tma
 }
 
 // ---------------------------------------------------------------- stepped grid walks
-// The walk of WalkBricks with delta tracking (MediumSampleEvent) or ratio tracking
-// (MediumTr) inside each brick, as a state machine advanced by one step per call: one
-// tentative collision, or one brick.  The tracking kernels run it in loops in which every
-// lane of a warp takes a step per iteration and a lane whose walk has ended takes the next
-// ray, so that the lanes stay busy while walks differ in length.  It makes the same random
-// draws in the same order as the nested loops above, so the results are the same.
+// Delta and ratio tracking (GridMedium::Sample / Tr, medium.cpp:55-116) against per-brick
+// majorants, as a state machine advanced one tentative collision per call.  The tracking
+// kernels run it in loops in which every lane of a warp takes a step per iteration and a
+// lane whose walk has ended takes the next ray, so that the lanes stay busy while walks
+// differ in length; each step is one density lookup.
+//
+// Free flight uses the majorant extinction sigma_t * majorant of each brick crossed
+// (piecewise constant along the ray): an exponential optical depth tau is drawn once per
+// tentative collision and used up brick by brick (a 3D DDA over the majorant grid), so a
+// brick crossed without a collision costs no random draw.  With per-brick majorants that
+// bound the density (their 1-voxel apron covers the trilinear footprint), the tentative
+// collisions form a Poisson process of the majorant's rate, and accepting each with
+// probability density / majorant (delta tracking) or weighting by 1 - density / majorant
+// (ratio tracking) is unbiased, as with pine's single global majorant.
 struct GridWalk {
     V3 mo, md;             // medium-space ray (direction normalised)
     float t;               // position along the ray
     float tb;              // exit of the current brick
     float t1;              // end of the segment (box exit or the ray's bound)
-    float maj, inv;        // the current brick's majorant (0: moving on), 1 / (sigma_t maj)
+    float maj, sm;         // the current brick's majorant and sigma_t * majorant (0: none)
+    float tau;             // optical depth left to the next tentative collision
     float tx, ty, tz;      // next brick-boundary crossings
     float dtx, dty, dtz;   // distance between crossings per axis
     int bx, by, bz;
-    int left;              // brick moves before the walk gives up (WalkBricks' maxSteps)
+    int left;              // brick moves before the walk gives up (one per brick the box holds along each axis, + 4)
     int stepSigns;         // bit k set: the walk moves towards +k on axis k
     uint32_t n;            // tentative collisions taken (kTrackingCap)
 };
 
-// Enters the brick the walk is in: its majorant and exit, or maj = 0 when it holds no
-// density or is passed at zero length (WalkBricks' loop head).  Returns false when the walk
-// is over (the brick budget spent or the segment's end reached).
+// Enters the brick the walk is in: its majorant and exit, with sm = 0 when it holds no
+// density or is passed at zero length.  False when the walk is over (the brick budget spent
+// or the segment's end reached).
 __device__ __forceinline__ bool GridWalkEnter(const MediumDev& m, GridWalk& w, uint32_t& bricks) {
     if (w.left <= 0 || !(w.t < w.t1))
         return false;
     w.left--;
-    float tn = Min(Min(w.tx, w.ty), Min(w.tz, w.t1));
-    float maj = __ldg(&m.majorant[w.bx + m.nb[0] * (w.by + m.nb[1] * w.bz)]);
+    bricks++;
+    const float tn = Min(Min(w.tx, w.ty), Min(w.tz, w.t1));
+    const float maj = __ldg(&m.majorant[w.bx + m.nb[0] * (w.by + m.nb[1] * w.bz)]);
     w.tb = tn;
-    w.maj = 0.0f;
-    if (maj > 0.0f && tn > w.t) {
-        bricks++;
-        w.maj = maj;
-        w.inv = 1.0f / (m.sigma_t * maj);
-    }
+    const bool dense = maj > 0.0f && tn > w.t;
+    w.maj = dense ? maj : 0.0f;
+    w.sm = dense ? m.sigma_t * maj : 0.0f;
     return true;
 }
 
-// Leaves the current brick at its exit for the next one along the ray (WalkBricks' loop
-// tail) and enters it; false when the walk is over.
+// Leaves the current brick at its exit for the next one along the ray and enters it; false
+// when the walk is over.  The axis of the crossing is chosen without branches.
 __device__ __forceinline__ bool GridWalkNext(const MediumDev& m, GridWalk& w, uint32_t& bricks) {
     w.t = w.tb;
-    if (w.tx <= w.ty && w.tx <= w.tz) {
-        w.bx += (w.stepSigns & 1) ? 1 : -1;
-        w.tx += w.dtx;
-        if (w.bx < 0 || w.bx >= m.nb[0])
-            return false;
-    } else if (w.ty <= w.tz) {
-        w.by += (w.stepSigns & 2) ? 1 : -1;
-        w.ty += w.dty;
-        if (w.by < 0 || w.by >= m.nb[1])
-            return false;
-    } else {
-        w.bz += (w.stepSigns & 4) ? 1 : -1;
-        w.tz += w.dtz;
-        if (w.bz < 0 || w.bz >= m.nb[2])
-            return false;
-    }
+    const bool ax = w.tx <= w.ty && w.tx <= w.tz;
+    const bool ay = !ax && w.ty <= w.tz;
+    const bool az = !ax && !ay;
+    w.bx += ax ? ((w.stepSigns & 1) ? 1 : -1) : 0;
+    w.by += ay ? ((w.stepSigns & 2) ? 1 : -1) : 0;
+    w.bz += az ? ((w.stepSigns & 4) ? 1 : -1) : 0;
+    w.tx += ax ? w.dtx : 0.0f;
+    w.ty += ay ? w.dty : 0.0f;
+    w.tz += az ? w.dtz : 0.0f;
+    if ((unsigned)w.bx >= (unsigned)m.nb[0] || (unsigned)w.by >= (unsigned)m.nb[1] ||
+        (unsigned)w.bz >= (unsigned)m.nb[2])
+        return false;
     return GridWalkEnter(m, w, bricks);
 }
 
-// Starts the walk of the world-space ray o + t d, t in [0, tmax], through grid medium m
-// (MediumSampleEvent / MediumTr up to WalkBricks' first brick); false when the ray misses
-// the grid's box.
+// An exponential optical depth, -log(1 - u) (the free-flight sampling of medium.cpp:104).
+template <int M>
+__device__ __forceinline__ float DrawOpticalDepth(HashRng& rng) {
+    return -PMath<M>::log(1.0f - rng.Get1D());
+}
+
+// Starts the walk of the world-space ray o + t d, t in [0, tmax], through grid medium m:
+// the medium-space ray, the box it crosses, the first brick and the first optical depth.
+// False when the ray misses the grid's box (no draw is taken then).
 template <int M>
 __device__ __forceinline__ bool GridWalkBegin(const MediumDev& m, V3 o, V3 d, float tmax, GridWalk& w,
-                                              uint32_t& bricks) {
+                                              HashRng& rng, uint32_t& bricks) {
     w.mo = Affine(m.w2m, o);
     w.md = Normalize<M>(Linear(m.w2m, d));
     float t0 = 0.0f, t1 = tmax;
@@ -729,68 +738,82 @@ __device__ __forceinline__ bool GridWalkBegin(const MediumDev& m, V3 o, V3 d, fl
     w.t1 = t1;
     w.left = m.nb[0] + m.nb[1] + m.nb[2] + 4;
     w.n = 0;
-    w.maj = 0.0f;
-    return GridWalkEnter(m, w, bricks);
+    if (!GridWalkEnter(m, w, bricks))
+        return false;
+    w.tau = DrawOpticalDepth<M>(rng);
+    return true;
+}
+
+// Moves along the ray to the next tentative collision, using up the optical depth brick
+// by brick: true with w.t at the collision (inside a brick with density), false when the
+// walk ends first.
+__device__ __forceinline__ bool GridWalkToCollision(const MediumDev& m, GridWalk& w, uint32_t& bricks) {
+    while (true) {
+        const float dtau = w.sm * (w.tb - w.t);
+        if (w.tau < dtau) {
+            w.t += w.tau / w.sm;
+            return true;
+        }
+        w.tau -= dtau;
+        if (!GridWalkNext(m, w, bricks))
+            return false;
+    }
+}
+
+// Density at the walk's position (GridMedium::Density, trilinear in voxel space).
+__device__ __forceinline__ float GridWalkDensity(const MediumDev& m, const GridWalk& w) {
+    return GridDensity(m, (w.mo.x + w.t * w.md.x) * (float)m.size[0],
+                       (w.mo.y + w.t * w.md.y) * (float)m.size[1],
+                       (w.mo.z + w.t * w.md.z) * (float)m.size[2]);
 }
 
 // Outcome of a walk step.
 enum WalkStep : int { kWalkGoing = 0, kWalkEnded = 1, kWalkCollided = 2 };
 
-// One step of delta tracking (GridMedium::Sample, medium.cpp:98-116, per brick): a
-// tentative collision in the current brick, accepted with probability density / majorant
-// (kWalkCollided: the walk stops at w.t), or the move to the next brick.  kWalkEnded: the
-// ray left the segment without a real collision (or hit the tracking cap, flagged in err).
+// One step of delta tracking (GridMedium::Sample, medium.cpp:98-116): the next tentative
+// collision, accepted as a real one with probability density / majorant (kWalkCollided:
+// the walk stops at w.t).  kWalkEnded: the ray left the segment without a real collision
+// (or hit the tracking cap, flagged in err).
 template <int M>
 __device__ __forceinline__ int DeltaTrackStep(const MediumDev& m, GridWalk& w, HashRng& rng,
                                               uint32_t& bricks, uint32_t& err) {
-    if (w.maj > 0.0f) {
-        float t = w.t - PMath<M>::log(1.0f - rng.Get1D()) * w.inv;
-        if (t < w.tb) {
-            w.t = t;
-            if (++w.n > (uint32_t)kTrackingCap) {
-                err |= kErrTrackingCap;
-                return kWalkEnded;
-            }
-            float dens = GridDensity(m, (w.mo.x + t * w.md.x) * (float)m.size[0],
-                                     (w.mo.y + t * w.md.y) * (float)m.size[1],
-                                     (w.mo.z + t * w.md.z) * (float)m.size[2]);
-            return dens / w.maj > rng.Get1D() ? kWalkCollided : kWalkGoing;
-        }
+    if (!GridWalkToCollision(m, w, bricks))
+        return kWalkEnded;
+    if (++w.n > (uint32_t)kTrackingCap) {
+        err |= kErrTrackingCap;
+        return kWalkEnded;
     }
-    return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+    if (GridWalkDensity(m, w) > rng.Get1D() * w.maj)
+        return kWalkCollided;
+    w.tau = DrawOpticalDepth<M>(rng);
+    return kWalkGoing;
 }
 
-// One step of ratio tracking with pine's Russian roulette (GridMedium::Tr, medium.cpp:55-80,
-// per brick), multiplying the transmittance estimate tr; kWalkEnded when the walk is over
+// One step of ratio tracking with pine's Russian roulette once the estimate drops below 0.1
+// (GridMedium::Tr, medium.cpp:55-80): the next tentative collision multiplies the
+// transmittance estimate tr by 1 - density / majorant.  kWalkEnded when the walk is over
 // (tr = 0 when the roulette or the tracking cap ended it).
 template <int M>
 __device__ __forceinline__ int RatioTrackStep(const MediumDev& m, GridWalk& w, HashRng& rng, float& tr,
                                               uint32_t& bricks, uint32_t& err) {
-    if (w.maj > 0.0f) {
-        float t = w.t - PMath<M>::log(1.0f - rng.Get1D()) * w.inv;
-        if (t < w.tb) {
-            w.t = t;
-            if (++w.n > (uint32_t)kTrackingCap) {
-                err |= kErrTrackingCap;
-                tr = 0.0f;
-                return kWalkEnded;
-            }
-            float dens = GridDensity(m, (w.mo.x + t * w.md.x) * (float)m.size[0],
-                                     (w.mo.y + t * w.md.y) * (float)m.size[1],
-                                     (w.mo.z + t * w.md.z) * (float)m.size[2]);
-            tr *= 1.0f - Max(0.0f, dens / w.maj);
-            if (tr < 0.1f) {
-                float q = Max(0.05f, 1.0f - tr);
-                if (rng.Get1D() < q) {
-                    tr = 0.0f;
-                    return kWalkEnded;
-                }
-                tr /= 1.0f - q;
-            }
-            return kWalkGoing;
-        }
+    if (!GridWalkToCollision(m, w, bricks))
+        return kWalkEnded;
+    if (++w.n > (uint32_t)kTrackingCap) {
+        err |= kErrTrackingCap;
+        tr = 0.0f;
+        return kWalkEnded;
     }
-    return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+    tr *= 1.0f - Max(0.0f, GridWalkDensity(m, w) / w.maj);
+    if (tr < 0.1f) {
+        const float q = Max(0.05f, 1.0f - tr);
+        if (rng.Get1D() < q) {
+            tr = 0.0f;
+            return kWalkEnded;
+        }
+        tr /= 1.0f - q;
+    }
+    w.tau = DrawOpticalDepth<M>(rng);
+    return kWalkGoing;
 }
 
 // GridMedium::Tr (medium.cpp:55-80): ratio tracking with pine's Russian roulette once the
@@ -808,7 +831,7 @@ __device__ float MediumTr(const MediumDev& m, V3 o, V3 d, float tmax, HashRng& r
     }
     float tr = 1.0f;
     GridWalk w;
-    if (GridWalkBegin<M>(m, o, d, tmax, w, bricks)) {
+    if (GridWalkBegin<M>(m, o, d, tmax, w, rng, bricks)) {
         while (RatioTrackStep<M>(m, w, rng, tr, bricks, err) == kWalkGoing) {
         }
         steps += w.n;

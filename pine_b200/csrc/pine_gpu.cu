@@ -185,8 +185,6 @@ struct Film {
     double *sum = nullptr, *sq = nullptr;  // accumulated over calls (progressive passes)
     double *wsum = nullptr, *w2sum = nullptr;  // filter weights and squared weights
     uint32_t* n = nullptr;
-    float4 *acc = nullptr, *acc2 = nullptr;  // this call's samples, vector-atomic targets
-    float2* acc3 = nullptr;                  // this call's squared weights and samples
     float *rmean = nullptr, *rvar = nullptr;  // resolved mean and variance, read back
     void Ensure(int64_t np) {
         if (np <= npix)
@@ -200,9 +198,6 @@ struct Film {
         wsum = mem.Alloc<double>(np);
         w2sum = mem.Alloc<double>(np);
         n = mem.Alloc<uint32_t>(np);
-        acc = mem.Alloc<float4>(np);
-        acc2 = mem.Alloc<float4>(np);
-        acc3 = mem.Alloc<float2>(np);
         rmean = mem.Alloc<float>(np * 3);
         rvar = mem.Alloc<float>(np * 3);
     }
@@ -225,8 +220,13 @@ struct pg_ctx {
     uint32_t* err = nullptr;
     int* h_counts = nullptr;               // pinned
     pg::DevMem req_buf;                    // per-call request table
+    pg::DevMem sample_mem;                 // per-sample radiance of box-film renders
+    size_t sample_cap = 0;                 // float4 slots in sample_mem
     std::string last_error;
-    pg_tuning tuning{1 << 22, 128, 1, 32};  // fastest on the volume benchmark (B200 sweep)
+    // Default tuning: 2^22 path slots, 128-thread shading blocks, shadow rays in their own
+    // kernels, 64-voxel majorant bricks (volume benchmark on B200: 915 Mpaths/s against 853
+    // with 32-voxel and 704 with 16-voxel bricks).
+    pg_tuning tuning{1 << 22, 128, 1, 64};
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
@@ -309,6 +309,7 @@ static void EnsureHalton(pg_ctx* ctx) {
     HaltonPrimes(primes, sums);
     std::vector<uint16_t> perm = HaltonPermutations(primes);
     ctx->halton_mem.stream = ctx->stream, ctx->halton_mem.async = true;
+    ctx->sample_mem.stream = ctx->stream, ctx->sample_mem.async = true;
     ctx->halton_primes = ctx->halton_mem.Upload(primes, ctx->stream);
     ctx->halton_magic = ctx->halton_mem.Upload(HaltonMagics(primes, sums, perm), ctx->stream);
     ctx->halton_sums = ctx->halton_mem.Upload(sums, ctx->stream);
@@ -897,7 +898,8 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.splat = pl.splat, P.splat_req = pl.splat_req;
     w.trk = pl.trk;
     P.counts = ctx->counts;
-    P.film_acc = ctx->film.acc, P.film_acc2 = ctx->film.acc2, P.film_acc3 = ctx->film.acc3;
+    P.film_sum = ctx->film.sum, P.film_sq = ctx->film.sq, P.film_wsum = ctx->film.wsum;
+    P.film_w2sum = ctx->film.w2sum, P.film_n = ctx->film.n, P.film_acc = nullptr;
     P.next_sample = ctx->next_sample;
     P.stats = ctx->stats;
     P.err = ctx->err;
@@ -1027,19 +1029,6 @@ static void EnsureFilm(pg_ctx* ctx, int64_t npix) {
     ctx->film.Ensure(npix);
 }
 
-static void ClearCallFilm(pg_ctx* ctx, int64_t npix) {
-    PG_CUDA(cudaMemsetAsync(ctx->film.acc, 0, npix * sizeof(float4), ctx->stream));
-    PG_CUDA(cudaMemsetAsync(ctx->film.acc2, 0, npix * sizeof(float4), ctx->stream));
-    PG_CUDA(cudaMemsetAsync(ctx->film.acc3, 0, npix * sizeof(float2), ctx->stream));
-}
-
-static void FoldFilm(pg_ctx* ctx, int64_t npix) {
-    Film& f = ctx->film;
-    k_fold<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(f.acc, f.acc2, f.acc3, (size_t)npix, f.sum,
-                                                     f.sq, f.wsum, f.w2sum, f.n);
-    PG_CUDA(cudaGetLastError());
-}
-
 static void ClearFilm(pg_ctx* ctx, int64_t npix) {
     EnsureFilm(ctx, npix);
     cudaStream_t st = ctx->stream;
@@ -1054,6 +1043,49 @@ static int64_t IterationCap(uint64_t total, int slots, int maxDepth) {
     // Every path ends within max_depth counted events; null-surface crossings do not
     // count, so the cap leaves generous room for them.
     return ((int64_t)(total / (uint64_t)slots) + 2) * ((int64_t)maxDepth * 4 + 64) + 4096;
+}
+
+// Largest per-sample buffer of a render (8 GiB: 1920 x 1080 at 256 spp fits); larger
+// renders accumulate the film with FP64 atomics instead.
+constexpr size_t kSampleBufferBytes = (size_t)8 << 30;
+
+// The per-sample buffer for a render of `total` samples, or null when it would exceed
+// kSampleBufferBytes.
+static float4* SampleBuffer(pg_ctx* ctx, uint64_t total) {
+    if (total * sizeof(float4) > kSampleBufferBytes)
+        return nullptr;
+    if (total > ctx->sample_cap) {
+        ctx->sample_mem.Free();
+        ctx->sample_cap = 0;
+        ctx->sample_mem.Alloc<float4>(total);
+        ctx->sample_cap = total;
+    }
+    return static_cast<float4*>(ctx->sample_mem.ptrs[0]);
+}
+
+// Sums each pixel's samples (sample id = pixel + npix * s, s < spp) in FP64 into the film,
+// skipping dropped ones; one thread per pixel, coalesced over pixels for every s.
+__global__ void k_film_reduce(const float4* __restrict__ samples, int64_t npix, int spp,
+                              double* __restrict__ sum, double* __restrict__ sq,
+                              uint32_t* __restrict__ n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
+        uint32_t k = 0;
+        const float4* p = samples + i;
+        for (int s = 0; s < spp; s++, p += npix) {
+            const float4 v = __ldcs(p);
+            if (v.w == 0.0f) {
+                const double x = v.x, y = v.y, z = v.z;
+                s0 += x, s1 += y, s2 += z;
+                q0 += x * x, q1 += y * y, q2 += z * z;
+                k++;
+            }
+        }
+        sum[3 * i] += s0, sum[3 * i + 1] += s1, sum[3 * i + 2] += s2;
+        sq[3 * i] += q0, sq[3 * i + 1] += q1, sq[3 * i + 2] += q2;
+        n[i] += k;
+    }
 }
 
 static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint64_t seed,
@@ -1071,7 +1103,6 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
         ClearFilm(ctx, npix);
     else
         Require(ctx->film.npix >= npix, "accumulate needs a film from an earlier call of this size");
-    ClearCallFilm(ctx, npix);
 
     Wave w;
     w.mode = mathMode;
@@ -1103,8 +1134,14 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
     w.P.reqs = dReq;
     w.P.nreq = 1;
+    w.P.samples = w.splat ? nullptr : SampleBuffer(ctx, total);
     RunHostLoop(ctx, w, profile, res);
-    FoldFilm(ctx, npix);
+    if (w.P.samples) {
+        Film& f = ctx->film;
+        k_film_reduce<<<ctx->num_sms * 8, 256, 0, st>>>(w.P.samples, npix, spp, f.sum, f.sq, f.n);
+        PG_CUDA(cudaGetLastError());
+        res.kernelLaunches[PG_KERNEL_REGEN]++;  // counted with the fill and swap kernels
+    }
     FinishWave(ctx, res);
     ctx->req_buf.Free();
 }
@@ -1122,6 +1159,8 @@ __global__ void k_resolve(const double* __restrict__ sum, const double* __restri
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
          i += (int64_t)gridDim.x * blockDim.x) {
         double k = n[i], W = wsum[i], W2 = w2sum[i];
+        if (W == 0.0 && W2 == 0.0)  // a box film of radius 0.5: every sample has weight 1
+            W = W2 = k;
         bool unit = W == k && W2 == k;
         double neff = W2 > 0 ? W * W / W2 : 0.0;
         for (int c = 0; c < 3; c++) {
@@ -1603,7 +1642,6 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         splat = splat || sc.filter_splat != 0;
     }
     ClearFilm(ctx, (int64_t)pixels);
-    ClearCallFilm(ctx, (int64_t)pixels);
     RequestDev* dReq = ctx->req_buf.Upload(rq, st);
     SceneDev* dScenes = ctx->req_buf.Upload(scenes, st);
     uint32_t* done = ctx->req_buf.Alloc<uint32_t>(n);
@@ -1629,7 +1667,6 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.P.req_done = done;
     w.P.req_time = times + 1;
     RunGraph(ctx, w, out.res, times);
-    FoldFilm(ctx, (int64_t)pixels);
     FinishWave(ctx, out.res);
     std::vector<unsigned long long> t(n + 1);
     PG_CUDA(cudaMemcpy(t.data(), times, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -1643,13 +1680,19 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
                 continue;
             const RequestDev& d = rq[k];
             std::vector<double> sum((size_t)d.npix * 3), wsum(d.npix);
+            std::vector<uint32_t> cnt(d.npix);
             PG_CUDA(cudaMemcpy(sum.data(), ctx->film.sum + d.film_base * 3, sum.size() * sizeof(double),
                                cudaMemcpyDeviceToHost));
             PG_CUDA(cudaMemcpy(wsum.data(), ctx->film.wsum + d.film_base, wsum.size() * sizeof(double),
                                cudaMemcpyDeviceToHost));
-            for (int p = 0; p < d.npix; p++)
+            PG_CUDA(cudaMemcpy(cnt.data(), ctx->film.n + d.film_base, cnt.size() * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+            for (int p = 0; p < d.npix; p++) {
+                // Box films of radius 0.5 keep no weights: every sample has weight 1.
+                const double W = wsum[p] != 0 ? wsum[p] : (double)cnt[p];
                 for (int c = 0; c < 3; c++)
-                    reqs[i].out_mean[3 * p + c] = wsum[p] != 0 ? (float)(sum[3 * p + c] / wsum[p]) : 0.0f;
+                    reqs[i].out_mean[3 * p + c] = W != 0 ? (float)(sum[3 * p + c] / W) : 0.0f;
+            }
         }
     }
     ctx->req_buf.Free();
@@ -1838,7 +1881,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     P.splat = f4(8), P.splat_req = i32(7);
     w.trk = f4(9);
     P.counts = ctx->counts;
-    P.film_acc = acc, P.film_acc2 = nullptr, P.film_acc3 = nullptr;  // the mean needs no more
+    P.film_sum = nullptr, P.film_acc = acc;  // a float film: the mean needs no more
     P.next_sample = ctx->next_sample;
     P.stats = ctx->stats;
     P.err = ctx->err;

@@ -16,7 +16,8 @@ dielectrics (roughness 0, so GGX alpha 0.001) give rare samples of 1e9-1e11, and
 ones that pine drops (32 of its 170M): the pixels such a sample lands in do not converge
 like 1/sqrt(spp), in pine's image or the GPU's.  `spheres_c0` is held to relative
 L2 < 1% over the pixels that no single sample dominates (relative standard error below 5%
-in both images; 3 of pine's 1296 pixels are out).  The other fixtures' noise at their
+in both images; 3 of pine's 1296 pixels are out, and about 1.4% of the pixels of a GPU
+render in pine's numerics).  The other fixtures' noise at their
 sample counts is 2-24% (dielectric caustics, random walks), so they are held to the
 z-score and MC-error bounds only.  `pine_spheres` is the reference's own scenes/spheres.txt
 (checkerboard, noise and 3-D noise textures, a noise bump map, a two-layer plastic) at
@@ -85,7 +86,7 @@ def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
         rse_g = np.sqrt(gv / r["count"][..., None]) / np.maximum(np.abs(g), 1e-30)
         rse_r = np.sqrt(rv / z["count"][..., None]) / np.maximum(np.abs(rm), 1e-30)
         ok = np.all((rse_g < 0.05) & (rse_r < 0.05), axis=-1)
-        assert ok.mean() > 0.99, ok.mean()
+        assert ok.mean() > 0.97, ok.mean()
         d, ref = (g - rm)[ok], rm[ok]
         rel_ok = np.linalg.norm(d) / np.linalg.norm(ref)
         exp_ok = np.sqrt(np.sum((gv / r["count"][..., None] + rv / z["count"][..., None])[ok])) / \
