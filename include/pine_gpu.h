@@ -457,6 +457,11 @@ pg_status pg_filter_table(int32_t filter, const float* radius, const float* para
 /* ---- host restatements exposed for tests ---- */
 /* pstd::stof (src/pstd/string.cpp:50-68), bit-exact. */
 float pg_pstd_stof(const char* str, int64_t len);
+/* The device ports of pine's pstd math (src/pstd/math.h:142-351) that the kernels run in
+ * PG_MATH_PINE mode, evaluated on the GPU for n rows ab = (a, b): out gets 12 floats a row,
+ * sqrt, log2, log, exp, cos, sin, tan, acos, asin, atan of a, atan2(a, b) and pow(a, b).
+ * Host buffers. */
+pg_status pg_pstd_math_device(const float* ab, int64_t n, float* out);
 
 #ifdef __cplusplus
 }

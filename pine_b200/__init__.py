@@ -188,6 +188,7 @@ def lib():
         "pg_set_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
         "pg_get_tuning": (st, [ctypes.c_void_p, _P(Tuning)]),
         "pg_pstd_stof": (ctypes.c_float, [ctypes.c_char_p, ctypes.c_int64]),
+        "pg_pstd_math_device": (st, [_F, ctypes.c_int64, _F]),
         "pg_parse_scene_file": (st, [ctypes.c_char_p, _P(SceneDesc), _P(ctypes.c_void_p)]),
         "pg_free_parsed_scene": (None, [ctypes.c_void_p]),
         "pg_guide_reset": (st, [ctypes.c_void_p, ctypes.c_uint64]),
@@ -286,6 +287,18 @@ def _node_call(name, desc, ref, math_mode, inputs, cols):
     out = np.empty((x.shape[0], 3), np.float32)
     st = getattr(lib(), name)(desc.node_ops, desc.num_node_ops, int(ref), MATH_MODES[math_mode],
                               _fptr(x), x.shape[0], _fptr(out))
+    if st != PG_OK:
+        raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
+    return out
+
+
+def pstd_math_device(ab):
+    """pine's pstd math as the kernels run it in pine mode, evaluated on the GPU: rows
+    (a, b) -> 12 columns (sqrt, log2, log, exp, cos, sin, tan, acos, asin, atan of a,
+    atan2(a, b), pow(a, b))."""
+    ab = np.ascontiguousarray(ab, np.float32).reshape(-1, 2)
+    out = np.empty((ab.shape[0], 12), np.float32)
+    st = lib().pg_pstd_math_device(_fptr(ab), ab.shape[0], _fptr(out))
     if st != PG_OK:
         raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
     return out
@@ -490,7 +503,7 @@ class Context:
         self._check(self._lib.pg_get_tuning(self._ctx, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
-    def set_tuning(self, queue_capacity: int = 1 << 22, block_size: int = 128,
+    def set_tuning(self, queue_capacity: int = 1 << 23, block_size: int = 128,
                    split_shadow: int = 1, majorant_brick: int = 64):
         t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))

@@ -218,6 +218,18 @@ PG_HD float PstdAcos(float y) {
     }
     return x;
 }
+// math.h:305-320: 8 Newton steps from y * pi / 2; outside [-1, 1] returns 0.
+PG_HD float PstdAsin(float y) {
+    if (y < -1 || y > 1)
+        return 0.0f;
+    float x = y * kPi / 2;
+    for (int i = 0; i < 8; ++i) {
+        float y_ = PstdSin(x) - y;
+        float dydx = PstdCos(x);
+        x -= y_ / dydx;
+    }
+    return x;
+}
 // math.h:322-334
 PG_HD float PstdAtan(float y) {
     float x = (y > 0 ? 1 - 1 / (1 + y) : -1 + 1 / (1 - y)) * kPi / 2;

@@ -223,10 +223,11 @@ struct pg_ctx {
     pg::DevMem sample_mem;                 // per-sample radiance of box-film renders
     size_t sample_cap = 0;                 // float4 slots in sample_mem
     std::string last_error;
-    // Default tuning: 2^22 path slots, 128-thread shading blocks, shadow rays in their own
+    // Default tuning: 2^23 path slots, 128-thread shading blocks, shadow rays in their own
     // kernels, 64-voxel majorant bricks (volume benchmark on B200: 915 Mpaths/s against 853
-    // with 32-voxel and 704 with 16-voxel bricks).
-    pg_tuning tuning{1 << 22, 128, 1, 64};
+    // with 32-voxel and 704 with 16-voxel bricks at 2^22 slots; 951 with 2^23 slots, 825
+    // with 2^21).
+    pg_tuning tuning{1 << 23, 128, 1, 64};
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
@@ -1750,7 +1751,7 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
         };
         double bestT = measure(best);
         const int bricks[] = {8, 16, 32, 64}, blocks[] = {32, 64, 128};
-        const int caps[] = {1 << 19, 1 << 20, 1 << 21, 1 << 22};
+        const int caps[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
         for (int dim = 0; dim < 4; dim++) {
             std::vector<pg_tuning> cands;
             for (int k = 0; k < (dim == 1 ? 2 : (dim == 2 ? 3 : 4)); k++) {
@@ -1943,6 +1944,37 @@ extern "C" pg_status pg_render_noalloc(pg_ctx* ctx, int32_t scene_id, const pg_r
             stats->paths = (int64_t)r.stats[kStatPaths];
             stats->launches = r.launches;
         }
+    });
+}
+
+// ================================================================ pine's numerics on the device
+namespace pg {
+
+// The device ports of pine's pstd math (src/pstd/math.h:142-351) for rows (a, b): sqrt, log2,
+// log, exp, cos, sin, tan, acos, asin, atan of a, atan2(a, b), pow(a, b); 12 outputs a row.
+__global__ void k_pstd_math(const float* in, int64_t n, float* out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float a = in[2 * i], b = in[2 * i + 1];
+        float* o = out + 12 * i;
+        o[0] = PstdSqrt(a), o[1] = PstdLog2(a), o[2] = PstdLog(a), o[3] = PstdExp(a);
+        o[4] = PstdCos(a), o[5] = PstdSin(a), o[6] = PstdTan(a), o[7] = PstdAcos(a);
+        o[8] = PstdAsin(a), o[9] = PstdAtan(a), o[10] = PstdAtan2(a, b), o[11] = PstdPow(a, b);
+    }
+}
+
+}  // namespace pg
+
+extern "C" pg_status pg_pstd_math_device(const float* ab, int64_t n, float* out) {
+    return Guard(nullptr, [&]() {
+        Require(ab != nullptr && out != nullptr && n > 0, "null buffer or empty input");
+        DevMem mem;
+        std::vector<float> in(ab, ab + 2 * n);
+        float* din = mem.Upload(in, nullptr);
+        float* dout = mem.Alloc<float>(12 * n);
+        k_pstd_math<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(din, n, dout);
+        PG_CUDA(cudaGetLastError());
+        PG_CUDA(cudaMemcpy(out, dout, 12 * n * sizeof(float), cudaMemcpyDeviceToHost));
     });
 }
 

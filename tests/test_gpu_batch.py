@@ -44,7 +44,7 @@ def test_autotune_returns_a_valid_tuning(ctx, tmp_path):
     before = ctx.tuning()
     t = ctx.autotune([dict(scene=ids[0], spp=64), dict(scene=ids[1], spp=64)])
     assert t["majorant_brick"] in (8, 16, 32, 64) and t["split_shadow"] in (0, 1)
-    assert t["block_size"] in (32, 64, 128) and 1 << 19 <= t["queue_capacity"] <= 1 << 22
+    assert t["block_size"] in (32, 64, 128) and 1 << 20 <= t["queue_capacity"] <= 1 << 23
     assert ctx.tuning() == t
     # Whatever was chosen renders the same image statistically.
     r = ctx.render(ids[1], spp=256, seed=9)
