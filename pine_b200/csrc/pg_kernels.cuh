@@ -835,8 +835,10 @@ __device__ __forceinline__ void PushGuide(const RenderParams& P, int slot, V3 p,
 }
 
 // MEDIA = false compiles the shading of scenes without participating media: the medium
-// code drops out, which frees registers for more resident warps.
-template <int M, bool FUSED, bool GUIDE, bool MEDIA, bool GEN>
+// code drops out, which frees registers for more resident warps.  SURF = false compiles
+// that of scenes of media alone (no surfaces: every ray leaves the medium or scatters in
+// it), without the surface and material code.
+template <int M, bool FUSED, bool GUIDE, bool MEDIA, bool GEN, bool SURF = true>
 __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const RequestDev& R, int i,
                          uint2* stack, ShadeCounters& ct, PendingShadow& ps, bool& finished,
                          V3& Lout, bool& deferred) {
@@ -850,8 +852,9 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             P.rec[kRecordStride * r + 4] = make_float4(Lw.x, Lw.y, Lw.z, 0.0f);
     }
     // Scenes without surfaces skip k_trace: every ray misses.
-    float4 h = (S.has_bvh || S.num_planes) ? P.hit[i]
-                                           : make_float4(kFloatMax, __int_as_float(-1), 0.0f, 0.0f);
+    float4 h = (SURF && (S.has_bvh || S.num_planes))
+                   ? P.hit[i]
+                   : make_float4(kFloatMax, __int_as_float(-1), 0.0f, 0.0f);
     V3 o = v3(ro.x, ro.y, ro.z), d = v3(rd.x, rd.y, rd.z);
     float bsdfPdf = ro.w;
     int medium = __float_as_int(rd.w);
@@ -863,7 +866,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     const bool walk = GEN && R.random_walk;
     Rng rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(Lw.w));
     int prim = __float_as_int(h.y);
-    bool found = prim != -1;
+    bool found = SURF && prim != -1;
     float tHit = found ? h.x : kFloatMax;
     finished = false;
     V3 no = o, nd = d;
@@ -1020,7 +1023,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
     }
 }
 
-template <int M, bool MULTI, bool FUSED, bool GUIDE, bool MEDIA, bool GEN>
+template <int M, bool MULTI, bool FUSED, bool GUIDE, bool MEDIA, bool GEN, bool SURF = true>
 __global__ void PG_SHADE_BOUNDS k_shade(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];
     __shared__ BlockQueues<1> q1;
@@ -1038,7 +1041,7 @@ __global__ void PG_SHADE_BOUNDS k_shade(const __grid_constant__ RenderParams P, 
         V3 L;
         bool deferred = false;
         if (live)
-            ShadeOne<M, FUSED, GUIDE, MEDIA, GEN>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
+            ShadeOne<M, FUSED, GUIDE, MEDIA, GEN, SURF>(P, SceneOf<MULTI>(P, S0, i), RequestOf<MULTI>(P, i), i,
                                       stack + threadIdx.x, ct, ps, finished, L, deferred);
         // A path that ends here with no shadow ray in flight is flushed now and its slot
         // takes the next camera sample; one with a shadow ray pending ends in k_shadow.

@@ -133,6 +133,9 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
         if (!FUSED && !w.media)
             k_shade<M, MULTI, false, false, false, GEN>
                 <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(P, w.S0);
+        else if (!FUSED && !w.surfaces)  // media alone: no surface or material code
+            k_shade<M, MULTI, false, false, true, GEN, false>
+                <<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, 0, st>>>(P, w.S0);
         else
             k_shade<M, MULTI, FUSED, false, true, GEN><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(P, w.S0);
     });

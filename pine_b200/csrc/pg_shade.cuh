@@ -704,13 +704,49 @@ __device__ __forceinline__ float DrawOpticalDepth(HashRng& rng) {
 // Starts the walk of the world-space ray o + t d, t in [0, tmax], through grid medium m:
 // the medium-space ray, the box it crosses, the first brick and the first optical depth.
 // False when the ray misses the grid's box (no draw is taken then).
+// AABB::Hit against the unit cube (geometry.cpp:67-87), as UnitBoxHit, with the inverse
+// direction given (zero components: inverse 0, the slab then only checks the origin).
+__device__ __forceinline__ bool UnitBoxHitInv(V3 o, V3 d, V3 inv, float& tmin, float& tmax) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const float oi = Comp(o, i), di = Comp(d, i), ii = Comp(inv, i);
+        float tn, tf;
+        if (di != 0.0f) {
+            tn = (0.0f - oi) * ii, tf = (1.0f - oi) * ii;
+            if (di < 0.0f) {
+                const float tmp = tn;
+                tn = tf;
+                tf = tmp;
+            }
+        } else {  // parallel to the slab: inside it or not
+            const bool in = oi >= 0.0f && oi <= 1.0f;
+            tn = in ? -kFloatMax : kFloatMax;
+            tf = in ? kFloatMax : -kFloatMax;
+        }
+        tmin = tn > tmin ? tn : tmin;
+        tmax = tf < tmax ? tf : tmax;
+        if (tmin > tmax)
+            return false;
+    }
+    return true;
+}
+
 template <int M>
 __device__ __forceinline__ bool GridWalkBegin(const MediumDev& m, V3 o, V3 d, float tmax, GridWalk& w,
                                               HashRng& rng, uint32_t& bricks) {
+    // The walk's geometry needs no correctly rounded division: the medium-space direction
+    // is normalised with a reciprocal square root and the slab and DDA distances use one
+    // approximate reciprocal per axis (about 2 ulp), shared by the box test and the DDA.
     w.mo = Affine(m.w2m, o);
-    w.md = Normalize<M>(Linear(m.w2m, d));
+    const V3 ld = Linear(m.w2m, d);
+    w.md = ld * rsqrtf(Dot(ld, ld));
+    if (!FiniteRay(w.mo, w.md))
+        return false;
+    const V3 inv = v3(w.md.x != 0.0f ? __fdividef(1.0f, w.md.x) : 0.0f,
+                      w.md.y != 0.0f ? __fdividef(1.0f, w.md.y) : 0.0f,
+                      w.md.z != 0.0f ? __fdividef(1.0f, w.md.z) : 0.0f);
     float t0 = 0.0f, t1 = tmax;
-    if (!FiniteRay(w.mo, w.md) || !UnitBoxHit(w.mo, w.md, t0, t1))
+    if (!(t0 <= t1) || !UnitBoxHitInv(w.mo, w.md, inv, t0, t1))
         return false;
     float sx = (float)m.size[0], sy = (float)m.size[1], sz = (float)m.size[2];
     V3 vo = v3(w.mo.x * sx, w.mo.y * sy, w.mo.z * sz), vd = v3(w.md.x * sx, w.md.y * sy, w.md.z * sz);
@@ -720,8 +756,8 @@ __device__ __forceinline__ bool GridWalkBegin(const MediumDev& m, V3 o, V3 d, fl
     w.by = min(max((int)floorf(py * inb), 0), m.nb[1] - 1);
     w.bz = min(max((int)floorf(pz * inb), 0), m.nb[2] - 1);
     w.stepSigns = (vd.x > 0.0f ? 1 : 0) | (vd.y > 0.0f ? 2 : 0) | (vd.z > 0.0f ? 4 : 0);
-    float inx = vd.x != 0.0f ? 1.0f / vd.x : 0.0f, iny = vd.y != 0.0f ? 1.0f / vd.y : 0.0f,
-          inz = vd.z != 0.0f ? 1.0f / vd.z : 0.0f;
+    // 1 / (md * size) per axis.
+    const float inx = __fdividef(inv.x, sx), iny = __fdividef(inv.y, sy), inz = __fdividef(inv.z, sz);
     auto nextT = [&](int b, bool pos, float vo_, float in) {
         if (in == 0.0f)
             return kFloatMax;
@@ -751,7 +787,7 @@ __device__ __forceinline__ bool GridWalkToCollision(const MediumDev& m, GridWalk
     while (true) {
         const float dtau = w.sm * (w.tb - w.t);
         if (w.tau < dtau) {
-            w.t += w.tau / w.sm;
+            w.t += __fdividef(w.tau, w.sm);
             return true;
         }
         w.tau -= dtau;
@@ -803,7 +839,7 @@ __device__ __forceinline__ int RatioTrackStep(const MediumDev& m, GridWalk& w, H
         tr = 0.0f;
         return kWalkEnded;
     }
-    tr *= 1.0f - Max(0.0f, GridWalkDensity(m, w) / w.maj);
+    tr *= 1.0f - Max(0.0f, __fdividef(GridWalkDensity(m, w), w.maj));
     if (tr < 0.1f) {
         const float q = Max(0.05f, 1.0f - tr);
         if (rng.Get1D() < q) {
