@@ -55,12 +55,13 @@ WORKLOADS = {
     "spheres": dict(kind="spheres", width=640, height=360, spp=64, max_depth=8),
     "mesh": dict(kind="mesh", width=1920, height=1080, spp=256, max_depth=16, subdiv=8),
 }
-# ncu cases (--profile-case): each workload's scene with one sample per pixel (the 512^3
-# grid and the 1.31M-triangle mesh are larger than L2 either way).
+# ncu cases (--profile-case): each workload's scene, full film, one sample per pixel (the
+# 512^3 grid and the 1.31M-triangle mesh are larger than L2 either way; at 1920x1080 the
+# mesh's traversal launches are full queues of 2M rays, under 1 GB on the device).
 PROFILE_CASES = {
     "volume": dict(WORKLOADS["volume"], spp=1),
     "spheres": dict(WORKLOADS["spheres"], spp=1),
-    "mesh": dict(WORKLOADS["mesh"], width=480, height=270, spp=1),
+    "mesh": dict(WORKLOADS["mesh"], spp=1),
 }
 
 
