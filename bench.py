@@ -88,6 +88,9 @@ def parse_args():
                     help="majorant brick edge in voxels (default: the library's tuning)")
     ap.add_argument("--queue-capacity", type=int, default=None,
                     help="path slots of the wavefront (default: the library's tuning)")
+    ap.add_argument("--sort-queue", type=int, choices=[0, 1], default=None,
+                    help="order the active list by medium cell before tracking (default: "
+                         "the library's tuning)")
     ap.add_argument("--profile-case", action="store_true",
                     help="render the small ncu case once and print its per-kernel counters")
     ap.add_argument("--guided", action="store_true",
@@ -365,6 +368,19 @@ def reference_arm(args, cfg, rank):
 
 
 # ---------------------------------------------------------------- our arm
+def apply_tuning(ctx, args):
+    """The library's tuning with the command line's overrides."""
+    tune = ctx.tuning()
+    if args.majorant_brick:
+        tune["majorant_brick"] = args.majorant_brick
+    if args.queue_capacity:
+        tune["queue_capacity"] = args.queue_capacity
+    if args.sort_queue is not None:
+        tune["sort_queue"] = args.sort_queue
+    ctx.set_tuning(**tune)
+    return tune
+
+
 def main():
     args = parse_args()
     SCENE_OPTS["sampler"], SCENE_OPTS["filter"] = args.sampler, args.filter
@@ -406,6 +422,7 @@ def main():
         case = PROFILE_CASES[args.workload]
         path = scene_path(case, args.cache, env)
         ctx = pb.Context(local)
+        apply_tuning(ctx, args)
         sid = ctx.load_scene(path)
         if args.guided:
             ctx.guide_reset(seed=0)
@@ -425,12 +442,7 @@ def main():
 
     ctx = pb.Context(local)
     ctx.set_bvh_builder(args.bvh)
-    tune = ctx.tuning()
-    if args.majorant_brick:
-        tune["majorant_brick"] = args.majorant_brick
-    if args.queue_capacity:
-        tune["queue_capacity"] = args.queue_capacity
-    ctx.set_tuning(**tune)
+    tune = apply_tuning(ctx, args)
     sid = ctx.load_scene(path)
     info = ctx.scene_info(sid)
     bvh = ctx.bvh_info(sid)

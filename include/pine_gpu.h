@@ -259,10 +259,12 @@ typedef struct pg_render_desc {
  * inference and guided direction sampling) and TRAIN (gradient and Adam between passes)
  * run only in guided renders.  TRACK (delta tracking of the extension rays through grid
  * media) runs in scenes with media; TRANSMIT (ratio tracking of the shadow rays) in scenes
- * with media and no surfaces, when shadow rays have their own kernel. */
+ * with media and no surfaces, when shadow rays have their own kernel.  SORT (the
+ * active list ordered by the grid-medium cell of each ray's origin) runs in scenes with grid
+ * media when the tuning's sort_queue is set. */
 enum { PG_KERNEL_REGEN = 0, PG_KERNEL_TRACE = 1, PG_KERNEL_SHADE = 2, PG_KERNEL_SHADOW = 3,
        PG_KERNEL_GUIDE = 4, PG_KERNEL_TRAIN = 5, PG_KERNEL_TRACK = 6, PG_KERNEL_TRANSMIT = 7,
-       PG_NUM_KERNELS = 8 };
+       PG_KERNEL_SORT = 8, PG_NUM_KERNELS = 9 };
 
 typedef struct pg_kernel_stats {
     int64_t launches;
@@ -379,6 +381,9 @@ typedef struct pg_tuning {
                                shading kernel */
     int32_t majorant_brick; /* voxels per edge of a grid medium's majorant brick: 8, 16, 32
                                or 64 */
+    int32_t sort_queue;     /* 1: in scenes with grid media, order each iteration's active
+                               list by the cell of the ray origins (8^3 cells per medium
+                               box) before the tracking kernels; 0: queue order */
 } pg_tuning;
 
 pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,

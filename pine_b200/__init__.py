@@ -39,7 +39,7 @@ class RenderDesc(ctypes.Structure):
                 ("accumulate", ctypes.c_int32), ("profile", ctypes.c_int32)]
 
 
-KERNELS = ["regen", "trace", "shade", "shadow", "guide", "train", "track", "transmit"]
+KERNELS = ["regen", "trace", "shade", "shadow", "guide", "train", "track", "transmit", "sort"]
 
 
 class KernelStats(ctypes.Structure):
@@ -129,7 +129,8 @@ SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
 
 class Tuning(ctypes.Structure):
     _fields_ = [("queue_capacity", ctypes.c_int32), ("block_size", ctypes.c_int32),
-                ("split_shadow", ctypes.c_int32), ("majorant_brick", ctypes.c_int32)]
+                ("split_shadow", ctypes.c_int32), ("majorant_brick", ctypes.c_int32),
+                ("sort_queue", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):
@@ -504,8 +505,9 @@ class Context:
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def set_tuning(self, queue_capacity: int = 1 << 23, block_size: int = 128,
-                   split_shadow: int = 1, majorant_brick: int = 64):
-        t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick))
+                   split_shadow: int = 1, majorant_brick: int = 64, sort_queue: int = 0):
+        t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick),
+                   int(sort_queue))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))
 
     @staticmethod

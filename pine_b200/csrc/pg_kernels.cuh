@@ -59,7 +59,7 @@ enum StatIndex {
     kStatShadowItems, kStatShadowSteps, kStatShadowBricks,
     kStatTraceItems, kStatRegenItems, kStatIterations, kStatGuided, kStatRecords,
     kStatTrainRows, kStatTrackItems, kStatTrackSteps, kStatTrackBricks, kStatTransmitItems,
-    kStatTransmitSteps, kStatTransmitBricks, kNumStats = 22
+    kStatTransmitSteps, kStatTransmitBricks, kStatSortItems, kNumStats = 23
 };
 
 enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlotDead = 3 };
@@ -67,7 +67,7 @@ enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlot
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
                   kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kCntTrackNext = 9,
-                  kCntTransmitNext = 10, kNumCounts = 11 };
+                  kCntTransmitNext = 10, kCntSorted = 11, kNumCounts = 12 };
 
 // k_track's result per slot (RenderParams::trk): the scattering position (world space) and,
 // in w, the tracking stream's next dimension with kTrackScattered set when the walk ended in
@@ -148,6 +148,12 @@ struct RenderParams {
     unsigned long long* req_time;  // globaltimer (ns) at each request's completion
     uint32_t* err;
     float4* trk;                 // k_track's result per slot (scenes with media)
+    // Queue sorting (scenes with grid media, k_sort_keys / k_sort_scatter): the active list
+    // reordered by the cell of each ray's origin, the entries' keys, and kSortBins counts,
+    // kSortBins cursors and a block counter (null: no sorting).
+    int* sorted;
+    uint16_t* sort_keys;
+    int* sort_bins;
     int transmitted;             // 1: k_transmit scaled sc by each shadow ray's transmittance
     int max_iter;
     int use_cond;                // k_swap sets the graph while-condition
@@ -239,8 +245,14 @@ __device__ __forceinline__ unsigned long long GlobalTimer() {
     return t;
 }
 
-__device__ __forceinline__ int* ActiveList(const RenderParams& P) {
+// The active list as the previous iteration queued it.
+__device__ __forceinline__ int* QueuedList(const RenderParams& P) {
     return P.lists + (size_t)(P.counts[kCntParity] & 1) * P.slots;
+}
+// The active list this iteration's kernels take their entries from: the queued list, or its
+// sorted copy once k_sort_keys has marked the queue sorted.
+__device__ __forceinline__ int* ActiveList(const RenderParams& P) {
+    return P.counts[kCntSorted] ? P.sorted : QueuedList(P);
 }
 __device__ __forceinline__ int* NextList(const RenderParams& P) {
     return P.lists + (size_t)((P.counts[kCntParity] + 1) & 1) * P.slots;
@@ -530,6 +542,7 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     c[kCntSplat] = 0;
     c[kCntTrackNext] = 0;
     c[kCntTransmitNext] = 0;
+    c[kCntSorted] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
     bool more = active > 0;
@@ -1144,13 +1157,161 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
     }
 }
 
+// ---------------------------------------------------------------- queue sorting
+// In scenes with grid media the active list is reordered at the start of each iteration
+// by the cell of each ray's origin in an 8 x 8 x 8 grid over its medium's box, in Morton
+// order (a counting sort: k_sort_keys counts, k_sort_scatter places).  The kernels take
+// queue entries in order, so the walks in flight at any moment start in a few neighbouring
+// cells: their density lookups share lines in L1 and stay in L2 instead of spreading over
+// the whole grid.  Nothing else depends on the order: a path's random streams follow its
+// sample, not its queue position, and the film is summed per sample.
+constexpr int kSortCells = 512;              // 8^3 cells of a grid medium's box
+constexpr int kSortBins = kSortCells + 1;    // + one bin for rays outside grid media
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;                // entries per thread and chunk in k_sort_scatter
+constexpr int kSortMinQueue = 1 << 16;       // shorter queues are left in queue order
+
+__device__ __forceinline__ uint32_t Spread3(uint32_t v) {
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+
+// The sort key of slot i: the Morton index of the cell of its ray origin in its grid
+// medium's unit box (origins outside the box go to the nearest cell), else kSortCells.
+template <bool MULTI>
+__device__ __forceinline__ int SortKey(const RenderParams& P, const SceneDev& S0, int i) {
+    const int medium = __float_as_int(P.ray_d[i].w);
+    if (medium < 0)
+        return kSortCells;
+    const MediumDev& m = SceneOf<MULTI>(P, S0, i).media[medium];
+    if (m.type != PG_MEDIUM_GRID)
+        return kSortCells;
+    const float4 ro = P.ray_o[i];
+    const V3 mo = Affine(m.w2m, v3(ro.x, ro.y, ro.z));
+    // Float-to-int conversion saturates (NaN gives 0), so the clamps bound every origin.
+    const int cx = min(max(__float2int_rd(mo.x * 8.0f), 0), 7);
+    const int cy = min(max(__float2int_rd(mo.y * 8.0f), 0), 7);
+    const int cz = min(max(__float2int_rd(mo.z * 8.0f), 0), 7);
+    return (int)(Spread3(cx) | (Spread3(cy) << 1) | (Spread3(cz) << 2));
+}
+
+// Counts the queued entries per key (and stores each entry's key).  The last block to
+// finish turns the counts into cursors (exclusive prefix sums), clears the counts and its
+// block counter for the next iteration, and marks the queue sorted.  Queues shorter than
+// kSortMinQueue are left as they are.
+template <bool MULTI>
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_keys(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    __shared__ int hist[kSortBins];
+    __shared__ int warpSums[kSortThreads / 32];
+    __shared__ bool lastBlock;
+    const int n = P.counts[kCntActive];
+    if (n < kSortMinQueue)
+        return;
+    int* bins = P.sort_bins;
+    for (int b = threadIdx.x; b < kSortBins; b += blockDim.x)
+        hist[b] = 0;
+    __syncthreads();
+    const int* src = QueuedList(P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int key = SortKey<MULTI>(P, S0, src[q]);
+        P.sort_keys[q] = (uint16_t)key;
+        atomicAdd(&hist[key], 1);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kSortBins; b += blockDim.x)
+        if (hist[b])
+            atomicAdd(&bins[b], hist[b]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        lastBlock = atomicAdd(&bins[2 * kSortBins], 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!lastBlock)
+        return;
+    __threadfence();
+    // Exclusive scan of the kSortBins counts: kPer consecutive bins per thread, then a scan
+    // of the threads' totals.
+    constexpr int kPer = (kSortBins + kSortThreads - 1) / kSortThreads;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int v[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const int b = t * kPer + k;
+        v[k] = b < kSortBins ? __ldcg(&bins[b]) : 0;
+        sum += v[k];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d)
+            incl += u;
+    }
+    if (lane == 31)
+        warpSums[warp] = incl;
+    __syncthreads();
+    int before = incl - sum;
+    for (int w = 0; w < warp; w++)
+        before += warpSums[w];
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const int b = t * kPer + k;
+        if (b < kSortBins) {
+            bins[kSortBins + b] = before;
+            bins[b] = 0;
+        }
+        before += v[k];
+    }
+    if (t == 0) {
+        bins[2 * kSortBins] = 0;
+        P.counts[kCntSorted] = 1;
+        P.stats[kStatSortItems] += (unsigned long long)n;
+    }
+}
+
+// Places each queued entry at its key's cursor: per chunk of kSortThreads * kSortItems
+// entries, ranks within the chunk from shared-memory counters and one global reservation per
+// key present in the chunk.  The sorted list is a permutation of the queued one.
+static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const __grid_constant__ RenderParams P) {
+    __shared__ int cnt[kSortBins];
+    __shared__ int base[kSortBins];
+    if (!P.counts[kCntSorted])
+        return;
+    const int n = P.counts[kCntActive];
+    const int* src = QueuedList(P);
+    int* cursor = P.sort_bins + kSortBins;
+    constexpr int kChunk = kSortThreads * kSortItems;
+    for (int c0 = blockIdx.x * kChunk; c0 < n; c0 += gridDim.x * kChunk) {
+        for (int b = threadIdx.x; b < kSortBins; b += blockDim.x)
+            cnt[b] = 0;
+        __syncthreads();
+        int key[kSortItems], rank[kSortItems], slot[kSortItems];
+#pragma unroll
+        for (int k = 0; k < kSortItems; k++) {
+            const int q = c0 + k * kSortThreads + (int)threadIdx.x;
+            key[k] = q < n ? (int)P.sort_keys[q] : -1;
+            slot[k] = q < n ? src[q] : 0;
+            rank[k] = key[k] >= 0 ? atomicAdd(&cnt[key[k]], 1) : 0;
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b < kSortBins; b += blockDim.x)
+            base[b] = cnt[b] ? atomicAdd(&cursor[b], cnt[b]) : 0;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kSortItems; k++)
+            if (key[k] >= 0)
+                P.sorted[base[key[k]] + rank[k]] = slot[k];
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- tracking kernels
 // Delta tracking of the extension rays (k_track) and ratio tracking of the shadow rays
 // (k_transmit) run in persistent warps: each lane walks one ray through the majorant bricks
 // a step at a time (GridWalk), and a warp takes new queue entries for its idle lanes once
 // kRefillLanes of them are idle (or all are), with one atomic on the queue's work counter.
 // A long walk then holds up one lane instead of its whole warp, and every iteration of the
-// loop is one short step with one memory lookup.
+// loop is one short action per lane: a brick crossing or a density lookup.
 #ifndef PG_REFILL_LANES
 #define PG_REFILL_LANES 8
 #endif
@@ -1227,7 +1388,7 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
             continue;
         }
         if (slot >= 0) {
-            const int r = DeltaTrackStep<M>(*med, w, rng, bricks, err);
+            const int r = DeltaTrackAction<M>(*med, w, rng, bricks, err);
             if (r != kWalkGoing) {
                 V3 p = v3(0.0f);
                 uint32_t wd = rng.dim;
@@ -1317,7 +1478,7 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
             continue;
         }
         if (entry >= 0) {
-            if (RatioTrackStep<M>(*med, w, rng, tr, bricks, err) != kWalkGoing) {
+            if (RatioTrackAction<M>(*med, w, rng, tr, bricks, err) != kWalkGoing) {
                 if (tr != 1.0f) {
                     float4* c = &P.sc[entry];
                     const float4 v = *c;

@@ -83,6 +83,7 @@ struct Wave {
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
     float4* trk = nullptr;  // per-slot results of k_track (required in scenes with media)
+    bool sort = false;      // order the active list by medium cell (k_sort_*) before tracking
 };
 
 // The parameters of one iteration's launches: k_track's results when it runs (scenes with
@@ -118,6 +119,13 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
     const RenderParams P = IterationParams(w, FUSED);
     // The tracking kernels are persistent: one full wave of resident blocks.
     const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
+    // Queue sorting: both kernels read the queue length on the device and do nothing for
+    // short queues; the host loop skips them there.
+    if (w.sort && P.trk && P.sorted && (persistent || n >= kSortMinQueue))
+        time(PG_KERNEL_SORT, [&]() {
+            k_sort_keys<MULTI><<<sms * 4, kSortThreads, 0, st>>>(P, w.S0);
+            k_sort_scatter<<<sms * 4, kSortThreads, 0, st>>>(P);
+        });
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
             k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(P, w.S0);

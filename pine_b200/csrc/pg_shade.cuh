@@ -852,6 +852,57 @@ __device__ __forceinline__ int RatioTrackStep(const MediumDev& m, GridWalk& w, H
     return kWalkGoing;
 }
 
+// The same walks one action at a time, for the tracking kernels' lane loops: either the
+// crossing into the next brick (when the optical depth left outlasts the current brick) or
+// one tentative collision with its density lookup.  A lane that crosses many bricks then
+// takes more loop iterations instead of holding its warp in an inner loop, and the sequence
+// of operations of each walk, hence its result, is the one of DeltaTrackStep/RatioTrackStep.
+template <int M>
+__device__ __forceinline__ int DeltaTrackAction(const MediumDev& m, GridWalk& w, HashRng& rng,
+                                                uint32_t& bricks, uint32_t& err) {
+    const float dtau = w.sm * (w.tb - w.t);
+    if (!(w.tau < dtau)) {
+        w.tau -= dtau;
+        return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+    }
+    w.t += __fdividef(w.tau, w.sm);
+    if (++w.n > (uint32_t)kTrackingCap) {
+        err |= kErrTrackingCap;
+        return kWalkEnded;
+    }
+    if (GridWalkDensity(m, w) > rng.Get1D() * w.maj)
+        return kWalkCollided;
+    w.tau = DrawOpticalDepth<M>(rng);
+    return kWalkGoing;
+}
+
+template <int M>
+__device__ __forceinline__ int RatioTrackAction(const MediumDev& m, GridWalk& w, HashRng& rng, float& tr,
+                                                uint32_t& bricks, uint32_t& err) {
+    const float dtau = w.sm * (w.tb - w.t);
+    if (!(w.tau < dtau)) {
+        w.tau -= dtau;
+        return GridWalkNext(m, w, bricks) ? kWalkGoing : kWalkEnded;
+    }
+    w.t += __fdividef(w.tau, w.sm);
+    if (++w.n > (uint32_t)kTrackingCap) {
+        err |= kErrTrackingCap;
+        tr = 0.0f;
+        return kWalkEnded;
+    }
+    tr *= 1.0f - Max(0.0f, __fdividef(GridWalkDensity(m, w), w.maj));
+    if (tr < 0.1f) {
+        const float q = Max(0.05f, 1.0f - tr);
+        if (rng.Get1D() < q) {
+            tr = 0.0f;
+            return kWalkEnded;
+        }
+        tr /= 1.0f - q;
+    }
+    w.tau = DrawOpticalDepth<M>(rng);
+    return kWalkGoing;
+}
+
 // GridMedium::Tr (medium.cpp:55-80): ratio tracking with pine's Russian roulette once the
 // transmittance estimate drops below 0.1, per majorant brick.  HomogeneousMedium::Tr
 // (medium.cpp:33-36).  For the shadow rays traced inside the shading or shadow kernels

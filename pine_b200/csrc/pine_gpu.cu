@@ -122,6 +122,9 @@ struct Pool {
     float4* splat = nullptr;   // queued samples of filtered films
     int* splat_req = nullptr;
     float4* trk = nullptr;     // k_track's result per slot
+    int* sorted = nullptr;     // the sorted active list, its keys and the bins (k_sort_*)
+    uint16_t* sort_keys = nullptr;
+    int* sort_bins = nullptr;
     void Ensure(int n) {
         if (n <= slots)
             return;
@@ -144,6 +147,9 @@ struct Pool {
         splat = mem.Alloc<float4>(n);
         splat_req = mem.Alloc<int>(n);
         trk = mem.Alloc<float4>(n);
+        sorted = mem.Alloc<int>(n);
+        sort_keys = mem.Alloc<uint16_t>(n);
+        sort_bins = mem.Alloc<int>(2 * kSortBins + 1);
     }
 };
 
@@ -227,7 +233,7 @@ struct pg_ctx {
     // kernels, 64-voxel majorant bricks (volume benchmark on B200: 915 Mpaths/s against 853
     // with 32-voxel and 704 with 16-voxel bricks at 2^22 slots; 951 with 2^23 slots, 825
     // with 2^21).
-    pg_tuning tuning{1 << 23, 128, 1, 64};
+    pg_tuning tuning{1 << 23, 128, 1, 64, 0};
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
@@ -898,6 +904,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.so = pl.so, P.sd = pl.sd, P.sc = pl.sc, P.skey = pl.skey;
     P.splat = pl.splat, P.splat_req = pl.splat_req;
     w.trk = pl.trk;
+    P.sorted = pl.sorted, P.sort_keys = pl.sort_keys, P.sort_bins = pl.sort_bins;
     P.counts = ctx->counts;
     P.film_sum = ctx->film.sum, P.film_sq = ctx->film.sq, P.film_wsum = ctx->film.wsum;
     P.film_w2sum = ctx->film.w2sum, P.film_n = ctx->film.n, P.film_acc = nullptr;
@@ -914,6 +921,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
     PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
     PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
+    PG_CUDA(cudaMemsetAsync(pl.sort_bins, 0, (2 * kSortBins + 1) * sizeof(int), st));
     if (w.guide) {
         GuidePool& gp = ctx->guide_pool;
         gp.Ensure(slots);
@@ -1112,6 +1120,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
+    w.sort = ctx->tuning.sort_queue != 0;
     w.guide = recordAccept != nullptr;
     w.media = sc.dev.num_media > 0;
     w.general = sc.general;
@@ -1479,11 +1488,11 @@ extern "C" pg_status pg_render(pg_ctx* ctx, int32_t scene_id, const pg_render_de
             stats->launches = r.launches;
             const int items[PG_NUM_KERNELS] = {kStatRegenItems, kStatTraceItems, kStatShadeItems,
                                                kStatShadowItems, kStatGuided, kStatTrainRows,
-                                               kStatTrackItems, kStatTransmitItems};
+                                               kStatTrackItems, kStatTransmitItems, kStatSortItems};
             const int steps[PG_NUM_KERNELS] = {-1, -1, kStatShadeSteps, kStatShadowSteps, -1, -1,
-                                               kStatTrackSteps, kStatTransmitSteps};
+                                               kStatTrackSteps, kStatTransmitSteps, -1};
             const int bricks[PG_NUM_KERNELS] = {-1, -1, kStatShadeBricks, kStatShadowBricks, -1, -1,
-                                                kStatTrackBricks, kStatTransmitBricks};
+                                                kStatTrackBricks, kStatTransmitBricks, -1};
             for (int k = 0; k < PG_NUM_KERNELS; k++) {
                 pg_kernel_stats& ks = stats->kernels[k];
                 ks.launches = r.kernelLaunches[k];
@@ -1658,6 +1667,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.general = general;
     w.splat = splat;
     w.fused = tune.split_shadow == 0;
+    w.sort = tune.sort_queue != 0;
     w.shadeBlock = tune.block_size;
     w.S0 = scenes[0];
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, tune.queue_capacity), total);
@@ -1708,7 +1718,8 @@ static bool ValidTuning(const pg_tuning& t) {
            t.block_size <= kMaxShadeBlock && (t.block_size & 31) == 0 &&
            (t.split_shadow == 0 || t.split_shadow == 1) &&
            (t.majorant_brick == 8 || t.majorant_brick == 16 || t.majorant_brick == 32 ||
-            t.majorant_brick == 64);
+            t.majorant_brick == 64) &&
+           (t.sort_queue == 0 || t.sort_queue == 1);
 }
 
 }  // namespace pg

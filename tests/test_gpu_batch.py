@@ -57,17 +57,40 @@ def test_autotune_returns_a_valid_tuning(ctx, tmp_path):
         ctx.release_scene(i)
 
 
-@pytest.mark.parametrize("split,brick", [(0, 8), (1, 32), (0, 16)])
-def test_tunings_agree(ctx, tmp_path, split, brick):
-    """Every shadow split and majorant brick size renders the same image statistically."""
+@pytest.mark.parametrize("split,brick,sort", [(0, 8, 0), (1, 32, 1), (0, 16, 1), (1, 64, 1)])
+def test_tunings_agree(ctx, tmp_path, split, brick, sort):
+    """Every shadow split, majorant brick size and queue order renders the same image
+    statistically."""
     z = golden("image_volume.npz")
     sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
     before = ctx.tuning()
     ctx.set_tuning(queue_capacity=1 << 20, block_size=128, split_shadow=split,
-                   majorant_brick=brick)
+                   majorant_brick=brick, sort_queue=sort)
     r = ctx.render(sid, spp=1024, seed=31)
     ctx.set_tuning(**before)
     se = np.sqrt(r["var"].astype(float) / 1024 + z["var"] / z["count"][..., None])
     v = se > 0
     assert np.mean(np.abs(r["mean"] - z["mean"])[v] / se[v] < 2.576) >= 0.98
+    ctx.release_scene(sid)
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_queue_sorting_changes_no_path(ctx, tmp_path, split):
+    """Ordering the active list by medium cell changes which lanes take which paths, not
+    the paths: a path's random streams follow its sample, and the film is summed per
+    sample, so the image is the same bit for bit with and without sorting."""
+    z = golden("image_volume.npz")
+    sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
+    before = ctx.tuning()
+    out = []
+    for sort in (0, 1):
+        ctx.set_tuning(**dict(before, queue_capacity=1 << 20, split_shadow=split, sort_queue=sort))
+        out.append(ctx.render(sid, spp=256, seed=7, math_mode="fast"))
+    ctx.set_tuning(**before)
+    assert out[0]["stats"]["kernels"]["sort"]["launches"] == 0
+    assert out[1]["stats"]["kernels"]["sort"]["launches"] > 0
+    assert out[1]["stats"]["kernels"]["sort"]["items"] > 0
+    np.testing.assert_array_equal(out[0]["count"], out[1]["count"])
+    np.testing.assert_array_equal(out[0]["mean"], out[1]["mean"])
+    np.testing.assert_array_equal(out[0]["var"], out[1]["var"])
     ctx.release_scene(sid)
