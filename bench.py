@@ -55,13 +55,14 @@ WORKLOADS = {
     "spheres": dict(kind="spheres", width=640, height=360, spp=64, max_depth=8),
     "mesh": dict(kind="mesh", width=1920, height=1080, spp=256, max_depth=16, subdiv=8),
 }
-# ncu cases (--profile-case): each workload's scene, full film, one sample per pixel (the
-# 512^3 grid and the 1.31M-triangle mesh are larger than L2 either way; at 1920x1080 the
-# mesh's traversal launches are full queues of 2M rays, under 1 GB on the device).
+# ncu cases (--profile-case): each workload's scene and film at a few samples per pixel, so
+# that the first wavefront launches are full queues of the default 2^23 path slots, as in
+# the benchmark (the 512^3 grid and the 1.31M-triangle mesh are larger than L2 either way;
+# a few GB on the device).
 PROFILE_CASES = {
-    "volume": dict(WORKLOADS["volume"], spp=1),
-    "spheres": dict(WORKLOADS["spheres"], spp=1),
-    "mesh": dict(WORKLOADS["mesh"], spp=1),
+    "volume": dict(WORKLOADS["volume"], spp=16),
+    "spheres": dict(WORKLOADS["spheres"], spp=32),
+    "mesh": dict(WORKLOADS["mesh"], spp=4),
 }
 
 
@@ -219,8 +220,9 @@ def hbm_peak():
 #   written; by k_transmit (ratio tracking of a shadow ray): 48 B ray read + 16 B
 #   contribution read and written;
 # * per volume tracking step 32 B (the 8 voxels of a trilinear lookup), 4 B per majorant
-#   brick entered.
-STATE_BYTES = {"shade": 128, "shadow": 64, "regen": 16, "track": 48, "transmit": 80}
+#   brick entered;
+# * a camera path started by k_regen: 80 B of new path state.
+STATE_BYTES = {"shade": 128, "shadow": 64, "regen": 80, "track": 48, "transmit": 80}
 
 
 def ray_bytes(prims, triangles):
@@ -264,7 +266,7 @@ def roofline(kernels, peak, peak_kind, b_ray, workload):
     tr = read_traffic() if workload == "volume" else {}
     if name in tr:
         traffic = tr[name] * per_launch_bytes
-        traffic_note = ("scaled from the 1-spp case: ncu DRAM bytes per algorithmic byte of the "
+        traffic_note = ("scaled from the 16-spp ncu case: DRAM bytes per algorithmic byte of the "
                         "kernel (profiles/volume_traffic.json) x this run's algorithmic bytes "
                         "per launch")
     out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

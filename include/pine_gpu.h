@@ -183,11 +183,23 @@ enum { PG_LIGHT_SAMPLER_POWER = 0, PG_LIGHT_SAMPLER_UNIFORM = 1 };
 
 /* Samplers.  PG_SAMPLER_HALTON draws pine's Halton sequence (HaltonSampler,
  * sampler.cpp:33-96: per-pixel index, digit permutations from pine's RNG at seed 0, pine's
- * float rounding), dimension by dimension in the order pine's PathIntegrator::Li asks for
- * them.  Pine's Uniform, Stratified, ZeroTwoSequence and Sobol samplers map to
- * PG_SAMPLER_INDEPENDENT, the library's counter-based stream (uniform, independent per
- * sample and dimension). */
-enum { PG_SAMPLER_INDEPENDENT = 0, PG_SAMPLER_HALTON = 1 };
+ * float rounding), and PG_SAMPLER_SOBOL pine's Sobol sequence (SobolSampler,
+ * sampler.cpp:129-220: 1024 dimensions, pixel-to-index map at the film's power-of-two
+ * resolution, the sampler's randomizer), dimension by dimension in the order pine's
+ * PathIntegrator::Li asks for them.  Pine's Uniform, Stratified and ZeroTwoSequence
+ * samplers map to PG_SAMPLER_INDEPENDENT, the library's counter-based stream (uniform,
+ * independent per sample and dimension). */
+enum { PG_SAMPLER_INDEPENDENT = 0, PG_SAMPLER_HALTON = 1, PG_SAMPLER_SOBOL = 2 };
+
+/* Sobol randomizeStrategy (SobolSampler::Create, sampler.cpp:268-277): "none",
+ * "binaryPermutate", "fastOwen" (the default) and "Owen"; another string keeps
+ * BinaryPermutate, as pine does. */
+enum {
+    PG_SOBOL_NONE = 0,
+    PG_SOBOL_BINARY_PERMUTATE = 1,
+    PG_SOBOL_FAST_OWEN = 2,
+    PG_SOBOL_OWEN = 3
+};
 
 /* Integrators.  PG_INTEGRATOR_PATH: PathIntegrator::Li (path.cpp:6-86), next-event
  * estimation with MIS and Russian roulette.  PG_INTEGRATOR_RANDOM_WALK:
@@ -225,7 +237,7 @@ typedef struct pg_scene_desc {
     const pg_node_op* node_ops;
     int32_t sampler;                 /* PG_SAMPLER_* */
     int32_t sampler_scramble;        /* Halton randomizeStrategy: 1 permutateDigits (pine's
-                                        default), 0 none */
+                                        default), 0 none; Sobol: PG_SOBOL_* */
     int32_t filter;                  /* PG_FILTER_* of the film; pine's default is
                                         LanczosSinc (filter.cpp:6) */
     float filter_radius[2];          /* a component <= 0 means pine's default 0.5; at most 16 */
@@ -452,10 +464,15 @@ pg_status pg_bump_normal(const pg_node_op* ops, int32_t num_ops, int32_t ref, in
  * x, pixel y, sample index, dimension >= 2), as HaltonSampler::StartPixel(p, 0), `sample`
  * StartNextSample calls and SampleDimension(dim) give them (sampler.cpp:62-96).
  * scramble: 1 permuted digits, 0 none.
+ * pg_sobol_sample: Sobol samples, rows as for pg_halton_sample (dimension 2..1023), as
+ * SobolSampler::StartPixel(p, sample) and SampleDimension(dim) give them
+ * (sampler.cpp:136-220); randomize: PG_SOBOL_*.
  * pg_filter_table: the film's 16 x 16 table of a filter (film.cpp:20-28), row-major in y;
  * radius and params as in pg_scene_desc. */
 pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scramble, const int64_t* rows,
                            int64_t n, float* out);
+pg_status pg_sobol_sample(int32_t width, int32_t height, int32_t randomize, const int64_t* rows,
+                          int64_t n, float* out);
 pg_status pg_filter_table(int32_t filter, const float* radius, const float* params,
                           float* table);
 

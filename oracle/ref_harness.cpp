@@ -479,6 +479,33 @@ int Halton(int w, int h, const char* strategy, const char* inPath, const char* o
     return 0;
 }
 
+// SobolSampler values (sampler.cpp:129-220) for a film size and randomize strategy at rows
+// of (pixel x, pixel y, sample index, dimension), as int64; out: one float per row.
+int Sobol(int w, int h, const char* strategy, const char* inPath, const char* outPath) {
+    FILE* f = std::fopen(inPath, "rb");
+    if (!f)
+        return 2;
+    std::vector<int64_t> rows;
+    int64_t buf[4];
+    while (std::fread(buf, sizeof(int64_t), 4, f) == 4)
+        rows.insert(rows.end(), buf, buf + 4);
+    std::fclose(f);
+    std::string text = std::string("sampler: Sobol{\n samplesPerPixel: 1\n randomizeStrategy: ") +
+                       strategy + "\n}\n";
+    Parameters params = Parse(text.c_str());
+    Parameters sp = params["sampler"];
+    sp.Set("filmSize", vec2i(w, h));
+    Sampler sampler = CreateSampler(sp);
+    SobolSampler& ss = sampler.Be<SobolSampler>();
+    std::vector<float> out(rows.size() / 4);
+    for (size_t i = 0; i < out.size(); i++) {
+        ss.StartPixel(vec2i((int)rows[4 * i], (int)rows[4 * i + 1]), (int)rows[4 * i + 2]);
+        out[i] = ss.SampleDimension((int)rows[4 * i + 3]);
+    }
+    WriteRaw(outPath, out.data(), out.size() * 4);
+    return 0;
+}
+
 // The film's filter table and radius for a scene (film.cpp:20-28); out: 2 + 256 floats.
 int FilterDump(const char* scenePath, const char* outPath) {
     FilterTable ft(scenePath);
@@ -557,6 +584,8 @@ int main(int argc, char** argv) {
         return Density(argv[2], argv[3], argv[4]);
     if (mode == "halton" && argc == 7)
         return Halton(std::atoi(argv[2]), std::atoi(argv[3]), argv[4], argv[5], argv[6]);
+    if (mode == "sobol" && argc == 7)
+        return Sobol(std::atoi(argv[2]), std::atoi(argv[3]), argv[4], argv[5], argv[6]);
     if (mode == "filter" && argc == 4)
         return FilterDump(argv[2], argv[3]);
     if (mode == "nodes" && argc == 5)

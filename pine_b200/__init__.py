@@ -120,7 +120,7 @@ class SceneDesc(ctypes.Structure):
                 ("filter_params", ctypes.c_float * 2), ("integrator", ctypes.c_int32)]
 
 
-SAMPLER_INDEPENDENT, SAMPLER_HALTON = 0, 1
+SAMPLER_INDEPENDENT, SAMPLER_HALTON, SAMPLER_SOBOL = 0, 1, 2
 FILTERS = {"Box": 0, "Triangle": 1, "Gaussian": 2, "Mitchell": 3, "LanczosSinc": 4}
 
 
@@ -210,6 +210,8 @@ def lib():
                                    _P(ctypes.c_int32), _P(ctypes.c_int64)]),
         "pg_halton_sample": (st, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                   _P(ctypes.c_int64), ctypes.c_int64, _F]),
+        "pg_sobol_sample": (st, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                 _P(ctypes.c_int64), ctypes.c_int64, _F]),
         "pg_filter_table": (st, [ctypes.c_int32, _F, _F, _F]),
         "pg_eval_nodes": (st, [_P(NodeOp), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                _F, ctypes.c_int64, _F]),
@@ -313,6 +315,22 @@ def halton_sample(width, height, rows, scramble=True):
     st = lib().pg_halton_sample(int(width), int(height), int(bool(scramble)),
                                 r.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), r.shape[0],
                                 _fptr(out))
+    if st != PG_OK:
+        raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
+    return out
+
+
+SOBOL_RANDOMIZERS = {"none": 0, "binaryPermutate": 1, "fastOwen": 2, "Owen": 3}
+
+
+def sobol_sample(width, height, rows, randomize="fastOwen"):
+    """pine's Sobol samples for a width x height film at rows (n x 4: pixel x, pixel y,
+    sample index, dimension) under a randomizeStrategy name; n floats."""
+    r = np.ascontiguousarray(rows, dtype=np.int64).reshape(-1, 4)
+    out = np.empty(r.shape[0], np.float32)
+    st = lib().pg_sobol_sample(int(width), int(height), SOBOL_RANDOMIZERS[randomize],
+                               r.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), r.shape[0],
+                               _fptr(out))
     if st != PG_OK:
         raise PgError(st, (lib().pg_last_error(None) or b"").decode(errors="replace"))
     return out

@@ -96,7 +96,7 @@ struct RequestDev {
     uint32_t key0_offset;             // sample_offset * npix (progressive passes)
     int max_depth;
     int sampler;                      // PG_SAMPLER_*
-    HaltonDev halton;                 // tables and film parameters of a Halton render
+    QmcDev qmc;                       // tables and film parameters of a Halton or Sobol render
     int filter_splat;                 // 0: box of radius 0.5 (one pixel, weight 1)
     float filter_radius[2];
     const float* filter_table;        // 16 x 16 filter values (film.cpp:20-28)
@@ -298,31 +298,32 @@ __device__ __forceinline__ int FindRequest(const RenderParams& P, unsigned long 
     return lo;
 }
 
-// Halton index of camera sample key0: its pixel's first index plus sample * stride.
-static __device__ __noinline__ uint64_t HaltonIndexOf(const RequestDev& R, uint32_t key0) {
+// Sequence index of camera sample key0 (sample s of its pixel): for Halton the pixel's
+// first index plus s * stride, for Sobol SobolIntervalToIndex of (s, pixel).
+static __device__ __noinline__ uint64_t QmcIndexOf(const RequestDev& R, uint32_t key0) {
     uint32_t s = key0 / (uint32_t)R.npix, pix = key0 - s * (uint32_t)R.npix;
     int px = (int)(pix % (uint32_t)R.width), py = (int)(pix / (uint32_t)R.width);
-    return HaltonPixelIndex(R.halton, px, py) + (uint64_t)s * R.halton.stride;
+    return QmcPixelIndex(R.qmc, s, px, py);
 }
 
-// The random stream of camera sample key0 from dimension `dim` on: pine's Halton sequence
-// at the sample's pixel and index for Halton renders, else the counter-based stream.  GEN
-// (general) kernel variants serve scenes with Halton sampling, filter splats or shader-node
-// materials; the others compile none of that code.
+// The random stream of camera sample key0 from dimension `dim` on: pine's Halton or Sobol
+// sequence at the sample's pixel and index for such renders, else the counter-based
+// stream.  GEN (general) kernel variants serve scenes with Halton or Sobol sampling, filter
+// splats or shader-node materials; the others compile none of that code.
 template <bool GEN>
 __device__ __forceinline__ Rng PathRng(const RequestDev& R, uint32_t key0, uint32_t dim) {
     Rng r{key0, R.key1, dim};
-    if (GEN && R.sampler == PG_SAMPLER_HALTON) {
-        uint64_t hidx = HaltonIndexOf(R, key0);
-        r.hal = &R.halton;
-        r.key0 = (uint32_t)hidx;
-        r.key1 = (uint32_t)(hidx >> 32);
+    if (GEN && R.sampler != PG_SAMPLER_INDEPENDENT) {
+        uint64_t idx = QmcIndexOf(R, key0);
+        r.hal = &R.qmc;
+        r.key0 = (uint32_t)idx;
+        r.key1 = (uint32_t)(idx >> 32);
     }
     return r;
 }
 template <bool GEN>
 __device__ __forceinline__ uint32_t FirstDim(const RequestDev& R) {
-    return GEN && R.sampler == PG_SAMPLER_HALTON ? 2u : 0u;  // StartPixel leaves it at 2
+    return GEN && R.sampler != PG_SAMPLER_INDEPENDENT ? 2u : 0u;  // StartPixel leaves it at 2
 }
 
 // Adds one sample's weighted radiance and its square to pixel pix of the FP64 film and

@@ -43,18 +43,36 @@ inline DivMagic MakeDivMagic(uint32_t d) {
     return DivMagic{(uint32_t)m, l, 1.0f / (float)d, 0.0f};
 }
 
-// Everything a path needs to draw its Halton samples; lives in device memory next to the
-// request it belongs to.
-struct HaltonDev {
+// ---------------------------------------------------------------- Sobol
+constexpr int kSobolDims = 1024;        // NSobolDimensions (util/sobolmetrices.h:10)
+constexpr int kSobolVdcCols = 52;       // SobolMatrixSize: columns of each VdC row
+constexpr int kSobolMaxLog2Scale = 25;  // rows of VdCSobolMatrices (films up to 2^25 wide)
+
+// Everything a path needs to draw pine's Halton or Sobol samples; lives in device memory
+// next to the request it belongs to.
+struct QmcDev {
+    int kind;                   // PG_SAMPLER_HALTON or PG_SAMPLER_SOBOL
+    int ndims;                  // dimensions before the counter restarts at 2 (Get1D)
+    int wrap2;                  // the counter from which Get2D restarts at 2: Halton
+                                // ndims - 1, Sobol ndims (pine checks only the first of
+                                // the pair's dimensions there)
+    uint32_t rotate;            // 0: pine's sequence; else the key of a per-dimension
+                                // Cranley-Patterson rotation (independent renders)
+    // Halton (HaltonSampler, sampler.cpp:33-96)
     const int* primes;          // the first 1000 primes
     const DivMagic* magic;      // division by each prime and its float constants
     const int* prime_sums;      // exclusive prefix sums: start of each prime's permutation
     const uint16_t* perm;       // digit permutations, concatenated in prime order
     int scramble;               // 1: permuted digits (pine's default), 0: plain radical inverse
-    uint32_t rotate;            // 0: pine's sequence; else the key of a per-dimension
-                                // Cranley-Patterson rotation (independent renders)
     uint32_t stride;            // baseScales.x * baseScales.y
     int scale[2], exps[2], inv[2];
+    // Sobol (SobolSampler, sampler.cpp:129-220)
+    const uint32_t* sobol;      // 1024 dimensions x 32 generator-matrix columns
+    const uint64_t* vdc;        // kSobolMaxLog2Scale rows of kSobolVdcCols: frame bits ->
+                                // pixel bits of the first two dimensions
+    const uint64_t* vdc_inv;    // the same rows of the inverse map: pixel bits -> index bits
+    int log2scale;              // log2(roundup2(max(film width, height)))
+    int randomize;              // PG_SOBOL_* (RandomizeStrategy)
 };
 
 // InverseRadicalInverse (lowdiscrepancy.h:44-53).
@@ -89,7 +107,7 @@ PG_HD uint32_t InverseRadicalInverseSmall(uint32_t inverse, int nDigits) {
 // HaltonSampler::StartPixel(p, 0) (sampler.cpp:62-75): the index of the pixel's first
 // sample; sample s of the pixel is this + s * stride.  pine sums in 64 bits; every term
 // here is below 128 * 243 * 243 < 2^23, so 32-bit arithmetic gives the same index.
-PG_HD uint64_t HaltonPixelIndex(const HaltonDev& h, int px, int py) {
+PG_HD uint64_t HaltonPixelIndex(const QmcDev& h, int px, int py) {
     if (h.stride <= 1)
         return 0;
     const uint32_t mx = (uint32_t)PstdMod(px, kHaltonMaxRes), my = (uint32_t)PstdMod(py, kHaltonMaxRes);
@@ -133,7 +151,7 @@ PG_HD float U64ToFloat(uint64_t v) {
 // order: 1/base, the running product of 1/base, the digits reversed into an integer, and
 // for the scrambled form the tail term perm[0] / (base + 1).  The digit loop runs in
 // 32-bit arithmetic while the index fits.
-PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
+PG_HD float HaltonRadical(const QmcDev& h, int dim, uint64_t a) {
     const int base = h.primes[dim];
     const uint16_t* perm = h.scramble ? h.perm + h.prime_sums[dim] : nullptr;
     const DivMagic mg = h.magic[dim];
@@ -181,10 +199,9 @@ PG_HD float HaltonRadical(const HaltonDev& h, int dim, uint64_t a) {
     return Min(v, kOneMinusEpsilon);
 }
 
-// A Halton sample of dimension `dim` at index `a`, rotated when the render asks for an
-// independent sequence.
-PG_HD float HaltonSample(const HaltonDev& h, uint64_t a, int dim) {
-    float v = HaltonRadical(h, dim, a);
+// The rotation of dimension `dim` for an independent render (seed != 0): a hashed offset
+// added modulo 1, which keeps the sequence's stratification.
+PG_HD float QmcRotate(const QmcDev& h, float v, int dim) {
     if (h.rotate) {
         uint64_t k = Hash64u(((uint64_t)h.rotate << 32) ^ (uint64_t)(uint32_t)dim);
         float shift = (float)(uint32_t)(k >> 40) * 0x1p-24f;
@@ -194,6 +211,114 @@ PG_HD float HaltonSample(const HaltonDev& h, uint64_t a, int dim) {
         v = Min(v, kOneMinusEpsilon);
     }
     return v;
+}
+
+// A Halton sample of dimension `dim` at index `a`.
+PG_HD float HaltonSample(const QmcDev& h, uint64_t a, int dim) {
+    return QmcRotate(h, HaltonRadical(h, dim, a), dim);
+}
+
+// MixBits (util/rng.h:46-53).
+PG_HD uint64_t MixBits64(uint64_t v) {
+    v ^= (v >> 31);
+    v *= 0x7fb5d329728ea185ULL;
+    v ^= (v >> 27);
+    v *= 0x81dadef4bc2dd44dULL;
+    v ^= (v >> 33);
+    return v;
+}
+PG_HD uint32_t ReverseBits32(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __brev(v);
+#else
+    v = (v << 16) | (v >> 16);
+    v = ((v & 0x00ff00ffu) << 8) | ((v & 0xff00ff00u) >> 8);
+    v = ((v & 0x0f0f0f0fu) << 4) | ((v & 0xf0f0f0f0u) >> 4);
+    v = ((v & 0x33333333u) << 2) | ((v & 0xccccccccu) >> 2);
+    return ((v & 0x55555555u) << 1) | ((v & 0xaaaaaaaau) >> 1);
+#endif
+}
+PG_HD float U32ToFloat(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __uint2float_rn(v);
+#else
+    return (float)v;
+#endif
+}
+
+// SobolIntervalToIndex (lowdiscrepancy.h:139-160): the index of sample `frame` of pixel
+// (px, py), whose first two Sobol dimensions fall in that pixel at resolution 2^m.  pine
+// keeps the index in 32 bits (`uint32_t index`), so it is truncated as there.
+PG_HD uint64_t SobolPixelIndex(const QmcDev& h, uint64_t frame, uint32_t px, uint32_t py) {
+    const int m = h.log2scale;
+    if (m == 0)
+        return frame;
+    uint32_t index = (uint32_t)(frame << (2 * m));
+    const uint64_t* row = h.vdc + (size_t)(m - 1) * kSobolVdcCols;
+    uint64_t delta = 0;
+    for (int c = 0; frame; c++, frame >>= 1)
+        if (frame & 1)
+            delta ^= row[c];
+    uint64_t b = (((uint64_t)px << m) | py) ^ delta;
+    const uint64_t* inv = h.vdc_inv + (size_t)(m - 1) * kSobolVdcCols;
+    for (int c = 0; b; c++, b >>= 1)
+        if (b & 1)
+            index ^= (uint32_t)inv[c];
+    return index;
+}
+
+// SobolSampler::SampleDimension (sampler.cpp:159-220) at Sobol index `a` (below 2^32):
+// SobolSample (lowdiscrepancy.h:129-137) with the randomizer of the sampler's strategy,
+// seeded by the low 32 bits of Hash(dim).
+PG_HD float SobolSampleDim(const QmcDev& h, uint32_t a, int dim) {
+    if (dim >= kSobolDims)  // pine's Get2D at dimension 1023 reads past its table
+        dim = 2;
+    const uint32_t* C = h.sobol + (size_t)dim * 32;
+    uint32_t v = 0;
+    for (int i = 0; a; i++, a >>= 1)
+        if (a & 1)
+            v ^= C[i];
+    const uint32_t seed = (uint32_t)Hash64u((uint64_t)(uint32_t)dim);
+    switch (h.randomize) {
+    case PG_SOBOL_BINARY_PERMUTATE:  // BinaryPermuteScrambler
+        v ^= seed;
+        break;
+    case PG_SOBOL_FAST_OWEN:  // FastOwenScramber
+        v = ReverseBits32(v);
+        v ^= v * 0x3d20adeau;
+        v += seed;
+        v *= (seed >> 16) | 1u;
+        v ^= v * 0x05526c56u;
+        v ^= v * 0x53a22864u;
+        v = ReverseBits32(v);
+        break;
+    case PG_SOBOL_OWEN:  // OwenScramber
+        if (seed & 1)
+            v ^= 1u << 31;
+        for (int b = 1; b < 32; b++) {
+            uint32_t mask = (~0u) << (32 - b);
+            if ((uint32_t)MixBits64((uint64_t)((v & mask) ^ seed)) & (1u << b))
+                v ^= 1u << (31 - b);
+        }
+        break;
+    default:
+        break;
+    }
+    return QmcRotate(h, Min(U32ToFloat(v) * 0x1p-32f, kOneMinusEpsilon), dim);
+}
+
+// A sample of dimension `dim` at sequence index `a` of either sampler.
+PG_HD float QmcSample(const QmcDev& h, uint64_t a, int dim) {
+    if (h.kind == PG_SAMPLER_SOBOL)
+        return SobolSampleDim(h, (uint32_t)a, dim);
+    return HaltonSample(h, a, dim);
+}
+
+// The sequence index of sample `s` of pixel (px, py).
+PG_HD uint64_t QmcPixelIndex(const QmcDev& h, uint32_t s, int px, int py) {
+    if (h.kind == PG_SAMPLER_SOBOL)
+        return SobolPixelIndex(h, s, (uint32_t)px, (uint32_t)py);
+    return HaltonPixelIndex(h, px, py) + (uint64_t)s * h.stride;
 }
 
 // ---------------------------------------------------------------- host tables
@@ -279,7 +404,7 @@ inline int64_t MultiplicativeInverse(int64_t a, int64_t n) {
 }
 
 // The per-film parameters of HaltonSampler's constructor (sampler.cpp:33-58).
-inline void HaltonFilmParams(HaltonDev& h, int width, int height) {
+inline void HaltonFilmParams(QmcDev& h, int width, int height) {
     const int size[2] = {width, height};
     for (int i = 0; i < 2; i++) {
         int base = i == 0 ? 2 : 3;
@@ -294,6 +419,122 @@ inline void HaltonFilmParams(HaltonDev& h, int width, int height) {
     h.inv[0] = (int)MultiplicativeInverse(h.scale[0], h.scale[1]);
     h.inv[1] = (int)MultiplicativeInverse(h.scale[1], h.scale[0]);
     h.stride = (uint32_t)(h.scale[0] * h.scale[1]);
+}
+
+// ---------------------------------------------------------------- Sobol tables
+// The generator matrices of pine's 1024 Sobol dimensions, as 32 columns per dimension
+// (column j is the contribution of index bit j, top bit first).  Dimension 0 is the van der
+// Corput sequence; dimension d >= 1 follows from its Joe-Kuo polynomial and initial
+// direction integers by the recurrence m_k = 2 a_1 m_{k-1} ^ ... ^ 2^{s-1} a_{s-1}
+// m_{k-s+1} ^ 2^s m_{k-s} ^ m_{k-s} (Bratley and Fox, ACM TOMS 14, 1988), column j =
+// m_{j+1} << (31 - j).
+#include "sobol_dirnums.inc"
+
+// The direction integers m_1..m_n of dimension `dim` (n <= 64).
+inline void SobolDirections(int dim, int n, std::vector<uint64_t>& m) {
+    m.assign(n, 1);
+    if (dim == 0)
+        return;
+    size_t pos = 0;
+    for (int d = 1; d < dim; d++) {
+        uint32_t p = kSobolDirNums[pos];
+        int s = 0;
+        while ((p >> (s + 1)) != 0)
+            s++;
+        pos += 1 + (size_t)s;
+    }
+    const uint32_t poly = kSobolDirNums[pos];
+    int s = 0;
+    while ((poly >> (s + 1)) != 0)
+        s++;
+    for (int k = 0; k < s && k < n; k++)
+        m[k] = kSobolDirNums[pos + 1 + k];
+    for (int k = s; k < n; k++) {
+        uint64_t v = m[k - s] ^ (m[k - s] << s);
+        for (int i = 1; i < s; i++)
+            if ((poly >> (s - i)) & 1)
+                v ^= m[k - i] << i;
+        m[k] = v;
+    }
+}
+
+inline std::vector<uint32_t> SobolMatrices() {
+    std::vector<uint32_t> out((size_t)kSobolDims * 32);
+    std::vector<uint64_t> m;
+    for (int dim = 0; dim < kSobolDims; dim++) {
+        if (dim == 0) {
+            for (int j = 0; j < 32; j++)
+                out[j] = 1u << (31 - j);
+            continue;
+        }
+        SobolDirections(dim, 32, m);
+        for (int j = 0; j < 32; j++)
+            out[(size_t)dim * 32 + j] = (uint32_t)(m[j] << (31 - j));
+    }
+    return out;
+}
+
+// The tables of SobolIntervalToIndex for every resolution 2^m, m = 1..25.  Index bit j
+// moves the first two dimensions' top m bits by contrib(j) = (x bits << m) | y bits, with
+// 64-bit columns (van der Corput bit j at 63 - j; dimension 1 column m_{j+1} << (63 - j)).
+// Row m - 1 of `vdc` holds contrib(2m + c) for frame bit c (c < 52 - 2m); row m - 1 of
+// `inv` holds, for each bit c of the 2m-bit pixel code, the low 2m index bits whose
+// contributions sum to that bit (the inverse of the 2m x 2m matrix of contrib(0..2m-1),
+// by Gaussian elimination over GF(2)).
+inline void SobolVdcTables(std::vector<uint64_t>& vdc, std::vector<uint64_t>& inv) {
+    vdc.assign((size_t)kSobolMaxLog2Scale * kSobolVdcCols, 0);
+    inv.assign((size_t)kSobolMaxLog2Scale * kSobolVdcCols, 0);
+    std::vector<uint64_t> m1;
+    SobolDirections(1, 64, m1);
+    for (int m = 1; m <= kSobolMaxLog2Scale; m++) {
+        auto contrib = [&](int j) -> uint64_t {
+            uint64_t c0 = j < 64 ? (1ull << (63 - j)) : 0;
+            uint64_t c1 = j < 64 ? (m1[j] << (63 - j)) : 0;
+            return ((c0 >> (64 - m)) << m) | (c1 >> (64 - m));
+        };
+        uint64_t* vrow = &vdc[(size_t)(m - 1) * kSobolVdcCols];
+        for (int c = 0; c < kSobolVdcCols - 2 * m; c++)
+            vrow[c] = contrib(2 * m + c);
+        // Row-reduce [contrib(j) | e_j]: pivots by highest bit, each with the index bits
+        // that produce it.
+        const int n = 2 * m;
+        uint64_t piv_v[64] = {}, piv_c[64] = {};
+        for (int j = 0; j < n; j++) {
+            uint64_t v = contrib(j), comb = 1ull << j;
+            for (int p = n - 1; p >= 0; p--)
+                if (((v >> p) & 1) && piv_v[p]) {
+                    v ^= piv_v[p];
+                    comb ^= piv_c[p];
+                }
+            if (v) {
+                int p = 63;
+                while (!((v >> p) & 1))
+                    p--;
+                piv_v[p] = v;
+                piv_c[p] = comb;
+            }
+        }
+        uint64_t* irow = &inv[(size_t)(m - 1) * kSobolVdcCols];
+        for (int c = 0; c < n; c++) {
+            uint64_t t = 1ull << c, comb = 0;
+            for (int p = n - 1; p >= 0; p--)
+                if (((t >> p) & 1) && piv_v[p]) {
+                    t ^= piv_v[p];
+                    comb ^= piv_c[p];
+                }
+            irow[c] = comb;  // t == 0: the matrix is invertible for every m
+        }
+    }
+}
+
+// SobolSampler's constructor (sampler.cpp:129-134): scale = roundup2(max(w, h)).
+inline int SobolLog2Scale(int width, int height) {
+    int mx = width > height ? width : height, scale = 1, l = 0;
+    while (scale < mx) {
+        scale <<= 1;
+        l++;
+    }
+    return l;
 }
 
 // ---------------------------------------------------------------- film filters

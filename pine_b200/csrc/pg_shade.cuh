@@ -28,21 +28,22 @@ struct HashRng {
     }
 };
 
-// Out of line, so that the Halton code adds nothing to the register allocation of the
-// kernels that only draw the counter-based stream.
-static __device__ __noinline__ float HaltonDraw(const HaltonDev* h, uint32_t lo, uint32_t hi, int dim) {
-    return HaltonSample(*h, ((uint64_t)hi << 32) | lo, dim);
+// Out of line, so that the Halton and Sobol code adds nothing to the register allocation
+// of the kernels that only draw the counter-based stream.
+static __device__ __noinline__ float HaltonDraw(const QmcDev* h, uint32_t lo, uint32_t hi, int dim) {
+    return QmcSample(*h, ((uint64_t)hi << 32) | lo, dim);
 }
 
-// A camera path of a Halton render draws pine's Halton sequence instead: `hal` set, the
-// sample's 64-bit Halton index in key1:key0, and `dim` pine's dimension counter, which
-// restarts at 2 after the last prime (HaltonSampler::Get1D/Get2D, sampler.cpp:76-87).
+// A camera path of a Halton or Sobol render draws pine's sequence instead: `hal` set, the
+// sample's sequence index in key1:key0, and `dim` pine's dimension counter, which restarts
+// at 2 after the last dimension (HaltonSampler::Get1D/Get2D, sampler.cpp:76-87;
+// SobolSampler::Get1D/Get2D, sampler.cpp:147-158).
 struct Rng {
     uint32_t key0, key1, dim;
-    const HaltonDev* hal = nullptr;
+    const QmcDev* hal = nullptr;
     __device__ __forceinline__ float Get1D() {
         if (hal) {
-            if (dim >= (uint32_t)kHaltonDims)
+            if (dim >= (uint32_t)hal->ndims)
                 dim = 2;
             return HaltonDraw(hal, key0, key1, (int)dim++);
         }
@@ -67,7 +68,7 @@ struct Rng {
     }
     __device__ __forceinline__ void Get2D(float& a, float& b) {
         if (hal) {
-            if (dim + 1 >= (uint32_t)kHaltonDims)
+            if (dim >= (uint32_t)hal->wrap2)
                 dim = 2;
             a = HaltonDraw(hal, key0, key1, (int)dim);
             b = HaltonDraw(hal, key0, key1, (int)dim + 1);

@@ -245,6 +245,9 @@ struct pg_ctx {
     const pg::DivMagic* halton_magic = nullptr;
     const int* halton_sums = nullptr;
     const uint16_t* halton_perm = nullptr;
+    const uint32_t* sobol_mat = nullptr;   // Sobol tables (built for the first Sobol scene)
+    const uint64_t* sobol_vdc = nullptr;
+    const uint64_t* sobol_vdc_inv = nullptr;
     int bvh_builder = PG_BVH_HOST;         // PG_BVH_*: how later scene uploads build their BVH
 };
 
@@ -324,6 +327,20 @@ static void EnsureHalton(pg_ctx* ctx) {
     PG_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+// The Sobol tables of the context: 1024 x 32 generator-matrix columns (128 KB) and the
+// pixel-to-index rows of every power-of-two resolution, built once.
+static void EnsureSobol(pg_ctx* ctx) {
+    if (ctx->sobol_mat)
+        return;
+    std::vector<uint64_t> vdc, inv;
+    SobolVdcTables(vdc, inv);
+    ctx->halton_mem.stream = ctx->stream, ctx->halton_mem.async = true;
+    ctx->sobol_mat = ctx->halton_mem.Upload(SobolMatrices(), ctx->stream);
+    ctx->sobol_vdc = ctx->halton_mem.Upload(vdc, ctx->stream);
+    ctx->sobol_vdc_inv = ctx->halton_mem.Upload(inv, ctx->stream);
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     DevMem upload;  // linear density grids: inputs of the majorant and brick builds only
     upload.stream = ctx->stream, upload.async = true;
@@ -338,8 +355,12 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     Require(d->camera.medium >= -1 && d->camera.medium < d->num_media, "camera medium out of range");
     for (int64_t i = 0; i < 3 * d->num_triangles; i++)
         Require((int64_t)d->indices[i] < d->num_vertices, "triangle index out of range");
-    Require(d->sampler == PG_SAMPLER_INDEPENDENT || d->sampler == PG_SAMPLER_HALTON,
+    Require(d->sampler == PG_SAMPLER_INDEPENDENT || d->sampler == PG_SAMPLER_HALTON ||
+                d->sampler == PG_SAMPLER_SOBOL,
             "unknown sampler");
+    Require(d->sampler != PG_SAMPLER_SOBOL ||
+                (d->sampler_scramble >= PG_SOBOL_NONE && d->sampler_scramble <= PG_SOBOL_OWEN),
+            "unknown Sobol randomizer");
     Require(d->filter >= PG_FILTER_BOX && d->filter <= PG_FILTER_LANCZOS_SINC, "unknown filter");
     Require(d->integrator == PG_INTEGRATOR_PATH || d->integrator == PG_INTEGRATOR_RANDOM_WALK,
             "unknown integrator");
@@ -780,16 +801,19 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
     S.has_null_surfaces = nullSurfaces ? 1 : 0;
     PG_CUDA(cudaStreamSynchronize(st));
 
-    // Sampler and film filter.  Halton renders always take the general splat, so that a
-    // sample on a pixel's edge reaches the neighbour as pine's film adds it; with the
+    // Sampler and film filter.  Halton and Sobol renders always take the general splat, so
+    // that a sample on a pixel's edge reaches the neighbour as pine's film adds it; with the
     // counter-based stream a box of radius 0.5 keeps one pixel per sample.
     sc->sampler = d->sampler;
-    sc->scramble = d->sampler_scramble ? 1 : 0;
+    sc->scramble = d->sampler == PG_SAMPLER_SOBOL ? d->sampler_scramble
+                                                  : (d->sampler_scramble ? 1 : 0);
     if (sc->sampler == PG_SAMPLER_HALTON)
         EnsureHalton(ctx);
+    if (sc->sampler == PG_SAMPLER_SOBOL)
+        EnsureSobol(ctx);
     sc->filter_radius[0] = fRadius[0];
     sc->filter_radius[1] = fRadius[1];
-    sc->filter_splat = sc->sampler == PG_SAMPLER_HALTON ||
+    sc->filter_splat = sc->sampler != PG_SAMPLER_INDEPENDENT ||
                        !(d->filter == PG_FILTER_BOX && fRadius[0] == 0.5f && fRadius[1] == 0.5f);
     sc->random_walk = d->integrator == PG_INTEGRATOR_RANDOM_WALK;
     sc->general = sc->filter_splat || d->num_node_ops > 0 || sc->random_walk;
@@ -820,21 +844,40 @@ static DeviceScene& GetScene(pg_ctx* ctx, int32_t id) {
     return *ctx->scenes[id];
 }
 
-// A request's sampler and film filter, for a film of rq.width x rq.height.  Halton renders
-// with seed 0 draw pine's own sequence; other seeds rotate it (Cranley-Patterson, one
-// offset per dimension), which keeps its stratification and makes renders independent.
+// A request's sampler and film filter, for a film of rq.width x rq.height (rq.total,
+// rq.npix and rq.key0_offset set).  Halton and Sobol renders with seed 0 draw pine's own
+// sequence; other seeds rotate it (Cranley-Patterson, one offset per dimension), which
+// keeps its stratification and makes renders independent.
 static void SetRequestSampling(pg_ctx* ctx, const DeviceScene& sc, RequestDev& rq, uint64_t seed) {
     rq.sampler = sc.sampler;
-    rq.halton = HaltonDev{};
+    rq.qmc = QmcDev{};
+    QmcDev& h = rq.qmc;
+    h.kind = sc.sampler;
+    h.rotate = seed == 0 ? 0u : ((uint32_t)Hash64u(seed) | 1u);
     if (sc.sampler == PG_SAMPLER_HALTON) {
-        HaltonDev& h = rq.halton;
+        h.ndims = kHaltonDims;
+        h.wrap2 = kHaltonDims - 1;
         h.primes = ctx->halton_primes;
         h.magic = ctx->halton_magic;
         h.prime_sums = ctx->halton_sums;
         h.perm = ctx->halton_perm;
         h.scramble = sc.scramble;
-        h.rotate = seed == 0 ? 0u : ((uint32_t)Hash64u(seed) | 1u);
         HaltonFilmParams(h, rq.width, rq.height);
+    } else if (sc.sampler == PG_SAMPLER_SOBOL) {
+        h.ndims = kSobolDims;
+        h.wrap2 = kSobolDims;
+        h.sobol = ctx->sobol_mat;
+        h.vdc = ctx->sobol_vdc;
+        h.vdc_inv = ctx->sobol_vdc_inv;
+        h.randomize = sc.scramble;
+        h.log2scale = SobolLog2Scale(rq.width, rq.height);
+        Require(h.log2scale <= kSobolMaxLog2Scale, "film too large for the Sobol sampler");
+        // Sample indices must stay within the frame columns of the film's resolution row
+        // (pine's table rows hold 52 - 2m of them).
+        const uint64_t frames = ((uint64_t)rq.key0_offset + rq.total) / (uint64_t)rq.npix;
+        const int cols = kSobolVdcCols - 2 * h.log2scale;
+        Require(cols >= 63 || frames <= (1ull << cols),
+                "too many samples per pixel for the Sobol sampler at this film size");
     }
     rq.filter_splat = sc.filter_splat;
     rq.filter_radius[0] = sc.filter_radius[0];
@@ -2268,7 +2311,9 @@ extern "C" pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scr
             perm = HaltonPermutations(primes);
             magic = HaltonMagics(primes, sums, perm);
         });
-        HaltonDev h{};
+        QmcDev h{};
+        h.kind = PG_SAMPLER_HALTON;
+        h.ndims = kHaltonDims;
         h.primes = primes.data();
         h.magic = magic.data();
         h.prime_sums = sums.data();
@@ -2280,6 +2325,39 @@ extern "C" pg_status pg_halton_sample(int32_t width, int32_t height, int32_t scr
             Require(r[2] >= 0 && r[3] >= 2 && r[3] < kHaltonDims, "bad sample index or dimension");
             uint64_t a = HaltonPixelIndex(h, (int)r[0], (int)r[1]) + (uint64_t)r[2] * h.stride;
             out[i] = HaltonSample(h, a, (int)r[3]);
+        }
+    });
+}
+
+extern "C" pg_status pg_sobol_sample(int32_t width, int32_t height, int32_t randomize,
+                                     const int64_t* rows, int64_t n, float* out) {
+    return Guard(nullptr, [&]() {
+        Require(width > 0 && height > 0, "film size must be positive");
+        Require(randomize >= PG_SOBOL_NONE && randomize <= PG_SOBOL_OWEN, "unknown randomizer");
+        Require(n >= 0 && (n == 0 || (rows && out)), "bad input or output arrays");
+        static std::vector<uint32_t> mat;
+        static std::vector<uint64_t> vdc, inv;
+        static std::once_flag once;
+        std::call_once(once, [] {
+            mat = SobolMatrices();
+            SobolVdcTables(vdc, inv);
+        });
+        QmcDev h{};
+        h.kind = PG_SAMPLER_SOBOL;
+        h.ndims = kSobolDims;
+        h.sobol = mat.data();
+        h.vdc = vdc.data();
+        h.vdc_inv = inv.data();
+        h.randomize = randomize;
+        h.log2scale = SobolLog2Scale(width, height);
+        Require(h.log2scale <= kSobolMaxLog2Scale, "film too large for the Sobol sampler");
+        for (int64_t i = 0; i < n; i++) {
+            const int64_t* r = rows + 4 * i;
+            Require(r[0] >= 0 && r[1] >= 0 && r[0] < width && r[1] < height, "pixel outside the film");
+            Require(r[2] >= 0 && r[2] <= INT32_MAX && r[3] >= 2 && r[3] < kSobolDims,
+                    "bad sample index or dimension");
+            uint64_t a = SobolPixelIndex(h, (uint64_t)r[2], (uint32_t)r[0], (uint32_t)r[1]);
+            out[i] = SobolSampleDim(h, (uint32_t)a, (int)r[3]);
         }
     });
 }

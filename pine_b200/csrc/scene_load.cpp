@@ -974,7 +974,16 @@ void LoadSceneFile(const std::string& path, HostScene& s) {
             // randomizeStrategy: "none" or "permutateDigits"; anything else keeps the
             // default (sampler.cpp:252-259).
             s.sampler_scramble = smp.String("randomizeStrategy", "permutateDigits") != "none";
-        } else if (stype != "Uniform" && stype != "Sobol") {
+        } else if (stype == "Sobol") {
+            s.sampler = PG_SAMPLER_SOBOL;
+            // SobolSampler::Create (sampler.cpp:268-277): BinaryPermutate unless the string
+            // names another strategy; the string's default is "fastOwen".
+            std::string rs = smp.String("randomizeStrategy", "fastOwen");
+            s.sampler_scramble = rs == "none"       ? PG_SOBOL_NONE
+                                 : rs == "fastOwen" ? PG_SOBOL_FAST_OWEN
+                                 : rs == "Owen"     ? PG_SOBOL_OWEN
+                                                    : PG_SOBOL_BINARY_PERMUTATE;
+        } else if (stype != "Uniform") {
             Warn("[Sampler][Create]Unknown type \"" + stype + "\"");
         }
         s.spp = smp.Int("samplesPerPixel", 1);

@@ -256,6 +256,51 @@ def sampler_filter_kat(tmp):
                         filter_tables=np.stack(tables), allow_pickle=True)
 
 
+SOBOL_FILMS = [(48, 27), (128, 36), (1280, 720), (7, 5), (1, 1), (1920, 1080)]
+SOBOL_STRATEGIES = ["none", "binaryPermutate", "fastOwen", "Owen"]
+
+
+def sobol_kat(tmp):
+    """pine's SobolSampler values at random (pixel, sample, dimension) rows for several film
+    sizes and every randomize strategy (sobol.npz)."""
+    rng = np.random.default_rng(5151)
+    rows_all, vals_all, meta = [], [], []
+    for (w, h) in SOBOL_FILMS:
+        for k, strat in enumerate(SOBOL_STRATEGIES):
+            n = 512
+            rows = np.stack([rng.integers(0, w, n), rng.integers(0, h, n),
+                             rng.integers(0, 4096, n), rng.integers(2, 1024, n)], 1)
+            rows[:64, 3] = np.arange(2, 66)
+            rows[64:80, 2] = rng.integers(1 << 16, 1 << 20, 16)  # many samples per pixel
+            rows[80:84, 3] = 1023
+            rows[84:88, 2] = 0
+            if w * h > 4096:  # keep the frame within the resolution's table row
+                rows[64:80, 2] = rng.integers(4096, 1 << 14, 16)
+            rows = rows.astype(np.int64)
+            rows.tofile(f"{tmp}/s.in")
+            run("sobol", str(w), str(h), strat, f"{tmp}/s.in", f"{tmp}/s.out")
+            rows_all.append(rows)
+            vals_all.append(np.fromfile(f"{tmp}/s.out", np.float32))
+            meta.append((w, h, k))
+    np.savez_compressed(f"{HERE}/sobol.npz", meta=np.array(meta, np.int32),
+                        strategies=np.array(SOBOL_STRATEGIES), rows=np.stack(rows_all),
+                        values=np.stack(vals_all))
+
+
+def sobol_case(tmp):
+    """The spheres fixture's scene with pine's Sobol sampler (fastOwen, the default) at 1024
+    spp: the GPU draws pine's sequence in pine's order, so its image follows pine's sample
+    by sample."""
+    z = np.load(f"{HERE}/image_spheres.npz", allow_pickle=True)
+    text = str(z["scene_text"])
+    assert "sampler: Halton{" in text
+    text = text.replace("sampler: Halton{", "sampler: Sobol{", 1)
+    path = f"{tmp}/sobol.txt"
+    with open(path, "w") as f:
+        f.write(text)
+    image_case("sobol", path, [])
+
+
 def filtered_case(tmp):
     """The spheres fixture's scene with a wide Gaussian filter (samples reach up to four
     pixels) at 256 spp."""
@@ -381,6 +426,9 @@ def main():
                 sampler_filter_kat(tmp)
             if "filtered" in only:
                 filtered_case(tmp)
+            if "sobol" in only:
+                sobol_kat(tmp)
+                sobol_case(tmp)
             if "randomwalk" in only:
                 randomwalk_case(tmp)
             if "pine_spheres" in only:
@@ -437,6 +485,8 @@ def main():
         sampler_filter_kat(tmp)
         filtered_case(tmp)
         randomwalk_case(tmp)
+        sobol_kat(tmp)
+        sobol_case(tmp)
     print("fixtures written to", HERE)
 
 

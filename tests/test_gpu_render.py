@@ -57,7 +57,7 @@ ONE_PIXEL = {"volume", "volume512", "spheres_c0", "mesh_full"}
 
 
 @pytest.mark.parametrize("name", ["spheres", "mesh", "volume", "pine_spheres", "filtered",
-                                  "randomwalk", "volume512", "spheres_c0", "mesh_full"])
+                                  "randomwalk", "sobol", "volume512", "spheres_c0", "mesh_full"])
 @pytest.mark.parametrize("math_mode", ["pine", "fast"])
 def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
     z = golden(f"image_{name}.npz")
@@ -95,11 +95,12 @@ def test_equal_spp_against_reference(ctx, tmp_path, name, math_mode):
     ctx.release_scene(sid)
 
 
-@pytest.mark.parametrize("name", ["spheres", "mesh", "pine_spheres", "filtered", "randomwalk"])
+@pytest.mark.parametrize("name", ["spheres", "mesh", "pine_spheres", "filtered", "randomwalk",
+                                  "sobol"])
 def test_halton_renders_follow_pine_sample_by_sample(ctx, tmp_path, name):
-    """Seed 0 draws pine's own Halton sequence in the order pine's PathIntegrator::Li
-    draws it, so with pine's numerics the GPU traces pine's paths: pixels agree far inside
-    Monte Carlo error, and filtered samples reach the same pixels."""
+    """Seed 0 draws pine's own Halton (or, for `sobol`, Sobol) sequence in the order pine's
+    PathIntegrator::Li draws it, so with pine's numerics the GPU traces pine's paths: pixels
+    agree far inside Monte Carlo error, and filtered samples reach the same pixels."""
     z = golden(f"image_{name}.npz")
     sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
     r = ctx.render(sid, spp=_spp(z), seed=0, math_mode="pine")

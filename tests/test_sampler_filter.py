@@ -1,7 +1,7 @@
-"""pine's Halton sampler and film filters on the host: the code the kernels run (through
-pg_halton_sample and pg_filter_table) against values pine itself produced
-(tests/golden/sampler_filter.npz, written by tests/golden/make_golden.py), and the scene
-loader's reading of sampler and filter blocks."""
+"""pine's Halton and Sobol samplers and film filters on the host: the code the kernels run
+(through pg_halton_sample, pg_sobol_sample and pg_filter_table) against values pine itself
+produced (tests/golden/sampler_filter.npz and sobol.npz, written by
+tests/golden/make_golden.py), and the scene loader's reading of sampler and filter blocks."""
 import numpy as np
 import pytest
 
@@ -26,6 +26,29 @@ def test_halton_rejects_bad_rows(pglib):
     for row in ([0, 0, 0, 1000], [0, 0, -1, 2], [0, 0, 0, 1]):
         with pytest.raises(pb.PgError):
             pb.halton_sample(8, 8, np.array([row]))
+
+
+S = golden("sobol.npz")
+
+
+@pytest.mark.parametrize("case", range(len(S["meta"])))
+def test_sobol_is_bit_exact_with_pine(pglib, case):
+    """Sobol matrices from the Joe-Kuo direction numbers, the pixel-to-index tables derived
+    from the first two dimensions, and each randomizer reproduce pine's values bit for bit."""
+    import pine_b200 as pb
+    w, h, k = (int(v) for v in S["meta"][case])
+    rows = S["rows"][case]
+    got = pb.sobol_sample(w, h, rows, randomize=str(S["strategies"][k]))
+    want = S["values"][case]
+    bad = got.view(np.uint32) != want.view(np.uint32)
+    assert not bad.any(), f"{bad.sum()} of {len(rows)} differ, first rows {rows[bad][:4]}"
+
+
+def test_sobol_rejects_bad_rows(pglib):
+    import pine_b200 as pb
+    for row in ([0, 0, 0, 1024], [0, 0, -1, 2], [0, 0, 0, 1], [8, 0, 0, 2]):
+        with pytest.raises(pb.PgError):
+            pb.sobol_sample(8, 8, np.array([row]))
 
 
 def _filter_args(block):
@@ -72,7 +95,11 @@ def _scene(tmp_path, sampler, film_extra):
     ("Halton{\n samplesPerPixel: 32\n }", 1, 32, 1),
     ("Halton{\n samplesPerPixel: 8\n randomizeStrategy: none\n }", 1, 8, 0),
     ("Uniform{\n samplesPerPixel: 5\n }", 0, 5, 1),
-    ("Sobol{\n samplesPerPixel: 16\n }", 0, 16, 1),
+    ("Sobol{\n samplesPerPixel: 16\n }", 2, 16, 2),
+    ("Sobol{\n samplesPerPixel: 4\n randomizeStrategy: none\n }", 2, 4, 0),
+    ("Sobol{\n samplesPerPixel: 4\n randomizeStrategy: Owen\n }", 2, 4, 3),
+    ("Sobol{\n samplesPerPixel: 4\n randomizeStrategy: binaryPermutate\n }", 2, 4, 1),
+    ("Sobol{\n samplesPerPixel: 4\n randomizeStrategy: other\n }", 2, 4, 1),
     ("Stratified{\n xPixelSamples: 3\n yPixelSamples: 4\n }", 0, 12, 1),
     ("ZeroTwoSequence{\n samplesPerPixel: 5\n }", 0, 8, 1),
 ])
