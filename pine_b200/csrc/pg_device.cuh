@@ -278,6 +278,63 @@ __device__ __forceinline__ bool TestPrim(const SceneDev& S, int idx, V3 o, V3 d,
     return ok;
 }
 
+// Tests the ray against the 8 quantised child boxes of node `node` (Ylitie, Karras and
+// Laine 2017): the children hit become the next node group (hit bits in the top byte,
+// octant-ordered) and the leaf primitives hit the next primitive group.
+__device__ __forceinline__ void VisitNode(const SceneDev& S, uint32_t node, V3 o, float ix, float iy,
+                                          float iz, uint32_t octInv, float tmin, float tmax,
+                                          uint2& ngroup, uint2& tgroup) {
+    const float4* nw = S.nodes[node].w;
+    float4 w0 = __ldg(&nw[0]), w1 = __ldg(&nw[1]), w2 = __ldg(&nw[2]),
+           w3 = __ldg(&nw[3]), w4 = __ldg(&nw[4]);
+    uint32_t eb = __float_as_uint(w0.w);
+    float sx = __uint_as_float((eb & 0xffu) << 23);
+    float sy = __uint_as_float(((eb >> 8) & 0xffu) << 23);
+    float sz = __uint_as_float(((eb >> 16) & 0xffu) << 23);
+    uint32_t imask = eb >> 24;
+    float ax = sx * ix, ay = sy * iy, az = sz * iz;
+    float bx = (w0.x - o.x) * ix, by = (w0.y - o.y) * iy, bz = (w0.z - o.z) * iz;
+    // Near/far plane words chosen by the ray octant.
+    uint32_t lox0 = __float_as_uint(w2.x), lox1 = __float_as_uint(w2.y);
+    uint32_t loy0 = __float_as_uint(w2.z), loy1 = __float_as_uint(w2.w);
+    uint32_t loz0 = __float_as_uint(w3.x), loz1 = __float_as_uint(w3.y);
+    uint32_t hix0 = __float_as_uint(w3.z), hix1 = __float_as_uint(w3.w);
+    uint32_t hiy0 = __float_as_uint(w4.x), hiy1 = __float_as_uint(w4.y);
+    uint32_t hiz0 = __float_as_uint(w4.z), hiz1 = __float_as_uint(w4.w);
+    uint32_t nx0 = ix < 0.0f ? hix0 : lox0, nx1 = ix < 0.0f ? hix1 : lox1;
+    uint32_t fx0 = ix < 0.0f ? lox0 : hix0, fx1 = ix < 0.0f ? lox1 : hix1;
+    uint32_t ny0 = iy < 0.0f ? hiy0 : loy0, ny1 = iy < 0.0f ? hiy1 : loy1;
+    uint32_t fy0 = iy < 0.0f ? loy0 : hiy0, fy1 = iy < 0.0f ? loy1 : hiy1;
+    uint32_t nz0 = iz < 0.0f ? hiz0 : loz0, nz1 = iz < 0.0f ? hiz1 : loz1;
+    uint32_t fz0 = iz < 0.0f ? loz0 : hiz0, fz1 = iz < 0.0f ? loz1 : hiz1;
+    uint32_t meta0 = __float_as_uint(w1.z), meta1 = __float_as_uint(w1.w);
+    uint32_t nodeHits = 0, primHits = 0;
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        uint32_t mw = s < 4 ? meta0 : meta1;
+        uint32_t meta = (mw >> (8 * (s & 3))) & 0xffu;
+        int bi = s & 3;
+        float qnx = ByteF(s < 4 ? nx0 : nx1, bi), qfx = ByteF(s < 4 ? fx0 : fx1, bi);
+        float qny = ByteF(s < 4 ? ny0 : ny1, bi), qfy = ByteF(s < 4 ? fy0 : fy1, bi);
+        float qnz = ByteF(s < 4 ? nz0 : nz1, bi), qfz = ByteF(s < 4 ? fz0 : fz1, bi);
+        float tn = fmaxf(fmaxf(fmaf(qnx, ax, bx), fmaf(qny, ay, by)),
+                         fmaxf(fmaf(qnz, az, bz), tmin));
+        float tf = fminf(fminf(fmaf(qfx, ax, bx), fmaf(qfy, ay, by)),
+                         fminf(fmaf(qfz, az, bz), tmax));
+        bool h = meta != 0u && tn <= tf;
+        if (h) {
+            if (imask & (1u << s)) {
+                nodeHits |= 1u << (s ^ octInv);
+            } else {
+                uint32_t cnt = meta >> 5, off = meta & 31u;
+                primHits |= ((1u << cnt) - 1u) << off;
+            }
+        }
+    }
+    ngroup = make_uint2(__float_as_uint(w1.x), (nodeHits << 24) | imask);
+    tgroup = make_uint2(__float_as_uint(w1.y), primHits);
+}
+
 // Closest hit (ANY = false) or first blocking hit (ANY = true) along [tmin, tmax].
 // `stack` points at this thread's first entry in shared memory; entries are `stride`
 // apart (the block size) so that a warp's accesses fall in distinct banks.
@@ -330,55 +387,7 @@ __device__ bool Traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, 
                 stack[sp * stride] = ngroup;
                 sp++;
             }
-            const float4* nw = S.nodes[node].w;
-            float4 w0 = __ldg(&nw[0]), w1 = __ldg(&nw[1]), w2 = __ldg(&nw[2]),
-                   w3 = __ldg(&nw[3]), w4 = __ldg(&nw[4]);
-            uint32_t eb = __float_as_uint(w0.w);
-            float sx = __uint_as_float((eb & 0xffu) << 23);
-            float sy = __uint_as_float(((eb >> 8) & 0xffu) << 23);
-            float sz = __uint_as_float(((eb >> 16) & 0xffu) << 23);
-            uint32_t imask = eb >> 24;
-            float ax = sx * ix, ay = sy * iy, az = sz * iz;
-            float bx = (w0.x - o.x) * ix, by = (w0.y - o.y) * iy, bz = (w0.z - o.z) * iz;
-            // Near/far plane words chosen by the ray octant.
-            uint32_t lox0 = __float_as_uint(w2.x), lox1 = __float_as_uint(w2.y);
-            uint32_t loy0 = __float_as_uint(w2.z), loy1 = __float_as_uint(w2.w);
-            uint32_t loz0 = __float_as_uint(w3.x), loz1 = __float_as_uint(w3.y);
-            uint32_t hix0 = __float_as_uint(w3.z), hix1 = __float_as_uint(w3.w);
-            uint32_t hiy0 = __float_as_uint(w4.x), hiy1 = __float_as_uint(w4.y);
-            uint32_t hiz0 = __float_as_uint(w4.z), hiz1 = __float_as_uint(w4.w);
-            uint32_t nx0 = ix < 0.0f ? hix0 : lox0, nx1 = ix < 0.0f ? hix1 : lox1;
-            uint32_t fx0 = ix < 0.0f ? lox0 : hix0, fx1 = ix < 0.0f ? lox1 : hix1;
-            uint32_t ny0 = iy < 0.0f ? hiy0 : loy0, ny1 = iy < 0.0f ? hiy1 : loy1;
-            uint32_t fy0 = iy < 0.0f ? loy0 : hiy0, fy1 = iy < 0.0f ? loy1 : hiy1;
-            uint32_t nz0 = iz < 0.0f ? hiz0 : loz0, nz1 = iz < 0.0f ? hiz1 : loz1;
-            uint32_t fz0 = iz < 0.0f ? loz0 : hiz0, fz1 = iz < 0.0f ? loz1 : hiz1;
-            uint32_t meta0 = __float_as_uint(w1.z), meta1 = __float_as_uint(w1.w);
-            uint32_t nodeHits = 0, primHits = 0;
-#pragma unroll
-            for (int s = 0; s < 8; s++) {
-                uint32_t mw = s < 4 ? meta0 : meta1;
-                uint32_t meta = (mw >> (8 * (s & 3))) & 0xffu;
-                int bi = s & 3;
-                float qnx = ByteF(s < 4 ? nx0 : nx1, bi), qfx = ByteF(s < 4 ? fx0 : fx1, bi);
-                float qny = ByteF(s < 4 ? ny0 : ny1, bi), qfy = ByteF(s < 4 ? fy0 : fy1, bi);
-                float qnz = ByteF(s < 4 ? nz0 : nz1, bi), qfz = ByteF(s < 4 ? fz0 : fz1, bi);
-                float tn = fmaxf(fmaxf(fmaf(qnx, ax, bx), fmaf(qny, ay, by)),
-                                 fmaxf(fmaf(qnz, az, bz), tmin));
-                float tf = fminf(fminf(fmaf(qfx, ax, bx), fmaf(qfy, ay, by)),
-                                 fminf(fmaf(qfz, az, bz), tmax));
-                bool h = meta != 0u && tn <= tf;
-                if (h) {
-                    if (imask & (1u << s)) {
-                        nodeHits |= 1u << (s ^ octInv);
-                    } else {
-                        uint32_t cnt = meta >> 5, off = meta & 31u;
-                        primHits |= ((1u << cnt) - 1u) << off;
-                    }
-                }
-            }
-            ngroup = make_uint2(__float_as_uint(w1.x), (nodeHits << 24) | imask);
-            tgroup = make_uint2(__float_as_uint(w1.y), primHits);
+            VisitNode(S, node, o, ix, iy, iz, octInv, tmin, tmax, ngroup, tgroup);
         }
         while (tgroup.y) {
             int bit = __ffs(tgroup.y) - 1;
@@ -403,6 +412,90 @@ __device__ bool Traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, 
         }
     }
     return found;
+}
+
+// ---------------------------------------------------------------- stepped closest hit
+// The closest-hit traversal of Traverse<false> over [0, inf) as a state machine advanced one
+// loop iteration at a time (TraceStep: one node's children tested, then the primitives of
+// the leaves it hit), so that a persistent warp can give a lane whose ray is done the next
+// ray while its other lanes keep walking.  Each ray takes the same steps in the same order
+// as in Traverse, so hits are identical.
+struct TraceWalk {
+    V3 o, d;
+    float ix, iy, iz;
+    uint32_t octInv;
+    uint2 ngroup, tgroup;
+    int sp, iter;
+    Hit hit;  // hit.t is the walk's tmax
+};
+
+// Starts the walk of ray o + t d: planes first (they lie outside the BVH), then the BVH
+// root.  False when there is no BVH: the walk is already over.
+__device__ __forceinline__ bool TraceBegin(const SceneDev& S, V3 o, V3 d, TraceWalk& w) {
+    w.o = o;
+    w.d = d;
+    w.hit.prim = -1;
+    w.hit.t = kFloatMax;
+    w.hit.u = w.hit.v = 0.0f;
+    for (int i = 0; i < S.num_planes; i++) {
+        const ShapeDev& sh = S.shapes[S.planes[i]];
+        float t;
+        if (IntersectPlane(o, d, 0.0f, w.hit.t, v3(sh.p[0], sh.p[1], sh.p[2]),
+                           v3(sh.p[3], sh.p[4], sh.p[5]), t)) {
+            w.hit.t = t;
+            w.hit.prim = -(2 + S.planes[i]);
+            w.hit.u = w.hit.v = 0.0f;
+        }
+    }
+    if (!S.has_bvh)
+        return false;
+    w.ix = SafeRcp(d.x), w.iy = SafeRcp(d.y), w.iz = SafeRcp(d.z);
+    const uint32_t oct = (w.ix < 0.0f ? 1u : 0u) | (w.iy < 0.0f ? 2u : 0u) | (w.iz < 0.0f ? 4u : 0u);
+    w.octInv = 7u - oct;
+    w.ngroup = make_uint2(0u, (1u << (24 + (0u ^ w.octInv))) | 1u);
+    w.tgroup = make_uint2(0u, 0u);
+    w.sp = 0;
+    w.iter = 0;
+    return true;
+}
+
+// One iteration of the traversal loop; false when the walk is over.  `stack` as in
+// Traverse, holding at most `cap` entries.
+__device__ __forceinline__ bool TraceStep(const SceneDev& S, TraceWalk& w, uint2* stack, int stride,
+                                          int cap, uint32_t& err) {
+    if (w.iter++ >= kTraversalCap) {
+        err |= kErrTraversalCap;
+        return false;
+    }
+    if (w.ngroup.y > 0x00ffffffu) {
+        uint32_t hits = w.ngroup.y >> 24;
+        uint32_t key = __ffs(hits) - 1;
+        w.ngroup.y &= ~(1u << (24 + key));
+        uint32_t slot = key ^ w.octInv;
+        uint32_t node = w.ngroup.x + __popc(w.ngroup.y & 0xffu & ((1u << slot) - 1u));
+        if (w.ngroup.y > 0x00ffffffu) {
+            if (w.sp >= cap) {
+                err |= kErrStackOverflow;
+                return false;
+            }
+            stack[w.sp * stride] = w.ngroup;
+            w.sp++;
+        }
+        VisitNode(S, node, w.o, w.ix, w.iy, w.iz, w.octInv, 0.0f, w.hit.t, w.ngroup, w.tgroup);
+    }
+    while (w.tgroup.y) {
+        int bit = __ffs(w.tgroup.y) - 1;
+        w.tgroup.y &= w.tgroup.y - 1u;
+        float tmax = w.hit.t;
+        TestPrim(S, (int)w.tgroup.x + bit, w.o, w.d, 0.0f, tmax, w.hit);
+    }
+    if (w.ngroup.y <= 0x00ffffffu) {
+        if (w.sp == 0)
+            return false;
+        w.sp--;
+        w.ngroup = stack[w.sp * stride];
+    }
+    return true;
 }
 
 }  // namespace pg

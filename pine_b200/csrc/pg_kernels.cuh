@@ -67,7 +67,7 @@ enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlot
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
                   kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kCntTrackNext = 9,
-                  kCntTransmitNext = 10, kCntSorted = 11, kNumCounts = 12 };
+                  kCntTransmitNext = 10, kCntSorted = 11, kCntTraceNext = 12, kNumCounts = 13 };
 
 // k_track's result per slot (RenderParams::trk): the scattering position (world space) and,
 // in w, the tracking stream's next dimension with kTrackScattered set when the walk ended in
@@ -155,6 +155,8 @@ struct RenderParams {
     uint16_t* sort_keys;
     int* sort_bins;
     int transmitted;             // 1: k_transmit scaled sc by each shadow ray's transmittance
+    int stack_cap;               // k_trace's traversal stack entries per thread (at least the
+                                 // BVH's depth + 2, at most kStackSize)
     int max_iter;
     int use_cond;                // k_swap sets the graph while-condition
     cudaGraphConditionalHandle cond;
@@ -543,6 +545,7 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     c[kCntSplat] = 0;
     c[kCntTrackNext] = 0;
     c[kCntTransmitNext] = 0;
+    c[kCntTraceNext] = 0;
     c[kCntSorted] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
@@ -557,28 +560,66 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
         cudaGraphSetConditional(P.cond, more ? 1u : 0u);
 }
 
+// k_trace: closest hits of the active rays in persistent warps.  Each lane walks one ray
+// through the BVH a loop iteration at a time (TraceStep: one node, then the primitives of
+// the leaves it hit), and a warp takes new queue entries for its idle lanes once
+// kTraceRefillLanes of them are idle (or all are), with one atomic on the queue's work
+// counter, so that a ray with many node visits holds up one lane instead of its warp.
+#ifndef PG_TRACE_REFILL_LANES
+#define PG_TRACE_REFILL_LANES 8
+#endif
+constexpr int kTraceRefillLanes = PG_TRACE_REFILL_LANES;
+constexpr int kTraceThreads = 128;
+
 template <bool MULTI>
-__global__ void k_trace(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+__global__ void __launch_bounds__(kTraceThreads, 8)
+    k_trace(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];
     const int n = P.counts[kCntActive];
     const int* active = ActiveList(P);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q - (int)threadIdx.x < n;
-         q += gridDim.x * blockDim.x) {
-        if (q < n) {
-            int i = active[q];
-            const SceneDev& S = SceneOf<MULTI>(P, S0, i);
-            float4 ro = P.ray_o[i], rd = P.ray_d[i];
-            Hit h;
-            uint32_t err = 0;
-            Traverse<false>(S, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), 0.0f, kFloatMax, h,
-                            stack + threadIdx.x, blockDim.x, err);
-            P.hit[i] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
-            if (err)
-                atomicOr(P.err, err);
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const SceneDev* S = &S0;
+    int slot = -1;
+    TraceWalk w;
+    uint32_t items = 0, err = 0;
+    bool more = true;
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, slot < 0);
+        if (more && (__popc(idle) >= kTraceRefillLanes || idle == 0xffffffffu)) {
+            int base = 0;
+            if (lane == 0)
+                base = atomicAdd(&P.counts[kCntTraceNext], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            more = base + __popc(idle) < n;
+            if (slot < 0) {
+                const int q = base + __popc(idle & below);
+                if (q < n) {
+                    const int i = active[q];
+                    items++;
+                    S = &SceneOf<MULTI>(P, S0, i);
+                    const float4 ro = P.ray_o[i], rd = P.ray_d[i];
+                    if (TraceBegin(*S, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), w))
+                        slot = i;
+                    else
+                        P.hit[i] = make_float4(w.hit.t, __int_as_float(w.hit.prim), w.hit.u, w.hit.v);
+                }
+            }
         }
-        WarpAdd(&P.stats[kStatRays], q < n ? 1u : 0u);
-        WarpAdd(&P.stats[kStatTraceItems], q < n ? 1u : 0u);
+        if (__ballot_sync(0xffffffffu, slot >= 0) == 0) {
+            if (!more)
+                break;
+            continue;
+        }
+        if (slot >= 0 && !TraceStep(*S, w, stack + threadIdx.x, blockDim.x, P.stack_cap, err)) {
+            P.hit[slot] = make_float4(w.hit.t, __int_as_float(w.hit.prim), w.hit.u, w.hit.v);
+            slot = -1;
+        }
     }
+    if (err)
+        atomicOr(P.err, err);
+    WarpAdd(&P.stats[kStatRays], items);
+    WarpAdd(&P.stats[kStatTraceItems], items);
 }
 
 struct SurfaceInfo {

@@ -82,6 +82,7 @@ struct Wave {
     int mode = PG_MATH_FAST;
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
+    int traceCap = kStackSize;  // k_trace's stack entries per thread (TraceCap of the scenes)
     float4* trk = nullptr;  // per-slot results of k_track (required in scenes with media)
     bool sort = false;      // order the active list by medium cell (k_sort_*) before tracking
 };
@@ -94,8 +95,29 @@ static RenderParams IterationParams(const Wave& w, bool fused) {
         throw Failure{PG_ERR_CUDA, "wavefront with media but no tracking buffer"};
     RenderParams P = w.P;
     P.trk = w.media ? w.trk : nullptr;
+    P.stack_cap = w.traceCap;
     P.transmitted = (P.trk && !fused && !w.surfaces) ? 1 : 0;
     return P;
+}
+
+// The traversal stack k_trace needs for a BVH of depth `depth` (8-wide levels below the
+// root): one entry per level pushed on the way down, with a margin, at most kStackSize.
+static inline int TraceCap(int depth) {
+    return std::min(kStackSize, std::max(4, depth + 2));
+}
+
+// k_trace's persistent grid: every block the SMs hold at once with this stack size.
+template <bool MULTI>
+static int TraceGrid(int sms, size_t smem) {
+    static int cachedBlocks[kStackSize + 1] = {};
+    const int entries = (int)(smem / (kTraceThreads * sizeof(uint2)));
+    int& nb = cachedBlocks[std::min(entries, kStackSize)];
+    if (nb == 0) {
+        int b = 0;
+        PG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trace<MULTI>, kTraceThreads, smem));
+        nb = std::max(1, b);
+    }
+    return sms * nb;
 }
 
 template <int M, bool MULTI, bool FUSED, bool GEN>
@@ -128,7 +150,8 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
         });
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
-            k_trace<MULTI><<<grid(tb, 12), tb, w.stackBytes, st>>>(P, w.S0);
+            const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
+            k_trace<MULTI><<<TraceGrid<MULTI>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
         });
     if (P.trk)
         time(PG_KERNEL_TRACK, [&]() {
@@ -203,7 +226,8 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
     const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
-            k_trace<false><<<grid(tb, 12), tb, w.stackBytes, st>>>(P, w.S0);
+            const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
+            k_trace<false><<<TraceGrid<false>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
         });
     if (P.trk)
         time(PG_KERNEL_TRACK, [&]() {

@@ -1159,6 +1159,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     Wave w;
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
+    w.traceCap = TraceCap(sc.bvh_depth);
     w.fused = ctx->tuning.split_shadow == 0;
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
@@ -1642,7 +1643,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     std::vector<SceneDev> scenes(n);
     uint64_t total = 0, pixels = 0;
     bool surfaces = false, media = false, general = false, splat = false;
-    int maxDepth = 1;
+    int maxDepth = 1, bvhDepth = 0;
     const int variant = MediaVariant(tune);
     // Shortest job first: requests take their sample ranges in increasing order of their
     // sample count, so small requests complete early (results keep the caller's order).
@@ -1690,6 +1691,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         s.cam.fov2d[0] = s.cam.fov2d[1] * ((float)w / (float)h);
         scenes[k] = s;
         surfaces = surfaces || sc.surfaces;
+        bvhDepth = std::max(bvhDepth, sc.bvh_depth);
         media = media || sc.dev.num_media > 0;
         general = general || sc.general;
         splat = splat || sc.filter_splat != 0;
@@ -1706,6 +1708,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.multi = true;
     w.mode = PG_MATH_FAST;
     w.surfaces = surfaces;
+    w.traceCap = TraceCap(bvhDepth);
     w.media = media;
     w.general = general;
     w.splat = splat;
@@ -1917,6 +1920,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     Wave w;
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
+    w.traceCap = TraceCap(sc.bvh_depth);
     w.media = sc.dev.num_media > 0;
     w.general = sc.general;
     w.splat = sc.filter_splat != 0;
