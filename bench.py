@@ -83,7 +83,7 @@ def parse_args():
     ap.add_argument("--filter", choices=["Box", "Triangle", "Gaussian", "Mitchell",
                                          "LanczosSinc"], default="Box",
                     help="the scene file's film filter (radius 0.5)")
-    ap.add_argument("--bvh", choices=["host", "gpu"], default="host",
+    ap.add_argument("--bvh", choices=["host", "gpu", "gpu_sah"], default="gpu_sah",
                     help="BVH builder for the scene upload")
     ap.add_argument("--majorant-brick", type=int, choices=[8, 16, 32, 64], default=None,
                     help="majorant brick edge in voxels (default: the library's tuning)")
@@ -574,8 +574,9 @@ def batch_eval(args):
     volume generators, resolution side uniform in 128..1024 with aspect uniform in
     1..16/9, spp log-uniform in 16..256.  The autotuner picks the tuning; then the whole
     set renders as one graph-captured batch (latency = completion time of each request from
-    the batch start, device clock) and, for comparison, one request at a time in order
-    (latency = the running sum of the single-request device times)."""
+    the batch start, device clock) and, for comparison, one request at a time (latency =
+    the running sum of the single-request device times), both in the caller's order and
+    shortest job first, the order the batch itself serves its requests in."""
     import pine_b200 as pb
     ctx = pb.Context(0)
     kinds = ["spheres", "mesh", "volume"]
@@ -599,19 +600,23 @@ def batch_eval(args):
     ctx.render_batch(reqs, outputs=False)  # warm-up
     b = ctx.render_batch(reqs, outputs=False)
     lat_b = np.array(b["request_seconds"])
-    seq, t = [], 0.0
-    for r in reqs:
-        t += ctx.render_batch([r], outputs=False)["seconds"]
-        seq.append(t)
-    lat_s = np.array(seq)
+    single = [ctx.render_batch([r], outputs=False)["seconds"] for r in reqs]
     pct = lambda a, q: float(np.percentile(a, q))
+
+    def sequential(order):
+        done = np.cumsum(np.asarray(single)[order])
+        t = float(done[-1])
+        return {"seconds": t, "value": paths / t / 1e6, "latency_p50_s": pct(done, 50),
+                "latency_p99_s": pct(done, 99)}
+
+    sjf = sorted(range(len(reqs)), key=lambda i: reqs[i]["width"] * reqs[i]["height"] * reqs[i]["spp"])
     ctx.close()
     return {"metric": "Mpaths/s", "workload": f"{len(reqs)} requests (seed {args.batch_seed}): {mix}",
             "paths": int(paths), "tuning": tuning,
             "batch": {"seconds": b["seconds"], "value": paths / b["seconds"] / 1e6,
                       "latency_p50_s": pct(lat_b, 50), "latency_p99_s": pct(lat_b, 99)},
-            "one_at_a_time": {"seconds": t, "value": paths / t / 1e6,
-                              "latency_p50_s": pct(lat_s, 50), "latency_p99_s": pct(lat_s, 99)}}
+            "one_at_a_time": sequential(list(range(len(reqs)))),
+            "one_at_a_time_shortest_first": sequential(sjf)}
 
 
 def guiding_eval(args, cfg, env):

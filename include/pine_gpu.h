@@ -358,10 +358,12 @@ pg_status pg_intersect_device(pg_ctx* ctx, int32_t scene_id, const float* d_rays
 /* ---- BVH construction ----
  * PG_BVH_HOST: binned SAH on the host threads (pine builds its binary BVH on one host
  * thread with a full SAH sweep, src/impl/accel/bvh.cpp:145-284).  PG_BVH_GPU: a linear BVH
- * built on the GPU (Morton order, radix tree, bottom-up boxes), faster to build and
- * slower to traverse.  Both collapse to the same 8-wide compressed format; closest hits do
- * not depend on the tree.  The choice applies to later pg_upload_scene calls. */
-enum { PG_BVH_HOST = 0, PG_BVH_GPU = 1 };
+ * built on the GPU (Morton order, radix tree, bottom-up boxes), fastest to build and
+ * slower to traverse.  PG_BVH_GPU_SAH: the host build's binned SAH tree (the same split
+ * decisions) built on the GPU, the default.  All collapse to the same 8-wide compressed
+ * format; closest hits do not depend on the tree.  The choice applies to later
+ * pg_upload_scene calls. */
+enum { PG_BVH_HOST = 0, PG_BVH_GPU = 1, PG_BVH_GPU_SAH = 2 };
 pg_status pg_set_bvh_builder(pg_ctx* ctx, int32_t builder);
 /* The BVH of a loaded scene: build time (host clock, seconds), depth and node count of the
  * 8-wide tree.  Any output may be NULL. */

@@ -435,9 +435,9 @@ class Context:
         return {"width": w.value, "height": h.value, "spp": s.value, "max_depth": d.value}
 
     def set_bvh_builder(self, builder: str):
-        """"host" (binned SAH on the host threads) or "gpu" (linear BVH on the GPU) for
-        later load_scene calls."""
-        self._check(self._lib.pg_set_bvh_builder(self._ctx, {"host": 0, "gpu": 1}[builder]))
+        """"host" (binned SAH on the host threads), "gpu" (linear BVH on the GPU) or
+        "gpu_sah" (the host's binned SAH tree, built on the GPU) for later load_scene calls."""
+        self._check(self._lib.pg_set_bvh_builder(self._ctx, {"host": 0, "gpu": 1, "gpu_sah": 2}[builder]))
 
     def bvh_info(self, scene: int):
         sec, depth, nodes = ctypes.c_double(), ctypes.c_int32(), ctypes.c_int64()

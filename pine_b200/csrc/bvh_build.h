@@ -62,4 +62,9 @@ WideBVH CollapseToWide(const std::vector<BNode>& nodes, int root,
 // build on (device memory is stream-ordered and released before returning).
 WideBVH BuildWideBVHGpu(const std::vector<Box>& boxes, void* stream);
 
+// The host build's binned SAH tree (same bins, costs, leaf rule and split decisions), built
+// on the GPU top-down (several blocks per node near the root, one warp per subtree below
+// 2048 primitives), then collapsed on the GPU like BuildWideBVHGpu's.
+WideBVH BuildWideBVHGpuSah(const std::vector<Box>& boxes, void* stream);
+
 }  // namespace pg

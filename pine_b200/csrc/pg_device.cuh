@@ -414,12 +414,14 @@ __device__ bool Traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, 
     return found;
 }
 
-// ---------------------------------------------------------------- stepped closest hit
-// The closest-hit traversal of Traverse<false> over [0, inf) as a state machine advanced one
-// loop iteration at a time (TraceStep: one node's children tested, then the primitives of
-// the leaves it hit), so that a persistent warp can give a lane whose ray is done the next
-// ray while its other lanes keep walking.  Each ray takes the same steps in the same order
-// as in Traverse, so hits are identical.
+// ---------------------------------------------------------------- stepped traversal
+// The traversal of Traverse over [0, tmax] as a state machine advanced one loop iteration
+// at a time (TraceStep: one node's children tested, then the primitives of the leaves it
+// hit), so that a persistent warp can give a lane whose ray is done the next ray while its
+// other lanes keep walking.  Closest hit (ANY = false): each ray takes the same steps in the
+// same order as in Traverse, so hits are identical.  First hit (ANY = true, scenes without
+// null surfaces): the walk ends at the first primitive hit, so whether the ray is blocked
+// is the same as Traverse<true>'s answer.
 struct TraceWalk {
     V3 o, d;
     float ix, iy, iz;
@@ -429,13 +431,16 @@ struct TraceWalk {
     Hit hit;  // hit.t is the walk's tmax
 };
 
-// Starts the walk of ray o + t d: planes first (they lie outside the BVH), then the BVH
-// root.  False when there is no BVH: the walk is already over.
-__device__ __forceinline__ bool TraceBegin(const SceneDev& S, V3 o, V3 d, TraceWalk& w) {
+// Starts the walk of ray o + t d, t in [0, tmax]: planes first (they lie outside the BVH),
+// then the BVH root.  False when the walk is already over (no BVH, or for ANY a plane
+// blocks the ray).
+template <bool ANY = false>
+__device__ __forceinline__ bool TraceBegin(const SceneDev& S, V3 o, V3 d, TraceWalk& w,
+                                           float tmax = kFloatMax) {
     w.o = o;
     w.d = d;
     w.hit.prim = -1;
-    w.hit.t = kFloatMax;
+    w.hit.t = tmax;
     w.hit.u = w.hit.v = 0.0f;
     for (int i = 0; i < S.num_planes; i++) {
         const ShapeDev& sh = S.shapes[S.planes[i]];
@@ -445,6 +450,8 @@ __device__ __forceinline__ bool TraceBegin(const SceneDev& S, V3 o, V3 d, TraceW
             w.hit.t = t;
             w.hit.prim = -(2 + S.planes[i]);
             w.hit.u = w.hit.v = 0.0f;
+            if (ANY)
+                return false;
         }
     }
     if (!S.has_bvh)
@@ -461,6 +468,7 @@ __device__ __forceinline__ bool TraceBegin(const SceneDev& S, V3 o, V3 d, TraceW
 
 // One iteration of the traversal loop; false when the walk is over.  `stack` as in
 // Traverse, holding at most `cap` entries.
+template <bool ANY = false>
 __device__ __forceinline__ bool TraceStep(const SceneDev& S, TraceWalk& w, uint2* stack, int stride,
                                           int cap, uint32_t& err) {
     if (w.iter++ >= kTraversalCap) {
@@ -487,7 +495,8 @@ __device__ __forceinline__ bool TraceStep(const SceneDev& S, TraceWalk& w, uint2
         int bit = __ffs(w.tgroup.y) - 1;
         w.tgroup.y &= w.tgroup.y - 1u;
         float tmax = w.hit.t;
-        TestPrim(S, (int)w.tgroup.x + bit, w.o, w.d, 0.0f, tmax, w.hit);
+        if (TestPrim(S, (int)w.tgroup.x + bit, w.o, w.d, 0.0f, tmax, w.hit) && ANY)
+            return false;
     }
     if (w.ngroup.y <= 0x00ffffffu) {
         if (w.sp == 0)

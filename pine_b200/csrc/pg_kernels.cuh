@@ -1134,6 +1134,58 @@ __global__ void PG_SHADE_BOUNDS k_shade(const __grid_constant__ RenderParams P, 
     }
 }
 
+// k_occlude: whether the queued shadow rays are blocked, in scenes with surfaces and
+// neither media nor null surfaces (Traverse<true>, RayIntegrator::IntersectTr,
+// integrator.cpp:68-87), in persistent warps as k_trace.  A blocked entry's unoccluded
+// contribution becomes zero; k_shadow then adds the entries to their paths.
+template <bool MULTI>
+__global__ void __launch_bounds__(kTraceThreads, 8)
+    k_occlude(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    extern __shared__ uint2 stack[];
+    const int n = P.counts[kCntShadow];
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const SceneDev* S = &S0;
+    int entry = -1;
+    TraceWalk w;
+    uint32_t err = 0;
+    bool more = true;
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, entry < 0);
+        if (more && (__popc(idle) >= kTraceRefillLanes || idle == 0xffffffffu)) {
+            int base = 0;
+            if (lane == 0)  // the shadow queue's work counter (k_transmit's in media scenes)
+                base = atomicAdd(&P.counts[kCntTransmitNext], __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            more = base + __popc(idle) < n;
+            if (entry < 0) {
+                const int q = base + __popc(idle & below);
+                if (q < n) {
+                    const float4 so = P.so[q], sd = P.sd[q];
+                    const int slot = (int)(__float_as_uint(P.sc[q].w) & ~kFinalShadow);
+                    S = &SceneOf<MULTI>(P, S0, slot);
+                    if (TraceBegin<true>(*S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), w, so.w))
+                        entry = q;
+                    else if (w.hit.prim != -1)
+                        P.sc[q] = make_float4(0.0f, 0.0f, 0.0f, P.sc[q].w);
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, entry >= 0) == 0) {
+            if (!more)
+                break;
+            continue;
+        }
+        if (entry >= 0 && !TraceStep<true>(*S, w, stack + threadIdx.x, blockDim.x, P.stack_cap, err)) {
+            if (w.hit.prim != -1)
+                P.sc[entry] = make_float4(0.0f, 0.0f, 0.0f, P.sc[entry].w);
+            entry = -1;
+        }
+    }
+    if (err)
+        atomicOr(P.err, err);
+}
+
 template <int M, bool MULTI, bool GUIDE, bool MEDIA, bool GEN>
 __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shadow(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
     extern __shared__ uint2 stack[];

@@ -83,20 +83,28 @@ struct Wave {
     int shadeBlock = 128;
     size_t stackBytes = (size_t)128 * kStackSize * sizeof(uint2);
     int traceCap = kStackSize;  // k_trace's stack entries per thread (TraceCap of the scenes)
+    bool nullSurfaces = false;  // some scene has surfaces without a material
     float4* trk = nullptr;  // per-slot results of k_track (required in scenes with media)
     bool sort = false;      // order the active list by medium cell (k_sort_*) before tracking
 };
 
+// Whether k_occlude decides the shadow rays' visibility before k_shadow: scenes with
+// surfaces and neither media nor null surfaces, shadow rays in their own kernel.
+static bool Occludes(const Wave& w, bool fused) {
+    return !fused && w.surfaces && !w.media && !w.nullSurfaces;
+}
+
 // The parameters of one iteration's launches: k_track's results when it runs (scenes with
-// media), and whether k_transmit applies the shadow rays' transmittance (media without
-// surfaces, shadow rays in their own kernel).
-static RenderParams IterationParams(const Wave& w, bool fused) {
+// media), and whether the shadow rays' transmittance is already applied when k_shadow runs
+// (k_transmit for media without surfaces, k_occlude for surfaces without media; shadow rays
+// in their own kernel).
+static RenderParams IterationParams(const Wave& w, bool fused, bool occlude = false) {
     if (w.media && !w.trk)
         throw Failure{PG_ERR_CUDA, "wavefront with media but no tracking buffer"};
     RenderParams P = w.P;
     P.trk = w.media ? w.trk : nullptr;
     P.stack_cap = w.traceCap;
-    P.transmitted = (P.trk && !fused && !w.surfaces) ? 1 : 0;
+    P.transmitted = ((P.trk && !fused && !w.surfaces) || occlude) ? 1 : 0;
     return P;
 }
 
@@ -120,6 +128,19 @@ static int TraceGrid(int sms, size_t smem) {
     return sms * nb;
 }
 
+template <bool MULTI>
+static int OccludeGrid(int sms, size_t smem) {
+    static int cachedBlocks[kStackSize + 1] = {};
+    const int entries = (int)(smem / (kTraceThreads * sizeof(uint2)));
+    int& nb = cachedBlocks[std::min(entries, kStackSize)];
+    if (nb == 0) {
+        int b = 0;
+        PG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_occlude<MULTI>, kTraceThreads, smem));
+        nb = std::max(1, b);
+    }
+    return sms * nb;
+}
+
 template <int M, bool MULTI, bool FUSED, bool GEN>
 static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, LaunchTimer* timer,
                        RenderResult* res) {
@@ -138,7 +159,8 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
         if (res)
             res->kernelLaunches[k]++;
     };
-    const RenderParams P = IterationParams(w, FUSED);
+    const bool occlude = Occludes(w, FUSED);
+    const RenderParams P = IterationParams(w, FUSED, occlude);
     // The tracking kernels are persistent: one full wave of resident blocks.
     const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     // Queue sorting: both kernels read the queue length on the device and do nothing for
@@ -171,15 +193,20 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
             k_shade<M, MULTI, FUSED, false, true, GEN><<<grid(w.shadeBlock, 2048 / w.shadeBlock), w.shadeBlock, shadeSmem, st>>>(P, w.S0);
     });
     if (!FUSED) {
-        if (P.transmitted)
+        if (P.transmitted && !occlude)
             time(PG_KERNEL_TRANSMIT, [&]() {
                 k_transmit<M, MULTI><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
             });
         time(PG_KERNEL_SHADOW, [&]() {
-            if (!w.media)
+            if (occlude) {
+                const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
+                k_occlude<MULTI><<<OccludeGrid<MULTI>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
+                k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, 0, st>>>(P, w.S0);
+            } else if (!w.media) {
                 k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
-            else
+            } else {
                 k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
+            }
         });
     }
     // Filtered films' splats and the queue swap; counted with the fill kernel.

@@ -248,7 +248,7 @@ struct pg_ctx {
     const uint32_t* sobol_mat = nullptr;   // Sobol tables (built for the first Sobol scene)
     const uint64_t* sobol_vdc = nullptr;
     const uint64_t* sobol_vdc_inv = nullptr;
-    int bvh_builder = PG_BVH_HOST;         // PG_BVH_*: how later scene uploads build their BVH
+    int bvh_builder = PG_BVH_GPU_SAH;      // PG_BVH_*: how later scene uploads build their BVH
 };
 
 namespace pg {
@@ -718,8 +718,9 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
         }
     }
     auto tb0 = std::chrono::steady_clock::now();
-    WideBVH bvh = ctx->bvh_builder == PG_BVH_GPU ? BuildWideBVHGpu(boxes, (void*)st)
-                                                 : BuildWideBVH(boxes);
+    WideBVH bvh = ctx->bvh_builder == PG_BVH_GPU       ? BuildWideBVHGpu(boxes, (void*)st)
+                  : ctx->bvh_builder == PG_BVH_GPU_SAH ? BuildWideBVHGpuSah(boxes, (void*)st)
+                                                       : BuildWideBVH(boxes);
     sc->bvh_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb0).count();
     sc->bvh_nodes = (int64_t)bvh.nodes.size();
     sc->prims = (int64_t)boxes.size();
@@ -1160,6 +1161,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
     w.traceCap = TraceCap(sc.bvh_depth);
+    w.nullSurfaces = sc.dev.has_null_surfaces != 0;
     w.fused = ctx->tuning.split_shadow == 0;
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
@@ -1644,6 +1646,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     uint64_t total = 0, pixels = 0;
     bool surfaces = false, media = false, general = false, splat = false;
     int maxDepth = 1, bvhDepth = 0;
+    bool nullSurfaces = false;
     const int variant = MediaVariant(tune);
     // Shortest job first: requests take their sample ranges in increasing order of their
     // sample count, so small requests complete early (results keep the caller's order).
@@ -1692,6 +1695,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         scenes[k] = s;
         surfaces = surfaces || sc.surfaces;
         bvhDepth = std::max(bvhDepth, sc.bvh_depth);
+        nullSurfaces = nullSurfaces || sc.dev.has_null_surfaces != 0;
         media = media || sc.dev.num_media > 0;
         general = general || sc.general;
         splat = splat || sc.filter_splat != 0;
@@ -1709,6 +1713,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.mode = PG_MATH_FAST;
     w.surfaces = surfaces;
     w.traceCap = TraceCap(bvhDepth);
+    w.nullSurfaces = nullSurfaces;
     w.media = media;
     w.general = general;
     w.splat = splat;
@@ -1921,6 +1926,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     w.mode = mathMode;
     w.surfaces = sc.surfaces;
     w.traceCap = TraceCap(sc.bvh_depth);
+    w.nullSurfaces = sc.dev.has_null_surfaces != 0;
     w.media = sc.dev.num_media > 0;
     w.general = sc.general;
     w.splat = sc.filter_splat != 0;
@@ -2380,7 +2386,8 @@ extern "C" pg_status pg_set_bvh_builder(pg_ctx* ctx, int32_t builder) {
     if (!ctx)
         return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
     return Guard(ctx, [&]() {
-        Require(builder == PG_BVH_HOST || builder == PG_BVH_GPU, "unknown BVH builder");
+        Require(builder == PG_BVH_HOST || builder == PG_BVH_GPU || builder == PG_BVH_GPU_SAH,
+                "unknown BVH builder");
         ctx->bvh_builder = builder;
     });
 }

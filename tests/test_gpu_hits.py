@@ -87,14 +87,15 @@ def test_full_size_mesh_hits(ctx, tmp_path):
     assert (rs == 0).sum() > n // 3  # most rays were aimed at the sphere
 
 
+@pytest.mark.parametrize("builder", ["gpu", "gpu_sah"])
 @pytest.mark.parametrize("name", ["spheres", "mesh"])
-def test_gpu_built_bvh_gives_the_same_hits(pglib, tmp_path, name):
-    """The linear BVH built on the GPU: closest hits do not depend on the tree, so they
-    match pine's exactly, as the host-built tree's do."""
+def test_gpu_built_bvh_gives_the_same_hits(pglib, tmp_path, name, builder):
+    """The trees built on the GPU (linear BVH; binned SAH): closest hits do not depend on the
+    tree, so they match pine's exactly, as the host-built tree's do."""
     z = golden(f"hits_{name}.npz")
     path = write_fixture_scene(z, str(tmp_path))
     with pb.Context(0) as ctx:
-        ctx.set_bvh_builder("gpu")
+        ctx.set_bvh_builder(builder)
         sid = ctx.load_scene(path)
         info = ctx.bvh_info(sid)
         assert info["nodes"] > 0 and info["depth"] > 0
@@ -110,8 +111,9 @@ def test_gpu_built_bvh_gives_the_same_hits(pglib, tmp_path, name):
 
 
 def test_gpu_built_bvh_on_the_full_mesh(pglib, tmp_path):
-    """The benchmark mesh (about 1.3M triangles): both builders' trees give the same
-    closest hits on 65536 random rays, and the GPU build is faster."""
+    """The benchmark mesh (about 1.3M triangles): every builder's tree gives the same
+    closest hits on 65536 random rays, the GPU builds are faster, and the GPU binned SAH
+    build makes the host build's tree (the same 8-wide node count and depth)."""
     from pine_b200 import scenegen
     path = scenegen.mesh_scene(str(tmp_path / "m.txt"), width=64, height=36, spp=1,
                                sampler="Uniform")
@@ -122,17 +124,21 @@ def test_gpu_built_bvh_on_the_full_mesh(pglib, tmp_path):
     rays = np.concatenate([o, d, np.zeros((65536, 1)), np.full((65536, 1), 3.4e38)], 1)
     out = {}
     with pb.Context(0) as ctx:
-        for builder in ("host", "gpu"):
+        for builder in ("host", "gpu", "gpu_sah"):
             ctx.set_bvh_builder(builder)
             sid = ctx.load_scene(path)
             out[builder] = ctx.intersect(sid, rays), ctx.bvh_info(sid)
             ctx.release_scene(sid)
     (hs, hp, ht, _), hi = out["host"]
-    (gs, gp, gt, _), gi = out["gpu"]
-    same = (hs == gs) & (hp == gp)
-    # Ties between two triangles at the same distance may go either way.
-    assert same.mean() > 0.9999
-    assert np.array_equal(ht[same].view(np.uint32), gt[same].view(np.uint32))
-    print(f"host build {hi['build_seconds']:.3f} s, GPU build {gi['build_seconds']:.3f} s; "
-          f"depth {hi['depth']} / {gi['depth']}, nodes {hi['nodes']} / {gi['nodes']}")
-    assert gi["build_seconds"] < hi["build_seconds"]
+    for builder in ("gpu", "gpu_sah"):
+        (gs, gp, gt, _), gi = out[builder]
+        same = (hs == gs) & (hp == gp)
+        # Ties between two triangles at the same distance may go either way.
+        assert same.mean() > 0.9999
+        assert np.array_equal(ht[same].view(np.uint32), gt[same].view(np.uint32))
+        print(f"{builder}: host build {hi['build_seconds']:.3f} s, GPU build "
+              f"{gi['build_seconds']:.3f} s; depth {hi['depth']} / {gi['depth']}, nodes "
+              f"{hi['nodes']} / {gi['nodes']}")
+        assert gi["build_seconds"] < hi["build_seconds"]
+    si = out["gpu_sah"][1]
+    assert (si["nodes"], si["depth"]) == (hi["nodes"], hi["depth"])
