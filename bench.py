@@ -89,7 +89,7 @@ def parse_args():
                     help="majorant brick edge in voxels (default: the library's tuning)")
     ap.add_argument("--queue-capacity", type=int, default=None,
                     help="path slots of the wavefront (default: the library's tuning)")
-    ap.add_argument("--sort-queue", type=int, choices=[0, 1], default=None,
+    ap.add_argument("--sort-queue", type=int, choices=[0, 1, 2], default=None,
                     help="order the active list by medium cell before tracking (default: "
                          "the library's tuning)")
     ap.add_argument("--profile-case", action="store_true",
@@ -110,6 +110,10 @@ def parse_args():
                     help="film size of the guiding evaluation (default: the workload's)")
     ap.add_argument("--guide-time-limit", type=float, default=90.0,
                     help="seconds of render time per method before extrapolating")
+    ap.add_argument("--guide-depth", type=int, default=0,
+                    help="--guiding-eval: guide vertices below this bounce depth (0: the library's default)")
+    ap.add_argument("--guide-budget", type=int, default=0,
+                    help="--guiding-eval: Adam steps per network (0: the library's default)")
     return ap.parse_args()
 
 
@@ -659,7 +663,9 @@ def guiding_eval(args, cfg, env):
                      "reference (s)",
            "workload": f"{args.workload}: " + describe(cfg) + f" at {size[0]}x{size[1]}",
            "math_mode": args.math,
-           "reference": {"spp": args.ref_spp, "rmse_floor": floor ** 0.5}}
+           "reference": {"spp": args.ref_spp, "rmse_floor": floor ** 0.5},
+           "guide_depth": args.guide_depth or "all", "guide_budget": args.guide_budget or 1024}
+    ctx.guide_config(args.guide_depth, args.guide_budget)
     for method in ("plain", "guided"):
         guided = method == "guided"
         if guided:

@@ -272,8 +272,8 @@ typedef struct pg_render_desc {
  * run only in guided renders.  TRACK (delta tracking of the extension rays through grid
  * media) runs in scenes with media; TRANSMIT (ratio tracking of the shadow rays) in scenes
  * with media and no surfaces, when shadow rays have their own kernel.  SORT (the
- * active list ordered by the grid-medium cell of each ray's origin) runs in scenes with grid
- * media when the tuning's sort_queue is set. */
+ * active list ordered by slot, or by the grid-medium cell of each ray's origin) runs as
+ * the tuning's sort_queue selects. */
 enum { PG_KERNEL_REGEN = 0, PG_KERNEL_TRACE = 1, PG_KERNEL_SHADE = 2, PG_KERNEL_SHADOW = 3,
        PG_KERNEL_GUIDE = 4, PG_KERNEL_TRAIN = 5, PG_KERNEL_TRACK = 6, PG_KERNEL_TRANSMIT = 7,
        PG_KERNEL_SORT = 8, PG_NUM_KERNELS = 9 };
@@ -395,9 +395,11 @@ typedef struct pg_tuning {
                                shading kernel */
     int32_t majorant_brick; /* voxels per edge of a grid medium's majorant brick: 8, 16, 32
                                or 64 */
-    int32_t sort_queue;     /* 1: in scenes with grid media, order each iteration's active
-                               list by the cell of the ray origins (8^3 cells per medium
-                               box) before the tracking kernels; 0: queue order */
+    int32_t sort_queue;     /* 2 (default): in scenes with surfaces, rebuild each
+                               iteration's active list in slot order, so that the kernels'
+                               warps read neighbouring path state; 1: in scenes with grid
+                               media, order it by the cell of the ray origins (8^3 cells per
+                               medium box) before the tracking kernels; 0: queue order */
 } pg_tuning;
 
 pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,
@@ -423,6 +425,11 @@ pg_status pg_get_tuning(pg_ctx* ctx, pg_tuning* tuning);
 /* Glorot-uniform weights from `seed`; Adam state, training budget and the guided pass
  * schedule start over. */
 pg_status pg_guide_reset(pg_ctx* ctx, uint64_t seed);
+/* Guided renders of this context: vertices at bounce depth < max_guided_depth (0 = the
+ * camera ray's first hit) sample with the network, deeper ones as the plain path tracer
+ * does (both unbiased); training stops after step_budget Adam steps per network.  A value
+ * <= 0 keeps the current setting. */
+pg_status pg_guide_config(pg_ctx* ctx, int32_t max_guided_depth, int32_t step_budget);
 pg_status pg_guide_get_weights(pg_ctx* ctx, float* weights);
 pg_status pg_guide_set_weights(pg_ctx* ctx, const float* weights);
 /* Raw outputs (n x 40) of n feature rows (n x 32), on the GPU. */

@@ -193,6 +193,7 @@ def lib():
         "pg_parse_scene_file": (st, [ctypes.c_char_p, _P(SceneDesc), _P(ctypes.c_void_p)]),
         "pg_free_parsed_scene": (None, [ctypes.c_void_p]),
         "pg_guide_reset": (st, [ctypes.c_void_p, ctypes.c_uint64]),
+        "pg_guide_config": (st, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
         "pg_guide_get_weights": (st, [ctypes.c_void_p, _F]),
         "pg_guide_set_weights": (st, [ctypes.c_void_p, _F]),
         "pg_guide_forward": (st, [ctypes.c_void_p, _F, ctypes.c_int64, _F]),
@@ -486,6 +487,11 @@ class Context:
     def guide_reset(self, seed: int = 0):
         self._check(self._lib.pg_guide_reset(self._ctx, int(seed)))
 
+    def guide_config(self, max_guided_depth: int = 0, step_budget: int = 0):
+        """Guided renders: network sampling at bounce depths below max_guided_depth, and
+        at most step_budget Adam steps per network (<= 0 keeps a setting)."""
+        self._check(self._lib.pg_guide_config(self._ctx, int(max_guided_depth), int(step_budget)))
+
     def guide_weights(self) -> np.ndarray:
         w = np.empty((6, 64, 64), np.float32)
         self._check(self._lib.pg_guide_get_weights(self._ctx, _fptr(w)))
@@ -523,7 +529,7 @@ class Context:
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def set_tuning(self, queue_capacity: int = 1 << 23, block_size: int = 128,
-                   split_shadow: int = 1, majorant_brick: int = 64, sort_queue: int = 0):
+                   split_shadow: int = 1, majorant_brick: int = 64, sort_queue: int = 2):
         t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick),
                    int(sort_queue))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))

@@ -34,7 +34,11 @@ constexpr int kTileRows = 128;
 constexpr int kTileBytes = kTileRows * kRowBytes;              // 16 KiB
 constexpr int kLayerBytes = kGuideDim * kRowBytes;             // 8 KiB
 constexpr int kWeightBytes = kGuideLayers * kLayerBytes;       // 48 KiB
-constexpr int kFwdSmem = kWeightBytes + 2 * kTileBytes + 1024;
+// Inference: W and one activation block, which each layer's epilogue overwrites with the
+// next layer's input once the layer's MMAs (the block's only reader) have completed; 65 KiB,
+// so three CTAs fit on an SM.
+constexpr int kFwdSmem = kWeightBytes + kTileBytes + 1024;
+constexpr int kFwdCtasPerSm = 3;
 // W, H0..H5, dZ, zero block.
 constexpr int kTrainSmem = kWeightBytes + 8 * kTileBytes + 1024;
 constexpr unsigned long long kWaitNs = 2000000000ull;
@@ -243,13 +247,14 @@ __device__ __forceinline__ void IssueForward(uint32_t tmem, const uint8_t* act, 
 // ---------------------------------------------------------------- inference
 __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict__ w16,
                                                        GuideInput in, int64_t nMax,
-                                                       float* __restrict__ out, uint32_t* err) {
+                                                       float* __restrict__ out, int lobes,
+                                                       uint32_t* err) {
     extern __shared__ uint8_t smemRaw[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmemSlot;
     __shared__ int abortFlag;
     uint8_t* sW = Align1024(smemRaw);
-    uint8_t* sA[2] = {sW + kWeightBytes, sW + kWeightBytes + kTileBytes};
+    uint8_t* sA = sW + kWeightBytes;
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0)
         abortFlag = 0;
@@ -261,14 +266,14 @@ __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict_
     const int64_t tiles = (n + kTileRows - 1) / kTileRows;
     for (int64_t t = blockIdx.x; t < tiles && !abortFlag; t += gridDim.x) {
         const int64_t row = t * kTileRows + tid;
-        LoadInputRow(in, row, row < n, sA[0], tid);
+        LoadInputRow(in, row, row < n, sA, tid);
         FenceProxyAsync();
         FenceBefore();
         __syncthreads();
         for (int l = 0; l < kGuideLayers; l++) {
             if (tid == 0) {
                 FenceAfter();
-                IssueForward(tmem, sA[l & 1], sW + l * kLayerBytes);
+                IssueForward(tmem, sA, sW + l * kLayerBytes);
                 Commit(&bar);
             }
             bool ok = __all_sync(0xffffffffu, BarWait(&bar, phase));
@@ -288,14 +293,21 @@ __global__ void __launch_bounds__(128) k_guide_forward(const __half* __restrict_
 #pragma unroll
                         for (int i = 0; i < 16; i++)
                             v[i] = fmaxf(v[i], 0.0f);
-                        StoreRow16(sA[(l + 1) & 1], tid, q, v);
+                        StoreRow16(sA, tid, q, v);
                     }
                 } else {
                     float o[48];
 #pragma unroll
                     for (int q = 0; q < 3; q++)
                         TmemLoad16(lane + 16 * q, o + 16 * q);
-                    if (row < n) {
+                    if (row < n && lobes) {
+                        float d[kGuideLobeRow];
+                        GuideLobesToRow(o, d);
+                        float4* dst = reinterpret_cast<float4*>(out + row * kGuideLobeRow);
+#pragma unroll
+                        for (int i = 0; i < kGuideLobeRow / 4; i++)
+                            dst[i] = make_float4(d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+                    } else if (row < n) {
                         float4* dst = reinterpret_cast<float4*>(out + row * kGuideOutputs);
 #pragma unroll
                         for (int i = 0; i < kGuideOutputs / 4; i++)
@@ -561,7 +573,7 @@ cudaError_t GuidePack(const GuideNetDev& net, cudaStream_t st) {
 }
 
 cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n, float* out,
-                         int sms, cudaStream_t st) {
+                         int sms, cudaStream_t st, bool lobes) {
     if (n <= 0)
         return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -569,8 +581,8 @@ cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n
     if (e != cudaSuccess)
         return e;
     int64_t tiles = (n + kTileRows - 1) / kTileRows;
-    int grid = (int)std::min<int64_t>(tiles, (int64_t)sms * 2);
-    k_guide_forward<<<grid, 128, kFwdSmem, st>>>(net.w16, in, n, out, net.err);
+    int grid = (int)std::min<int64_t>(tiles, (int64_t)sms * kFwdCtasPerSm);
+    k_guide_forward<<<grid, 128, kFwdSmem, st>>>(net.w16, in, n, out, lobes ? 1 : 0, net.err);
     return cudaGetLastError();
 }
 

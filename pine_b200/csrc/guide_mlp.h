@@ -41,10 +41,11 @@ void GuideNetBind(GuideNetDev& net, void* mem, int blocks);
 // Rebuilds the FP16 image from the FP32 master weights.
 cudaError_t GuidePack(const GuideNetDev& net, cudaStream_t st);
 
-// Raw network outputs (n x 40 FP32) of n input rows.  With in.count the grid is sized for
-// up to `n` rows and the kernel reads the actual count on the device.
+// Raw network outputs (n x 40 FP32) of n input rows, or with `lobes` the mixture as the
+// renderer reads it (n x kGuideLobeRow: GuideLobesToRow).  With in.count the grid is sized
+// for up to `n` rows and the kernel reads the actual count on the device.
 cudaError_t GuideForward(const GuideNetDev& net, const GuideInput& in, int64_t n, float* out,
-                         int sms, cudaStream_t st);
+                         int sms, cudaStream_t st, bool lobes = false);
 
 // Mean over the n rows of the gradient of -weight * log q(dir) with respect to the FP32
 // weights (net.grad) and the loss sum (net.loss).  dirw: n x float4 (dir.xyz, weight);

@@ -29,6 +29,8 @@ constexpr int kGuideDim = 64;        // padded row width of every layer
 constexpr int kGuideLayers = 6;      // weight matrices
 constexpr int kGuideLobes = 8;
 constexpr int kGuideOutputs = 40;    // 5 per lobe
+constexpr int kGuideLobeFloats = 6;  // a lobe as the renderer reads it: mu.xyz, kappa, weight, logNorm
+constexpr int kGuideLobeRow = kGuideLobes * kGuideLobeFloats;
 constexpr int kGuideBins = 5;        // one-blob bins per angle
 constexpr float kGuideLogKappaMin = -3.0f, kGuideLogKappaMax = 7.0f;
 constexpr int kGuideWeights = kGuideLayers * kGuideDim * kGuideDim;
@@ -118,6 +120,35 @@ PG_HD float GuidePdf(const VmfLobe* lobes, V3 w) {
     return p;
 }
 
+// The mixture of one row of raw outputs, written as kGuideLobeRow floats (each lobe's axis,
+// concentration, weight and log normaliser): inference stores this form, so that the
+// sampling kernel reads each lobe when it needs it instead of holding the mixture.
+PG_HD void GuideLobesToRow(const float* raw, float* dst) {
+    VmfLobe lobes[kGuideLobes];
+    GuideMixture(raw, lobes);
+    for (int i = 0; i < kGuideLobes; i++) {
+        float* d = dst + kGuideLobeFloats * i;
+        d[0] = lobes[i].mu.x, d[1] = lobes[i].mu.y, d[2] = lobes[i].mu.z;
+        d[3] = lobes[i].kappa, d[4] = lobes[i].weight, d[5] = lobes[i].logNorm;
+    }
+}
+PG_HD VmfLobe GuideRowLobe(const float* row, int i) {
+    const float* d = row + kGuideLobeFloats * i;
+    VmfLobe l;
+    l.mu = v3(d[0], d[1], d[2]);
+    l.kappa = d[3], l.weight = d[4], l.logNorm = d[5];
+    return l;
+}
+// GuidePdf and GuideSample on a stored row.
+PG_HD float GuidePdfRow(const float* row, V3 w) {
+    float p = 0.0f;
+    for (int i = 0; i < kGuideLobes; i++) {
+        const VmfLobe l = GuideRowLobe(row, i);
+        p += l.weight * VmfPdf(l, w);
+    }
+    return p;
+}
+
 // Orthonormal basis around a unit vector (Duff et al. 2017, "Building an Orthonormal
 // Basis, Revisited").
 PG_HD void GuideBasis(V3 n, V3& b1, V3& b2) {
@@ -159,6 +190,27 @@ PG_HD V3 GuideSample(const VmfLobe* lobes, float u0, float u1, float u2) {
         }
     }
     const VmfLobe& l = lobes[k];
+    float u = Max(u1, 1e-7f);
+    float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * l.kappa)) / l.kappa;
+    w = Clamp(w, -1.0f, 1.0f);
+    float s = sqrtf(Max(0.0f, 1.0f - w * w));
+    float phi = 2 * kPi * u2;
+    V3 b1, b2;
+    GuideBasis(l.mu, b1, b2);
+    return b1 * (s * cosf(phi)) + b2 * (s * sinf(phi)) + l.mu * w;
+}
+
+PG_HD V3 GuideSampleRow(const float* row, float u0, float u1, float u2) {
+    int k = kGuideLobes - 1;
+    float c = 0.0f;
+    for (int i = 0; i < kGuideLobes; i++) {
+        c += row[kGuideLobeFloats * i + 4];
+        if (u0 < c) {
+            k = i;
+            break;
+        }
+    }
+    const VmfLobe l = GuideRowLobe(row, k);
     float u = Max(u1, 1e-7f);
     float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * l.kappa)) / l.kappa;
     w = Clamp(w, -1.0f, 1.0f);

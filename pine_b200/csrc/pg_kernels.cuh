@@ -162,12 +162,13 @@ struct RenderParams {
     cudaGraphConditionalHandle cond;
     // Guided rendering only.
     float4* gq;                  // guide queue, kGuideEntry float4 per entry
-    const float* graw;           // network outputs per guide entry (kGuideOutputs floats)
+    const float* graw;           // the mixture per guide entry (kGuideLobeRow floats)
     float4* rec;                 // training records, kRecordStride float4 each
     float4* rec_dirw;            // per record: sampled direction, target weight
     int* rec_last;               // per slot: newest record of its path, -1 none
     int rec_cap;
     float rec_accept;            // probability of recording a continuing guided vertex
+    int guide_depth;             // vertices at a bounce depth below this are guided
 };
 
 __device__ __forceinline__ int WarpAppend(int* counter, bool pred) {
@@ -961,7 +962,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
             if (!walk)
                 NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, ev.p, v3(0.0f), -d, false, nullptr,
                                            nullptr, m.g, medium, medium, beta, L, stack, ct, ps);
-            if (GUIDE) {
+            if (GUIDE && depth < P.guide_depth) {
                 PushGuide(P, i, ev.p, v3(0.0f), false, medium, -d, ps.idx, medium, medium);
                 deferred = true;
             } else {
@@ -1025,7 +1026,7 @@ __device__ void ShadeOne(const RenderParams& P, const SceneDev& S, const Request
                 if (!walk)
                     NextEvent<M, FUSED, MEDIA>(P, S, i, R.key1, rng, si.p, si.n, -d, true, &mat, &fr,
                                                0.0f, medIn, medOut, beta, L, stack, ct, ps);
-                if (GUIDE && GuideEligible(mat)) {
+                if (GUIDE && GuideEligible(mat) && depth < P.guide_depth) {
                     PushGuide(P, i, si.p, si.n, true, sh.material, -d, ps.idx, medIn, medOut);
                     deferred = true;
                 } else {
@@ -1399,6 +1400,19 @@ static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const __gr
     }
 }
 
+// ---------------------------------------------------------------- slot order
+// Flags the slots of the queued active list (sort_keys as one flag per slot); a CUB select
+// of the flagged slot indices then writes them in ascending order to P.sorted.
+static __global__ void k_slot_mark(const __grid_constant__ RenderParams P) {
+    const int n = P.counts[kCntActive];
+    const int* q = QueuedList(P);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        P.sort_keys[q[i]] = 1;
+}
+static __global__ void k_slot_sorted(const __grid_constant__ RenderParams P) {
+    P.counts[kCntSorted] = 1;
+}
+
 // ---------------------------------------------------------------- tracking kernels
 // Delta tracking of the extension rays (k_track) and ratio tracking of the shadow rays
 // (k_transmit) run in persistent warps: each lane walks one ray through the majorant bricks
@@ -1616,8 +1630,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
     V3 beta = v3(bt.x, bt.y, bt.z);
     int depth = __float_as_int(bt.w);
     Rng rng = PathRng<true>(R, P.sample[i], __float_as_uint(Lw.w));
-    VmfLobe lobes[kGuideLobes];
-    GuideMixture(P.graw + (size_t)kGuideOutputs * q, lobes);
+    const float* lobes = P.graw + (size_t)kGuideLobeRow * q;
     const GuideFrameT gf = GuideFrame(surface, n, wi);  // the mixture's frame
     const float uSel = rng.Get1D();
     V3 w = v3(0.0f, 0.0f, 1.0f), f = v3(0.0f);
@@ -1641,7 +1654,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
         } else {
             float u0 = rng.Get1D(), u1, u2;
             rng.Get2D(u1, u2);
-            w = gf.ToWorld(GuideSample(lobes, u0, u1, u2));
+            w = gf.ToWorld(GuideSampleRow(lobes, u0, u1, u2));
             MaterialEval<M>(mat, wiL, fr.ToLocal(w), f, pdfB);
             ok = true;
         }
@@ -1655,14 +1668,14 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
         } else {
             float u0 = rng.Get1D(), u1, u2;
             rng.Get2D(u1, u2);
-            w = gf.ToWorld(GuideSample(lobes, u0, u1, u2));
+            w = gf.ToWorld(GuideSampleRow(lobes, u0, u1, u2));
             pdfB = PhaseHG<M>(Dot(wi, w), m.g);
         }
         f = v3(pdfB);
         ok = pdfB > 0.0f;
     }
     const V3 wl = gf.ToLocal(w);
-    const float pc = ok ? 0.5f * pdfB + 0.5f * GuidePdf(lobes, wl) : 0.0f;
+    const float pc = ok ? 0.5f * pdfB + 0.5f * GuidePdfRow(lobes, wl) : 0.0f;
     bool finished = !(pc > 0.0f) || !isfinite(pc);
     const V3 betaVertex = beta;
     if (!finished) {

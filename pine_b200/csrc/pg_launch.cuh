@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <utility>
 #include <vector>
@@ -86,6 +88,10 @@ struct Wave {
     bool nullSurfaces = false;  // some scene has surfaces without a material
     float4* trk = nullptr;  // per-slot results of k_track (required in scenes with media)
     bool sort = false;      // order the active list by medium cell (k_sort_*) before tracking
+    bool slotSort = false;  // order the active list by slot (k_slot_mark + CUB select)
+    void* selectTemp = nullptr;
+    size_t selectBytes = 0;
+    int* selectCount = nullptr;
 };
 
 // Whether k_occlude decides the shadow rays' visibility before k_shadow: scenes with
@@ -170,6 +176,16 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
             k_sort_keys<MULTI><<<sms * 4, kSortThreads, 0, st>>>(P, w.S0);
             k_sort_scatter<<<sms * 4, kSortThreads, 0, st>>>(P);
         });
+    // Slot order (scenes with surfaces): the active list rebuilt as the ascending list of its
+    // slots, so that each warp's entries read neighbouring path-state slots.
+    if (w.slotSort && w.surfaces)
+        time(PG_KERNEL_SORT, [&]() {
+            PG_CUDA(cudaMemsetAsync(P.sort_keys, 0, (size_t)P.slots * sizeof(uint16_t), st));
+            k_slot_mark<<<sms * 4, 256, 0, st>>>(P);
+            PG_CUDA(cub::DeviceSelect::Flagged(w.selectTemp, w.selectBytes, cub::CountingInputIterator<int>(0),
+                                               P.sort_keys, P.sorted, w.selectCount, P.slots, st));
+            k_slot_sorted<<<1, 1, 0, st>>>(P);
+        });
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
             const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
@@ -249,7 +265,8 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
         if (res)
             res->kernelLaunches[k]++;
     };
-    const RenderParams P = IterationParams(w, FUSED);
+    const bool occlude = Occludes(w, FUSED);
+    const RenderParams P = IterationParams(w, FUSED, occlude);
     const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     if (w.surfaces)
         time(PG_KERNEL_TRACE, [&]() {
@@ -274,16 +291,22 @@ static void LaunchGuidedBody(const LaunchEnv& env, Wave& w, int n, LaunchTimer* 
         for (int k = 0; k < 3; k++)
             in.lo[k] = w.S0.guide_lo[k], in.inv[k] = w.S0.guide_inv[k];
         in.count = &P.counts[kCntGuide];
-        PG_CUDA(GuideForward(*env.guide, in, n, const_cast<float*>(P.graw), sms, st));
+        PG_CUDA(GuideForward(*env.guide, in, n, const_cast<float*>(P.graw), sms, st, true));
         k_guide_sample<M><<<grid(tb, 12), tb, 0, st>>>(P, w.S0);
     });
     if (!FUSED) {
-        if (P.transmitted)
+        if (P.transmitted && !occlude)
             time(PG_KERNEL_TRANSMIT, [&]() {
                 k_transmit<M, false><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
             });
         time(PG_KERNEL_SHADOW, [&]() {
-            k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
+            if (occlude) {
+                const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
+                k_occlude<false><<<OccludeGrid<false>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
+                k_shadow<M, false, true, false, true><<<grid(tb, 12), tb, 0, st>>>(P, w.S0);
+            } else {
+                k_shadow<M, false, true, true, true><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
+            }
         });
     }
     time(PG_KERNEL_REGEN, [&]() {

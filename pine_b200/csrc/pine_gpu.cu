@@ -111,6 +111,16 @@ struct DeviceScene {
 
 
 // ---------------------------------------------------------------- path pool
+// Scratch bytes of the CUB select that rebuilds an active list of up to n slots in slot
+// order (sort_queue 2).
+static size_t SlotSortScratch(int n) {
+    size_t bytes = 0;
+    PG_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, cub::CountingInputIterator<int>(0),
+                                       static_cast<const uint16_t*>(nullptr), static_cast<int*>(nullptr),
+                                       static_cast<int*>(nullptr), n));
+    return std::max<size_t>(bytes, 256);
+}
+
 struct Pool {
     DevMem mem;
     int slots = 0;
@@ -125,6 +135,9 @@ struct Pool {
     int* sorted = nullptr;     // the sorted active list, its keys and the bins (k_sort_*)
     uint16_t* sort_keys = nullptr;
     int* sort_bins = nullptr;
+    void* select_temp = nullptr;  // slot-order sorting: CUB select's scratch and count
+    size_t select_bytes = 0;
+    int* select_count = nullptr;
     void Ensure(int n) {
         if (n <= slots)
             return;
@@ -150,6 +163,9 @@ struct Pool {
         sorted = mem.Alloc<int>(n);
         sort_keys = mem.Alloc<uint16_t>(n);
         sort_bins = mem.Alloc<int>(2 * kSortBins + 1);
+        select_bytes = SlotSortScratch(n);
+        select_temp = mem.Alloc<uint8_t>(select_bytes);
+        select_count = mem.Alloc<int>(1);
     }
 };
 
@@ -158,6 +174,8 @@ struct Pool {
 constexpr int kRecordCap = 1 << 20;     // training records per pass
 constexpr int kTrainBatch = 1 << 18;    // records per Adam step
 constexpr float kGuideLr = 1e-2f;
+constexpr int kGuideDepthDefault = 1 << 30;        // every eligible vertex is guided
+constexpr int64_t kGuideStepBudgetDefault = 1024;  // Adam steps per network (pg_guide_reset)
 
 // Zeroes every allocation of mem (on its stream when it is stream-ordered).
 static void ZeroAll(DevMem& mem);
@@ -176,7 +194,7 @@ struct GuidePool {
         mem.Free();
         slots = n;
         gq = mem.Alloc<float4>((size_t)kGuideEntry * n);
-        graw = mem.Alloc<float>((size_t)kGuideOutputs * n);
+        graw = mem.Alloc<float>((size_t)kGuideLobeRow * n);
         rec_last = mem.Alloc<int>(n);
         rec = mem.Alloc<float4>((size_t)kRecordStride * kRecordCap);
         rec_dirw = mem.Alloc<float4>(kRecordCap);
@@ -233,13 +251,15 @@ struct pg_ctx {
     // kernels, 64-voxel majorant bricks (volume benchmark on B200: 915 Mpaths/s against 853
     // with 32-voxel and 704 with 16-voxel bricks at 2^22 slots; 951 with 2^23 slots, 825
     // with 2^21).
-    pg_tuning tuning{1 << 23, 128, 1, 64, 0};
+    pg_tuning tuning{1 << 23, 128, 1, 64, 2};
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
     pg::GuidePool guide_pool;              // guided-render queues and training records
     int guide_pass = 1;                    // samples per pixel of the next guided pass
     int64_t guide_steps = 0;               // Adam steps taken since the network was reset
+    int guide_depth = pg::kGuideDepthDefault;  // guided vertices: bounce depth below this
+    int64_t guide_budget = pg::kGuideStepBudgetDefault;  // Adam steps per network
     pg::DevMem halton_mem;                 // Halton tables (built for the first Halton scene)
     const int* halton_primes = nullptr;
     const pg::DivMagic* halton_magic = nullptr;
@@ -949,6 +969,7 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.splat = pl.splat, P.splat_req = pl.splat_req;
     w.trk = pl.trk;
     P.sorted = pl.sorted, P.sort_keys = pl.sort_keys, P.sort_bins = pl.sort_bins;
+    w.selectTemp = pl.select_temp, w.selectBytes = pl.select_bytes, w.selectCount = pl.select_count;
     P.counts = ctx->counts;
     P.film_sum = ctx->film.sum, P.film_sq = ctx->film.sq, P.film_wsum = ctx->film.wsum;
     P.film_w2sum = ctx->film.w2sum, P.film_n = ctx->film.n, P.film_acc = nullptr;
@@ -1166,13 +1187,15 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
-    w.sort = ctx->tuning.sort_queue != 0;
+    w.sort = ctx->tuning.sort_queue == 1;
+    w.slotSort = ctx->tuning.sort_queue == 2;
     w.guide = recordAccept != nullptr;
     w.media = sc.dev.num_media > 0;
     w.general = sc.general;
     w.splat = sc.filter_splat != 0;
     if (w.guide)
         w.P.rec_accept = *recordAccept;
+    w.P.guide_depth = ctx->guide_depth;
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, ctx->tuning.queue_capacity), total);
     PrepareWave(ctx, w, slots, total, (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30));
     RequestDev rq{};
@@ -1308,10 +1331,19 @@ extern "C" void pg_destroy(pg_ctx* ctx) {
     ctx->scenes.clear();
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    // Every device buffer is released here, while the stream its stream-ordered frees are
+    // queued on still exists (a DevMem left to its destructor would free on a destroyed
+    // stream).
     ctx->pool.mem.Free();
     ctx->film.mem.Free();
     ctx->small.Free();
-    ctx->halton_mem.Free();  // stream-ordered: freed while the stream still exists
+    ctx->req_buf.Free();
+    ctx->sample_mem.Free();
+    ctx->guide_mem.Free();
+    ctx->guide_pool.mem.Free();
+    ctx->halton_mem.Free();
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
     if (ctx->h_counts)
         cudaFreeHost(ctx->h_counts);
     if (ctx->ev0)
@@ -1412,7 +1444,6 @@ static GuideNetDev& EnsureGuide(pg_ctx* ctx);
 // the context's training budget.  Everything is queued on the stream without host
 // synchronisation.  Returns the steps taken; *rows the rows trained on.
 constexpr int kMinTrainSteps = 16, kMaxTrainSteps = 32;
-constexpr int64_t kGuideStepBudget = 1024;  // Adam steps per network (pg_guide_reset)
 
 static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec, int64_t& rows) {
     GuideNetDev& net = ctx->guide;
@@ -1423,7 +1454,7 @@ static int64_t TrainOnRecords(pg_ctx* ctx, const DeviceScene& sc, int64_t nrec, 
         return 0;
     int64_t steps = std::min<int64_t>(
         kMaxTrainSteps, std::max<int64_t>(kMinTrainSteps, (nrec + kTrainBatch - 1) / kTrainBatch));
-    steps = std::min<int64_t>(steps, kGuideStepBudget - ctx->guide_steps);
+    steps = std::min<int64_t>(steps, ctx->guide_budget - ctx->guide_steps);
     for (int64_t k = 0; k < steps; k++) {
         int64_t b = (k * kTrainBatch) % nrec;
         int64_t nb = std::min<int64_t>(kTrainBatch, nrec - b);
@@ -1454,7 +1485,7 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
                          RenderResult& res) {
     Require(!sc.random_walk, "guided rendering needs the Path integrator");
     EnsureGuide(ctx);
-    float accept = ctx->guide_steps < kGuideStepBudget ? 1.0f : 0.0f;
+    float accept = ctx->guide_steps < ctx->guide_budget ? 1.0f : 0.0f;
     int done = 0;
     while (done < spp) {
         int passSpp = ctx->guide_pass;
@@ -1476,7 +1507,7 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
         // While training, a pass is at most what fills the record buffer, so that the
         // network takes its Adam steps after every kRecordCap vertices or so.
         const double perSpp = (double)r.stats[kStatGuided] / sp;
-        if (ctx->guide_steps < kGuideStepBudget && perSpp > 0)
+        if (ctx->guide_steps < ctx->guide_budget && perSpp > 0)
             ctx->guide_pass = std::max(1, std::min(ctx->guide_pass, (int)(kRecordCap / perSpp)));
         if (accept > 0.0f) {
             int nrec = 0;
@@ -1492,7 +1523,7 @@ static void RenderGuided(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, ui
             res.seconds += dt;
             // Record about kRecordCap vertices in the next pass, none once the budget is spent.
             int next = ctx->guide_pass;
-            accept = ctx->guide_steps >= kGuideStepBudget ? 0.0f
+            accept = ctx->guide_steps >= ctx->guide_budget ? 0.0f
                      : perSpp > 0 ? (float)std::min(1.0, kRecordCap / (perSpp * next))
                                   : 1.0f;
         }
@@ -1718,7 +1749,8 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
     w.general = general;
     w.splat = splat;
     w.fused = tune.split_shadow == 0;
-    w.sort = tune.sort_queue != 0;
+    w.sort = tune.sort_queue == 1;
+    w.slotSort = tune.sort_queue == 2;
     w.shadeBlock = tune.block_size;
     w.S0 = scenes[0];
     int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, tune.queue_capacity), total);
@@ -1770,7 +1802,7 @@ static bool ValidTuning(const pg_tuning& t) {
            (t.split_shadow == 0 || t.split_shadow == 1) &&
            (t.majorant_brick == 8 || t.majorant_brick == 16 || t.majorant_brick == 32 ||
             t.majorant_brick == 64) &&
-           (t.sort_queue == 0 || t.sort_queue == 1);
+           (t.sort_queue >= 0 && t.sort_queue <= 2);
 }
 
 }  // namespace pg
@@ -1794,8 +1826,8 @@ extern "C" pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_
 }
 
 // Coordinate descent over the tuning space on a 1/8-spp sample of the request mix: brick
-// size, shadow split, shading block size, queue capacity, each chosen with the others
-// fixed, keeping a value only when it is at least 2% faster.
+// size, shadow split, shading block size, queue capacity, queue order, each chosen with
+// the others fixed, keeping a value only when it is at least 2% faster.
 extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n, pg_tuning* chosen) {
     if (!ctx)
         return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
@@ -1814,9 +1846,9 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
         double bestT = measure(best);
         const int bricks[] = {8, 16, 32, 64}, blocks[] = {32, 64, 128};
         const int caps[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
-        for (int dim = 0; dim < 4; dim++) {
+        for (int dim = 0; dim < 5; dim++) {
             std::vector<pg_tuning> cands;
-            for (int k = 0; k < (dim == 1 ? 2 : (dim == 2 ? 3 : 4)); k++) {
+            for (int k = 0; k < (dim == 1 ? 2 : (dim == 2 || dim == 4 ? 3 : 4)); k++) {
                 pg_tuning t = best;
                 if (dim == 0)
                     t.majorant_brick = bricks[k];
@@ -1824,8 +1856,10 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
                     t.split_shadow = k;
                 else if (dim == 2)
                     t.block_size = std::min(blocks[k], kMaxShadeBlock);
-                else
+                else if (dim == 3)
                     t.queue_capacity = caps[k];
+                else
+                    t.sort_queue = k;
                 cands.push_back(t);
             }
             for (auto& t : cands) {
@@ -2136,6 +2170,17 @@ extern "C" pg_status pg_guide_reset(pg_ctx* ctx, uint64_t seed) {
         EnsureGuide(ctx);
         GuideInit(ctx, seed);
         PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" pg_status pg_guide_config(pg_ctx* ctx, int32_t max_guided_depth, int32_t step_budget) {
+    if (!ctx)
+        return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
+    return Guard(ctx, [&]() {
+        if (max_guided_depth > 0)
+            ctx->guide_depth = max_guided_depth;
+        if (step_budget > 0)
+            ctx->guide_budget = step_budget;
     });
 }
 

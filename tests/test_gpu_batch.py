@@ -94,3 +94,23 @@ def test_queue_sorting_changes_no_path(ctx, tmp_path, split):
     np.testing.assert_array_equal(out[0]["mean"], out[1]["mean"])
     np.testing.assert_array_equal(out[0]["var"], out[1]["var"])
     ctx.release_scene(sid)
+
+
+def test_slot_order_changes_no_path(ctx, tmp_path):
+    """Rebuilding the active list in slot order (the default in scenes with surfaces) only
+    changes which lanes take which paths: the spheres scene with the counter-based stream
+    and a box film renders the same image bit for bit in queue order and in slot order."""
+    z = golden("image_spheres_c0.npz")
+    sid = ctx.load_scene(write_fixture_scene(z, str(tmp_path)))
+    before = ctx.tuning()
+    out = []
+    for sort in (0, 2):
+        ctx.set_tuning(**dict(before, queue_capacity=1 << 20, sort_queue=sort))
+        out.append(ctx.render(sid, spp=256, seed=5, math_mode="fast"))
+    ctx.set_tuning(**before)
+    assert out[0]["stats"]["kernels"]["sort"]["launches"] == 0
+    assert out[1]["stats"]["kernels"]["sort"]["launches"] > 0
+    np.testing.assert_array_equal(out[0]["count"], out[1]["count"])
+    np.testing.assert_array_equal(out[0]["mean"], out[1]["mean"])
+    np.testing.assert_array_equal(out[0]["var"], out[1]["var"])
+    ctx.release_scene(sid)
