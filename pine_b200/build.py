@@ -27,7 +27,7 @@ SOURCES = ["pine_gpu.cu", "pg_kernels_pine.cu", "pg_kernels_fast.cu", "guide_mlp
            "scene_load.cpp", "bvh_build.cpp", "bvh_gpu.cu"]
 HEADERS = ["pg_math.h", "pg_device.cuh", "pg_shade.cuh", "pg_kernels.cuh", "scene_load.h",
            "bvh_build.h", "guide_net.cuh", "guide_mlp.h", "pg_nodes.h", "pg_sampler.h",
-           "pg_launch.cuh", "pg_error.h"]
+           "pg_launch.cuh", "pg_error.h", "sobol_dirnums.inc"]
 
 
 def _nvcc() -> str:

@@ -67,7 +67,8 @@ enum SlotState : int { kSlotEmpty = 0, kSlotActive = 1, kSlotFinished = 2, kSlot
 // Counters in device memory (RenderParams::counts).
 enum CountIndex { kCntActive = 0, kCntShadow = 1, kCntNext = 2, kCntFinished = 3, kCntParity = 4,
                   kCntIter = 5, kCntGuide = 6, kCntRecords = 7, kCntSplat = 8, kCntTrackNext = 9,
-                  kCntTransmitNext = 10, kCntSorted = 11, kCntTraceNext = 12, kNumCounts = 13 };
+                  kCntTransmitNext = 10, kCntSorted = 11, kCntTraceNext = 12, kCntOccludeNext = 13,
+                  kNumCounts = 14 };
 
 // k_track's result per slot (RenderParams::trk): the scattering position (world space) and,
 // in w, the tracking stream's next dimension with kTrackScattered set when the walk ended in
@@ -155,6 +156,8 @@ struct RenderParams {
     uint16_t* sort_keys;
     int* sort_bins;
     int transmitted;             // 1: k_transmit scaled sc by each shadow ray's transmittance
+    int per_entry;               // 1: k_transmit and k_occlude each take the entries of their
+                                 // kind of scene and mark them kShadowDone (mixed batches)
     int stack_cap;               // k_trace's traversal stack entries per thread (at least the
                                  // BVH's depth + 2, at most kStackSize)
     int max_iter;
@@ -547,6 +550,7 @@ static __global__ void k_swap(const __grid_constant__ RenderParams P) {
     c[kCntTrackNext] = 0;
     c[kCntTransmitNext] = 0;
     c[kCntTraceNext] = 0;
+    c[kCntOccludeNext] = 0;
     c[kCntSorted] = 0;
     c[kCntParity] ^= 1;
     int it = ++c[kCntIter];
@@ -785,11 +789,16 @@ struct ShadeCounters {
 };
 
 // The shadow-queue entry a shading step produced (-1: none).  The top bit of the slot
-// word of an entry marks the path's last shadow ray: k_shadow then finishes the path.
+// word of an entry marks the path's last shadow ray: k_shadow then finishes the path.  In
+// batches that mix scenes with media and scenes with surfaces (RenderParams::per_entry),
+// the next bit marks an entry whose transmittance k_transmit or k_occlude has already
+// applied to its contribution.
 struct PendingShadow {
     int idx = -1;
 };
 constexpr uint32_t kFinalShadow = 0x80000000u;
+constexpr uint32_t kShadowDone = 0x40000000u;
+constexpr uint32_t kShadowSlot = 0x3fffffffu;
 
 // Next-event estimation (RayIntegrator::EstimateDirect, integrator.cpp:88-119): picks a
 // light, samples it, evaluates the BSDF (surface) or phase function (medium) and either
@@ -1155,20 +1164,28 @@ __global__ void __launch_bounds__(kTraceThreads, 8)
         const unsigned idle = __ballot_sync(0xffffffffu, entry < 0);
         if (more && (__popc(idle) >= kTraceRefillLanes || idle == 0xffffffffu)) {
             int base = 0;
-            if (lane == 0)  // the shadow queue's work counter (k_transmit's in media scenes)
-                base = atomicAdd(&P.counts[kCntTransmitNext], __popc(idle));
+            if (lane == 0)
+                base = atomicAdd(&P.counts[kCntOccludeNext], __popc(idle));
             base = __shfl_sync(0xffffffffu, base, 0);
             more = base + __popc(idle) < n;
             if (entry < 0) {
                 const int q = base + __popc(idle & below);
                 if (q < n) {
                     const float4 so = P.so[q], sd = P.sd[q];
-                    const int slot = (int)(__float_as_uint(P.sc[q].w) & ~kFinalShadow);
-                    S = &SceneOf<MULTI>(P, S0, slot);
-                    if (TraceBegin<true>(*S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), w, so.w))
-                        entry = q;
-                    else if (w.hit.prim != -1)
-                        P.sc[q] = make_float4(0.0f, 0.0f, 0.0f, P.sc[q].w);
+                    const uint32_t word = __float_as_uint(P.sc[q].w);
+                    S = &SceneOf<MULTI>(P, S0, (int)(word & kShadowSlot));
+                    // Mixed batches: this kernel takes the entries of scenes with surfaces
+                    // and neither media nor null surfaces, and marks them done.
+                    const bool mine = !P.per_entry || ((S->has_bvh || S->num_planes) && S->num_media == 0 &&
+                                                       !S->has_null_surfaces);
+                    if (mine) {
+                        if (P.per_entry)
+                            reinterpret_cast<uint32_t*>(&P.sc[q])[3] = word | kShadowDone;
+                        if (TraceBegin<true>(*S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), w, so.w))
+                            entry = q;
+                        else if (w.hit.prim != -1)
+                            P.sc[q] = make_float4(0.0f, 0.0f, 0.0f, P.sc[q].w);
+                    }
                 }
             }
         }
@@ -1203,12 +1220,12 @@ __global__ void __launch_bounds__(128, MEDIA ? PG_SHADOW_MIN_BLOCKS : 7) k_shado
         if (q < n) {
             float4 so = P.so[q], sd = P.sd[q], sc = P.sc[q];
             uint32_t w = __float_as_uint(sc.w);
-            slot = (int)(w & ~kFinalShadow);
+            slot = (int)(w & kShadowSlot);
             last = (w & kFinalShadow) != 0;
             const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
             V3 tr = v3(1.0f);
-            if (P.transmitted) {
-                traced = 1;  // k_transmit already applied the transmittance to sc
+            if (P.transmitted || (w & kShadowDone)) {
+                traced = 1;  // k_transmit or k_occlude already applied the transmittance to sc
             } else {
                 HashRng rng{P.sample[slot], P.skey[q], 0};
                 tr = ShadowTr<M, MEDIA>(S, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
@@ -1530,8 +1547,14 @@ __device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const Scene
     if (medium < 0)
         return false;
     const float4 so = P.so[q], sc = P.sc[q];
-    const int slot = (int)(__float_as_uint(sc.w) & ~kFinalShadow);
+    const int slot = (int)(__float_as_uint(sc.w) & kShadowSlot);
     const SceneDev& S = SceneOf<MULTI>(P, S0, slot);
+    if (P.per_entry) {
+        // Mixed batches: this kernel takes the entries of scenes without surfaces.
+        if (S.has_bvh || S.num_planes)
+            return false;
+        reinterpret_cast<uint32_t*>(&P.sc[q])[3] = __float_as_uint(sc.w) | kShadowDone;
+    }
     med = &S.media[medium];
     if (med->type != PG_MEDIUM_GRID) {
         // HomogeneousMedium::Tr (medium.cpp:33-36): closed form.

@@ -104,14 +104,23 @@ static bool Occludes(const Wave& w, bool fused) {
 // media), and whether the shadow rays' transmittance is already applied when k_shadow runs
 // (k_transmit for media without surfaces, k_occlude for surfaces without media; shadow rays
 // in their own kernel).
-static RenderParams IterationParams(const Wave& w, bool fused, bool occlude = false) {
+static RenderParams IterationParams(const Wave& w, bool fused, bool occlude = false,
+                                    bool perEntry = false) {
     if (w.media && !w.trk)
         throw Failure{PG_ERR_CUDA, "wavefront with media but no tracking buffer"};
     RenderParams P = w.P;
     P.trk = w.media ? w.trk : nullptr;
     P.stack_cap = w.traceCap;
     P.transmitted = ((P.trk && !fused && !w.surfaces) || occlude) ? 1 : 0;
+    P.per_entry = perEntry ? 1 : 0;
     return P;
+}
+
+// Batches that mix scenes with media and scenes with surfaces: k_transmit takes the shadow
+// rays of the scenes without surfaces, k_occlude those of the scenes with surfaces and
+// neither media nor null surfaces, and k_shadow traces the rest itself.
+static bool PerEntryShadows(const Wave& w, bool fused) {
+    return w.multi && !fused && w.surfaces && w.media;
 }
 
 // The traversal stack k_trace needs for a BVH of depth `depth` (8-wide levels below the
@@ -166,7 +175,8 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
             res->kernelLaunches[k]++;
     };
     const bool occlude = Occludes(w, FUSED);
-    const RenderParams P = IterationParams(w, FUSED, occlude);
+    const bool perEntry = PerEntryShadows(w, FUSED);
+    const RenderParams P = IterationParams(w, FUSED, occlude, perEntry);
     // The tracking kernels are persistent: one full wave of resident blocks.
     const int trackGrid = sms * PG_TRACK_MIN_BLOCKS;
     // Queue sorting: both kernels read the queue length on the device and do nothing for
@@ -213,11 +223,19 @@ static void LaunchBody(const LaunchEnv& env, Wave& w, int n, bool persistent, La
             time(PG_KERNEL_TRANSMIT, [&]() {
                 k_transmit<M, MULTI><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
             });
+        if (perEntry)
+            time(PG_KERNEL_TRANSMIT, [&]() {
+                k_transmit<M, MULTI><<<trackGrid, kTrackThreads, 0, st>>>(P, w.S0);
+            });
         time(PG_KERNEL_SHADOW, [&]() {
             if (occlude) {
                 const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
                 k_occlude<MULTI><<<OccludeGrid<MULTI>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
                 k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, 0, st>>>(P, w.S0);
+            } else if (perEntry) {
+                const size_t smem = (size_t)kTraceThreads * w.traceCap * sizeof(uint2);
+                k_occlude<MULTI><<<OccludeGrid<MULTI>(sms, smem), kTraceThreads, smem, st>>>(P, w.S0);
+                k_shadow<M, MULTI, false, true, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
             } else if (!w.media) {
                 k_shadow<M, MULTI, false, false, GEN><<<grid(tb, 12), tb, stackBytes, st>>>(P, w.S0);
             } else {
