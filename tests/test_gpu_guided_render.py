@@ -111,12 +111,17 @@ def _zfrac(a, b):
     return np.mean(np.abs(z) < 2.576), z
 
 
-@pytest.mark.parametrize("name,spp", [("spheres", 256), ("volume", 128)])
-def test_guided_matches_plain_within_mc_error(ctx, tmp_path, name, spp):
+@pytest.mark.parametrize("name,spp,depth", [("spheres", 256, 0), ("volume", 128, 0),
+                                           ("spheres", 256, 1), ("volume", 128, 2)])
+def test_guided_matches_plain_within_mc_error(ctx, tmp_path, name, spp, depth):
+    """Guided renders have the plain tracer's expectation, with every eligible vertex
+    guided (depth 0: the default) or only those below a bounce depth (pg_guide_config)."""
     sid = ctx.load_scene(write_fixture_scene(golden(f"image_{name}.npz"), str(tmp_path)))
     plain = ctx.render(sid, spp=spp, seed=1, math_mode="fast")
+    ctx.guide_config(max_guided_depth=depth if depth else 1 << 30)
     ctx.guide_reset(seed=0)
     guided = ctx.render(sid, spp=spp, seed=2, math_mode="fast", guiding=True)
+    ctx.guide_config(max_guided_depth=1 << 30)
     st = guided["stats"]
     assert st["kernels"]["guide"]["items"] > 0 and st["kernels"]["train"]["items"] > 0
     assert st["dropped"] == 0 and st["paths"] == plain["stats"]["paths"]
