@@ -112,6 +112,10 @@ struct SceneDev {
     const pg_node_op* node_ops;  // shader-node programs of the materials
     float guide_lo[3];       // scene bounds the guiding network's position encoding maps
     float guide_inv[3];      // to [0,1]^3: lo and 1 / extent
+    // Single-request waves of a scene whose only medium is a grid: a copy of that medium in
+    // the kernel parameters, so that the tracking kernels read its fields as constants.
+    int single_grid;
+    MediumDev grid0;
 };
 
 // Error flags written by kernels (bitmask), converted to pg_status on the host.

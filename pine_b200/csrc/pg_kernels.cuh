@@ -1448,10 +1448,17 @@ constexpr int kTrackThreads = 128;
 #define PG_TRACK_MIN_BLOCKS 8
 #endif
 
+// The medium a tracking lane walks: with SINGLE (a single-request wave whose scene has one
+// grid medium) the copy in the kernel parameters, else the lane's medium.
+template <bool SINGLE>
+__device__ __forceinline__ const MediumDev& WalkMedium(const SceneDev& S0, const MediumDev* med) {
+    return SINGLE ? S0.grid0 : *med;
+}
+
 // Starts slot i's delta-tracking walk when its ray is in a grid medium: false when there is
 // nothing to walk (no grid medium: the shading kernel tracks inline; or the ray misses the
 // grid: the result, no collision, is written here).
-template <int M, bool MULTI, bool GEN>
+template <int M, bool MULTI, bool GEN, bool SINGLE>
 __device__ __forceinline__ bool TrackBegin(const RenderParams& P, const SceneDev& S0, int i, GridWalk& w,
                                            HashRng& rng, const MediumDev*& med, uint32_t& bricks) {
     const float4 rd = P.ray_d[i];
@@ -1459,9 +1466,11 @@ __device__ __forceinline__ bool TrackBegin(const RenderParams& P, const SceneDev
     if (medium < 0)
         return false;
     const SceneDev& S = SceneOf<MULTI>(P, S0, i);
-    med = &S.media[medium];
-    if (med->type != PG_MEDIUM_GRID)
-        return false;
+    if (!SINGLE) {
+        med = &S.media[medium];
+        if (med->type != PG_MEDIUM_GRID)
+            return false;
+    }
     const float4 ro = P.ray_o[i];
     // The segment ends at the surface k_trace found (path.cpp:13-17).
     float tHit = kFloatMax;
@@ -1472,15 +1481,15 @@ __device__ __forceinline__ bool TrackBegin(const RenderParams& P, const SceneDev
     }
     const RequestDev& R = RequestOf<MULTI>(P, i);
     rng = PathRng<GEN>(R, P.sample[i], __float_as_uint(P.L[i].w)).Tracking();
-    if (GridWalkBegin<M>(*med, v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), tHit, w, rng, bricks))
+    if (GridWalkBegin<M>(WalkMedium<SINGLE>(S0, med), v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), tHit,
+                         w, rng, bricks))
         return true;
     reinterpret_cast<uint4*>(P.trk)[i] = make_uint4(0u, 0u, 0u, rng.dim);
     return false;
 }
 
-template <int M, bool MULTI, bool GEN>
-__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
-    k_track(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+template <int M, bool MULTI, bool GEN, bool SINGLE>
+__device__ __forceinline__ void TrackLoop(const RenderParams& P, const SceneDev& S0) {
     const int n = P.counts[kCntActive];
     const int* active = ActiveList(P);
     const int lane = threadIdx.x & 31;
@@ -1504,7 +1513,7 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
                 if (q < n) {
                     const int i = active[q];
                     items++;
-                    if (TrackBegin<M, MULTI, GEN>(P, S0, i, w, rng, med, bricks))
+                    if (TrackBegin<M, MULTI, GEN, SINGLE>(P, S0, i, w, rng, med, bricks))
                         slot = i;
                 }
             }
@@ -1515,12 +1524,13 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
             continue;
         }
         if (slot >= 0) {
-            const int r = DeltaTrackAction<M>(*med, w, rng, bricks, err);
+            const MediumDev& m = WalkMedium<SINGLE>(S0, med);
+            const int r = DeltaTrackAction<M>(m, w, rng, bricks, err);
             if (r != kWalkGoing) {
                 V3 p = v3(0.0f);
                 uint32_t wd = rng.dim;
                 if (r == kWalkCollided) {
-                    p = Affine(med->m2w, w.mo + w.t * w.md);
+                    p = Affine(m.m2w, w.mo + w.t * w.md);
                     wd |= kTrackScattered;
                 }
                 reinterpret_cast<uint4*>(P.trk)[slot] =
@@ -1538,10 +1548,19 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
     WarpAdd(&P.stats[kStatSteps], steps);
 }
 
+template <int M, bool MULTI, bool GEN>
+__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
+    k_track(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    if (!MULTI && S0.single_grid)
+        TrackLoop<M, MULTI, GEN, true>(P, S0);
+    else
+        TrackLoop<M, MULTI, GEN, false>(P, S0);
+}
+
 // Starts the ratio-tracking walk of shadow-queue entry q (scenes without surfaces: the
 // transmittance is the medium's alone, RayIntegrator::IntersectTr, integrator.cpp:68-87);
 // false when there is nothing to walk, with the entry's contribution already final.
-template <int M, bool MULTI>
+template <int M, bool MULTI, bool SINGLE>
 __device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const SceneDev& S0, int q, GridWalk& w,
                                               HashRng& rng, const MediumDev*& med, uint32_t& bricks) {
     const float4 sd = P.sd[q];
@@ -1558,7 +1577,7 @@ __device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const Scene
         reinterpret_cast<uint32_t*>(&P.sc[q])[3] = __float_as_uint(sc.w) | kShadowDone;
     }
     med = &S.media[medium];
-    if (med->type != PG_MEDIUM_GRID) {
+    if (!SINGLE && med->type != PG_MEDIUM_GRID) {
         // HomogeneousMedium::Tr (medium.cpp:33-36): closed form.
         const MediumDev& m = *med;
         const float t = so.w;
@@ -1568,14 +1587,14 @@ __device__ __forceinline__ bool TransmitBegin(const RenderParams& P, const Scene
         return false;
     }
     rng = HashRng{P.sample[slot], P.skey[q], 0};
-    return GridWalkBegin<M>(*med, v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w, w, rng, bricks);
+    return GridWalkBegin<M>(WalkMedium<SINGLE>(S0, med), v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z), so.w,
+                            w, rng, bricks);
 }
 
 // Ratio tracking of the shadow queue (the media-only scenes' k_shadow work): scales each
 // entry's unoccluded contribution by its transmittance; k_shadow then adds it to the path.
-template <int M, bool MULTI>
-__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
-    k_transmit(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+template <int M, bool MULTI, bool SINGLE>
+__device__ __forceinline__ void TransmitLoop(const RenderParams& P, const SceneDev& S0) {
     const int n = P.counts[kCntShadow];
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -1598,7 +1617,7 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
                 const int q = base + __popc(idle & below);
                 if (q < n) {
                     items++;
-                    if (TransmitBegin<M, MULTI>(P, S0, q, w, rng, med, bricks)) {
+                    if (TransmitBegin<M, MULTI, SINGLE>(P, S0, q, w, rng, med, bricks)) {
                         entry = q;
                         tr = 1.0f;
                     }
@@ -1611,7 +1630,7 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
             continue;
         }
         if (entry >= 0) {
-            if (RatioTrackAction<M>(*med, w, rng, tr, bricks, err) != kWalkGoing) {
+            if (RatioTrackAction<M>(WalkMedium<SINGLE>(S0, med), w, rng, tr, bricks, err) != kWalkGoing) {
                 if (tr != 1.0f) {
                     float4* c = &P.sc[entry];
                     const float4 v = *c;
@@ -1628,6 +1647,15 @@ __global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
     WarpAdd(&P.stats[kStatTransmitSteps], steps);
     WarpAdd(&P.stats[kStatTransmitBricks], bricks);
     WarpAdd(&P.stats[kStatSteps], steps);
+}
+
+template <int M, bool MULTI>
+__global__ void __launch_bounds__(kTrackThreads, PG_TRACK_MIN_BLOCKS)
+    k_transmit(const __grid_constant__ RenderParams P, const __grid_constant__ SceneDev S0) {
+    if (!MULTI && S0.single_grid)
+        TransmitLoop<M, MULTI, true>(P, S0);
+    else
+        TransmitLoop<M, MULTI, false>(P, S0);
 }
 
 // Guided direction sampling for the vertices in the guide queue, from the network's

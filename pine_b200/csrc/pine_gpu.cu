@@ -95,6 +95,8 @@ struct DeviceScene {
     SceneDev dev{};
     DevMem mem;
     const MediumDev* media_dev[4] = {nullptr, nullptr, nullptr, nullptr};  // per brick size
+    bool single_grid = false;   // the scene's only medium is a grid: grid0 holds it
+    MediumDev grid0[4] = {};    // per brick size
     int width = 0, height = 0, spp = 1, max_depth = 4;
     int sampler = PG_SAMPLER_INDEPENDENT, scramble = 1;
     int filter_splat = 0;                  // 0: one pixel per sample, weight 1
@@ -816,6 +818,10 @@ static void UploadScene(pg_ctx* ctx, const pg_scene_desc* d, int32_t* sceneId) {
             mv[i].inv_bsize = 1.0f / kBrickSizes[v];
         }
         sc->media_dev[v] = sc->mem.Upload(mv, st);
+        if (d->num_media == 1 && mv[0].type == PG_MEDIUM_GRID) {
+            sc->single_grid = true;
+            sc->grid0[v] = mv[0];
+        }
     }
     S.media = sc->media_dev[0];
     S.num_media = d->num_media;
@@ -1187,6 +1193,8 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
+    w.S0.single_grid = sc.single_grid ? 1 : 0;
+    w.S0.grid0 = sc.grid0[MediaVariant(ctx->tuning)];
     w.sort = ctx->tuning.sort_queue == 1;
     w.slotSort = ctx->tuning.sort_queue == 2;
     w.guide = recordAccept != nullptr;
@@ -1968,6 +1976,8 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     w.shadeBlock = ctx->tuning.block_size;
     w.S0 = sc.dev;
     w.S0.media = sc.media_dev[MediaVariant(ctx->tuning)];
+    w.S0.single_grid = sc.single_grid ? 1 : 0;
+    w.S0.grid0 = sc.grid0[MediaVariant(ctx->tuning)];
     const int slots = (int)std::min<uint64_t>((uint64_t)kNoAllocSlots, total);
     RenderParams& P = w.P;
     P.slots = slots;
