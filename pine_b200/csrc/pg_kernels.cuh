@@ -109,6 +109,7 @@ struct RenderParams {
     int nreq;
     unsigned long long total;    // samples over all requests
     const RequestDev* reqs;
+    RequestDev req0;             // single-request waves: a copy of reqs[0], read as constants
     const SceneDev* scenes;      // one per request (batched renders)
     int* slot_req;               // request of each slot (batched renders)
     float4* ray_o;               // o.xyz, bsdfPdf
@@ -272,7 +273,7 @@ __device__ __forceinline__ const SceneDev& SceneOf(const RenderParams& P, const 
 }
 template <bool MULTI>
 __device__ __forceinline__ const RequestDev& RequestOf(const RenderParams& P, int slot) {
-    return P.reqs[MULTI ? P.slot_req[slot] : 0];
+    return MULTI ? P.reqs[P.slot_req[slot]] : P.req0;
 }
 
 template <int M>
@@ -449,7 +450,7 @@ static __device__ void FinalizeRecords(const RenderParams& P, int i, V3 L, bool 
 template <int M, bool MULTI, bool GEN>
 __device__ void SpawnPath(const RenderParams& P, const SceneDev& S0, int i, unsigned long long id) {
     int r = MULTI ? FindRequest(P, id) : 0;
-    const RequestDev& R = P.reqs[r];
+    const RequestDev& R = MULTI ? P.reqs[r] : P.req0;
     if (MULTI)
         P.slot_req[i] = r;
     const SceneDev& S = MULTI ? P.scenes[r] : S0;
@@ -530,7 +531,7 @@ __global__ void k_splat(const __grid_constant__ RenderParams P) {
     const int n = P.counts[kCntSplat];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const float4 e = P.splat[q];
-        const RequestDev& R = P.reqs[MULTI ? P.splat_req[q] : 0];
+        const RequestDev& R = MULTI ? P.reqs[P.splat_req[q]] : P.req0;
         const uint32_t key0 = __float_as_uint(e.w);
         const uint32_t pix = (key0 - R.key0_offset) % (uint32_t)R.npix;
         SplatSample(P, R, key0, pix, v3(e.x, e.y, e.z));
@@ -1673,7 +1674,7 @@ __device__ void GuideOne(const RenderParams& P, const SceneDev& S, int q, int& s
                  g2 = P.gq[kGuideEntry * q + 2], g3 = P.gq[kGuideEntry * q + 3];
     const int i = __float_as_int(g0.w);
     slot = i;
-    const RequestDev& R = P.reqs[0];
+    const RequestDev& R = P.req0;
     const V3 p = v3(g0.x, g0.y, g0.z), n = v3(g1.x, g1.y, g1.z), wi = v3(g2.x, g2.y, g2.z);
     const bool surface = !isnan(g1.x);
     const int id = __float_as_int(g1.w), shadowIdx = __float_as_int(g2.w);

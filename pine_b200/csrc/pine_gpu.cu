@@ -1220,6 +1220,7 @@ static void RenderFilm(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, uint
     RequestDev* dReq = ctx->req_buf.Alloc<RequestDev>(1);
     PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
     w.P.reqs = dReq;
+    w.P.req0 = rq;
     w.P.nreq = 1;
     w.P.samples = w.splat ? nullptr : SampleBuffer(ctx, total);
     RunHostLoop(ctx, w, profile, res);
@@ -2018,6 +2019,7 @@ static void RenderNoAlloc(pg_ctx* ctx, DeviceScene& sc, int spp, int maxDepth, u
     rq.max_depth = maxDepth;
     SetRequestSampling(ctx, sc, rq, seed);
     PG_CUDA(cudaMemcpyAsync(dReq, &rq, sizeof(rq), cudaMemcpyHostToDevice, st));
+    w.P.req0 = rq;
     RunHostLoop(ctx, w, false, res);
     k_noalloc_mean<<<ctx->num_sms * 4, 256, 0, st>>>(acc, npix, meanDevice);
     PG_CUDA(cudaGetLastError());
