@@ -580,7 +580,11 @@ def batch_eval(args):
     set renders as one graph-captured batch (latency = completion time of each request from
     the batch start, device clock) and, for comparison, one request at a time (latency =
     the running sum of the single-request device times), both in the caller's order and
-    shortest job first, the order the batch itself serves its requests in."""
+    shortest job first, the order the batch itself serves its requests in.  The batch is
+    timed all three ways the tuning allows: one wave per scene, one per scene kind and one
+    for the whole batch.
+    `wall_*` adds the host's share (graph capture, launches, synchronisation): the
+    render_batch call's wall time, and the sum of the single calls' wall times."""
     import pine_b200 as pb
     ctx = pb.Context(0)
     kinds = ["spheres", "mesh", "volume"]
@@ -601,24 +605,57 @@ def batch_eval(args):
         mix[k] += 1
     paths = sum(r["width"] * r["height"] * r["spp"] for r in reqs)
     tuning = ctx.autotune(reqs)
-    ctx.render_batch(reqs, outputs=False)  # warm-up
-    b = ctx.render_batch(reqs, outputs=False)
-    lat_b = np.array(b["request_seconds"])
-    single = [ctx.render_batch([r], outputs=False)["seconds"] for r in reqs]
     pct = lambda a, q: float(np.percentile(a, q))
+    batches = {}
+    for g in (2, 1, 0):  # one wave per scene, per scene kind, one for the whole batch
+        ctx.set_tuning(**dict(tuning, group_kinds=g))
+        ctx.render_batch(reqs, outputs=False)  # warm-up
+        t0 = time.perf_counter()
+        b = ctx.render_batch(reqs, outputs=False)
+        wall = time.perf_counter() - t0
+        lat = np.array(b["request_seconds"])
+        batches[g] = {"seconds": b["seconds"], "value": paths / b["seconds"] / 1e6,
+                      "latency_p50_s": pct(lat, 50), "latency_p99_s": pct(lat, 99),
+                      "wall_seconds": wall, "wall_value": paths / wall / 1e6}
+    # The batch at every queue capacity the autotuner chooses from.
+    sweep = {}
+    for cap in (1 << 20, 1 << 21, 1 << 22, 1 << 23):
+        ctx.set_tuning(**dict(tuning, queue_capacity=cap))
+        ctx.render_batch(reqs, outputs=False)
+        sweep[cap] = paths / ctx.render_batch(reqs, outputs=False)["seconds"] / 1e6
+    ctx.set_tuning(**tuning)
+    single, single_wall = [], []
+    for r in reqs:
+        t0 = time.perf_counter()
+        single.append(ctx.render_batch([r], outputs=False)["seconds"])
+        single_wall.append(time.perf_counter() - t0)
 
     def sequential(order):
         done = np.cumsum(np.asarray(single)[order])
         t = float(done[-1])
+        wall = float(np.sum(single_wall))
         return {"seconds": t, "value": paths / t / 1e6, "latency_p50_s": pct(done, 50),
-                "latency_p99_s": pct(done, 99)}
+                "latency_p99_s": pct(done, 99), "wall_seconds": wall, "wall_value": paths / wall / 1e6}
 
+    # Each kind batched alone, against the same requests one at a time (device seconds).
+    per_kind = {}
+    for k in kinds:
+        idx = [i for i, r in enumerate(reqs) if r["scene"] == sids[k]]
+        sub = [reqs[i] for i in idx]
+        ctx.render_batch(sub, outputs=False)
+        per_kind[k] = {"requests": len(sub),
+                       "batch_seconds": ctx.render_batch(sub, outputs=False)["seconds"],
+                       "one_at_a_time_seconds": float(np.sum(np.asarray(single)[idx]))}
     sjf = sorted(range(len(reqs)), key=lambda i: reqs[i]["width"] * reqs[i]["height"] * reqs[i]["spp"])
     ctx.close()
     return {"metric": "Mpaths/s", "workload": f"{len(reqs)} requests (seed {args.batch_seed}): {mix}",
             "paths": int(paths), "tuning": tuning,
-            "batch": {"seconds": b["seconds"], "value": paths / b["seconds"] / 1e6,
-                      "latency_p50_s": pct(lat_b, 50), "latency_p99_s": pct(lat_b, 99)},
+            "batch": batches[tuning["group_kinds"]],
+            "batch_wave_per_scene": batches[2],
+            "batch_wave_per_kind": batches[1],
+            "batch_one_wave": batches[0],
+            "batch_mpaths_per_s_by_queue_capacity": sweep,
+            "per_kind": per_kind,
             "one_at_a_time": sequential(list(range(len(reqs)))),
             "one_at_a_time_shortest_first": sequential(sjf)}
 

@@ -370,7 +370,7 @@ pg_status pg_set_bvh_builder(pg_ctx* ctx, int32_t builder);
 pg_status pg_scene_bvh_info(pg_ctx* ctx, int32_t scene_id, double* build_seconds,
                             int32_t* wide_depth, int64_t* wide_nodes);
 
-/* ---- batched requests (many renders in one persistent, graph-captured launch) ---- */
+/* ---- batched requests (many renders in persistent, graph-captured waves) ---- */
 typedef struct pg_request {
     int32_t scene_id;
     int32_t width, height;  /* <= 0: the scene's film size */
@@ -400,6 +400,12 @@ typedef struct pg_tuning {
                                warps read neighbouring path state; 1: in scenes with grid
                                media, order it by the cell of the ray origins (8^3 cells per
                                medium box) before the tracking kernels; 0: queue order */
+    int32_t group_kinds;    /* pg_render_batch only: how requests split into waves, each
+                               one graph launch with only the kernel variants its scenes
+                               need, enqueued back to back in increasing order of their
+                               samples.  2 (default): one wave per scene; 1: one per scene
+                               kind (surfaces only, media only, both, general materials,
+                               filtered films); 0: one wave for the whole batch */
 } pg_tuning;
 
 pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_t n,

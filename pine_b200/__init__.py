@@ -130,7 +130,7 @@ SHAPE_SPHERE, SHAPE_PLANE, SHAPE_TRIANGLE, SHAPE_RECT, SHAPE_MESH = range(5)
 class Tuning(ctypes.Structure):
     _fields_ = [("queue_capacity", ctypes.c_int32), ("block_size", ctypes.c_int32),
                 ("split_shadow", ctypes.c_int32), ("majorant_brick", ctypes.c_int32),
-                ("sort_queue", ctypes.c_int32)]
+                ("sort_queue", ctypes.c_int32), ("group_kinds", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):
@@ -529,9 +529,10 @@ class Context:
         return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def set_tuning(self, queue_capacity: int = 1 << 23, block_size: int = 128,
-                   split_shadow: int = 1, majorant_brick: int = 64, sort_queue: int = 2):
+                   split_shadow: int = 1, majorant_brick: int = 64, sort_queue: int = 2,
+                   group_kinds: int = 2):
         t = Tuning(int(queue_capacity), int(block_size), int(split_shadow), int(majorant_brick),
-                   int(sort_queue))
+                   int(sort_queue), int(group_kinds))
         self._check(self._lib.pg_set_tuning(self._ctx, ctypes.byref(t)))
 
     @staticmethod

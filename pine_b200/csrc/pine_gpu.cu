@@ -252,8 +252,8 @@ struct pg_ctx {
     // Default tuning: 2^23 path slots, 128-thread shading blocks, shadow rays in their own
     // kernels, 64-voxel majorant bricks (volume benchmark on B200: 915 Mpaths/s against 853
     // with 32-voxel and 704 with 16-voxel bricks at 2^22 slots; 951 with 2^23 slots, 825
-    // with 2^21).
-    pg_tuning tuning{1 << 23, 128, 1, 64, 2};
+    // with 2^21); slot order; a batch's waves one per scene.
+    pg_tuning tuning{1 << 23, 128, 1, 64, 2, 2};
     int num_sms = 148;
     pg::DevMem guide_mem;                  // guiding network (allocated on first use)
     pg::GuideNetDev guide;
@@ -941,6 +941,12 @@ __global__ void k_iota(int* a, int n) {
 __global__ void k_timestamp(unsigned long long* t) {
     *t = GlobalTimer();
 }
+// Queue counters at the start of a wave: all zero but the finished list, which holds every
+// slot.
+__global__ void k_reset_counts(int* counts, int slots) {
+    for (int i = threadIdx.x; i < kNumCounts; i += blockDim.x)
+        counts[i] = i == kCntFinished ? slots : 0;
+}
 
 static void DispatchRegen(pg_ctx* ctx, Wave& w, LaunchTimer* timer, RenderResult* res) {
     LaunchEnv env{ctx->stream, ctx->num_sms, &ctx->guide};
@@ -959,10 +965,9 @@ static void DispatchBody(pg_ctx* ctx, Wave& w, int n, bool persistent, LaunchTim
         DispatchBodyFast(env, w, n, persistent, timer, res);
 }
 
-// Fills the pool pointers of a wave and resets its queues: every slot starts empty and
-// listed as finished, so the first k_regen fills all of them.
-static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int maxIter) {
-    cudaStream_t st = ctx->stream;
+// Fills the pool pointers of a wave.  The pool grows to `slots` if it is smaller, which
+// moves it: bind every wave of a set only after growing the pool to the set's largest.
+static void BindWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int maxIter) {
     ctx->pool.Ensure(slots);
     Pool& pl = ctx->pool;
     RenderParams& P = w.P;
@@ -983,24 +988,38 @@ static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int max
     P.stats = ctx->stats;
     P.err = ctx->err;
     P.max_iter = maxIter;
-    PG_CUDA(cudaMemsetAsync(pl.state, 0, (size_t)slots * sizeof(int), st));
-    k_iota<<<ctx->num_sms * 4, 256, 0, st>>>(pl.finished, slots);
-    PG_CUDA(cudaGetLastError());
-    std::vector<int> c(kNumCounts, 0);
-    c[kCntFinished] = slots;
-    PG_CUDA(cudaMemcpyAsync(ctx->counts, c.data(), kNumCounts * sizeof(int), cudaMemcpyHostToDevice, st));
-    PG_CUDA(cudaMemsetAsync(ctx->next_sample, 0, sizeof(unsigned long long), st));
-    PG_CUDA(cudaMemsetAsync(ctx->stats, 0, kNumStats * sizeof(unsigned long long), st));
-    PG_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), st));
-    PG_CUDA(cudaMemsetAsync(pl.sort_bins, 0, (2 * kSortBins + 1) * sizeof(int), st));
     if (w.guide) {
         GuidePool& gp = ctx->guide_pool;
         gp.Ensure(slots);
         P.gq = gp.gq, P.graw = gp.graw, P.rec = gp.rec, P.rec_dirw = gp.rec_dirw;
         P.rec_last = gp.rec_last;
         P.rec_cap = kRecordCap;
-        PG_CUDA(cudaMemsetAsync(gp.rec_last, 0xff, (size_t)slots * sizeof(int), st));
     }
+}
+
+// Resets a bound wave's queues on the stream: every slot starts empty and listed as
+// finished, so the first k_regen fills all of them.  `counters`: also zero the statistics
+// and the device error word (waves of one batch share them).
+static void ResetWave(pg_ctx* ctx, const Wave& w, bool counters) {
+    cudaStream_t st = ctx->stream;
+    const RenderParams& P = w.P;
+    PG_CUDA(cudaMemsetAsync(P.state, 0, (size_t)P.slots * sizeof(int), st));
+    k_iota<<<ctx->num_sms * 4, 256, 0, st>>>(P.finished, P.slots);
+    k_reset_counts<<<1, 32, 0, st>>>(P.counts, P.slots);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemsetAsync(P.next_sample, 0, sizeof(unsigned long long), st));
+    if (counters) {
+        PG_CUDA(cudaMemsetAsync(P.stats, 0, kNumStats * sizeof(unsigned long long), st));
+        PG_CUDA(cudaMemsetAsync(P.err, 0, sizeof(uint32_t), st));
+    }
+    PG_CUDA(cudaMemsetAsync(P.sort_bins, 0, (2 * kSortBins + 1) * sizeof(int), st));
+    if (w.guide)
+        PG_CUDA(cudaMemsetAsync(P.rec_last, 0xff, (size_t)P.slots * sizeof(int), st));
+}
+
+static void PrepareWave(pg_ctx* ctx, Wave& w, int slots, uint64_t total, int maxIter) {
+    BindWave(ctx, w, slots, total, maxIter);
+    ResetWave(ctx, w, true);
 }
 
 // Host-driven loop: the active count is read back after each k_swap so that every launch
@@ -1023,34 +1042,38 @@ static void RunHostLoop(pg_ctx* ctx, Wave& w, bool profile, RenderResult& res) {
     timer.Collect(res);
 }
 
+// An instantiated wave graph.  Destroying it while its launch runs is allowed: CUDA frees
+// an executable graph that is still in flight when that launch completes.
+struct WaveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    WaveGraph() = default;
+    WaveGraph(const WaveGraph&) = delete;
+    WaveGraph& operator=(const WaveGraph&) = delete;
+    ~WaveGraph() {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+    }
+};
+
 // Device-driven loop: after the initial fill, the whole render is one CUDA graph whose
 // while-node repeats trace/shade/shadow/swap with persistent (fixed, grid-stride) launches
 // until k_swap finds the active queue empty or the iteration cap reached.  The condition
-// starts at 1: the fill always leaves at least one active path.
-static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res, unsigned long long* startTime) {
+// starts at 1: the fill always leaves at least one active path.  Capturing enqueues nothing.
+static void CaptureWave(pg_ctx* ctx, Wave& w, WaveGraph& g) {
     cudaStream_t st = ctx->stream;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    PG_CUDA(cudaGraphCreate(&graph, 0));
-    struct Cleanup {
-        cudaGraph_t& g;
-        cudaGraphExec_t& e;
-        ~Cleanup() {
-            if (e)
-                cudaGraphExecDestroy(e);
-            if (g)
-                cudaGraphDestroy(g);
-        }
-    } cleanup{graph, exec};
+    PG_CUDA(cudaGraphCreate(&g.graph, 0));
     cudaGraphConditionalHandle cond;
-    PG_CUDA(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+    PG_CUDA(cudaGraphConditionalHandleCreate(&cond, g.graph, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = cond;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
-    PG_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    PG_CUDA(cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     w.P.use_cond = 1;
     w.P.cond = cond;
@@ -1065,17 +1088,18 @@ static void RunGraph(pg_ctx* ctx, Wave& w, RenderResult& res, unsigned long long
         le = cudaGetLastError();  // a launch the capture refused
     cudaGraph_t captured = nullptr;
     cudaError_t ce = cudaStreamEndCapture(st, &captured);  // always ends the capture
+    w.P.use_cond = 0;
     if (le != cudaSuccess)
         throw Failure{PG_ERR_CUDA, std::string("graph capture launch: ") + cudaGetErrorString(le)};
     if (ce != cudaSuccess)
         throw Failure{PG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)};
-    PG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    w.P.use_cond = 0;
-    PG_CUDA(cudaEventRecord(ctx->ev0, st));
-    if (startTime)
-        k_timestamp<<<1, 1, 0, st>>>(startTime);
+    PG_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+}
+
+// Enqueues a captured wave: its initial fill, then its graph.
+static void LaunchWave(pg_ctx* ctx, Wave& w, const WaveGraph& g) {
     DispatchRegen(ctx, w, nullptr, nullptr);
-    PG_CUDA(cudaGraphLaunch(exec, st));
+    PG_CUDA(cudaGraphLaunch(g.exec, ctx->stream));
 }
 
 // Ends the timed region (after the film fold) and collects counters and device errors.
@@ -1675,44 +1699,78 @@ struct BatchOutcome {
     std::vector<double> requestSeconds;
 };
 
-// Renders many requests in one graph-captured persistent wavefront.  sppDivisor > 1 runs
-// a proportionally smaller sample of each request (used by the autotuner).
+// The wavefront kernels a scene needs: surface traversal, grid-medium tracking, the
+// general shading code (node graphs, bump maps, samplers other than independent), the splat
+// queue of filtered films, null-surface crossings.  A wave whose requests share one kind
+// launches only that kind's kernel variants.
+static int SceneKind(const DeviceScene& sc) {
+    return (sc.surfaces ? 1 : 0) | (sc.dev.num_media > 0 ? 2 : 0) | (sc.general ? 4 : 0) |
+           (sc.filter_splat != 0 ? 8 : 0) | (sc.dev.has_null_surfaces != 0 ? 16 : 0);
+}
+
+// Renders many requests as graph-captured persistent wavefronts: one wave for the whole
+// set (tune.group_kinds 0), one per scene kind (1) or one per scene (2), waves in
+// increasing order of their samples.  Within a wave requests take their sample ranges shortest first, so small
+// requests complete early (results keep the caller's order).  sppDivisor > 1 runs a
+// proportionally smaller sample of each request (used by the autotuner).
 static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning& tune,
                      bool outputs, int sppDivisor, BatchOutcome& out) {
     Require(reqs != nullptr && n > 0 && n <= (1 << 16), "bad request array");
     cudaStream_t st = ctx->stream;
-    std::vector<RequestDev> rq(n);
-    std::vector<SceneDev> scenes(n);
-    uint64_t total = 0, pixels = 0;
-    bool surfaces = false, media = false, general = false, splat = false;
-    int maxDepth = 1, bvhDepth = 0;
-    bool nullSurfaces = false;
     const int variant = MediaVariant(tune);
-    // Shortest job first: requests take their sample ranges in increasing order of their
-    // sample count, so small requests complete early (results keep the caller's order).
     std::vector<uint64_t> cost(n);
+    std::vector<int> kind(n);
     for (int i = 0; i < n; i++) {
         const pg_request& r = reqs[i];
         DeviceScene& sc = GetScene(ctx, r.scene_id);
+        Require(r.spp > 0, "request spp must be positive");
         int w = r.width > 0 ? r.width : sc.width, h = r.height > 0 ? r.height : sc.height;
         cost[i] = (uint64_t)std::max(w, 1) * std::max(h, 1) * (uint64_t)std::max(r.spp, 1);
+        kind[i] = tune.group_kinds == 2 ? r.scene_id : (tune.group_kinds == 1 ? SceneKind(sc) : 0);
     }
-    std::vector<int> order(n);
+    std::vector<int> byCost(n);
     for (int i = 0; i < n; i++)
-        order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] < cost[b]; });
+        byCost[i] = i;
+    std::stable_sort(byCost.begin(), byCost.end(), [&](int a, int b) { return cost[a] < cost[b]; });
+    // Waves: groups ordered by their total samples; order[] is the serving order, wave g
+    // serves order[groups[g] .. groups[g + 1]).
+    std::vector<int> kinds;
+    std::vector<uint64_t> kindCost;
+    for (int i = 0; i < n; i++) {
+        size_t g = std::find(kinds.begin(), kinds.end(), kind[i]) - kinds.begin();
+        if (g == kinds.size()) {
+            kinds.push_back(kind[i]);
+            kindCost.push_back(0);
+        }
+        kindCost[g] += cost[i];
+    }
+    std::vector<size_t> kindOrder(kinds.size());
+    for (size_t g = 0; g < kinds.size(); g++)
+        kindOrder[g] = g;
+    std::stable_sort(kindOrder.begin(), kindOrder.end(),
+                     [&](size_t a, size_t b) { return kindCost[a] < kindCost[b]; });
+    std::vector<int> order, groups;
+    for (size_t g : kindOrder) {
+        groups.push_back((int)order.size());
+        for (int i : byCost)
+            if (kind[i] == kinds[g])
+                order.push_back(i);
+    }
+    groups.push_back(n);
+
+    std::vector<RequestDev> rq(n);
+    std::vector<SceneDev> scenes(n);
+    uint64_t pixels = 0;
     for (int k = 0; k < n; k++) {
         const int i = order[k];
         const pg_request& r = reqs[i];
         DeviceScene& sc = GetScene(ctx, r.scene_id);
         int w = r.width > 0 ? r.width : sc.width, h = r.height > 0 ? r.height : sc.height;
-        Require(r.spp > 0, "request spp must be positive");
         int spp = std::max(1, r.spp / std::max(1, sppDivisor));
         int md = r.max_depth > 0 ? r.max_depth : sc.max_depth;
         uint64_t cnt = (uint64_t)w * h * spp;
         Require(cnt < (1ull << 32), "a request's width*height*spp must stay below 2^32");
         RequestDev& d = rq[k];
-        d.sample_begin = total;
         d.total = (uint32_t)cnt;
         d.npix = w * h;
         d.width = w;
@@ -1723,9 +1781,7 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         d.key0_offset = 0;
         d.max_depth = md;
         SetRequestSampling(ctx, sc, d, r.seed);
-        total += cnt;
         pixels += (uint64_t)w * h;
-        maxDepth = std::max(maxDepth, md);
         SceneDev s = sc.dev;
         s.media = sc.media_dev[variant];
         // The request's film size sets the aspect ratio (camera.h:29-30).
@@ -1733,43 +1789,82 @@ static void RunBatch(pg_ctx* ctx, const pg_request* reqs, int n, const pg_tuning
         s.cam.height = h;
         s.cam.fov2d[0] = s.cam.fov2d[1] * ((float)w / (float)h);
         scenes[k] = s;
-        surfaces = surfaces || sc.surfaces;
-        bvhDepth = std::max(bvhDepth, sc.bvh_depth);
-        nullSurfaces = nullSurfaces || sc.dev.has_null_surfaces != 0;
-        media = media || sc.dev.num_media > 0;
-        general = general || sc.general;
-        splat = splat || sc.filter_splat != 0;
     }
     ClearFilm(ctx, (int64_t)pixels);
-    RequestDev* dReq = ctx->req_buf.Upload(rq, st);
-    SceneDev* dScenes = ctx->req_buf.Upload(scenes, st);
     uint32_t* done = ctx->req_buf.Alloc<uint32_t>(n);
     unsigned long long* times = ctx->req_buf.Alloc<unsigned long long>(n + 1);
     PG_CUDA(cudaMemsetAsync(done, 0, n * sizeof(uint32_t), st));
     PG_CUDA(cudaMemsetAsync(times, 0, (n + 1) * sizeof(unsigned long long), st));
 
-    Wave w;
-    w.multi = true;
-    w.mode = PG_MATH_FAST;
-    w.surfaces = surfaces;
-    w.traceCap = TraceCap(bvhDepth);
-    w.nullSurfaces = nullSurfaces;
-    w.media = media;
-    w.general = general;
-    w.splat = splat;
-    w.fused = tune.split_shadow == 0;
-    w.sort = tune.sort_queue == 1;
-    w.slotSort = tune.sort_queue == 2;
-    w.shadeBlock = tune.block_size;
-    w.S0 = scenes[0];
-    int slots = (int)std::min<uint64_t>((uint64_t)std::max(1024, tune.queue_capacity), total);
-    PrepareWave(ctx, w, slots, total, (int)std::min<int64_t>(IterationCap(total, slots, maxDepth), 1 << 30));
-    w.P.reqs = dReq;
-    w.P.nreq = n;
-    w.P.scenes = dScenes;
-    w.P.req_done = done;
-    w.P.req_time = times + 1;
-    RunGraph(ctx, w, out.res, times);
+    // Per wave: its samples (ids start at 0 in each wave, requests' ranges in serving
+    // order) and the union of its scenes' needs.
+    struct WaveSpec {
+        uint64_t total = 0;
+        int maxDepth = 1, bvhDepth = 0;
+        bool surfaces = false, media = false, general = false, splat = false, nullSurfaces = false;
+    };
+    std::vector<WaveSpec> specs(groups.size() - 1);
+    for (size_t g = 0; g + 1 < groups.size(); g++) {
+        WaveSpec& ws = specs[g];
+        for (int k = groups[g]; k < groups[g + 1]; k++) {
+            const DeviceScene& sc = GetScene(ctx, reqs[order[k]].scene_id);
+            rq[k].sample_begin = ws.total;
+            ws.total += rq[k].total;
+            ws.maxDepth = std::max(ws.maxDepth, rq[k].max_depth);
+            ws.surfaces = ws.surfaces || sc.surfaces;
+            ws.bvhDepth = std::max(ws.bvhDepth, sc.bvh_depth);
+            ws.nullSurfaces = ws.nullSurfaces || sc.dev.has_null_surfaces != 0;
+            ws.media = ws.media || sc.dev.num_media > 0;
+            ws.general = ws.general || sc.general;
+            ws.splat = ws.splat || sc.filter_splat != 0;
+        }
+    }
+    RequestDev* dReqAll = ctx->req_buf.Upload(rq, st);
+    SceneDev* dScenesAll = ctx->req_buf.Upload(scenes, st);
+    // Every wave is bound and captured first, then all are enqueued back to back, so no host
+    // work (capture, instantiation, synchronisation) separates them on the device.
+    const size_t nw = specs.size();
+    std::vector<int> slots(nw);
+    for (size_t g = 0; g < nw; g++) {
+        slots[g] = (int)std::min<uint64_t>((uint64_t)std::max(1024, tune.queue_capacity), specs[g].total);
+        ctx->pool.Ensure(slots[g]);
+    }
+    std::vector<Wave> waves(nw);
+    std::vector<WaveGraph> graphs(nw);
+    for (size_t g = 0; g < nw; g++) {
+        const int k0 = groups[g], k1 = groups[g + 1];
+        const WaveSpec& ws = specs[g];
+        Wave& w = waves[g];
+        w.multi = true;
+        w.mode = PG_MATH_FAST;
+        w.surfaces = ws.surfaces;
+        w.traceCap = TraceCap(ws.bvhDepth);
+        w.nullSurfaces = ws.nullSurfaces;
+        w.media = ws.media;
+        w.general = ws.general;
+        w.splat = ws.splat;
+        w.fused = tune.split_shadow == 0;
+        w.sort = tune.sort_queue == 1;
+        w.slotSort = tune.sort_queue == 2;
+        w.shadeBlock = tune.block_size;
+        w.S0 = scenes[k0];
+        BindWave(ctx, w, slots[g], ws.total,
+                 (int)std::min<int64_t>(IterationCap(ws.total, slots[g], ws.maxDepth), 1 << 30));
+        w.P.reqs = dReqAll + k0;
+        w.P.nreq = k1 - k0;
+        w.P.scenes = dScenesAll + k0;
+        w.P.req_done = done + k0;
+        w.P.req_time = times + 1 + k0;
+        CaptureWave(ctx, w, graphs[g]);
+    }
+    ResetWave(ctx, waves[0], true);
+    PG_CUDA(cudaEventRecord(ctx->ev0, st));
+    k_timestamp<<<1, 1, 0, st>>>(times);  // latencies count from here
+    for (size_t g = 0; g < nw; g++) {
+        if (g > 0)
+            ResetWave(ctx, waves[g], false);  // statistics and errors accumulate over the waves
+        LaunchWave(ctx, waves[g], graphs[g]);
+    }
     FinishWave(ctx, out.res);
     std::vector<unsigned long long> t(n + 1);
     PG_CUDA(cudaMemcpy(t.data(), times, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -1811,7 +1906,7 @@ static bool ValidTuning(const pg_tuning& t) {
            (t.split_shadow == 0 || t.split_shadow == 1) &&
            (t.majorant_brick == 8 || t.majorant_brick == 16 || t.majorant_brick == 32 ||
             t.majorant_brick == 64) &&
-           (t.sort_queue >= 0 && t.sort_queue <= 2);
+           (t.sort_queue >= 0 && t.sort_queue <= 2) && (t.group_kinds >= 0 && t.group_kinds <= 2);
 }
 
 }  // namespace pg
@@ -1835,8 +1930,9 @@ extern "C" pg_status pg_render_batch(pg_ctx* ctx, const pg_request* reqs, int32_
 }
 
 // Coordinate descent over the tuning space on a 1/8-spp sample of the request mix: brick
-// size, shadow split, shading block size, queue capacity, queue order, each chosen with
-// the others fixed, keeping a value only when it is at least 2% faster.
+// size, shadow split, shading block size, queue capacity, queue order, grouping by scene
+// kind, each chosen with the others fixed, keeping a value only when it is at least 2%
+// faster.
 extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n, pg_tuning* chosen) {
     if (!ctx)
         return Fail(nullptr, Failure{PG_ERR_INVALID_ARG, "null context"});
@@ -1855,9 +1951,10 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
         double bestT = measure(best);
         const int bricks[] = {8, 16, 32, 64}, blocks[] = {32, 64, 128};
         const int caps[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
-        for (int dim = 0; dim < 5; dim++) {
+        const int values[6] = {4, 2, 3, 4, 3, 3};  // candidates per dimension
+        for (int dim = 0; dim < 6; dim++) {
             std::vector<pg_tuning> cands;
-            for (int k = 0; k < (dim == 1 ? 2 : (dim == 2 || dim == 4 ? 3 : 4)); k++) {
+            for (int k = 0; k < values[dim]; k++) {
                 pg_tuning t = best;
                 if (dim == 0)
                     t.majorant_brick = bricks[k];
@@ -1867,8 +1964,10 @@ extern "C" pg_status pg_autotune(pg_ctx* ctx, const pg_request* reqs, int32_t n,
                     t.block_size = std::min(blocks[k], kMaxShadeBlock);
                 else if (dim == 3)
                     t.queue_capacity = caps[k];
-                else
+                else if (dim == 4)
                     t.sort_queue = k;
+                else
+                    t.group_kinds = k;
                 cands.push_back(t);
             }
             for (auto& t : cands) {

@@ -38,6 +38,40 @@ def test_batch_matches_individual_renders(ctx, tmp_path):
         ctx.release_scene(i)
 
 
+@pytest.mark.parametrize("group", [1, 2])
+def test_grouped_batch_matches_one_launch(ctx, tmp_path, group):
+    """Splitting a mixed batch into waves (one per scene kind or one per scene, each
+    launching only its scenes' kernels) keeps every request's random streams, so its images
+    match those of the one-wave batch up to float rounding; latencies stay within the
+    batch's time, which spans all the waves."""
+    names = ["spheres", "volume", "mesh"]
+    ids = [ctx.load_scene(write_fixture_scene(golden(f"image_{n}.npz"), str(tmp_path / n)))
+           for n in names]
+    reqs = [dict(scene=ids[1], spp=128, seed=1),
+            dict(scene=ids[0], spp=64, seed=2),
+            dict(scene=ids[2], spp=64, seed=3),
+            dict(scene=ids[0], spp=16, width=17, height=9, seed=4),
+            dict(scene=ids[1], spp=32, width=40, height=30, seed=5)]
+    before = ctx.tuning()
+    outs = []
+    for g in (0, group):
+        ctx.set_tuning(**dict(before, group_kinds=g))
+        outs.append(ctx.render_batch(reqs))
+    ctx.set_tuning(**before)
+    assert outs[0]["paths"] == outs[1]["paths"]
+    for o in outs:
+        t = np.array(o["request_seconds"])
+        assert (t > 0).all() and (t <= o["seconds"] * 1.01 + 1e-3).all()
+    for a, b in zip(outs[0]["means"], outs[1]["means"]):
+        assert a.shape == b.shape and np.isfinite(b).all()
+        scale = max(float(a.mean()), 1e-6)
+        close = np.abs(a - b) <= 1e-4 * np.abs(a) + 1e-5 * scale
+        assert close.mean() >= 0.99
+        assert abs(float(a.mean()) - float(b.mean())) <= 1e-3 * scale
+    for i in ids:
+        ctx.release_scene(i)
+
+
 def test_autotune_returns_a_valid_tuning(ctx, tmp_path):
     ids = [ctx.load_scene(write_fixture_scene(golden(f"image_{n}.npz"), str(tmp_path / n)))
            for n in ["volume", "spheres"]]
@@ -45,6 +79,7 @@ def test_autotune_returns_a_valid_tuning(ctx, tmp_path):
     t = ctx.autotune([dict(scene=ids[0], spp=64), dict(scene=ids[1], spp=64)])
     assert t["majorant_brick"] in (8, 16, 32, 64) and t["split_shadow"] in (0, 1)
     assert t["block_size"] in (32, 64, 128) and 1 << 20 <= t["queue_capacity"] <= 1 << 23
+    assert t["sort_queue"] in (0, 1, 2) and t["group_kinds"] in (0, 1, 2)
     assert ctx.tuning() == t
     # Whatever was chosen renders the same image statistically.
     r = ctx.render(ids[1], spp=256, seed=9)
