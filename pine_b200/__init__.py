@@ -554,8 +554,8 @@ class Context:
         return arr, outs
 
     def render_batch(self, reqs, outputs: bool = True):
-        """Renders many requests (dicts: scene, spp, width, height, max_depth, seed) in one
-        graph-captured wavefront.  Returns per-request means, per-request completion times
+        """Renders many requests (dicts: scene, spp, width, height, max_depth, seed) in
+        graph-captured wavefronts (one wave per scene with the default tuning).  Returns per-request means, per-request completion times
         (seconds from the batch start) and the batch's device time."""
         sizes = []
         for r in reqs:
