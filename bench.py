@@ -98,7 +98,7 @@ def parse_args():
                     help="with --profile-case: render it guided (one pass, then training)")
     ap.add_argument("--batch-eval", action="store_true",
                     help="the 64-request batch: aggregate Mpaths/s and per-request latency "
-                         "p50/p99, one graph-captured launch vs one request at a time")
+                         "p50/p99, graph-captured waves vs one request at a time")
     ap.add_argument("--batch-requests", type=int, default=64)
     ap.add_argument("--batch-seed", type=int, default=0)
     ap.add_argument("--guiding-eval", action="store_true",
@@ -577,10 +577,10 @@ def batch_eval(args):
     """The batched-requests workload: requests drawn by seed from the spheres, mesh and
     volume generators, resolution side uniform in 128..1024 with aspect uniform in
     1..16/9, spp log-uniform in 16..256.  The autotuner picks the tuning; then the whole
-    set renders as one graph-captured batch (latency = completion time of each request from
-    the batch start, device clock) and, for comparison, one request at a time (latency =
-    the running sum of the single-request device times), both in the caller's order and
-    shortest job first, the order the batch itself serves its requests in.  The batch is
+    set renders as one batch of graph-captured waves (latency = completion time of each
+    request from the batch start, device clock) and, for comparison, one request at a time
+    (latency = the running sum of the single-request device times), both in the caller's
+    order and shortest job first, the order a wave serves its requests in.  The batch is
     timed all three ways the tuning allows: one wave per scene, one per scene kind and one
     for the whole batch.
     `wall_*` adds the host's share (graph capture, launches, synchronisation): the

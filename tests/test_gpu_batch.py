@@ -1,4 +1,4 @@
-"""Batched requests in one graph-captured persistent wavefront (pg_render_batch) and the
+"""Batched requests in graph-captured persistent wavefronts (pg_render_batch) and the
 autotuner (pg_autotune)."""
 
 import numpy as np
